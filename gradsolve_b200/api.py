@@ -1,0 +1,266 @@
+"""Public API: ``solve`` and ``grad_closure`` with the reference's signatures and routing
+contract, served by the B200 kernels.
+
+Mirrors gradsolve/api.py:291-400 (``solve``) and :792-1030 (``grad_closure``):
+  * ``engine="auto"`` picks the Rosenbrock23 engine for stiff problems and the Tsit5
+    engine otherwise (gradsolve/dispatch.py:235-258); the reference's engine names for this
+    path (``warp_replay``, ``tsit5_replay``, ``warp_ode``, ``cuda_tsit5``; ``warp_rosenbrock``,
+    ``cuda_rosenbrock23``) are accepted and served by the matching B200 engine, which the
+    ``.route`` records;
+  * the closure records the accepted-dt mesh ONCE at (y0, params) and is differentiable in
+    the inputs ``wrt`` selects (``"params"``, ``"y0"`` or ``("y0", "params")``,
+    gradsolve/api.py:721-758); the gradient is the frozen-controller discrete adjoint;
+  * every result and closure carries ``.route`` (gradsolve/base.py:116-140);
+  * ``remat`` maps onto the checkpoint policy: True -> sqrt(N) segments, False -> every
+    state stored, None -> chosen by the memory budget (gradsolve/dispatch.py:268-293 picks
+    ``jax.checkpoint`` for the same trade).
+
+Inputs may be numpy arrays or torch tensors; closures return float64 CUDA tensors and are
+differentiated with ``torch.autograd`` (``loss.backward()`` / ``torch.autograd.grad``).
+There is no CPU path: ``device`` must name a CUDA device.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Callable, Optional
+
+import numpy as np
+import torch
+
+from . import engine
+from .base import Route, SolveResult
+from .fields import FieldSpec, field_for, kernel_params
+from .torch_adapter import ReplayState, replay_apply
+
+ENGINE_TSIT5 = "b200_tsit5"
+ENGINE_ROS23 = "b200_rosenbrock23"
+
+# reference engine names on this path -> the B200 engine that serves them
+ALIASES = {
+    "warp_replay": ENGINE_TSIT5, "tsit5_replay": ENGINE_TSIT5, "warp_ode": ENGINE_TSIT5,
+    "cuda_tsit5": ENGINE_TSIT5,
+    "warp_rosenbrock": ENGINE_ROS23, "cuda_rosenbrock23": ENGINE_ROS23,
+}
+
+DEFAULT_MAX_STEPS = {ENGINE_TSIT5: 4096, ENGINE_ROS23: 50000}  # warp_replay.py:121, :296
+
+
+@dataclass(frozen=True)
+class EngineSpec:
+    """One engine (gradsolve/api.py:48-71): name, supports(problem), solve, reverse."""
+    name: str
+    method: str
+    supports: Callable
+    solve: Callable
+    reverse: Optional[Callable] = None
+
+
+def _supports_tsit5(problem) -> bool:
+    return field_for(problem) is not None
+
+
+def _supports_ros23(problem) -> bool:
+    spec = field_for(problem)
+    return spec is not None and spec.stiff_ok
+
+
+def _device(device) -> torch.device:
+    dev = torch.device(device if device is not None else "cuda")
+    if dev.type != "cuda":
+        raise ValueError(
+            f"gradsolve_b200 runs on CUDA devices only (got device={device!r}); there is no "
+            "CPU path")
+    if not torch.cuda.is_available():
+        raise RuntimeError("gradsolve_b200 needs a CUDA device, and none is visible")
+    return dev
+
+
+def _as_tensor(x, dev: torch.device) -> torch.Tensor:
+    if isinstance(x, torch.Tensor):
+        return x.to(device=dev, dtype=torch.float64)
+    return torch.as_tensor(np.asarray(x, dtype=np.float64), device=dev)
+
+
+def _prepare(problem, y0, params, dev):
+    spec = field_for(problem)
+    if spec is None:
+        raise ValueError(
+            f"gradsolve_b200 has no registered field for problem {getattr(problem, 'name', '?')!r}"
+            "; supported names: 'diffeqgpu_lorenz', 'lorenz', 'vdp', 'lotka_volterra', "
+            "'linear_ladder_<D>' (D in 1,2,3,4,8), 'robertson'")
+    y0_np = y0 if isinstance(y0, torch.Tensor) else np.asarray(y0, dtype=np.float64)
+    if y0_np.ndim == 1:
+        y0_np = y0_np[None, :]
+    if y0_np.shape[-1] != spec.dim:
+        raise ValueError(f"y0 must be (n, {spec.dim}) for {problem.name!r}; got {tuple(y0_np.shape)}")
+    if isinstance(params, torch.Tensor):
+        p_t = params.to(device=dev, dtype=torch.float64)
+        if p_t.ndim == 1:
+            p_t = p_t[:, None]
+    else:
+        p_np = np.asarray(params, dtype=np.float64)
+        if p_np.ndim == 1:
+            p_np = p_np[:, None]
+        p_t = torch.as_tensor(p_np, device=dev)
+    y0_t = _as_tensor(y0_np, dev).contiguous()
+    if p_t.shape[0] != y0_t.shape[0]:
+        raise ValueError(f"y0 has {y0_t.shape[0]} trajectories but params has {p_t.shape[0]}")
+    if p_t.shape[1] < spec.nparam:
+        if not spec.key.startswith("linear_"):
+            kernel_params(spec, np.zeros((1, p_t.shape[1])))  # raises the column-count error
+        p_t = torch.nn.functional.pad(p_t, (0, spec.nparam - p_t.shape[1]))
+    pk = p_t[:, : spec.nparam].contiguous()
+    return spec, y0_t, p_t.contiguous(), pk
+
+
+def _resolve(problem, engine_name: str, reasons: list) -> str:
+    if engine_name == "auto":
+        return ENGINE_ROS23 if getattr(problem, "is_stiff", False) else ENGINE_TSIT5
+    if engine_name in ENGINE_REGISTRY:
+        return engine_name
+    if engine_name in ALIASES:
+        reasons.append(f"served-by-{ALIASES[engine_name]}")
+        return ALIASES[engine_name]
+    raise ValueError(f"unknown engine {engine_name!r}; known: {sorted(ENGINE_REGISTRY)} + "
+                     f"reference names {sorted(ALIASES)}")
+
+
+def _t1_arg(problem, t1, dev):
+    if t1 is None:
+        return float(problem.t1), None
+    t1a = np.asarray(t1, dtype=np.float64)
+    if t1a.ndim == 0:
+        return float(t1a), None
+    return float(t1a.max()), torch.as_tensor(t1a, device=dev).contiguous()
+
+
+def _engine_solve(name):
+    method = ENGINE_REGISTRY[name].method
+
+    def run(problem, y0, params, *, rtol, atol, device="cuda", max_steps=None, t1=None):
+        dev = _device(device)
+        spec, y0_t, _p, pk = _prepare(problem, y0, params, dev)
+        t1s, t1v = _t1_arg(problem, t1, dev)
+        ms = int(max_steps or 100000)
+        r = engine.forward_record(method, spec, y0_t, pk, t0=float(problem.t0), t1=t1s,
+                                  t1v=t1v, rtol=rtol, atol=atol, max_steps=ms, record=False)
+        yf = r.y_final.cpu().numpy()
+        st = r.status.cpu().numpy()
+        yf[st != 0] = np.nan  # failed rows NaN'd, as the reference driver does (warp_ode.py:319)
+        return SolveResult(y_final=yf, accepted_steps=r.n_acc.cpu().numpy().astype(np.int64),
+                           rejected_steps=r.n_rej.cpu().numpy().astype(np.int64), solver=name)
+    return run
+
+
+def solve(problem, y0, params, *, saveat=None, engine: str = "auto", rtol: float = 1e-6,
+          atol: float = 1e-9, device: str = "cuda", max_steps: Optional[int] = None,
+          t1=None, **unused) -> SolveResult:
+    """Forward ensemble solve (gradsolve/api.py:291-400).  Routes like the reference and
+    returns a host ``SolveResult`` with true per-trajectory accepted/rejected counts.
+    ``t1`` (optional) overrides ``problem.t1`` with a scalar or per-trajectory end times."""
+    if saveat is not None:
+        raise NotImplementedError("saveat is not available on the B200 engines yet")
+    reasons: list[str] = []
+    name = _resolve(problem, engine, reasons)
+    spec = ENGINE_REGISTRY[name]
+    if not spec.supports(problem):
+        raise ValueError(f"engine {name!r} does not support problem {problem.name!r}")
+    res = spec.solve(problem, y0, params, rtol=rtol, atol=atol, device=device,
+                     max_steps=max_steps, t1=t1)
+    res.solver = name
+    res.route = Route(requested=engine, actual=name, reason="; ".join(reasons) or None)
+    return res
+
+
+_VALID_WRT = "'params', 'y0', or ('y0', 'params')"
+
+
+def _normalize_wrt(wrt) -> tuple:
+    if wrt == "params":
+        return ("params",)
+    if wrt == "y0":
+        return ("y0",)
+    if isinstance(wrt, (tuple, list, set, frozenset)) and set(wrt) == {"y0", "params"}:
+        return ("y0", "params")
+    raise ValueError(f"invalid wrt={wrt!r}; expected {_VALID_WRT}")
+
+
+def build_replay_state(problem, y0, params, *, method: str, rtol: float, atol: float,
+                       device="cuda", max_steps: Optional[int] = None, checkpoint="auto",
+                       t1=None, precision: str = "float64"):
+    """Record the mesh once and return (ReplayState, y0 tensor, params tensor)."""
+    dev = _device(device)
+    spec, y0_t, p_t, pk = _prepare(problem, y0, params, dev)
+    t1s, t1v = _t1_arg(problem, t1, dev)
+    ms = int(max_steps or 100000)
+    r = engine.forward_record(method, spec, y0_t, pk, t0=float(problem.t0), t1=t1s, t1v=t1v,
+                              rtol=rtol, atol=atol, max_steps=ms, checkpoint=checkpoint,
+                              precision=precision)
+    engine.raise_on_failed(r, ms, t1s)
+    state = ReplayState(r, y0_t, pk, spec.nparam, precision=precision)
+    return state, y0_t, p_t
+
+
+def _make_reverse(name):
+    method = ENGINE_REGISTRY[name].method
+
+    def reverse(problem, y0, params, *, rtol, atol, device="cuda", remat=None, wrt=("params",),
+                max_steps=None, checkpoint=None, t1=None, precision="float64"):
+        if checkpoint is None:
+            checkpoint = "auto" if remat is None else ("sqrt" if remat else "all")
+        ms = max_steps or DEFAULT_MAX_STEPS[name]
+        state, y0_t, p_t = build_replay_state(problem, y0, params, method=method, rtol=rtol,
+                                              atol=atol, device=device, max_steps=ms,
+                                              checkpoint=checkpoint, t1=t1,
+                                              precision=precision)
+        dev = y0_t.device
+
+        def kernel(z, p):
+            return replay_apply(state, _as_tensor(z, dev), _as_tensor(p, dev))
+
+        if wrt == ("y0",):
+            fn = lambda z: kernel(z, p_t)  # noqa: E731
+        elif wrt == ("params",):
+            fn = lambda p: kernel(y0_t, p)  # noqa: E731
+        else:
+            fn = lambda z, p: kernel(z, p)  # noqa: E731
+        fn.state = state
+        return fn
+    return reverse
+
+
+def grad_closure(problem, y0, params, *, wrt="params", saveat=None, precision: str = "float64",
+                 engine: str = "auto", rtol: float = 1e-6, atol: float = 1e-9,
+                 device: str = "cuda", remat: Optional[bool] = None,
+                 max_steps: Optional[int] = None, checkpoint=None, t1=None, **unused):
+    """Record the frozen step mesh at (y0, params) and return a differentiable closure
+    (gradsolve/api.py:792-1030).  ``closure(params) -> y_final`` (n, dim) for the default
+    ``wrt="params"``; ``closure(y0)`` for ``wrt="y0"``; ``closure(y0, params)`` for both.
+    The closure carries ``.route`` and ``.state`` (the device record)."""
+    wrt_t = _normalize_wrt(wrt)
+    if saveat is not None:
+        raise NotImplementedError("saveat is not available on the B200 engines yet")
+    if precision not in ("float64",):
+        raise ValueError(f"precision {precision!r} is not available; use 'float64'")
+    reasons: list[str] = []
+    name = _resolve(problem, engine, reasons)
+    spec = ENGINE_REGISTRY[name]
+    if not spec.supports(problem):
+        raise ValueError(f"engine {name!r} does not support problem {problem.name!r}")
+    fn = spec.reverse(problem, y0, params, rtol=rtol, atol=atol, device=device, remat=remat,
+                      wrt=wrt_t, max_steps=max_steps, checkpoint=checkpoint, t1=t1,
+                      precision=precision)
+    fn.route = Route(requested=engine, actual=name, reason="; ".join(reasons) or None)
+    return fn
+
+
+ENGINE_REGISTRY: dict[str, EngineSpec] = {}
+for _name, _method, _sup in ((ENGINE_TSIT5, engine.METHOD_TSIT5, _supports_tsit5),
+                             (ENGINE_ROS23, engine.METHOD_ROS23, _supports_ros23)):
+    ENGINE_REGISTRY[_name] = EngineSpec(_name, _method, _sup, None, None)
+for _name in list(ENGINE_REGISTRY):
+    _s = ENGINE_REGISTRY[_name]
+    ENGINE_REGISTRY[_name] = EngineSpec(_s.name, _s.method, _s.supports, _engine_solve(_name),
+                                        _make_reverse(_name))
+
+__all__ = ["solve", "grad_closure", "ENGINE_REGISTRY", "ALIASES", "FieldSpec"]

@@ -1,0 +1,374 @@
+// gs_abi.cu -- the extern "C" entry points of libgsolve.so (declared in include/gsolve.h).
+//
+// Host-side argument checking, field dispatch to the templated kernels, and launch on the
+// caller's stream.  The library allocates nothing and keeps no state besides the
+// per-thread error message.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/gsolve.h"
+#include "gs_fields.cuh"
+#include "gs_ros23.cuh"
+#include "gs_tableau.cuh"
+#include "gs_tsit5.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_check(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(GS_ERR_CUDA, std::string("CUDA: ") + what + ": " + cudaGetErrorString(e));
+  return GS_OK;
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+bool aligned8(const void* p) { return ((uintptr_t)p & 7u) == 0; }
+
+constexpr int kBlock = 128;
+
+unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+int field_dims(int field, int* D, int* P) {
+  switch (field) {
+    case gs::FIELD_LORENZ: *D = 3; *P = 1; return GS_OK;
+    case gs::FIELD_VDP: *D = 2; *P = 1; return GS_OK;
+    case gs::FIELD_LOTKA_VOLTERRA: *D = 2; *P = 4; return GS_OK;
+    case gs::FIELD_ROBERTSON: *D = 3; *P = 3; return GS_OK;
+    case gs::FIELD_LORENZ3: *D = 3; *P = 3; return GS_OK;
+    case 4001: *D = 1; *P = 1; return GS_OK;
+    case 4002: *D = 2; *P = 1; return GS_OK;
+    case 4003: *D = 3; *P = 1; return GS_OK;
+    case 4004: *D = 4; *P = 1; return GS_OK;
+    case 4008: *D = 8; *P = 1; return GS_OK;
+  }
+  return fail(GS_ERR_FIELD, "unknown field code " + std::to_string(field));
+}
+
+// Non-stiff fields usable by the Tsit5 kernels.
+#define GS_TSIT5_DISPATCH(field, FN, ...)                                                   \
+  switch (field) {                                                                          \
+    case gs::FIELD_LORENZ: return FN<gs::Lorenz>(__VA_ARGS__);                              \
+    case gs::FIELD_LORENZ3: return FN<gs::Lorenz3>(__VA_ARGS__);                            \
+    case gs::FIELD_VDP: return FN<gs::VdP>(__VA_ARGS__);                                    \
+    case gs::FIELD_LOTKA_VOLTERRA: return FN<gs::LotkaVolterra>(__VA_ARGS__);               \
+    case gs::FIELD_ROBERTSON: return FN<gs::Robertson>(__VA_ARGS__);                        \
+    case 4001: return FN<gs::Linear<1>>(__VA_ARGS__);                                       \
+    case 4002: return FN<gs::Linear<2>>(__VA_ARGS__);                                       \
+    case 4003: return FN<gs::Linear<3>>(__VA_ARGS__);                                       \
+    case 4004: return FN<gs::Linear<4>>(__VA_ARGS__);                                       \
+    case 4008: return FN<gs::Linear<8>>(__VA_ARGS__);                                       \
+    default: return fail(GS_ERR_FIELD, "unknown field code " + std::to_string(field));      \
+  }
+
+// Fields with an analytic Jacobian, usable by the Rosenbrock23 kernels.
+#define GS_ROS23_DISPATCH(field, FN, ...)                                                   \
+  switch (field) {                                                                          \
+    case gs::FIELD_ROBERTSON: return FN<gs::Robertson>(__VA_ARGS__);                        \
+    case 4001: return FN<gs::Linear<1>>(__VA_ARGS__);                                       \
+    case 4002: return FN<gs::Linear<2>>(__VA_ARGS__);                                       \
+    case 4003: return FN<gs::Linear<3>>(__VA_ARGS__);                                       \
+    case 4004: return FN<gs::Linear<4>>(__VA_ARGS__);                                       \
+    case 4008: return FN<gs::Linear<8>>(__VA_ARGS__);                                       \
+    default:                                                                                \
+      return fail(GS_ERR_FIELD,                                                             \
+                  "field " + std::to_string(field) + " has no analytic Jacobian for Rosenbrock23"); \
+  }
+
+template <class F>
+int launch_tsit5_record(const gs::RecordArgs& a, cudaStream_t s) {
+  gs::tsit5_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+  return cuda_check("tsit5_record_kernel");
+}
+template <class F>
+int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s) {
+  gs::tsit5_replay_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+  return cuda_check("tsit5_replay_kernel");
+}
+template <class F>
+int launch_tsit5_adjoint(const gs::AdjointArgs& a, cudaStream_t s) {
+  gs::tsit5_adjoint_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+  return cuda_check("tsit5_adjoint_kernel");
+}
+template <class F>
+int launch_ros23_record(const gs::RecordArgs& a, cudaStream_t s) {
+  gs::ros23_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+  return cuda_check("ros23_record_kernel");
+}
+template <class F>
+int launch_ros23_replay(const gs::ReplayArgs& a, cudaStream_t s) {
+  gs::ros23_replay_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+  return cuda_check("ros23_replay_kernel");
+}
+template <class F>
+int launch_ros23_adjoint(const gs::AdjointArgs& a, cudaStream_t s) {
+  gs::ros23_adjoint_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+  return cuda_check("ros23_adjoint_kernel");
+}
+
+__global__ void device_tableau_kernel(double* out) {
+  using T = gs::Tsit5;
+  using C = gs::Ctrl;
+  using R = gs::Ros23;
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const double v[41] = {T::C2,  T::C3,  T::C4,  T::C5,  T::A21, T::A31, T::A32, T::A41, T::A42,
+                        T::A43, T::A51, T::A52, T::A53, T::A54, T::A61, T::A62, T::A63, T::A64,
+                        T::A65, T::B1,  T::B2,  T::B3,  T::B4,  T::B5,  T::B6,  T::B7,  T::E1,
+                        T::E2,  T::E3,  T::E4,  T::E5,  T::E6,  T::E7,  C::SAFETY, C::ERR_FLOOR,
+                        C::FAC_MIN, C::FAC_MAX, T::ORDER_EXP, R::D, R::E32, R::ORDER_EXP};
+  for (int i = 0; i < 41; ++i) out[i] = v[i];
+}
+
+__global__ void record_from_padded_kernel(long long n, long long S, const double* dts,
+                                          long long ld, double* rec, int cap, int* n_steps) {
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const double* row = dts + j * ld;
+  long long last = 0;
+  for (long long s = 0; s < S; ++s)
+    if (row[s] != 0.0) last = s + 1;
+  const long long nch = (last + 3) / 4;
+  for (long long c = 0; c < nch; ++c) {
+    double v[4];
+    for (int q = 0; q < 4; ++q) {
+      const long long s = c * 4 + q;
+      v[q] = s < last ? row[s] : 0.0;
+    }
+    gs::store_rec_chunk(rec, n, j, (int)c, v[0], v[1], v[2], v[3]);
+  }
+  n_steps[j] = (int)last;
+  (void)cap;
+}
+
+__global__ void record_to_padded_kernel(long long n, const double* rec, const int* n_acc,
+                                        long long S, double* dts) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * S) return;
+  const long long j = idx / S, s = idx % S;
+  dts[idx] = s < n_acc[j] ? rec[gs::rec_index(j, s, n)] : 0.0;
+}
+
+int check_record_args(const char* who, long long n, const double* y0, const double* p,
+                      double rtol, double atol, int max_steps, int cap, int ckpt_every,
+                      const double* rec, const double* ckpt, const double* yf, const int* n_acc,
+                      const int* n_rej, const int* status) {
+  const std::string w(who);
+  if (n < 0) return fail(GS_ERR_ARG, w + ": n < 0");
+  if (!y0 || !p || !yf || !n_acc || !n_rej || !status)
+    return fail(GS_ERR_ARG, w + ": y0, p, y_final, n_acc, n_rej and status are required");
+  if (!aligned8(y0) || !aligned8(p) || !aligned8(yf))
+    return fail(GS_ERR_ARG, w + ": float64 arrays must be 8-byte aligned");
+  if (!(rtol >= 0.0) || !(atol >= 0.0)) return fail(GS_ERR_ARG, w + ": rtol/atol must be >= 0");
+  if (max_steps < 0) return fail(GS_ERR_ARG, w + ": max_steps < 0");
+  if ((rec || ckpt) && cap < 1) return fail(GS_ERR_ARG, w + ": cap must be >= 1 with a record");
+  if (rec && !aligned16(rec)) return fail(GS_ERR_ARG, w + ": rec must be 16-byte aligned");
+  if (ckpt) {
+    if (!aligned16(ckpt)) return fail(GS_ERR_ARG, w + ": ckpt must be 16-byte aligned");
+    if (ckpt_every < 1 || ckpt_every > gs::KMAX)
+      return fail(GS_ERR_ARG, w + ": ckpt_every must be in [1, " + std::to_string(gs::KMAX) + "]");
+  }
+  return GS_OK;
+}
+
+int check_adjoint_args(const char* who, long long n, const double* p, const double* rec,
+                       const int* n_acc, int cap, const double* ckpt, int ckpt_every,
+                       const double* ybar) {
+  const std::string w(who);
+  if (n < 0) return fail(GS_ERR_ARG, w + ": n < 0");
+  if (!p || !rec || !n_acc || !ckpt || !ybar)
+    return fail(GS_ERR_ARG, w + ": p, rec, n_acc, ckpt and ybar are required");
+  if (cap < 1) return fail(GS_ERR_ARG, w + ": cap must be >= 1");
+  if (!aligned16(rec) || !aligned16(ckpt))
+    return fail(GS_ERR_ARG, w + ": rec and ckpt must be 16-byte aligned");
+  if (ckpt_every < 1 || ckpt_every > gs::KMAX)
+    return fail(GS_ERR_ARG, w + ": ckpt_every must be in [1, " + std::to_string(gs::KMAX) + "]");
+  return GS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gs_version(void) { return 100; }
+
+const char* gs_last_error(void) { return g_err.c_str(); }
+
+int gs_field_dims(int field, int* D, int* P) {
+  if (!D || !P) return fail(GS_ERR_ARG, "gs_field_dims: null output");
+  return field_dims(field, D, P);
+}
+
+int gs_tableau(double* out, int len) {
+  using T = gs::Tsit5;
+  using C = gs::Ctrl;
+  using R = gs::Ros23;
+  if (!out || len < 41) return fail(GS_ERR_ARG, "gs_tableau: need 41 doubles");
+  const double v[41] = {T::C2,  T::C3,  T::C4,  T::C5,  T::A21, T::A31, T::A32, T::A41, T::A42,
+                        T::A43, T::A51, T::A52, T::A53, T::A54, T::A61, T::A62, T::A63, T::A64,
+                        T::A65, T::B1,  T::B2,  T::B3,  T::B4,  T::B5,  T::B6,  T::B7,  T::E1,
+                        T::E2,  T::E3,  T::E4,  T::E5,  T::E6,  T::E7,  C::SAFETY, C::ERR_FLOOR,
+                        C::FAC_MIN, C::FAC_MAX, T::ORDER_EXP, R::D, R::E32, R::ORDER_EXP};
+  for (int i = 0; i < 41; ++i) out[i] = v[i];
+  return GS_OK;
+}
+
+int gs_device_tableau(double* out_dev, void* stream) {
+  if (!out_dev) return fail(GS_ERR_ARG, "gs_device_tableau: null output");
+  device_tableau_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(out_dev);
+  return cuda_check("device_tableau_kernel");
+}
+
+size_t gs_record_bytes(long long n, int cap) {
+  if (n <= 0 || cap <= 0) return 0;
+  return (size_t)((cap + 3) / 4) * (size_t)n * 4u * sizeof(double);
+}
+
+int gs_ckpt_slots(int cap, int ckpt_every) {
+  if (cap <= 0 || ckpt_every <= 0) return 0;
+  return (cap + ckpt_every - 1) / ckpt_every + 1;
+}
+
+size_t gs_ckpt_bytes(int field, long long n, int cap, int ckpt_every) {
+  int D, P;
+  if (field_dims(field, &D, &P) != GS_OK || n <= 0) return 0;
+  return (size_t)gs_ckpt_slots(cap, ckpt_every) * (size_t)n * (size_t)gs::ckpt_width(D) *
+         sizeof(double);
+}
+
+int gs_max_ckpt_every(void) { return gs::KMAX; }
+
+int gs_tsit5_fwd_record(int field, int precision, long long n, const double* y0,
+                        const double* p, double t0, const double* t1v, double t1, double rtol,
+                        double atol, double dt0, int max_steps, int cap, int ckpt_every,
+                        double* rec, double* ckpt, double* y_final, int* n_acc, int* n_rej,
+                        int* status, void* stream) {
+  if (precision != GS_PREC_F64)
+    return fail(GS_ERR_PRECISION, "gs_tsit5_fwd_record: precision mode not built");
+  int rc = check_record_args("gs_tsit5_fwd_record", n, y0, p, rtol, atol, max_steps, cap,
+                             ckpt_every, rec, ckpt, y_final, n_acc, n_rej, status);
+  if (rc) return rc;
+  int D, P;
+  if ((rc = field_dims(field, &D, &P))) return rc;
+  if (n == 0) return GS_OK;
+  gs::RecordArgs a{n, y0, p, t0, t1, rtol, atol, dt0, t1v, max_steps, cap, ckpt_every,
+                   gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status};
+  GS_TSIT5_DISPATCH(field, launch_tsit5_record, a, (cudaStream_t)stream)
+}
+
+int gs_tsit5_replay(int field, int precision, long long n, const double* y0, const double* p,
+                    double t0, const double* rec, const int* n_acc, int cap, int ckpt_every,
+                    double* ckpt, double* y_final, void* stream) {
+  if (precision != GS_PREC_F64)
+    return fail(GS_ERR_PRECISION, "gs_tsit5_replay: precision mode not built");
+  if (n < 0) return fail(GS_ERR_ARG, "gs_tsit5_replay: n < 0");
+  if (!y0 || !p || !rec || !n_acc || !y_final)
+    return fail(GS_ERR_ARG, "gs_tsit5_replay: y0, p, rec, n_acc and y_final are required");
+  if (cap < 1 || !aligned16(rec)) return fail(GS_ERR_ARG, "gs_tsit5_replay: bad record");
+  if (ckpt && (!aligned16(ckpt) || ckpt_every < 1 || ckpt_every > gs::KMAX))
+    return fail(GS_ERR_ARG, "gs_tsit5_replay: bad checkpoint buffer or interval");
+  int D, P, rc;
+  if ((rc = field_dims(field, &D, &P))) return rc;
+  if (n == 0) return GS_OK;
+  gs::ReplayArgs a{n, y0, p, t0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every), ckpt,
+                   y_final};
+  GS_TSIT5_DISPATCH(field, launch_tsit5_replay, a, (cudaStream_t)stream)
+}
+
+int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, const double* rec,
+                     const int* n_acc, int cap, const double* ckpt, int ckpt_every,
+                     const double* ybar, double* gy0, double* gp, void* stream) {
+  if (precision != GS_PREC_F64)
+    return fail(GS_ERR_PRECISION, "gs_tsit5_adjoint: precision mode not built");
+  int rc = check_adjoint_args("gs_tsit5_adjoint", n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar);
+  if (rc) return rc;
+  int D, P;
+  if ((rc = field_dims(field, &D, &P))) return rc;
+  if (n == 0) return GS_OK;
+  gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp};
+  GS_TSIT5_DISPATCH(field, launch_tsit5_adjoint, a, (cudaStream_t)stream)
+}
+
+int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,
+                        const double* p, double t0, const double* t1v, double t1, double rtol,
+                        double atol, double dt0, int max_steps, int cap, int ckpt_every,
+                        double* rec, double* ckpt, double* y_final, int* n_acc, int* n_rej,
+                        int* status, void* stream) {
+  if (precision != GS_PREC_F64)
+    return fail(GS_ERR_PRECISION, "gs_ros23_fwd_record: precision mode not built");
+  int rc = check_record_args("gs_ros23_fwd_record", n, y0, p, rtol, atol, max_steps, cap,
+                             ckpt_every, rec, ckpt, y_final, n_acc, n_rej, status);
+  if (rc) return rc;
+  int D, P;
+  if ((rc = field_dims(field, &D, &P))) return rc;
+  if (n == 0) return GS_OK;
+  gs::RecordArgs a{n, y0, p, t0, t1, rtol, atol, dt0, t1v, max_steps, cap, ckpt_every,
+                   gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status};
+  GS_ROS23_DISPATCH(field, launch_ros23_record, a, (cudaStream_t)stream)
+}
+
+int gs_ros23_replay(int field, int precision, long long n, const double* y0, const double* p,
+                    double t0, const double* rec, const int* n_acc, int cap, int ckpt_every,
+                    double* ckpt, double* y_final, void* stream) {
+  if (precision != GS_PREC_F64)
+    return fail(GS_ERR_PRECISION, "gs_ros23_replay: precision mode not built");
+  if (n < 0) return fail(GS_ERR_ARG, "gs_ros23_replay: n < 0");
+  if (!y0 || !p || !rec || !n_acc || !y_final)
+    return fail(GS_ERR_ARG, "gs_ros23_replay: y0, p, rec, n_acc and y_final are required");
+  if (cap < 1 || !aligned16(rec)) return fail(GS_ERR_ARG, "gs_ros23_replay: bad record");
+  if (ckpt && (!aligned16(ckpt) || ckpt_every < 1 || ckpt_every > gs::KMAX))
+    return fail(GS_ERR_ARG, "gs_ros23_replay: bad checkpoint buffer or interval");
+  int D, P, rc;
+  if ((rc = field_dims(field, &D, &P))) return rc;
+  if (n == 0) return GS_OK;
+  gs::ReplayArgs a{n, y0, p, t0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every), ckpt,
+                   y_final};
+  GS_ROS23_DISPATCH(field, launch_ros23_replay, a, (cudaStream_t)stream)
+}
+
+int gs_ros23_adjoint(int field, int precision, long long n, const double* p, const double* rec,
+                     const int* n_acc, int cap, const double* ckpt, int ckpt_every,
+                     const double* ybar, double* gy0, double* gp, void* stream) {
+  if (precision != GS_PREC_F64)
+    return fail(GS_ERR_PRECISION, "gs_ros23_adjoint: precision mode not built");
+  int rc = check_adjoint_args("gs_ros23_adjoint", n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar);
+  if (rc) return rc;
+  int D, P;
+  if ((rc = field_dims(field, &D, &P))) return rc;
+  if (n == 0) return GS_OK;
+  gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp};
+  GS_ROS23_DISPATCH(field, launch_ros23_adjoint, a, (cudaStream_t)stream)
+}
+
+int gs_record_from_padded(long long n, long long S, const double* dts, long long ld,
+                          double* rec, int cap, int* n_steps, void* stream) {
+  if (n < 0 || S < 0 || ld < S) return fail(GS_ERR_ARG, "gs_record_from_padded: bad sizes");
+  if (S > cap) return fail(GS_ERR_ARG, "gs_record_from_padded: S exceeds the record capacity");
+  if (!rec || !n_steps || (S > 0 && !dts))
+    return fail(GS_ERR_ARG, "gs_record_from_padded: null buffer");
+  if (!aligned16(rec)) return fail(GS_ERR_ARG, "gs_record_from_padded: rec must be 16-byte aligned");
+  if (n == 0) return GS_OK;
+  record_from_padded_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(n, S, dts, ld, rec,
+                                                                               cap, n_steps);
+  return cuda_check("record_from_padded_kernel");
+}
+
+int gs_record_to_padded(long long n, int cap, const double* rec, const int* n_acc, long long S,
+                        double* dts, void* stream) {
+  if (n < 0 || S < 0 || S > cap) return fail(GS_ERR_ARG, "gs_record_to_padded: bad sizes");
+  if (!rec || !n_acc || (n * S > 0 && !dts)) return fail(GS_ERR_ARG, "gs_record_to_padded: null buffer");
+  if (n == 0 || S == 0) return GS_OK;
+  const long long total = n * S;
+  record_to_padded_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+      n, rec, n_acc, S, dts);
+  return cuda_check("record_to_padded_kernel");
+}
+
+}  // extern "C"

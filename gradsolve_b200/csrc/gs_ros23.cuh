@@ -1,0 +1,391 @@
+// gs_ros23.cuh -- adaptive Rosenbrock23 (ode23s, autonomous) forward with dt record, its
+// frozen-mesh replay and the hand-written reverse-replay adjoint (float64).
+//
+// Forward: the fused kernel of gradsolve/warp/_warp_rosenbrock.py:383-452, specified by
+// tests/_oracles/gradsolve_g2_spike_oracle.py:138-184:
+//   W = I - d*h*J(y);  k1 = W\f(y);  k2 = W\(f(y + h/2 k1) - k1) + k1;  ynew = y + h k2;
+//   k3 = W\(f(ynew) - e32 (k2 - F1) - 2 (k1 - F0));  err_vec = h/6 (k1 - 2 k2 + k3);
+//   WRMS norm, accept iff err <= 1, dt = h*clip(0.9*max(err,1e-10)^(-1/3), 0.2, 5) after both
+//   outcomes.  W is factored once per attempt (partial pivoting, division by the pivot) and
+//   the three solves reuse the factors: the same operations, in the same order, as the
+//   reference kernel's three fresh eliminations (_gauss_solve, :346-381), because a row swap
+//   moves the stored multipliers with the row.  The 3x3 LU stays in registers.
+// Replay: gradsolve/solvers/rosenbrock23_step.py:47-66 (no k3) with the analytic Jacobian.
+// Adjoint: reverse of that step, including the second-order term through W = I - d dt J(y,p):
+//   Wbar = -(W^-T k2bar) k2'^T - (W^-T k1bar) k1^T,  then  d<-d dt Wbar, J(y,p)>/d(y,p).
+// Record, checkpoint and segment scheme: as the Tsit5 kernels (gs_tsit5.cuh).
+#pragma once
+#include "gs_fields.cuh"
+#include "gs_tableau.cuh"
+#include "gs_tsit5.cuh"
+
+namespace gs {
+
+template <int D>
+struct LU {
+  double a[D * D];  // L (unit, below diagonal) and U (on/above), row-swapped
+  int piv[D];
+};
+
+template <int D>
+__device__ __forceinline__ void lu_factor(LU<D>& f) {
+#pragma unroll
+  for (int col = 0; col < D; ++col) {
+    int pv = col;
+    double big = fabs(f.a[col * D + col]);
+#pragma unroll
+    for (int r = col + 1; r < D; ++r) {
+      const double v = fabs(f.a[r * D + col]);
+      if (v > big) {
+        big = v;
+        pv = r;
+      }
+    }
+    f.piv[col] = pv;
+    if (pv != col) {
+#pragma unroll
+      for (int c = 0; c < D; ++c) {
+        // select-based swap keeps the matrix in registers (no dynamic indexing)
+#pragma unroll
+        for (int r = col + 1; r < D; ++r) {
+          if (r == pv) {
+            const double tmp = f.a[col * D + c];
+            f.a[col * D + c] = f.a[r * D + c];
+            f.a[r * D + c] = tmp;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int r = col + 1; r < D; ++r) {
+      const double factor = f.a[r * D + col] / f.a[col * D + col];
+      f.a[r * D + col] = factor;
+#pragma unroll
+      for (int c = col + 1; c < D; ++c) f.a[r * D + c] = f.a[r * D + c] - factor * f.a[col * D + c];
+    }
+  }
+}
+
+// x = W^-1 b
+template <int D>
+__device__ __forceinline__ void lu_solve(const LU<D>& f, const double* b, double* x) {
+#pragma unroll
+  for (int i = 0; i < D; ++i) x[i] = b[i];
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+#pragma unroll
+    for (int r = k + 1; r < D; ++r) {
+      if (r == f.piv[k]) {
+        const double tmp = x[k];
+        x[k] = x[r];
+        x[r] = tmp;
+      }
+    }
+#pragma unroll
+    for (int r = k + 1; r < D; ++r) x[r] = x[r] - f.a[r * D + k] * x[k];
+  }
+#pragma unroll
+  for (int ii = 0; ii < D; ++ii) {
+    const int i = D - 1 - ii;
+    double s = x[i];
+#pragma unroll
+    for (int c = i + 1; c < D; ++c) s = s - f.a[i * D + c] * x[c];
+    x[i] = s / f.a[i * D + i];
+  }
+}
+
+// x = W^-T b   (W = P^T L U  =>  W^T = U^T L^T P)
+template <int D>
+__device__ __forceinline__ void lu_solve_t(const LU<D>& f, const double* b, double* x) {
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    double s = b[i];
+#pragma unroll
+    for (int jj = 0; jj < i; ++jj) s = s - f.a[jj * D + i] * x[jj];
+    x[i] = s / f.a[i * D + i];
+  }
+#pragma unroll
+  for (int ii = 0; ii < D; ++ii) {
+    const int i = D - 1 - ii;
+    double s = x[i];
+#pragma unroll
+    for (int r = i + 1; r < D; ++r) s = s - f.a[r * D + i] * x[r];
+    x[i] = s;
+  }
+#pragma unroll
+  for (int kk = 0; kk < D; ++kk) {
+    const int k = D - 1 - kk;
+#pragma unroll
+    for (int r = k + 1; r < D; ++r) {
+      if (r == f.piv[k]) {
+        const double tmp = x[k];
+        x[k] = x[r];
+        x[r] = tmp;
+      }
+    }
+  }
+}
+
+template <class F>
+__device__ __forceinline__ void ros23_build_w(const double* y, const double* p, double h,
+                                              LU<F::D>& W) {
+  constexpr int D = F::D;
+  double J[D * D];
+  F::jac(y, p, J);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+#pragma unroll
+    for (int c = 0; c < D; ++c) W.a[i * D + c] = -Ros23::D * h * J[i * D + c];
+    W.a[i * D + i] = W.a[i * D + i] + 1.0;
+  }
+  lu_factor<D>(W);
+}
+
+// Shared part of the attempt and of the replay step: W factored, F0, k1, F1, k2, ynew.
+template <class F>
+struct RosCore {
+  static constexpr int D = F::D;
+  LU<D> W;
+  double F0[D], k1[D], F1[D], k2[D];
+};
+
+template <class F>
+__device__ __forceinline__ void ros23_core(const double* y, const double* p, double h,
+                                           RosCore<F>& c, double* ynew) {
+  constexpr int D = F::D;
+  double s[D];
+  ros23_build_w<F>(y, p, h, c.W);
+  F::rhs(y, p, c.F0);
+  lu_solve<D>(c.W, c.F0, c.k1);
+#pragma unroll
+  for (int i = 0; i < D; ++i) s[i] = y[i] + 0.5 * h * c.k1[i];
+  F::rhs(s, p, c.F1);
+#pragma unroll
+  for (int i = 0; i < D; ++i) s[i] = c.F1[i] - c.k1[i];
+  lu_solve<D>(c.W, s, c.k2);
+#pragma unroll
+  for (int i = 0; i < D; ++i) c.k2[i] = c.k2[i] + c.k1[i];
+#pragma unroll
+  for (int i = 0; i < D; ++i) ynew[i] = y[i] + h * c.k2[i];
+}
+
+template <class F>
+__device__ __forceinline__ void ros23_replay_step(double* y, const double* p, double dt) {
+  constexpr int D = F::D;
+  RosCore<F> c;
+  double yn[D];
+  ros23_core<F>(y, p, dt, c, yn);
+#pragma unroll
+  for (int i = 0; i < D; ++i) y[i] = yn[i];
+}
+
+template <class F>
+__device__ __forceinline__ void ros23_step_vjp(const double* y, const double* p, double dt,
+                                               double* lam, double* gp) {
+  constexpr int D = F::D;
+  LU<D> W;
+  double F0[D], k1[D], s1[D], F1[D], r2[D], k2p[D];
+  ros23_build_w<F>(y, p, dt, W);
+  F::rhs(y, p, F0);
+  lu_solve<D>(W, F0, k1);
+#pragma unroll
+  for (int i = 0; i < D; ++i) s1[i] = y[i] + 0.5 * dt * k1[i];
+  F::rhs(s1, p, F1);
+#pragma unroll
+  for (int i = 0; i < D; ++i) r2[i] = F1[i] - k1[i];
+  lu_solve<D>(W, r2, k2p);
+
+  double yb[D], k2b[D], k1b[D], r2b[D], s1b[D], r1b[D], G[D * D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    yb[i] = lam[i];
+    k2b[i] = dt * lam[i];
+    k1b[i] = k2b[i];
+    s1b[i] = 0.0;
+  }
+  lu_solve_t<D>(W, k2b, r2b);
+  const double scale = Ros23::D * dt;  // G = -d dt Wbar, Wbar = -(r2b k2p^T + r1b k1^T)
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+#pragma unroll
+    for (int c = 0; c < D; ++c) G[i * D + c] = scale * (r2b[i] * k2p[c]);
+    k1b[i] -= r2b[i];
+  }
+  F::vjp(s1, p, r2b, s1b, gp);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    yb[i] += s1b[i];
+    k1b[i] += 0.5 * dt * s1b[i];
+  }
+  lu_solve_t<D>(W, k1b, r1b);
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int c = 0; c < D; ++c) G[i * D + c] += scale * (r1b[i] * k1[c]);
+  F::vjp(y, p, r1b, yb, gp);
+  F::jac_contract_grad(y, p, G, yb, gp);
+#pragma unroll
+  for (int i = 0; i < D; ++i) lam[i] = yb[i];
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
+  constexpr int D = F::D, P = F::P;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  double y[D], p[P], ynew[D], ev[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) y[i] = a.y0[j * D + i];
+#pragma unroll
+  for (int i = 0; i < P; ++i) p[i] = a.p[j * P + i];
+  double t = a.t0;
+  const double t1 = a.t1v ? a.t1v[j] : a.t1;
+  double dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
+  const bool rec_on = a.rec != nullptr;
+  const bool ck_on = a.ckpt != nullptr;
+  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
+  int acc = 0, rej = 0, st = 0, ck_cnt = 0, ck_slot = 0;
+  double b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
+  for (int it = 0; it < a.max_steps; ++it) {
+    if (t >= t1) break;
+    const double h = (t1 - t < dt) ? (t1 - t) : dt;
+    if (t + h == t) {  // the step no longer advances time
+      st = 2;
+      break;
+    }
+    RosCore<F> c;
+    ros23_core<F>(y, p, h, c, ynew);
+    double F2[D], r3[D], k3[D];
+    F::rhs(ynew, p, F2);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      r3[i] = F2[i] - Ros23::E32 * (c.k2[i] - c.F1[i]) - 2.0 * (c.k1[i] - c.F0[i]);
+    lu_solve<D>(c.W, r3, k3);
+#pragma unroll
+    for (int i = 0; i < D; ++i) ev[i] = (h / 6.0) * (c.k1[i] - 2.0 * c.k2[i] + k3[i]);
+    const double err = wrms_norm<D>(ev, y, ynew, a.rtol, a.atol);
+    if (!(err == err)) {
+      st = 1;
+      break;
+    }
+    if (err <= 1.0) {
+      if ((rec_on || ck_on) && acc >= a.cap) {
+        st = 3;
+        break;
+      }
+      t = t + h;
+#pragma unroll
+      for (int i = 0; i < D; ++i) y[i] = ynew[i];
+      if (rec_on) {
+        b0 = b1;
+        b1 = b2;
+        b2 = b3;
+        b3 = h;
+        if ((acc & 3) == 3) store_rec_chunk(a.rec, a.n, j, acc >> 2, b0, b1, b2, b3);
+      }
+      ++acc;
+      if (ck_on && ++ck_cnt == a.ck_every) {
+        ck_cnt = 0;
+        if (++ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, ck_slot, y, t);
+      }
+    } else {
+      ++rej;
+    }
+    dt = step_controller(err, h, Ros23::ORDER_EXP);
+  }
+  if (st == 0 && !(t >= t1)) st = 1;
+  if (rec_on) {
+    switch (acc & 3) {
+      case 1: store_rec_chunk(a.rec, a.n, j, acc >> 2, b3, 0.0, 0.0, 0.0); break;
+      case 2: store_rec_chunk(a.rec, a.n, j, acc >> 2, b2, b3, 0.0, 0.0); break;
+      case 3: store_rec_chunk(a.rec, a.n, j, acc >> 2, b1, b2, b3, 0.0); break;
+      default: break;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
+  a.n_acc[j] = acc;
+  a.n_rej[j] = rej;
+  a.status[j] = st;
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) ros23_replay_kernel(const ReplayArgs a) {
+  constexpr int D = F::D, P = F::P;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  double y[D], p[P];
+#pragma unroll
+  for (int i = 0; i < D; ++i) y[i] = a.y0[j * D + i];
+#pragma unroll
+  for (int i = 0; i < P; ++i) p[i] = a.p[j * P + i];
+  const int na = a.n_acc[j];
+  double t = a.t0;
+  const bool ck_on = a.ckpt != nullptr;
+  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
+  int ck_cnt = 0, ck_slot = 0;
+  for (int s = 0; s < na; ++s) {
+    const double dt = load_rec(a.rec, a.n, j, s);
+    ros23_replay_step<F>(y, p, dt);
+    t = t + dt;
+    if (ck_on && ++ck_cnt == a.ck_every) {
+      ck_cnt = 0;
+      if (++ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, ck_slot, y, t);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) ros23_adjoint_kernel(const AdjointArgs a) {
+  constexpr int D = F::D, P = F::P;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  double p[P], lam[D], gp[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    p[i] = a.p[j * P + i];
+    gp[i] = 0.0;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
+  const int na = a.n_acc[j];
+  const int K = a.ck_every;
+  const int nseg = (na + K - 1) / K;
+  double seg[KMAX][D];
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int start = sg * K;
+    double y[D];
+    load_ckpt<D>(a.ckpt, a.n, j, sg, y);
+#pragma unroll
+    for (int i = 0; i < D; ++i) seg[0][i] = y[i];
+    for (int q = 1; q < K; ++q) {
+      const int s = start + q - 1;
+      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      if (dt != 0.0) ros23_replay_step<F>(y, p, dt);
+#pragma unroll
+      for (int i = 0; i < D; ++i) seg[q][i] = y[i];
+    }
+    for (int q = K - 1; q >= 0; --q) {
+      const int s = start + q;
+      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      if (dt != 0.0) {
+        double ys[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) ys[i] = seg[q][i];
+        ros23_step_vjp<F>(ys, p, dt, lam, gp);
+      }
+    }
+  }
+  if (a.gy0) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) a.gy0[j * D + i] = lam[i];
+  }
+  if (a.gp) {
+#pragma unroll
+    for (int i = 0; i < P; ++i) a.gp[j * P + i] = gp[i];
+  }
+}
+
+}  // namespace gs

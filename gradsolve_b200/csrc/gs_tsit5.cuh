@@ -1,0 +1,505 @@
+// gs_tsit5.cuh -- adaptive Tsit5 forward with dt record, frozen-mesh replay, and the
+// hand-written reverse-replay adjoint (float64).
+//
+// One thread integrates one trajectory; state, stages and the step-size controller live in
+// registers.  The forward follows tsit5_adaptive (gradsolve/solvers/tsit5_replay.py:62-124):
+// FSAL reuse of k7 on accept, WRMS error norm sc = atol + rtol*max(|y|,|y5|), accept iff
+// err <= 1, dt = h * clip(0.9 * max(err,1e-10)^-0.2, 0.2, 5) after accept AND reject, last
+// step clamped to h = min(dt, t1 - t), at most max_steps attempts.
+//
+// Memory layouts (all in HBM, all 64-bit indexed):
+//   y0, y_final, gy0, ybar : (n, D) row-major float64 (the Python API's layout)
+//   p, gp                   : (n, P) row-major float64
+//   dt record               : chunk-interleaved, 4 steps per 32-byte sector:
+//                             step s of trajectory j lives at ((s/4)*n + j)*4 + s%4.
+//                             A thread buffers 4 accepted dt's in registers and writes the
+//                             whole sector at once (two 16-byte stores), so the record is
+//                             written and read in full sectors even though trajectories
+//                             accept steps at different times.  Entries past n_acc[j] in
+//                             trajectory j's last sector are 0 (identity steps).
+//   checkpoints             : slot c of trajectory j = (y after c*K accepted steps, t), at
+//                             ((c*n + j) * CW) with CW = D+1 rounded up to even (16-byte
+//                             aligned); slot 0 is (y0, t0).  K = ckpt_every.
+//
+// The adjoint walks each trajectory's record backwards in segments of K steps.  For a
+// segment it reloads the checkpoint, recomputes the K-1 interior states into a per-thread
+// array, then applies the step VJPs in reverse.  Every trajectory runs whole segments
+// (n_acc padded up to a multiple of K with dt = 0 identity steps, which are exact
+// identities in value and gradient, gradsolve/solvers/tsit5_step.py:84-86), so the lanes of
+// a warp stay in the same phase (recompute vs VJP) instead of diverging.  With K = 1 every
+// state is a checkpoint and nothing is recomputed.
+#pragma once
+#include "gs_fields.cuh"
+#include "gs_tableau.cuh"
+
+namespace gs {
+
+constexpr int KMAX = 64;  // largest checkpoint interval the adjoint supports
+
+GS_HD int ckpt_width(int D) { return (D + 2) & ~1; }
+
+GS_HD size_t rec_index(long long j, long long s, long long n) {
+  return ((size_t)(s >> 2) * (size_t)n + (size_t)j) * 4u + (size_t)(s & 3);
+}
+
+// numpy's add.reduce order for a length-D array (sequential below 8 terms, 8-way pairwise
+// from 8 up): the reference's np.mean((e/sc)**2).
+template <int D>
+__device__ __forceinline__ double wrms_sum(const double* q) {
+  if constexpr (D < 8) {
+    double s = q[0];
+#pragma unroll
+    for (int i = 1; i < D; ++i) s += q[i];
+    return s;
+  } else {
+    double r[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r[j] = q[j];
+    constexpr int full = D - (D % 8);
+#pragma unroll
+    for (int i = 8; i < full; i += 8)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) r[j] += q[i + j];
+    double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+#pragma unroll
+    for (int i = full; i < D; ++i) res += q[i];
+    return res;
+  }
+}
+
+template <int D>
+__device__ __forceinline__ double wrms_norm(const double* e, const double* y, const double* yn,
+                                            double rtol, double atol) {
+  double q[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    const double sc = atol + rtol * fmax(fabs(y[i]), fabs(yn[i]));
+    const double c = e[i] / sc;
+    q[i] = c * c;
+  }
+  return sqrt(wrms_sum<D>(q) / (double)D);
+}
+
+__device__ __forceinline__ double step_controller(double err, double h, double order_exp) {
+  const double e = err > Ctrl::ERR_FLOOR ? err : Ctrl::ERR_FLOOR;
+  double fac = Ctrl::SAFETY * pow(e, order_exp);
+  fac = fac > Ctrl::FAC_MIN ? fac : Ctrl::FAC_MIN;
+  fac = Ctrl::FAC_MAX < fac ? Ctrl::FAC_MAX : fac;
+  return h * fac;
+}
+
+// --- the shared stage arithmetic ------------------------------------------------------
+// Stages 2..6 inputs and k2..k6 from (y, k1, h).  Used by the forward, the replay and the
+// adjoint's recomputation so every kernel evaluates the same expressions.
+template <class F>
+struct Stages {
+  static constexpr int D = F::D;
+  double k2[D], k3[D], k4[D], k5[D], k6[D];
+};
+
+template <class F>
+__device__ __forceinline__ void tsit5_k2_to_k6(const double* y, const double* p, const double* k1,
+                                               double h, Stages<F>& S) {
+  constexpr int D = F::D;
+  using T = Tsit5;
+  double s[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) s[i] = y[i] + h * (T::A21 * k1[i]);
+  F::rhs(s, p, S.k2);
+#pragma unroll
+  for (int i = 0; i < D; ++i) s[i] = y[i] + h * (T::A31 * k1[i] + T::A32 * S.k2[i]);
+  F::rhs(s, p, S.k3);
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+    s[i] = y[i] + h * (T::A41 * k1[i] + T::A42 * S.k2[i] + T::A43 * S.k3[i]);
+  F::rhs(s, p, S.k4);
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+    s[i] = y[i] + h * (T::A51 * k1[i] + T::A52 * S.k2[i] + T::A53 * S.k3[i] + T::A54 * S.k4[i]);
+  F::rhs(s, p, S.k5);
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+    s[i] = y[i] + h * (T::A61 * k1[i] + T::A62 * S.k2[i] + T::A63 * S.k3[i] + T::A64 * S.k4[i] +
+                       T::A65 * S.k5[i]);
+  F::rhs(s, p, S.k6);
+}
+
+template <class F>
+__device__ __forceinline__ void tsit5_y5(const double* y, const double* k1, const Stages<F>& S,
+                                         double h, double* y5) {
+  using T = Tsit5;
+#pragma unroll
+  for (int i = 0; i < F::D; ++i)
+    y5[i] = y[i] + h * (T::B1 * k1[i] + T::B2 * S.k2[i] + T::B3 * S.k3[i] + T::B4 * S.k4[i] +
+                        T::B5 * S.k5[i] + T::B6 * S.k6[i]);
+}
+
+// One replay step (gradsolve/solvers/tsit5_step.py:80-102).  The B7*k7 term of the
+// reference is an exact +0 (B7 == 0), so k7 is not evaluated here.
+template <class F>
+__device__ __forceinline__ void tsit5_replay_step(double* y, const double* p, double dt) {
+  constexpr int D = F::D;
+  double k1[D], yn[D];
+  Stages<F> S;
+  F::rhs(y, p, k1);
+  tsit5_k2_to_k6<F>(y, p, k1, dt, S);
+  tsit5_y5<F>(y, k1, S, dt, yn);
+#pragma unroll
+  for (int i = 0; i < D; ++i) y[i] = yn[i];
+}
+
+// Reverse of one replay step at (y, dt): lam <- (dy'/dy)^T lam, gp += (dy'/dp)^T lam.
+// Stage 7 carries weight B7 == 0, so its cotangent is exactly zero and it is skipped.
+template <class F>
+__device__ __forceinline__ void tsit5_step_vjp(const double* y, const double* p, double dt,
+                                               double* lam, double* gp) {
+  constexpr int D = F::D;
+  using T = Tsit5;
+  double k1[D], s2[D], s3[D], s4[D], s5[D], s6[D];
+  {
+    double k2[D], k3[D], k4[D], k5[D];
+    F::rhs(y, p, k1);
+#pragma unroll
+    for (int i = 0; i < D; ++i) s2[i] = y[i] + dt * (T::A21 * k1[i]);
+    F::rhs(s2, p, k2);
+#pragma unroll
+    for (int i = 0; i < D; ++i) s3[i] = y[i] + dt * (T::A31 * k1[i] + T::A32 * k2[i]);
+    F::rhs(s3, p, k3);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      s4[i] = y[i] + dt * (T::A41 * k1[i] + T::A42 * k2[i] + T::A43 * k3[i]);
+    F::rhs(s4, p, k4);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      s5[i] = y[i] + dt * (T::A51 * k1[i] + T::A52 * k2[i] + T::A53 * k3[i] + T::A54 * k4[i]);
+    F::rhs(s5, p, k5);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      s6[i] = y[i] + dt * (T::A61 * k1[i] + T::A62 * k2[i] + T::A63 * k3[i] + T::A64 * k4[i] +
+                           T::A65 * k5[i]);
+  }
+  double g[D], kb1[D], kb2[D], kb3[D], kb4[D], kb5[D], kb6[D], sb[D], yb[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    g[i] = dt * lam[i];
+    yb[i] = lam[i];
+    kb1[i] = T::B1 * g[i];
+    kb2[i] = T::B2 * g[i];
+    kb3[i] = T::B3 * g[i];
+    kb4[i] = T::B4 * g[i];
+    kb5[i] = T::B5 * g[i];
+    kb6[i] = T::B6 * g[i];
+  }
+  // stage 6
+#pragma unroll
+  for (int i = 0; i < D; ++i) sb[i] = 0.0;
+  F::vjp(s6, p, kb6, sb, gp);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    yb[i] += sb[i];
+    const double u = dt * sb[i];
+    kb1[i] += T::A61 * u;
+    kb2[i] += T::A62 * u;
+    kb3[i] += T::A63 * u;
+    kb4[i] += T::A64 * u;
+    kb5[i] += T::A65 * u;
+  }
+  // stage 5
+#pragma unroll
+  for (int i = 0; i < D; ++i) sb[i] = 0.0;
+  F::vjp(s5, p, kb5, sb, gp);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    yb[i] += sb[i];
+    const double u = dt * sb[i];
+    kb1[i] += T::A51 * u;
+    kb2[i] += T::A52 * u;
+    kb3[i] += T::A53 * u;
+    kb4[i] += T::A54 * u;
+  }
+  // stage 4
+#pragma unroll
+  for (int i = 0; i < D; ++i) sb[i] = 0.0;
+  F::vjp(s4, p, kb4, sb, gp);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    yb[i] += sb[i];
+    const double u = dt * sb[i];
+    kb1[i] += T::A41 * u;
+    kb2[i] += T::A42 * u;
+    kb3[i] += T::A43 * u;
+  }
+  // stage 3
+#pragma unroll
+  for (int i = 0; i < D; ++i) sb[i] = 0.0;
+  F::vjp(s3, p, kb3, sb, gp);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    yb[i] += sb[i];
+    const double u = dt * sb[i];
+    kb1[i] += T::A31 * u;
+    kb2[i] += T::A32 * u;
+  }
+  // stage 2
+#pragma unroll
+  for (int i = 0; i < D; ++i) sb[i] = 0.0;
+  F::vjp(s2, p, kb2, sb, gp);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    yb[i] += sb[i];
+    kb1[i] += T::A21 * (dt * sb[i]);
+  }
+  // stage 1 (s1 = y)
+  F::vjp(y, p, kb1, yb, gp);
+#pragma unroll
+  for (int i = 0; i < D; ++i) lam[i] = yb[i];
+}
+
+// --- kernel arguments -----------------------------------------------------------------
+struct RecordArgs {
+  long long n;
+  const double* y0;
+  const double* p;
+  double t0, t1, rtol, atol, dt0;
+  const double* t1v;  // per-trajectory end times or null
+  int max_steps, cap, ck_every, ck_slots;
+  double* rec;   // chunked dt record or null
+  double* ckpt;  // checkpoints or null
+  double* yf;
+  int* n_acc;
+  int* n_rej;
+  int* status;
+};
+
+struct AdjointArgs {
+  long long n;
+  const double* p;
+  const double* rec;
+  const int* n_acc;
+  const double* ckpt;
+  int ck_every;
+  const double* ybar;
+  double* gy0;
+  double* gp;
+};
+
+struct ReplayArgs {
+  long long n;
+  const double* y0;
+  const double* p;
+  double t0;
+  const double* rec;
+  const int* n_acc;
+  int ck_every, ck_slots;
+  double* ckpt;
+  double* yf;
+};
+
+template <int D>
+__device__ __forceinline__ void store_ckpt(double* ckpt, long long n, long long j, int slot,
+                                           const double* y, double t) {
+  constexpr int CW = (D + 2) & ~1;
+  double v[CW];
+#pragma unroll
+  for (int i = 0; i < D; ++i) v[i] = y[i];
+  v[D] = t;
+#pragma unroll
+  for (int i = D + 1; i < CW; ++i) v[i] = 0.0;
+  double2* dst = reinterpret_cast<double2*>(ckpt + ((size_t)slot * (size_t)n + (size_t)j) * CW);
+#pragma unroll
+  for (int i = 0; i < CW / 2; ++i) dst[i] = make_double2(v[2 * i], v[2 * i + 1]);
+}
+
+template <int D>
+__device__ __forceinline__ double load_ckpt(const double* ckpt, long long n, long long j, int slot,
+                                            double* y) {
+  constexpr int CW = (D + 2) & ~1;
+  const double2* src =
+      reinterpret_cast<const double2*>(ckpt + ((size_t)slot * (size_t)n + (size_t)j) * CW);
+  double v[CW];
+#pragma unroll
+  for (int i = 0; i < CW / 2; ++i) {
+    const double2 w = __ldg(src + i);
+    v[2 * i] = w.x;
+    v[2 * i + 1] = w.y;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) y[i] = v[i];
+  return v[D];
+}
+
+__device__ __forceinline__ void store_rec_chunk(double* rec, long long n, long long j, int chunk,
+                                                double a, double b, double c, double d) {
+  double2* dst = reinterpret_cast<double2*>(rec + ((size_t)chunk * (size_t)n + (size_t)j) * 4u);
+  dst[0] = make_double2(a, b);
+  dst[1] = make_double2(c, d);
+}
+
+__device__ __forceinline__ double load_rec(const double* rec, long long n, long long j,
+                                           long long s) {
+  return __ldg(rec + rec_index(j, s, n));
+}
+
+// --- forward adaptive solve with record --------------------------------------------------
+template <class F>
+__global__ void __launch_bounds__(128) tsit5_record_kernel(const RecordArgs a) {
+  constexpr int D = F::D, P = F::P;
+  using T = Tsit5;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  double y[D], p[P], k1[D], y5[D], k7[D], e[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) y[i] = a.y0[j * D + i];
+#pragma unroll
+  for (int i = 0; i < P; ++i) p[i] = a.p[j * P + i];
+  double t = a.t0;
+  const double t1 = a.t1v ? a.t1v[j] : a.t1;
+  double dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
+  const bool rec_on = a.rec != nullptr;
+  const bool ck_on = a.ckpt != nullptr;
+  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
+  F::rhs(y, p, k1);
+  int acc = 0, rej = 0, st = 0, ck_cnt = 0, ck_slot = 0;
+  double b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
+  for (int it = 0; it < a.max_steps; ++it) {
+    if (t >= t1) break;
+    const double h = (t1 - t < dt) ? (t1 - t) : dt;
+    Stages<F> S;
+    tsit5_k2_to_k6<F>(y, p, k1, h, S);
+    tsit5_y5<F>(y, k1, S, h, y5);
+    F::rhs(y5, p, k7);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      e[i] = h * (T::E1 * k1[i] + T::E2 * S.k2[i] + T::E3 * S.k3[i] + T::E4 * S.k4[i] +
+                  T::E5 * S.k5[i] + T::E6 * S.k6[i] + T::E7 * k7[i]);
+    const double err = wrms_norm<D>(e, y, y5, a.rtol, a.atol);
+    if (!(err == err)) {  // NaN error: dt would turn NaN and the loop could never finish
+      st = 1;
+      break;
+    }
+    if (err <= 1.0) {
+      if ((rec_on || ck_on) && acc >= a.cap) {
+        st = 3;
+        break;
+      }
+      t = t + h;
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        y[i] = y5[i];
+        k1[i] = k7[i];
+      }
+      if (rec_on) {
+        b0 = b1;
+        b1 = b2;
+        b2 = b3;
+        b3 = h;
+        if ((acc & 3) == 3) store_rec_chunk(a.rec, a.n, j, acc >> 2, b0, b1, b2, b3);
+      }
+      ++acc;
+      if (ck_on && ++ck_cnt == a.ck_every) {
+        ck_cnt = 0;
+        if (++ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, ck_slot, y, t);
+      }
+    } else {
+      ++rej;
+    }
+    dt = step_controller(err, h, T::ORDER_EXP);
+  }
+  if (st == 0 && !(t >= t1)) st = 1;
+  if (rec_on) {
+    switch (acc & 3) {  // zero-padded last sector
+      case 1: store_rec_chunk(a.rec, a.n, j, acc >> 2, b3, 0.0, 0.0, 0.0); break;
+      case 2: store_rec_chunk(a.rec, a.n, j, acc >> 2, b2, b3, 0.0, 0.0); break;
+      case 3: store_rec_chunk(a.rec, a.n, j, acc >> 2, b1, b2, b3, 0.0); break;
+      default: break;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
+  a.n_acc[j] = acc;
+  a.n_rej[j] = rej;
+  a.status[j] = st;
+}
+
+// --- frozen-mesh replay (values), optionally writing checkpoints -------------------------
+template <class F>
+__global__ void __launch_bounds__(128) tsit5_replay_kernel(const ReplayArgs a) {
+  constexpr int D = F::D, P = F::P;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  double y[D], p[P];
+#pragma unroll
+  for (int i = 0; i < D; ++i) y[i] = a.y0[j * D + i];
+#pragma unroll
+  for (int i = 0; i < P; ++i) p[i] = a.p[j * P + i];
+  const int na = a.n_acc[j];
+  double t = a.t0;
+  const bool ck_on = a.ckpt != nullptr;
+  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
+  int ck_cnt = 0, ck_slot = 0;
+  for (int s = 0; s < na; ++s) {
+    const double dt = load_rec(a.rec, a.n, j, s);
+    tsit5_replay_step<F>(y, p, dt);
+    t = t + dt;
+    if (ck_on && ++ck_cnt == a.ck_every) {
+      ck_cnt = 0;
+      if (++ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, ck_slot, y, t);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
+}
+
+// --- reverse-replay adjoint ---------------------------------------------------------------
+template <class F>
+__global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a) {
+  constexpr int D = F::D, P = F::P;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  double p[P], lam[D], gp[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    p[i] = a.p[j * P + i];
+    gp[i] = 0.0;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
+  const int na = a.n_acc[j];
+  const int K = a.ck_every;
+  const int nseg = (na + K - 1) / K;
+  double seg[KMAX][D];  // interior states of the current segment (per-thread local memory)
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int start = sg * K;
+    double y[D];
+    load_ckpt<D>(a.ckpt, a.n, j, sg, y);
+#pragma unroll
+    for (int i = 0; i < D; ++i) seg[0][i] = y[i];
+    for (int q = 1; q < K; ++q) {
+      const int s = start + q - 1;
+      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      if (dt != 0.0) tsit5_replay_step<F>(y, p, dt);
+#pragma unroll
+      for (int i = 0; i < D; ++i) seg[q][i] = y[i];
+    }
+    for (int q = K - 1; q >= 0; --q) {
+      const int s = start + q;
+      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      if (dt != 0.0) {
+        double ys[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) ys[i] = seg[q][i];
+        tsit5_step_vjp<F>(ys, p, dt, lam, gp);
+      }
+    }
+  }
+  if (a.gy0) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) a.gy0[j * D + i] = lam[i];
+  }
+  if (a.gp) {
+#pragma unroll
+    for (int i = 0; i < P; ++i) a.gp[j * P + i] = gp[i];
+  }
+}
+
+}  // namespace gs

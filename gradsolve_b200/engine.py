@@ -1,0 +1,210 @@
+"""Device-level driver: owns the workspaces and calls the libgsolve entry points.
+
+PyTorch is used only as the device allocator and stream provider (tensors on the current
+CUDA device, the current stream); all arithmetic happens in libgsolve.so.  The functions
+here work on device tensors and return device tensors; the public API (``api.py``) and the
+autograd adapter (``torch_adapter.py``) sit on top.
+
+Record capacity follows the reference's device recorder (gradsolve/solvers/record_jax.py:
+171-213): start with a bounded capacity, and if any trajectory reports a full record
+(status 3) double it (up to ``max_steps``) and run again.  Failures then raise with the
+reference's messages ("exhausted max_steps", "underflow").
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import Optional
+
+import torch
+
+from . import _lib
+from .fields import FieldSpec
+
+METHOD_TSIT5 = "tsit5"
+METHOD_ROS23 = "rosenbrock23"
+_PREC = {"float64": _lib.GS_PREC_F64, "mixed": _lib.GS_PREC_MIXED}
+
+# default record capacity before growth (the reference's device recorder starts at 1024)
+DEFAULT_CAP0 = 1024
+
+
+def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def ckpt_width(dim: int) -> int:
+    return (dim + 2) & ~1
+
+
+def choose_ckpt_every(policy, dim: int, n: int, cap: int, budget_bytes: Optional[int]) -> int:
+    """Checkpoint interval K.
+
+    ``policy``: an int K; ``"all"`` (K = 1, every state stored, no recomputation);
+    ``"sqrt"`` (K = ceil(sqrt(cap)), the sqrt(N) segment scheme); ``"auto"``: K = 1 when the
+    full state record fits ``budget_bytes`` (default: a quarter of the free device memory),
+    else the sqrt(N) scheme."""
+    kmax = _lib.lib().gs_max_ckpt_every()
+    if isinstance(policy, int):
+        if not 1 <= policy <= kmax:
+            raise ValueError(f"checkpoint interval must be in [1, {kmax}]; got {policy}")
+        return policy
+    sq = max(2, min(kmax, int(math.ceil(math.sqrt(max(cap, 1))))))
+    if policy == "all":
+        return 1
+    if policy == "sqrt":
+        return sq
+    if policy != "auto":
+        raise ValueError(f"checkpoint policy must be 'auto', 'all', 'sqrt' or an int; got {policy!r}")
+    if budget_bytes is None:
+        free, _total = torch.cuda.mem_get_info()
+        budget_bytes = free // 4
+    full = (cap + 1) * n * ckpt_width(dim) * 8
+    return 1 if full <= budget_bytes else sq
+
+
+@dataclass
+class Record:
+    """Everything the forward leaves on the device for the adjoint."""
+    method: str
+    spec: FieldSpec
+    n: int
+    t0: float
+    cap: int
+    ckpt_every: int
+    rec: torch.Tensor        # chunked dt record (flat float64)
+    ckpt: torch.Tensor       # checkpoints (flat float64)
+    y_final: torch.Tensor    # (n, D)
+    n_acc: torch.Tensor      # (n,) int32
+    n_rej: torch.Tensor      # (n,) int32
+    status: torch.Tensor     # (n,) int32
+
+    def padded_dts(self, S: Optional[int] = None) -> torch.Tensor:
+        """The record in the reference's (n, S) zero-padded layout."""
+        if S is None:
+            S = int(self.n_acc.max().item()) if self.n else 0
+        out = torch.zeros((self.n, S), dtype=torch.float64, device=self.rec.device)
+        _lib.check(_lib.lib().gs_record_to_padded(self.n, self.cap, _ptr(self.rec),
+                                                  _ptr(self.n_acc), S, _ptr(out), _stream()),
+                   "gs_record_to_padded")
+        return out
+
+
+def _alloc_record(n: int, cap: int, dim: int, K: int, device) -> tuple:
+    L = _lib.lib()
+    rec_elems = L.gs_record_bytes(n, cap) // 8
+    slots = L.gs_ckpt_slots(cap, K)
+    rec = torch.empty(max(rec_elems, 2), dtype=torch.float64, device=device)
+    ckpt = torch.empty(max(slots * n * ckpt_width(dim), 2), dtype=torch.float64, device=device)
+    return rec, ckpt
+
+
+def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tensor, *,
+                   t0: float, t1: float, rtol: float, atol: float, dt0: Optional[float] = None,
+                   t1v: Optional[torch.Tensor] = None, max_steps: int = 100000,
+                   cap0: int = DEFAULT_CAP0, checkpoint="auto",
+                   budget_bytes: Optional[int] = None, precision: str = "float64",
+                   record: bool = True) -> Record:
+    """Adaptive solve on the device; with ``record`` the dts and checkpoints are kept.
+
+    ``y0`` (n, D) and ``p`` (n, P) float64 contiguous device tensors."""
+    n = y0.shape[0]
+    device = y0.device
+    L = _lib.lib()
+    fn = L.gs_tsit5_fwd_record if method == METHOD_TSIT5 else L.gs_ros23_fwd_record
+    yf = torch.empty_like(y0)
+    n_acc = torch.empty(n, dtype=torch.int32, device=device)
+    n_rej = torch.empty(n, dtype=torch.int32, device=device)
+    status = torch.empty(n, dtype=torch.int32, device=device)
+    dt0_arg = -1.0 if dt0 is None else float(dt0)
+    if not record:
+        _lib.check(fn(spec.code, _PREC[precision], n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
+                      float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), 0, 1, None,
+                      None, _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status), _stream()),
+                   fn.__name__)
+        empty = torch.empty(0, dtype=torch.float64, device=device)
+        return Record(method, spec, n, float(t0), 0, 1, empty, empty, yf, n_acc, n_rej, status)
+    cap = max(1, min(int(cap0), int(max_steps)))
+    while True:
+        K = choose_ckpt_every(checkpoint, spec.dim, n, cap, budget_bytes)
+        rec, ckpt = _alloc_record(n, cap, spec.dim, K, device)
+        _lib.check(fn(spec.code, _PREC[precision], n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
+                      float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), cap, K,
+                      _ptr(rec), _ptr(ckpt), _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status),
+                      _stream()), fn.__name__)
+        if n == 0 or cap >= max_steps or not bool((status == 3).any().item()):
+            break
+        cap = min(2 * cap, int(max_steps))
+    return Record(method, spec, n, float(t0), cap, K, rec, ckpt, yf, n_acc, n_rej, status)
+
+
+def raise_on_failed(r: Record, max_steps: int, t1) -> None:
+    """Refuse an incomplete mesh, with the reference's messages
+    (gradsolve/warp/warp_replay.py:167-173, gradsolve/solvers/record_jax.py:201-211)."""
+    if r.n == 0:
+        return
+    bad = torch.nonzero(r.status != 0).flatten()
+    if bad.numel() == 0:
+        return
+    i = int(bad[0].item())
+    st = int(r.status[i].item())
+    if st == 2:
+        raise RuntimeError(
+            f"record: trajectory {i} reached the step-size underflow floor before t1={t1} — a "
+            "singular or non-finite field (check the RHS; loosen the tol or shorten the "
+            "horizon); the recorded dt sequence is degenerate and a frozen replay of it would "
+            "be silently wrong.")
+    raise RuntimeError(
+        f"record: {bad.numel()} trajectories (rows {bad[:8].tolist()}...) exhausted "
+        f"max_steps={max_steps} before t1 — the recorded dt sequence is incomplete and a "
+        "frozen replay of it would be silently wrong. Increase max_steps, loosen the tol, "
+        "or shorten the horizon.")
+
+
+def replay(r: Record, y0: torch.Tensor, p: torch.Tensor, *, write_ckpt: bool = True,
+           precision: str = "float64") -> torch.Tensor:
+    """Frozen-mesh replay at (y0, p); refreshes the checkpoints for a following adjoint."""
+    L = _lib.lib()
+    fn = L.gs_tsit5_replay if r.method == METHOD_TSIT5 else L.gs_ros23_replay
+    yf = torch.empty_like(y0)
+    _lib.check(fn(r.spec.code, _PREC[precision], r.n, _ptr(y0), _ptr(p), float(r.t0), _ptr(r.rec),
+                  _ptr(r.n_acc), max(r.cap, 1), r.ckpt_every,
+                  _ptr(r.ckpt) if write_ckpt else None, _ptr(yf), _stream()), fn.__name__)
+    return yf
+
+
+def adjoint(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
+            want_p: bool = True, precision: str = "float64"):
+    """(dL/dy0, dL/dp) for cotangent ybar = dL/dy_final, using the record's checkpoints."""
+    L = _lib.lib()
+    fn = L.gs_tsit5_adjoint if r.method == METHOD_TSIT5 else L.gs_ros23_adjoint
+    gy0 = torch.empty((r.n, r.spec.dim), dtype=torch.float64, device=p.device) if want_y0 else None
+    gp = torch.empty((r.n, p.shape[1]), dtype=torch.float64, device=p.device) if want_p else None
+    ybar = ybar.contiguous()
+    _lib.check(fn(r.spec.code, _PREC[precision], r.n, _ptr(p), _ptr(r.rec), _ptr(r.n_acc),
+                  max(r.cap, 1), _ptr(r.ckpt), r.ckpt_every, _ptr(ybar), _ptr(gy0), _ptr(gp),
+                  _stream()), fn.__name__)
+    return gy0, gp
+
+
+def record_from_padded(method: str, spec: FieldSpec, dts: torch.Tensor, t0: float,
+                       checkpoint="auto", budget_bytes: Optional[int] = None) -> Record:
+    """A Record built from a padded (n, S) dt array (e.g. the reference's own record).
+    Checkpoints are filled by the next ``replay``."""
+    dts = dts.contiguous()
+    n, S = dts.shape
+    cap = max(S, 1)
+    K = choose_ckpt_every(checkpoint, spec.dim, n, cap, budget_bytes)
+    rec, ckpt = _alloc_record(n, cap, spec.dim, K, dts.device)
+    n_steps = torch.empty(n, dtype=torch.int32, device=dts.device)
+    _lib.check(_lib.lib().gs_record_from_padded(n, S, _ptr(dts), S, _ptr(rec), cap,
+                                                _ptr(n_steps), _stream()),
+               "gs_record_from_padded")
+    zeros = torch.zeros(n, dtype=torch.int32, device=dts.device)
+    yf = torch.empty((n, spec.dim), dtype=torch.float64, device=dts.device)
+    return Record(method, spec, n, float(t0), cap, K, rec, ckpt, yf, n_steps, zeros,
+                  zeros.clone())

@@ -1,0 +1,32 @@
+"""Algorithmic work per unit, for roofline reporting.
+
+Counted once per (method, field) by the counting oracle (``+ - * /`` = 1 each, so a fused
+multiply-add = 2; ``sqrt``/``pow``/``abs``/``max`` = 1 each) on the reference's expressions:
+  F_att  one adaptive attempt; F_step one replay step (the zero-weight k7 stage excluded);
+  F_vjp  the backward sweep of one step (forward recomputation excluded).
+Per trajectory:
+  solve    F = (n_acc + n_rej) * F_att
+  gradient F = (n_acc + n_rej) * F_att + n_acc * (F_step + F_vjp)
+tests/test_flops.py re-derives the numbers.
+"""
+from __future__ import annotations
+
+COUNTS = {
+    ("tsit5", "lorenz"): dict(F_att=269, F_step=198, F_vjp=228),
+    ("tsit5", "lv"): dict(F_att=193, F_step=144, F_vjp=204),
+    ("tsit5", "vdp"): dict(F_att=175, F_step=126, F_vjp=186),
+    ("rosenbrock23", "robertson"): dict(F_att=205, F_step=115, F_vjp=191),
+}
+
+
+def solve_flops(method: str, field: str, attempts: int) -> int:
+    return COUNTS[(method, field)]["F_att"] * int(attempts)
+
+
+def adjoint_flops(method: str, field: str, accepted: int) -> int:
+    c = COUNTS[(method, field)]
+    return (c["F_step"] + c["F_vjp"]) * int(accepted)
+
+
+def gradient_flops(method: str, field: str, attempts: int, accepted: int) -> int:
+    return solve_flops(method, field, attempts) + adjoint_flops(method, field, accepted)

@@ -1,0 +1,88 @@
+"""``torch.autograd.Function`` around the frozen-mesh replay and its hand-written adjoint.
+
+This is the PyTorch face of the reference's closure contract
+(gradsolve/warp/warp_replay.py:186-237, gradsolve/solvers/tsit5_replay.py:192-232): the
+mesh is recorded ONCE at (y0, params0); the closure's forward re-integrates that frozen
+mesh at the (y0, params) it is given (the replay value, ``warp_replay.py:30-55``), and its
+backward is the discrete adjoint of that replay with the dts held fixed -- computed by the
+reverse-replay kernel instead of by ``jax.grad``.
+
+When the closure is called at exactly the recording point (same y0 and params, bitwise),
+the recording pass already produced the replay's value and checkpoints (the adaptive
+forward and the replay evaluate the same expressions in the same order), so no second
+forward is launched.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import engine
+
+
+class ReplayState:
+    """The frozen record plus bookkeeping shared by every call of one closure."""
+
+    def __init__(self, record: engine.Record, y0_rec: torch.Tensor, p_rec: torch.Tensor,
+                 nparam: int, precision: str = "float64", reuse_recording: bool = True):
+        self.record = record
+        self.y0_rec = y0_rec
+        self.p_rec = p_rec
+        self.nparam = nparam
+        self.precision = precision
+        self.version = 0           # bumps whenever the checkpoints are rewritten
+        self.ckpt_point = (y0_rec, p_rec) if reuse_recording else None
+
+    def kernel_p(self, p: torch.Tensor) -> torch.Tensor:
+        if p.shape[1] < self.nparam:  # only fields that ignore their parameter get here
+            p = torch.nn.functional.pad(p, (0, self.nparam - p.shape[1]))
+        return p[:, : self.nparam].contiguous()
+
+    def run_forward(self, y0: torch.Tensor, p: torch.Tensor) -> torch.Tensor:
+        pk = self.kernel_p(p)
+        if (self.ckpt_point is not None and torch.equal(y0, self.ckpt_point[0])
+                and torch.equal(pk, self.ckpt_point[1])):
+            return self.record.y_final.clone()
+        yf = engine.replay(self.record, y0.contiguous(), pk, write_ckpt=True,
+                           precision=self.precision)
+        self.ckpt_point = (y0.detach().clone(), pk.detach().clone())
+        self.version += 1
+        return yf
+
+
+class _ReplayFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, y0, p, state):
+        y0 = y0.contiguous()
+        p = p.contiguous()
+        yf = state.run_forward(y0, p)
+        ctx.state = state
+        ctx.version = state.version
+        ctx.save_for_backward(y0, p)
+        return yf
+
+    @staticmethod
+    def backward(ctx, ybar):
+        state: ReplayState = ctx.state
+        y0, p = ctx.saved_tensors
+        pk = state.kernel_p(p)
+        if state.version != ctx.version or state.ckpt_point is None or not (
+                torch.equal(y0, state.ckpt_point[0]) and torch.equal(pk, state.ckpt_point[1])):
+            # another forward of the same closure rewrote the checkpoints: rebuild ours
+            engine.replay(state.record, y0, pk, write_ckpt=True, precision=state.precision)
+            state.ckpt_point = (y0.detach().clone(), pk.detach().clone())
+            state.version += 1
+        need_y0, need_p = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        gy0, gpk = engine.adjoint(state.record, pk, ybar.to(torch.float64),
+                                  want_y0=need_y0, want_p=need_p, precision=state.precision)
+        gp = None
+        if need_p:
+            if p.shape[1] == state.nparam:
+                gp = gpk
+            else:
+                gp = torch.zeros_like(p)
+                gp[:, : state.nparam] = gpk
+        return gy0, gp, None
+
+
+def replay_apply(state: ReplayState, y0: torch.Tensor, p: torch.Tensor) -> torch.Tensor:
+    return _ReplayFn.apply(y0, p, state)

@@ -1,0 +1,175 @@
+/*
+ * gsolve.h -- C ABI of libgsolve.so, the B200 (sm_100a) ensemble adaptive ODE solve and
+ * record-and-replay discrete adjoint.
+ *
+ * Plain C: device pointers, sizes and a CUDA stream passed as void*.  No framework types.
+ * Every entry point returns an int status (GS_OK or a negative GS_ERR_*); the message of the
+ * last failure on the calling thread is available from gs_last_error().  Per-trajectory
+ * outcomes (reached t1, max_steps exhausted, record full) are DATA in the status[] output,
+ * not call errors, exactly as the reference's kernels report them
+ * (gradsolve/warp/_warp_kernel.py:396-399, gradsolve/solvers/record_jax.py:71).
+ *
+ * All launches are asynchronous on `stream` (NULL = the legacy default stream).  Calls are
+ * stateless and re-entrant; the library allocates no device memory: the caller owns every
+ * buffer (the workspace size helpers below give the record and checkpoint sizes).
+ *
+ * Layouts (float64 unless stated):
+ *   y0, y_final, ybar, gy0 : (n, D) row-major        p, gp : (n, P) row-major
+ *   rec   : dt record, chunk-interleaved: step s of trajectory j at ((s/4)*n + j)*4 + s%4,
+ *           cap steps per trajectory; 16-byte aligned.  gs_record_bytes() gives its size.
+ *   ckpt  : checkpoints, slot c of trajectory j = (state after c*K accepted steps, time) at
+ *           (c*n + j)*CW doubles, CW = D+1 rounded up to even; 16-byte aligned.
+ *           gs_ckpt_bytes() gives its size for (field, n, cap, K).
+ *   n_acc, n_rej, status : (n,) int32.
+ * Field codes: GS_FIELD_LORENZ (D=3,P=1: rho), GS_FIELD_VDP (D=2,P=1: mu),
+ *   GS_FIELD_LOTKA_VOLTERRA (D=2,P=4: alpha,beta,gamma,delta), GS_FIELD_LINEAR*1000 + D
+ *   (D in 1,2,3,4,8; P=1, ignored), GS_FIELD_ROBERTSON (D=3,P=3: k1,k2,k3; stiff),
+ *   GS_FIELD_LORENZ3 (D=3,P=3: sigma,beta,rho).
+ */
+#ifndef GSOLVE_H_
+#define GSOLVE_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GS_OK 0
+#define GS_ERR_ARG (-1)      /* invalid argument (null pointer, bad size, misalignment) */
+#define GS_ERR_FIELD (-2)    /* unknown field code, or field not available for the method */
+#define GS_ERR_CUDA (-3)     /* a CUDA launch or runtime call failed */
+#define GS_ERR_PRECISION (-4)/* precision mode not available for this entry point */
+
+#define GS_FIELD_LORENZ 1
+#define GS_FIELD_VDP 2
+#define GS_FIELD_LOTKA_VOLTERRA 3
+#define GS_FIELD_LINEAR 4
+#define GS_FIELD_ROBERTSON 10
+#define GS_FIELD_LORENZ3 11
+
+#define GS_PREC_F64 0   /* everything float64 */
+#define GS_PREC_MIXED 1 /* float32 stages/RHS; float64 time, controller, error norm, state */
+
+/* per-trajectory status values written to status[] */
+#define GS_TRAJ_OK 0          /* reached t1 */
+#define GS_TRAJ_MAX_STEPS 1   /* max_steps attempts exhausted (or non-finite error) */
+#define GS_TRAJ_UNDERFLOW 2   /* step size underflow (Rosenbrock23 only) */
+#define GS_TRAJ_RECORD_FULL 3 /* more than cap accepted steps; grow the record and retry */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int gs_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* gs_last_error(void);
+
+/* State dimension D and parameter count P of a field code.  Replaces the registry lookup
+ * of gradsolve/warp/_warp_kernel.py:229-286 (_field_entry / field_dim). */
+int gs_field_dims(int field, int* D, int* P);
+
+/* Host copy of the method constants in this order: C2..C5 (4), A21..A65 (15), B1..B7 (7),
+ * E1..E7 (7), SAFETY, ERR_FLOOR, FAC_MIN, FAC_MAX, TSIT5_EXP (5), ROS_D, ROS_E32, ROS_EXP (3):
+ * 41 values.  The constants of gradsolve/solvers/tsit5_step.py:26-77 and
+ * gradsolve/warp/_warp_rosenbrock.py:62-70.  len must be >= 41. */
+int gs_tableau(double* out, int len);
+
+/* The same 41 constants as compiled into device code, written by a kernel to a device
+ * buffer of 41 doubles. */
+int gs_device_tableau(double* out_dev, void* stream);
+
+/* Bytes of a dt record for n trajectories of capacity cap. */
+size_t gs_record_bytes(long long n, int cap);
+
+/* Number of checkpoint slots for capacity cap and interval K (ceil(cap/K) + 1). */
+int gs_ckpt_slots(int cap, int ckpt_every);
+
+/* Bytes of the checkpoint buffer for (field, n, cap, K); 0 for an unknown field. */
+size_t gs_ckpt_bytes(int field, long long n, int cap, int ckpt_every);
+
+/* Largest checkpoint interval K the adjoint kernels accept. */
+int gs_max_ckpt_every(void);
+
+/*
+ * Adaptive Tsit5 forward solve that records the accepted step sizes.
+ * Replaces gradsolve/warp/_warp_kernel.py:325-399 (_tsit5_adaptive_general, record == 1)
+ * as launched by gradsolve/warp/warp_ode.py:215-327 (_launch), and the host recorder
+ * gradsolve/solvers/tsit5_replay.py:62-124 (tsit5_adaptive) it is specified by.
+ *   t1v  : per-trajectory end times (n,) or NULL for the scalar t1.
+ *   dt0  : first step; <= 0 selects (t1_j - t0)/100 per trajectory (warp_replay.py:157).
+ *   rec  : dt record of capacity cap, or NULL (no record).
+ *   ckpt : checkpoints every ckpt_every accepted steps (1..gs_max_ckpt_every()), or NULL.
+ *   A trajectory that would accept more than cap steps stops with status 3 when rec or ckpt
+ *   is given.  y_final is the last reached state (rows with status != 0 are not NaN'd here;
+ *   the reference's driver does that, gradsolve/warp/warp_ode.py:319).
+ */
+int gs_tsit5_fwd_record(int field, int precision, long long n, const double* y0,
+                        const double* p, double t0, const double* t1v, double t1, double rtol,
+                        double atol, double dt0, int max_steps, int cap, int ckpt_every,
+                        double* rec, double* ckpt, double* y_final, int* n_acc, int* n_rej,
+                        int* status, void* stream);
+
+/*
+ * Frozen-mesh replay: re-integrate n_acc[j] recorded steps of trajectory j with fixed
+ * steps.  Replaces gradsolve/warp/warp_replay.py:30-55 (replay_solve_jax) over
+ * gradsolve/solvers/tsit5_step.py:80-102 (tsit5_step).  Optionally writes checkpoints
+ * (ckpt != NULL), so a record that came from elsewhere (gs_record_from_padded) can feed
+ * gs_tsit5_adjoint.
+ */
+int gs_tsit5_replay(int field, int precision, long long n, const double* y0, const double* p,
+                    double t0, const double* rec, const int* n_acc, int cap, int ckpt_every,
+                    double* ckpt, double* y_final, void* stream);
+
+/*
+ * Discrete adjoint of the frozen-mesh replay: given ybar = dL/dy_final, writes
+ * gy0 = dL/dy0 and gp = dL/dp (either may be NULL) with the recorded dts held fixed -- the
+ * gradient jax.grad takes through replay_solve_jax (gradsolve/warp/warp_replay.py:30-55,
+ * closures :186-237; gradsolve/solvers/tsit5_replay.py:192-232).  Needs the checkpoints of
+ * the forward (or of gs_tsit5_replay) with the same ckpt_every.
+ */
+int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, const double* rec,
+                     const int* n_acc, int cap, const double* ckpt, int ckpt_every,
+                     const double* ybar, double* gy0, double* gp, void* stream);
+
+/*
+ * Adaptive Rosenbrock23 (ode23s, autonomous) forward with dt record.  Replaces
+ * gradsolve/warp/_warp_rosenbrock.py:383-452 (_rosenbrock23_adaptive, record == 1) as
+ * launched by gradsolve/warp/warp_rosenbrock.py:166-218 (_launch); specified by
+ * tests/_oracles/gradsolve_g2_spike_oracle.py:138-184.  Same arguments and outputs as
+ * gs_tsit5_fwd_record; fields need an analytic Jacobian (GS_FIELD_ROBERTSON, linear).
+ * Additionally stops with status 2 when a step no longer advances time (t + h == t).
+ */
+int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,
+                        const double* p, double t0, const double* t1v, double t1, double rtol,
+                        double atol, double dt0, int max_steps, int cap, int ckpt_every,
+                        double* rec, double* ckpt, double* y_final, int* n_acc, int* n_rej,
+                        int* status, void* stream);
+
+/* Frozen-mesh Rosenbrock23 replay.  Replaces gradsolve/warp/warp_replay.py:267-293
+ * (replay_solve_rosenbrock_jax) over gradsolve/solvers/rosenbrock23_step.py:47-66. */
+int gs_ros23_replay(int field, int precision, long long n, const double* y0, const double* p,
+                    double t0, const double* rec, const int* n_acc, int cap, int ckpt_every,
+                    double* ckpt, double* y_final, void* stream);
+
+/* Discrete adjoint of the Rosenbrock23 replay (the gradient jax.grad takes through
+ * gradsolve/warp/warp_replay.py:344-384), including the second-order term through
+ * W = I - d*dt*J(y, p). */
+int gs_ros23_adjoint(int field, int precision, long long n, const double* p, const double* rec,
+                     const int* n_acc, int cap, const double* ckpt, int ckpt_every,
+                     const double* ybar, double* gy0, double* gp, void* stream);
+
+/*
+ * Record conversion between the reference's padded (n, S) layout (row j = trajectory j's
+ * accepted dts, zero padded; gradsolve/warp/warp_replay.py:181-182) and the chunked record.
+ * from_padded also writes n_steps[j] = index of the last non-zero dt + 1 (zero steps
+ * before it are kept: they are identity steps).  dts row stride is ld (>= S).
+ */
+int gs_record_from_padded(long long n, long long S, const double* dts, long long ld,
+                          double* rec, int cap, int* n_steps, void* stream);
+int gs_record_to_padded(long long n, int cap, const double* rec, const int* n_acc, long long S,
+                        double* dts, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSOLVE_H_ */

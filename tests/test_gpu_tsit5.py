@@ -1,0 +1,236 @@
+"""Parity of the CUDA Tsit5 path (libgsolve.so, through the C ABI) with the reference.
+
+Bars (float64):
+  * forward record vs the reference's own tsit5_adaptive (tests/golden/): accepted and
+    rejected counts identical; dts and y_final within 1e-10 relative (the kernel fuses
+    multiply-adds, the reference does not, so bitwise equality is not expected);
+  * replay of the reference's own recorded dts: y_final within 1e-10 relative of the
+    oracle's replay;
+  * gradients of the replay (dts frozen) within 1e-9 relative of the oracle's reverse pass
+    and of torch-float64 autograd, and within 1e-6 of central finite differences
+    (tests/test_adjoint_replay.py:174-216 of the reference).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+CASES = [("lorenz_small", "lorenz"), ("lorenz_scale", "lorenz"), ("vdp_batch", "vdp"),
+         ("lv_mixed", "lv"), ("linear3", "linear_3")]
+
+
+def rel(a, b, floor=1e-300):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor))) if a.size else 0.0
+
+
+def _spec(field):
+    from gradsolve_b200.fields import field_spec
+    return field_spec(field)
+
+
+def _record(gslib, cuda, field, g, **kw):
+    from gradsolve_b200 import engine
+    spec = _spec(field)
+    y0 = torch.tensor(g["y0"], device=cuda)
+    p = torch.tensor(g["params"][:, : spec.nparam], device=cuda).contiguous()
+    r = engine.forward_record("tsit5", spec, y0, p, t0=float(g["t0"]), t1=float(g["t1"]),
+                              rtol=float(g["rtol"]), atol=float(g["atol"]),
+                              max_steps=kw.pop("max_steps", 100000), **kw)
+    torch.cuda.synchronize()
+    return spec, y0, p, r
+
+
+@pytest.mark.parametrize("case,field", CASES)
+def test_forward_record_matches_reference(gslib, cuda, case, field):
+    g = load_golden(case)
+    spec, y0, p, r = _record(gslib, cuda, field, g)
+    np.testing.assert_array_equal(r.status.cpu().numpy(), g["status"])
+    np.testing.assert_array_equal(r.n_acc.cpu().numpy(), g["n_acc"])
+    np.testing.assert_array_equal(r.n_rej.cpu().numpy(), g["n_rej"])
+    dts = r.padded_dts().cpu().numpy()
+    assert dts.shape == g["dts"].shape
+    assert rel(dts, g["dts"]) <= 1e-10
+    assert rel(r.y_final.cpu().numpy(), g["y_final"], 1e-12) <= 1e-10
+
+
+@pytest.mark.parametrize("case,field", CASES)
+def test_record_padding_contract(gslib, cuda, case, field):
+    g = load_golden(case)
+    spec, y0, p, r = _record(gslib, cuda, field, g)
+    S = int(r.n_acc.max().item())
+    dts = r.padded_dts(S + 3).cpu().numpy()
+    n_acc = r.n_acc.cpu().numpy()
+    for j in range(dts.shape[0]):
+        assert np.all(dts[j, : n_acc[j]] > 0)
+        assert np.all(dts[j, n_acc[j]:] == 0)
+        assert abs(dts[j].sum() - (float(g["t1"]) - float(g["t0"]))) <= 1e-12
+
+
+@pytest.mark.parametrize("case,field", CASES)
+def test_forward_value_equals_replay_value(gslib, cuda, case, field):
+    """The recording pass and the frozen-mesh replay evaluate the same expressions, so the
+    closure may reuse the recording pass at the recording point: y_final bitwise equal."""
+    from gradsolve_b200 import engine
+    g = load_golden(case)
+    spec, y0, p, r = _record(gslib, cuda, field, g, checkpoint=1)
+    yf_fwd = r.y_final.clone()
+    ck_fwd = r.ckpt.clone()
+    yf_rep = engine.replay(r, y0, p, write_ckpt=True)
+    torch.cuda.synchronize()
+    assert torch.equal(yf_fwd, yf_rep)
+    n_acc = r.n_acc.cpu().numpy()
+    slots = int(n_acc.max()) + 1
+    a = ck_fwd[: slots * r.n * 4].view(slots, r.n, 4).cpu().numpy()
+    b = r.ckpt[: slots * r.n * 4].view(slots, r.n, 4).cpu().numpy()
+    for j in range(r.n):  # only the slots this trajectory wrote (0..n_acc[j])
+        np.testing.assert_array_equal(a[: n_acc[j] + 1, j, : spec.dim + 1],
+                                      b[: n_acc[j] + 1, j, : spec.dim + 1])
+
+
+def _replay_reference_dts(cuda, field, g, checkpoint="sqrt"):
+    from gradsolve_b200 import engine
+    spec = _spec(field)
+    dts = torch.tensor(g["dts"], device=cuda)
+    r = engine.record_from_padded("tsit5", spec, dts, float(g["t0"]), checkpoint=checkpoint)
+    y0 = torch.tensor(g["y0"], device=cuda)
+    p = torch.tensor(g["params"][:, : spec.nparam], device=cuda).contiguous()
+    yf = engine.replay(r, y0, p, write_ckpt=True)
+    return spec, r, y0, p, yf
+
+
+@pytest.mark.parametrize("case,field", CASES)
+def test_replay_of_reference_dts(gslib, oracle, cuda, case, field):
+    g = load_golden(case)
+    spec, r, y0, p, yf = _replay_reference_dts(cuda, field, g)
+    ref = oracle.replay("tsit5", field, g["y0"], g["params"], g["dts"])
+    assert rel(yf.cpu().numpy(), ref, 1e-12) <= 1e-10
+
+
+@pytest.mark.parametrize("checkpoint", [1, 3, 8, 64, "sqrt"])
+@pytest.mark.parametrize("case,field", CASES)
+def test_adjoint_of_reference_dts(gslib, oracle, cuda, case, field, checkpoint):
+    from gradsolve_b200 import engine
+    g = load_golden(case)
+    spec, r, y0, p, yf = _replay_reference_dts(cuda, field, g, checkpoint=checkpoint)
+    ybar = 2.0 * yf
+    gy0, gp = engine.adjoint(r, p, ybar)
+    torch.cuda.synchronize()
+    oy, op = oracle.replay_vjp("tsit5", field, g["y0"], g["params"], g["dts"], ybar.cpu().numpy())
+    assert rel(gy0.cpu().numpy(), oy, 1e-8) <= 1e-9
+    if not field.startswith("linear_"):
+        assert rel(gp.cpu().numpy(), op[:, : spec.nparam], 1e-8) <= 1e-9
+
+
+def test_checkpoint_interval_does_not_change_the_gradient(gslib, cuda):
+    """Segments recompute the same states the record stored (same expressions), so every
+    checkpoint interval gives the same gradient bit for bit."""
+    from gradsolve_b200 import engine
+    g = load_golden("lorenz_scale")
+    outs = []
+    for K in (1, 2, 7, 26, 64):
+        spec, y0, p, r = _record(gslib, cuda, "lorenz", g, checkpoint=K)
+        gy0, gp = engine.adjoint(r, p, 2.0 * r.y_final)
+        outs.append((gy0.cpu().numpy(), gp.cpu().numpy()))
+    for gy, gpp in outs[1:]:
+        np.testing.assert_array_equal(gy, outs[0][0])
+        np.testing.assert_array_equal(gpp, outs[0][1])
+
+
+@pytest.mark.parametrize("case,field", [("vdp_batch", "vdp"), ("lorenz_small", "lorenz"),
+                                        ("lv_mixed", "lv")])
+def test_adjoint_vs_torch_autograd_and_fd(gslib, oracle, cuda, case, field):
+    from gradsolve_b200 import engine
+    g = load_golden(case)
+    g = {k: (v[:6] if getattr(v, "ndim", 0) >= 1 and v.shape[0] == g["y0"].shape[0] else v)
+         for k, v in g.items()}
+    spec, r, y0, p, yf = _replay_reference_dts(cuda, field, g)
+    gy0, gp = engine.adjoint(r, p, 2.0 * yf)
+    ty, tp = oracle.torch_replay_grad("tsit5", field, g["y0"], g["params"][:, : spec.nparam],
+                                      g["dts"], 2.0 * yf.cpu().numpy())
+    assert rel(gy0.cpu().numpy(), ty, 1e-8) <= 1e-9
+    assert rel(gp.cpu().numpy(), tp, 1e-8) <= 1e-9
+
+    def loss(q):
+        qq = torch.tensor(q, device=cuda).contiguous()
+        return float((engine.replay(r, y0, qq, write_ckpt=False) ** 2).sum().item())
+
+    fd = oracle.fd_grad(loss, g["params"][:, : spec.nparam].copy())
+    assert rel(gp.cpu().numpy(), fd, 1e-8) < 1e-6
+
+
+def test_empty_and_single_trajectory(gslib, cuda):
+    from gradsolve_b200 import engine
+    spec = _spec("lorenz")
+    for n in (0, 1):
+        y0 = torch.ones((n, 3), dtype=torch.float64, device=cuda)
+        p = torch.full((n, 1), 28.0, dtype=torch.float64, device=cuda)
+        r = engine.forward_record("tsit5", spec, y0, p, t0=0.0, t1=1.0, rtol=1e-6, atol=1e-9)
+        gy0, gp = engine.adjoint(r, p, torch.ones_like(y0))
+        torch.cuda.synchronize()
+        assert gy0.shape == (n, 3) and gp.shape == (n, 1)
+        assert r.status.numel() == n
+
+
+def test_max_steps_exhaustion_and_record_growth(gslib, oracle, cuda):
+    from gradsolve_b200 import engine
+    g = load_golden("lorenz_scale")
+    spec = _spec("lorenz")
+    y0 = torch.tensor(g["y0"], device=cuda)
+    p = torch.tensor(g["params"], device=cuda)
+    kw = dict(t0=0.0, t1=10.0, rtol=1e-8, atol=1e-8)
+    r = engine.forward_record("tsit5", spec, y0, p, max_steps=50, **kw)
+    assert (r.status.cpu().numpy() == 1).all()
+    with pytest.raises(RuntimeError, match="exhausted max_steps"):
+        engine.raise_on_failed(r, 50, 10.0)
+    # a record capacity of 8 forces several grow-and-retry rounds; the result is unchanged
+    r2 = engine.forward_record("tsit5", spec, y0, p, max_steps=100000, cap0=8, **kw)
+    assert r2.cap >= int(g["n_acc"].max())
+    np.testing.assert_array_equal(r2.n_acc.cpu().numpy(), g["n_acc"])
+    assert rel(r2.y_final.cpu().numpy(), g["y_final"], 1e-12) <= 1e-10
+
+
+def test_nan_parameter_and_reversed_interval(gslib, cuda):
+    from gradsolve_b200 import engine
+    spec = _spec("lorenz")
+    y0 = torch.tensor([[1.0, 0.0, 0.0], [1.0, 0.0, 0.0]], dtype=torch.float64, device=cuda)
+    p = torch.tensor([[float("nan")], [28.0]], dtype=torch.float64, device=cuda)
+    r = engine.forward_record("tsit5", spec, y0, p, t0=0.0, t1=1.0, rtol=1e-6, atol=1e-9)
+    st = r.status.cpu().numpy()
+    assert st[0] == 1 and st[1] == 0
+    # t1 < t0: the loop never starts (t >= t1), zero steps, y unchanged (reference semantics)
+    r = engine.forward_record("tsit5", spec, y0[1:], p[1:], t0=1.0, t1=0.5, rtol=1e-6,
+                              atol=1e-9)
+    assert int(r.n_acc.item()) == 0 and int(r.status.item()) == 0
+    assert torch.equal(r.y_final, y0[1:])
+
+
+def test_per_trajectory_end_times(gslib, oracle, cuda):
+    from gradsolve_b200 import engine
+    spec = _spec("vdp")
+    rng = np.random.default_rng(5)
+    n = 64
+    y0 = rng.uniform(-2, 2, (n, 2))
+    mu = 10 ** rng.uniform(-1, 0.9, (n, 1))
+    t1v = 10 ** rng.uniform(-1, np.log10(20), n)
+    r = engine.forward_record("tsit5", spec, torch.tensor(y0, device=cuda),
+                              torch.tensor(mu, device=cuda), t0=0.0, t1=float(t1v.max()),
+                              t1v=torch.tensor(t1v, device=cuda), rtol=1e-6, atol=1e-9)
+    ref = oracle.record("tsit5", "vdp", y0, mu, 0.0, 0.0, 1e-6, 1e-9, t1v=t1v)
+    np.testing.assert_array_equal(r.n_acc.cpu().numpy(), ref["n_acc"])
+    assert rel(r.y_final.cpu().numpy(), ref["y_final"], 1e-12) <= 1e-10
+
+
+def test_device_tableau_equals_host(gslib, cuda):
+    import ctypes
+    out = torch.zeros(41, dtype=torch.float64, device=cuda)
+    gslib.check(gslib.lib().gs_device_tableau(out.data_ptr(), None), "gs_device_tableau")
+    host = (ctypes.c_double * 41)()
+    gslib.lib().gs_tableau(host, 41)
+    np.testing.assert_array_equal(out.cpu().numpy(), np.array(host[:]))

@@ -81,13 +81,18 @@ def _as_tensor(x, dev: torch.device) -> torch.Tensor:
     return torch.as_tensor(np.asarray(x, dtype=np.float64), device=dev)
 
 
-def _prepare(problem, y0, params, dev):
+def _require_field(problem) -> FieldSpec:
     spec = field_for(problem)
     if spec is None:
         raise ValueError(
             f"gradsolve_b200 has no registered field for problem {getattr(problem, 'name', '?')!r}"
             "; supported names: 'diffeqgpu_lorenz', 'lorenz', 'vdp', 'lotka_volterra', "
             "'linear_ladder_<D>' (D in 1,2,3,4,8), 'robertson'")
+    return spec
+
+
+def _prepare(problem, y0, params, dev):
+    spec = _require_field(problem)
     y0_np = y0 if isinstance(y0, torch.Tensor) else np.asarray(y0, dtype=np.float64)
     if y0_np.ndim == 1:
         y0_np = y0_np[None, :]
@@ -161,6 +166,7 @@ def solve(problem, y0, params, *, saveat=None, engine: str = "auto", rtol: float
     if saveat is not None:
         raise NotImplementedError("saveat is not available on the B200 engines yet")
     reasons: list[str] = []
+    _require_field(problem)
     name = _resolve(problem, engine, reasons)
     spec = ENGINE_REGISTRY[name]
     if not spec.supports(problem):
@@ -243,6 +249,7 @@ def grad_closure(problem, y0, params, *, wrt="params", saveat=None, precision: s
     if precision not in ("float64",):
         raise ValueError(f"precision {precision!r} is not available; use 'float64'")
     reasons: list[str] = []
+    _require_field(problem)
     name = _resolve(problem, engine, reasons)
     spec = ENGINE_REGISTRY[name]
     if not spec.supports(problem):

@@ -162,6 +162,7 @@ int check_record_args(const char* who, long long n, const double* y0, const doub
                       const int* n_rej, const int* status) {
   const std::string w(who);
   if (n < 0) return fail(GS_ERR_ARG, w + ": n < 0");
+  if (n == 0) return GS_OK;  // empty ensemble: nothing is read or written
   if (!y0 || !p || !yf || !n_acc || !n_rej || !status)
     return fail(GS_ERR_ARG, w + ": y0, p, y_final, n_acc, n_rej and status are required");
   if (!aligned8(y0) || !aligned8(p) || !aligned8(yf))
@@ -183,6 +184,7 @@ int check_adjoint_args(const char* who, long long n, const double* p, const doub
                        const double* ybar) {
   const std::string w(who);
   if (n < 0) return fail(GS_ERR_ARG, w + ": n < 0");
+  if (n == 0) return GS_OK;
   if (!p || !rec || !n_acc || !ckpt || !ybar)
     return fail(GS_ERR_ARG, w + ": p, rec, n_acc, ckpt and ybar are required");
   if (cap < 1) return fail(GS_ERR_ARG, w + ": cap must be >= 1");
@@ -269,6 +271,7 @@ int gs_tsit5_replay(int field, int precision, long long n, const double* y0, con
   if (precision != GS_PREC_F64)
     return fail(GS_ERR_PRECISION, "gs_tsit5_replay: precision mode not built");
   if (n < 0) return fail(GS_ERR_ARG, "gs_tsit5_replay: n < 0");
+  if (n == 0) return GS_OK;
   if (!y0 || !p || !rec || !n_acc || !y_final)
     return fail(GS_ERR_ARG, "gs_tsit5_replay: y0, p, rec, n_acc and y_final are required");
   if (cap < 1 || !aligned16(rec)) return fail(GS_ERR_ARG, "gs_tsit5_replay: bad record");
@@ -320,6 +323,7 @@ int gs_ros23_replay(int field, int precision, long long n, const double* y0, con
   if (precision != GS_PREC_F64)
     return fail(GS_ERR_PRECISION, "gs_ros23_replay: precision mode not built");
   if (n < 0) return fail(GS_ERR_ARG, "gs_ros23_replay: n < 0");
+  if (n == 0) return GS_OK;
   if (!y0 || !p || !rec || !n_acc || !y_final)
     return fail(GS_ERR_ARG, "gs_ros23_replay: y0, p, rec, n_acc and y_final are required");
   if (cap < 1 || !aligned16(rec)) return fail(GS_ERR_ARG, "gs_ros23_replay: bad record");

@@ -170,7 +170,7 @@ def cpu_gradient_rate(target_s: float = 12.0, threads: int = 0) -> dict:
 
     m = max(64, cores * 16)
     dt = run(m)
-    m2 = int(min(1 << 16, max(m, m * target_s / max(dt, 1e-3))))
+    m2 = int(min(1 << 20, max(m, m * target_s / max(dt, 1e-3))))
     dt2 = run(m2)
     return {"value": m2 / dt2, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{m2} trajectories of the same workload (seed 1000), C restatement of "
@@ -289,6 +289,9 @@ def run_b200(args) -> None:
             events[3].record(stream)
         return r, gp
 
+    # clocks are sampled from the start of the warm-up to the end of the timed steps
+    clocks = ClockSampler(local)
+    clocks.start()
     # warm-up (also sizes the record so the timed steps never regrow it)
     for _ in range(args.warmup):
         r, gp = step()
@@ -299,11 +302,9 @@ def run_b200(args) -> None:
     S = int(r.n_acc.max().item())
     K = r.ckpt_every
 
-    clocks = ClockSampler(local)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks.start()
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     for k in range(args.steps):
         flush.zero_()  # L2 flush between timed steps (outside the events)

@@ -5,6 +5,7 @@
 // per-thread error message.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -376,3 +377,108 @@ int gs_record_to_padded(long long n, int cap, const double* rec, const int* n_ac
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Replay gradient without device allocation (gs_tsit5_vjp_static).
+//
+// Some callers cannot call cudaMalloc: a custom call running inside JAX/XLA, where XLA has
+// already reserved most of the device memory for its own pool and owns the rest, and
+// latency-critical callers for which the device-wide synchronisation of cudaMalloc and
+// cudaFree is not acceptable.  This entry point gives them the replay gradient of
+// gs_tsit5_replay + gs_tsit5_adjoint using a scratch array that lives in the library
+// itself: the dt record, the checkpoints and the per-trajectory step counts are placed in
+// g_vjp_scratch, a file-scope __device__ array of GS_STATIC_SCRATCH_BYTES bytes that every
+// GPU which loads the library holds until the process exits.
+//
+// The array's name is only a host-side stand-in in host code, so its device address is
+// looked up with cudaGetSymbolAddress, once per device, by the first call made on that
+// device (with that device current); that first call should therefore come before any
+// stream capture.  Every call shares the one array and it keeps the contents of the last
+// call; nothing in it has to start at zero, because every region a call reads is written
+// earlier in the same call.  Calls that overlap on the GPU (on different streams of the
+// same device) race on the array and must be serialised by the caller.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+__device__ __align__(256) unsigned char g_vjp_scratch[GS_STATIC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::atomic<void*> g_vjp_scratch_addr[kMaxDevices];
+
+int vjp_scratch_address(void** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess)
+    return fail(GS_ERR_CUDA, std::string("CUDA: cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices)
+    return fail(GS_ERR_ARG, "gs_tsit5_vjp_static: device ordinal " + std::to_string(dev) +
+                                " is beyond the supported " + std::to_string(kMaxDevices));
+  void* p = g_vjp_scratch_addr[dev].load(std::memory_order_acquire);
+  if (!p) {
+    e = cudaGetSymbolAddress(&p, g_vjp_scratch);
+    if (e != cudaSuccess)
+      return fail(GS_ERR_CUDA, std::string("CUDA: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_vjp_scratch_addr[dev].store(p, std::memory_order_release);
+  }
+  *out = p;
+  return GS_OK;
+}
+
+size_t round256(size_t b) { return (b + 255u) & ~size_t(255); }
+
+template <class F>
+int launch_tsit5_vjp_static(long long n, long long S, long long ld, const double* y0,
+                            const double* p, double t0, const double* dts, const double* ybar,
+                            double* y_final, double* gy0, double* gp, unsigned char* base,
+                            int cap, int K, size_t off_rec, size_t off_ckpt, cudaStream_t s) {
+  int* n_steps = reinterpret_cast<int*>(base);
+  double* rec = reinterpret_cast<double*>(base + off_rec);
+  double* ckpt = reinterpret_cast<double*>(base + off_ckpt);
+  record_from_padded_kernel<<<grid_for(n), kBlock, 0, s>>>(n, S, dts, ld, rec, cap, n_steps);
+  int rc = cuda_check("record_from_padded_kernel");
+  if (rc) return rc;
+  gs::ReplayArgs ra{n, y0, p, t0, rec, n_steps, K, gs_ckpt_slots(cap, K), ckpt, y_final};
+  gs::tsit5_replay_kernel<F><<<grid_for(n), kBlock, 0, s>>>(ra);
+  if ((rc = cuda_check("tsit5_replay_kernel"))) return rc;
+  gs::AdjointArgs aa{n, p, rec, n_steps, ckpt, K, ybar, gy0, gp};
+  gs::tsit5_adjoint_kernel<F><<<grid_for(n), kBlock, 0, s>>>(aa);
+  return cuda_check("tsit5_adjoint_kernel");
+}
+
+}  // namespace
+
+extern "C" int gs_tsit5_vjp_static(int field, long long n, const double* y0, const double* p,
+                                   double t0, const double* dts, long long S, long long ld,
+                                   const double* ybar, double* y_final, double* gy0,
+                                   double* gp, void* stream) {
+  if (n < 0 || S < 0 || ld < S) return fail(GS_ERR_ARG, "gs_tsit5_vjp_static: bad sizes");
+  int D, P, rc;
+  if ((rc = field_dims(field, &D, &P))) return rc;
+  if (n == 0) return GS_OK;
+  if (!y0 || !p || !ybar || !y_final || (S > 0 && !dts))
+    return fail(GS_ERR_ARG, "gs_tsit5_vjp_static: y0, p, dts, ybar and y_final are required");
+  if (!aligned8(y0) || !aligned8(p) || !aligned8(ybar) || !aligned8(y_final) ||
+      (dts && !aligned8(dts)))
+    return fail(GS_ERR_ARG, "gs_tsit5_vjp_static: float64 arrays must be 8-byte aligned");
+  if (S > (long long)INT32_MAX / 2)
+    return fail(GS_ERR_ARG, "gs_tsit5_vjp_static: S too large");
+  const int cap = S > 0 ? (int)S : 1;
+  int K = 1;
+  while ((long long)K * K < cap && K < gs::KMAX) ++K;  // ceil(sqrt(S)), at most KMAX
+  const size_t b_steps = round256((size_t)n * sizeof(int));
+  const size_t b_rec = round256(gs_record_bytes(n, cap));
+  const size_t b_ckpt = round256(gs_ckpt_bytes(field, n, cap, K));
+  const size_t need = b_steps + b_rec + b_ckpt;
+  if (need > (size_t)GS_STATIC_SCRATCH_BYTES)
+    return fail(GS_ERR_ARG, "gs_tsit5_vjp_static: n=" + std::to_string(n) + ", S=" +
+                                std::to_string(S) + " needs " + std::to_string(need) +
+                                " bytes of scratch; the static scratch holds " +
+                                std::to_string((size_t)GS_STATIC_SCRATCH_BYTES) +
+                                " bytes (use gs_tsit5_replay + gs_tsit5_adjoint with "
+                                "caller-allocated buffers for larger ensembles)");
+  void* base = nullptr;
+  if ((rc = vjp_scratch_address(&base))) return rc;
+  GS_TSIT5_DISPATCH(field, launch_tsit5_vjp_static, n, S, ld, y0, p, t0, dts, ybar, y_final,
+                    gy0, gp, static_cast<unsigned char*>(base), cap, K, b_steps,
+                    b_steps + b_rec, (cudaStream_t)stream)
+}

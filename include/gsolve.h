@@ -168,6 +168,32 @@ int gs_record_from_padded(long long n, long long S, const double* dts, long long
 int gs_record_to_padded(long long n, int cap, const double* rec, const int* n_acc, long long S,
                         double* dts, void* stream);
 
+/* Size of the library's own device scratch used by gs_tsit5_vjp_static: 64 MiB, held by
+ * every GPU that loads the library until the process exits. */
+#define GS_STATIC_SCRATCH_BYTES (64ull << 20)
+
+/*
+ * Replay gradient that allocates nothing.  No counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc -- a custom call inside JAX/XLA, where XLA has already
+ * reserved most of the device memory for its own pool, and latency-critical callers that
+ * cannot accept the device-wide synchronisation of cudaMalloc/cudaFree.
+ * Given the recorded dts in the reference's padded (n, S) layout (row stride ld >= S), it
+ * replays them at (y0, p) into y_final and writes gy0 = dL/dy0 and gp = dL/dp (either may
+ * be NULL) for the cotangent ybar = dL/dy_final: the result of gs_record_from_padded +
+ * gs_tsit5_replay + gs_tsit5_adjoint, computed with the dt record, checkpoints and step
+ * counts in a static device array inside the library instead of caller buffers.
+ * Limits: the record + checkpoints + counts must fit GS_STATIC_SCRATCH_BYTES (roughly
+ * n * S <= 7.5e6 steps for the 3-state fields); larger problems return GS_ERR_ARG with the
+ * numbers -- use the allocating entry points for them.
+ * The first call on each device looks up the array's device address (cudaGetSymbolAddress,
+ * with that device current); make that first call before any stream capture.  All calls
+ * share the one array, which keeps the last call's contents: calls that overlap on the GPU
+ * race and must be serialised by the caller.  Non-stiff (Tsit5) fields only.
+ */
+int gs_tsit5_vjp_static(int field, long long n, const double* y0, const double* p, double t0,
+                        const double* dts, long long S, long long ld, const double* ybar,
+                        double* y_final, double* gy0, double* gp, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -249,6 +249,33 @@ def run_reference(args) -> None:
 # ------------------------------------------------------------------------------------
 # the B200 arm
 # ------------------------------------------------------------------------------------
+def _time_steps(torch, step, steps, flush, stream):
+    """Run `steps` timed steps (L2 flushed before each, outside the events); returns the
+    per-step (forward, adjoint, whole) milliseconds and the last step's outputs."""
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(steps)]
+    out = None
+    for k in range(steps):
+        flush.zero_()
+        out = step(ev[k])
+    torch.cuda.synchronize()
+    fwd = [e[0].elapsed_time(e[1]) for e in ev]
+    adj = [e[2].elapsed_time(e[3]) for e in ev]
+    whole = [e[0].elapsed_time(e[3]) for e in ev]
+    return fwd, adj, whole, out
+
+
+def _grad_err(g, ref):
+    """Per-trajectory relative error of gradient rows g vs ref (both (n, P) tensors)."""
+    import torch
+    num = (g - ref).abs().amax(dim=1)
+    den = ref.abs().amax(dim=1).clamp_min(1e-300)
+    q = (num / den).double()
+    rel_l2 = float(((g - ref).norm() / ref.norm()).item())
+    return {"max": float(q.max().item()), "median": float(q.median().item()),
+            "p99": float(torch.quantile(q[: min(q.numel(), 1 << 24)], 0.99).item()),
+            "rel_l2": rel_l2}
+
+
 def run_b200(args) -> None:
     import torch
     import torch.distributed as dist
@@ -274,26 +301,29 @@ def run_b200(args) -> None:
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
     inv = 1.0 / (n * 3 * world)
 
-    def step(events=None):
-        if events:
-            events[0].record(stream)
-        r = engine.forward_record("tsit5", spec, y0, rho, t0=T0, t1=T1, rtol=RTOL, atol=ATOL,
-                                  max_steps=100000, cap0=args.cap, checkpoint=args.checkpoint)
-        if events:
-            events[1].record(stream)
-        ybar = (2.0 * inv) * r.y_final
-        if events:
-            events[2].record(stream)
-        gy0, gp = engine.adjoint(r, rho, ybar, want_y0=False)
-        if events:
-            events[3].record(stream)
-        return r, gp
+    def make_step(precision):
+        def step(events=None):
+            if events:
+                events[0].record(stream)
+            r = engine.forward_record("tsit5", spec, y0, rho, t0=T0, t1=T1, rtol=RTOL,
+                                      atol=ATOL, max_steps=100000, cap0=args.cap,
+                                      checkpoint=args.checkpoint, precision=precision)
+            if events:
+                events[1].record(stream)
+            ybar = (2.0 * inv) * r.y_final
+            if events:
+                events[2].record(stream)
+            _gy0, gp = engine.adjoint(r, rho, ybar, want_y0=False, precision=precision)
+            if events:
+                events[3].record(stream)
+            return r, gp
+        return step
 
     # clocks are sampled from the start of the warm-up to the end of the timed steps
     clocks = ClockSampler(local)
     clocks.start()
-    # warm-up (also sizes the record so the timed steps never regrow it)
-    for _ in range(args.warmup):
+    step = make_step("float64")
+    for _ in range(args.warmup):  # warm-up (also sizes the record so timed steps never regrow)
         r, gp = step()
     torch.cuda.synchronize()
     assert int((r.status != 0).sum().item()) == 0, "warm-up solve failed"
@@ -301,30 +331,48 @@ def run_b200(args) -> None:
     acc = int(r.n_acc.to(torch.int64).sum().item())
     S = int(r.n_acc.max().item())
     K = r.ckpt_every
-
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
-    for k in range(args.steps):
-        flush.zero_()  # L2 flush between timed steps (outside the events)
-        r, gp = step(ev[k])
-    torch.cuda.synchronize()
+    fwd_ms, adj_ms, step_ms, (r, gp) = _time_steps(torch, step, args.steps, flush, stream)
     if world > 1:
         dist.barrier()
-    clk = clocks.stop()
-    fwd_ms = [e[0].elapsed_time(e[1]) for e in ev]
-    adj_ms = [e[2].elapsed_time(e[3]) for e in ev]
-    step_ms = [e[0].elapsed_time(e[3]) for e in ev]
     ms_per_step = float(np.mean(step_ms))
     if world > 1:
         t = torch.tensor([ms_per_step], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_per_step = float(t.item())
     value = n * world / (ms_per_step * 1e-3)
-
-    # gradient sanity on this rank (finite, and matches the loss direction)
     assert torch.isfinite(gp).all()
+
+    # ---- the float32-stage variant on the same workload, and its accuracy ---------------
+    mixed = None
+    if not args.no_mixed:
+        mstep = make_step("mixed")
+        for _ in range(args.warmup):
+            rm, gpm = mstep()
+        m_fwd, m_adj, m_step, (rm, gpm) = _time_steps(torch, mstep, args.steps, flush, stream)
+        m_ms = float(np.mean(m_step))
+        if world > 1:
+            t = torch.tensor([m_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            m_ms = float(t.item())
+        # same mesh: the float64 record replayed and differentiated with float32 stages
+        ybar64 = (2.0 * inv) * r.y_final
+        yf_sm = engine.replay(r, y0, rho, write_ckpt=True, precision="mixed")
+        _g, gp_sm = engine.adjoint(r, rho, ybar64, want_y0=False, precision="mixed")
+        n_acc_diff = (rm.n_acc.to(torch.int64) - r.n_acc.to(torch.int64)).abs()
+        yrel = ((yf_sm - r.y_final).abs() / r.y_final.abs().clamp_min(1e-300)).amax(dim=1)
+        mixed = {"value": n * world / (m_ms * 1e-3), "ms_per_step": m_ms,
+                 "fwd_ms": float(np.mean(m_fwd)), "adj_ms": float(np.mean(m_adj)),
+                 "speedup_vs_f64": ms_per_step / m_ms,
+                 "grad_rel_err_own_mesh": _grad_err(gpm, gp),
+                 "grad_rel_err_same_mesh": _grad_err(gp_sm, gp),
+                 "y_final_rel_err_same_mesh_max": float(yrel.max().item()),
+                 "y_final_rel_err_same_mesh_median": float(yrel.median().item()),
+                 "n_acc_diff_max": int(n_acc_diff.max().item()),
+                 "meets_1e-6": _grad_err(gp_sm, gp)["max"] <= 1e-6}
+    clk = clocks.stop()
 
     # ---- e2e through the public API, host buffers, H2D + D2H inside the timed region ----
     e2e = None
@@ -336,8 +384,8 @@ def run_b200(args) -> None:
         prob = LorenzProblem()
 
         def e2e_step():
-            clo = gsb.grad_closure(prob, y0_h, rho_h, rtol=RTOL, atol=ATOL, remat=True,
-                                   max_steps=100000, device=dev)
+            clo = gsb.grad_closure(prob, y0_h, rho_h, rtol=RTOL, atol=ATOL,
+                                   checkpoint=args.checkpoint, max_steps=100000, device=dev)
             p = clo.state.p_rec.clone().requires_grad_(True)
             yf = clo(p)
             loss = (yf * yf).sum() * inv
@@ -412,7 +460,7 @@ def run_b200(args) -> None:
                    "l2": "flushed between timed steps (record traffic also >> L2)"},
         "gpu_launches": 2 * args.steps,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-        "fwd_ms": fwd_avg, "adj_ms": adj_avg,
+        "fwd_ms": fwd_avg, "adj_ms": adj_avg, "mixed": mixed,
     }
     print(json.dumps(line), flush=True)
     if world > 1:
@@ -431,6 +479,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-mixed", action="store_true")
     args = ap.parse_args()
     if args.checkpoint not in ("sqrt", "all", "auto"):
         args.checkpoint = int(args.checkpoint)

@@ -28,6 +28,7 @@ import numpy as np
 import torch
 
 from . import engine
+from . import engine as engine_mod
 from .base import Route, SolveResult
 from .fields import FieldSpec, field_for, kernel_params
 from .torch_adapter import ReplayState, replay_apply
@@ -246,14 +247,22 @@ def grad_closure(problem, y0, params, *, wrt="params", saveat=None, precision: s
     wrt_t = _normalize_wrt(wrt)
     if saveat is not None:
         raise NotImplementedError("saveat is not available on the B200 engines yet")
-    if precision not in ("float64",):
-        raise ValueError(f"precision {precision!r} is not available; use 'float64'")
     reasons: list[str] = []
+    if precision == "float32":
+        # the reference's f32 route (record and replay all in float32, gradsolve/api.py:
+        # 253-274) is served by the mixed mode: float32 stages, float64 state/controller
+        precision = "mixed"
+        reasons.append("float32-served-by-mixed")
+    if precision not in ("float64", "mixed"):
+        raise ValueError(f"unknown precision {precision!r}; known: 'float64', 'mixed', "
+                         "'float32'")
     _require_field(problem)
     name = _resolve(problem, engine, reasons)
     spec = ENGINE_REGISTRY[name]
     if not spec.supports(problem):
         raise ValueError(f"engine {name!r} does not support problem {problem.name!r}")
+    if precision == "mixed" and spec.method != engine_mod.METHOD_TSIT5:
+        raise ValueError("precision='mixed' is available on the Tsit5 engine only")
     fn = spec.reverse(problem, y0, params, rtol=rtol, atol=atol, device=device, remat=remat,
                       wrt=wrt_t, max_steps=max_steps, checkpoint=checkpoint, t1=t1,
                       precision=precision)

@@ -12,6 +12,7 @@
 
 #include "../../include/gsolve.h"
 #include "gs_fields.cuh"
+#include "gs_mixed.cuh"
 #include "gs_ros23.cuh"
 #include "gs_tableau.cuh"
 #include "gs_tsit5.cuh"
@@ -84,18 +85,31 @@ int field_dims(int field, int* D, int* P) {
                   "field " + std::to_string(field) + " has no analytic Jacobian for Rosenbrock23"); \
   }
 
+// mixed = float32 stages (GS_PREC_MIXED, gs_mixed.cuh), else float64 throughout.
 template <class F>
-int launch_tsit5_record(const gs::RecordArgs& a, cudaStream_t s) {
+int launch_tsit5_record(const gs::RecordArgs& a, cudaStream_t s, bool mixed) {
+  if (mixed) {
+    gs::tsit5_mixed_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    return cuda_check("tsit5_mixed_record_kernel");
+  }
   gs::tsit5_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
   return cuda_check("tsit5_record_kernel");
 }
 template <class F>
-int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s) {
+int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed) {
+  if (mixed) {
+    gs::tsit5_mixed_replay_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    return cuda_check("tsit5_mixed_replay_kernel");
+  }
   gs::tsit5_replay_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
   return cuda_check("tsit5_replay_kernel");
 }
 template <class F>
-int launch_tsit5_adjoint(const gs::AdjointArgs& a, cudaStream_t s) {
+int launch_tsit5_adjoint(const gs::AdjointArgs& a, cudaStream_t s, bool mixed) {
+  if (mixed) {
+    gs::tsit5_mixed_adjoint_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    return cuda_check("tsit5_mixed_adjoint_kernel");
+  }
   gs::tsit5_adjoint_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
   return cuda_check("tsit5_adjoint_kernel");
 }
@@ -253,8 +267,8 @@ int gs_tsit5_fwd_record(int field, int precision, long long n, const double* y0,
                         double atol, double dt0, int max_steps, int cap, int ckpt_every,
                         double* rec, double* ckpt, double* y_final, int* n_acc, int* n_rej,
                         int* status, void* stream) {
-  if (precision != GS_PREC_F64)
-    return fail(GS_ERR_PRECISION, "gs_tsit5_fwd_record: precision mode not built");
+  if (precision != GS_PREC_F64 && precision != GS_PREC_MIXED)
+    return fail(GS_ERR_PRECISION, "gs_tsit5_fwd_record: unknown precision mode " + std::to_string(precision));
   int rc = check_record_args("gs_tsit5_fwd_record", n, y0, p, rtol, atol, max_steps, cap,
                              ckpt_every, rec, ckpt, y_final, n_acc, n_rej, status);
   if (rc) return rc;
@@ -263,14 +277,15 @@ int gs_tsit5_fwd_record(int field, int precision, long long n, const double* y0,
   if (n == 0) return GS_OK;
   gs::RecordArgs a{n, y0, p, t0, t1, rtol, atol, dt0, t1v, max_steps, cap, ckpt_every,
                    gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status};
-  GS_TSIT5_DISPATCH(field, launch_tsit5_record, a, (cudaStream_t)stream)
+  GS_TSIT5_DISPATCH(field, launch_tsit5_record, a, (cudaStream_t)stream,
+                    precision == GS_PREC_MIXED)
 }
 
 int gs_tsit5_replay(int field, int precision, long long n, const double* y0, const double* p,
                     double t0, const double* rec, const int* n_acc, int cap, int ckpt_every,
                     double* ckpt, double* y_final, void* stream) {
-  if (precision != GS_PREC_F64)
-    return fail(GS_ERR_PRECISION, "gs_tsit5_replay: precision mode not built");
+  if (precision != GS_PREC_F64 && precision != GS_PREC_MIXED)
+    return fail(GS_ERR_PRECISION, "gs_tsit5_replay: unknown precision mode " + std::to_string(precision));
   if (n < 0) return fail(GS_ERR_ARG, "gs_tsit5_replay: n < 0");
   if (n == 0) return GS_OK;
   if (!y0 || !p || !rec || !n_acc || !y_final)
@@ -283,21 +298,23 @@ int gs_tsit5_replay(int field, int precision, long long n, const double* y0, con
   if (n == 0) return GS_OK;
   gs::ReplayArgs a{n, y0, p, t0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every), ckpt,
                    y_final};
-  GS_TSIT5_DISPATCH(field, launch_tsit5_replay, a, (cudaStream_t)stream)
+  GS_TSIT5_DISPATCH(field, launch_tsit5_replay, a, (cudaStream_t)stream,
+                    precision == GS_PREC_MIXED)
 }
 
 int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, const double* rec,
                      const int* n_acc, int cap, const double* ckpt, int ckpt_every,
                      const double* ybar, double* gy0, double* gp, void* stream) {
-  if (precision != GS_PREC_F64)
-    return fail(GS_ERR_PRECISION, "gs_tsit5_adjoint: precision mode not built");
+  if (precision != GS_PREC_F64 && precision != GS_PREC_MIXED)
+    return fail(GS_ERR_PRECISION, "gs_tsit5_adjoint: unknown precision mode " + std::to_string(precision));
   int rc = check_adjoint_args("gs_tsit5_adjoint", n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar);
   if (rc) return rc;
   int D, P;
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (n == 0) return GS_OK;
   gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp};
-  GS_TSIT5_DISPATCH(field, launch_tsit5_adjoint, a, (cudaStream_t)stream)
+  GS_TSIT5_DISPATCH(field, launch_tsit5_adjoint, a, (cudaStream_t)stream,
+                    precision == GS_PREC_MIXED)
 }
 
 int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,

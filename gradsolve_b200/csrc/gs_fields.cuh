@@ -17,6 +17,9 @@
 //
 // Contract of each field F (R = double or float):
 //   rhs(y, p, dy)                 dy = f(y, p)           (all fields are autonomous)
+//   rhs_delta(y, p, d, df)        df = f(y + d, p) - f(y, p), expanded so that no large
+//                                 terms cancel (used by the float32-stage kernels, where y
+//                                 is the float64 state rounded to float and d is small)
 //   vjp(y, p, w, gy, gp)          gy += (df/dy)^T w, gp += (df/dp)^T w
 //   jac(y, p, J)                  J = df/dy, row-major D x D          (stiff fields)
 //   jac_contract_grad(y,p,G,gy,gp) gy += d/dy <G, J(y,p)>, gp += d/dp <G, J(y,p)>
@@ -47,6 +50,15 @@ struct Lorenz {
     dy[2] = y[0] * y[1] - beta * y[2];
   }
   template <class R>
+  static GS_HD void rhs_delta(const R* y, const R* p, const R* d, R* df) {
+    const R sigma = R(10.0);
+    const R beta = R(8.0) / R(3.0);
+    const R rho = p[0];
+    df[0] = sigma * (d[1] - d[0]);
+    df[1] = rho * d[0] - d[1] - (y[0] * d[2] + d[0] * (y[2] + d[2]));
+    df[2] = y[0] * d[1] + d[0] * (y[1] + d[1]) - beta * d[2];
+  }
+  template <class R>
   static GS_HD void vjp(const R* y, const R* p, const R* w, R* gy, R* gp) {
     const R sigma = R(10.0);
     const R beta = R(8.0) / R(3.0);
@@ -68,6 +80,13 @@ struct Lorenz3 {
     dy[2] = y[0] * y[1] - beta * y[2];
   }
   template <class R>
+  static GS_HD void rhs_delta(const R* y, const R* p, const R* d, R* df) {
+    const R sigma = p[0], beta = p[1], rho = p[2];
+    df[0] = sigma * (d[1] - d[0]);
+    df[1] = rho * d[0] - d[1] - (y[0] * d[2] + d[0] * (y[2] + d[2]));
+    df[2] = y[0] * d[1] + d[0] * (y[1] + d[1]) - beta * d[2];
+  }
+  template <class R>
   static GS_HD void vjp(const R* y, const R* p, const R* w, R* gy, R* gp) {
     const R sigma = p[0], beta = p[1], rho = p[2];
     gy[0] += -sigma * w[0] + (rho - y[2]) * w[1] + y[1] * w[2];
@@ -87,6 +106,13 @@ struct VdP {
     dy[0] = v;
     dy[1] = mu * ((R(1.0) - x * x) * v - x);
   }
+  // f1(x+dx, v+dv) - f1(x, v) = mu [ (1 - x^2) dv - (2x + dx) dx (v + dv) - dx ]
+  template <class R>
+  static GS_HD void rhs_delta(const R* y, const R* p, const R* d, R* df) {
+    const R x = y[0], v = y[1], mu = p[0], dx = d[0], dv = d[1];
+    df[0] = dv;
+    df[1] = mu * ((R(1.0) - x * x) * dv - (R(2.0) * x + dx) * dx * (v + dv) - dx);
+  }
   template <class R>
   static GS_HD void vjp(const R* y, const R* p, const R* w, R* gy, R* gp) {
     const R x = y[0], v = y[1], mu = p[0];
@@ -103,6 +129,13 @@ struct LotkaVolterra {
     const R x = y[0], u = y[1];
     dy[0] = p[0] * x - p[1] * x * u;
     dy[1] = p[3] * x * u - p[2] * u;
+  }
+  // (x+dx)(u+du) - x u = x du + dx (u + du)
+  template <class R>
+  static GS_HD void rhs_delta(const R* y, const R* p, const R* d, R* df) {
+    const R dxu = y[0] * d[1] + d[0] * (y[1] + d[1]);
+    df[0] = p[0] * d[0] - p[1] * dxu;
+    df[1] = p[3] * dxu - p[2] * d[1];
   }
   template <class R>
   static GS_HD void vjp(const R* y, const R* p, const R* w, R* gy, R* gp) {
@@ -123,6 +156,11 @@ struct Linear {
   static GS_HD void rhs(const R* y, const R*, R* dy) {
 #pragma unroll
     for (int i = 0; i < D; ++i) dy[i] = R(1.01) * y[i];
+  }
+  template <class R>
+  static GS_HD void rhs_delta(const R*, const R*, const R* d, R* df) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) df[i] = R(1.01) * d[i];
   }
   template <class R>
   static GS_HD void vjp(const R*, const R*, const R* w, R* gy, R*) {
@@ -149,6 +187,16 @@ struct Robertson {
     dy[0] = -k1 * a + k3 * b * c;
     dy[1] = k1 * a - k3 * b * c - k2 * b * b;
     dy[2] = k2 * b * b;
+  }
+  // with e = (b+db)(c+dc) - b c = b dc + db (c + dc) and q = (b+db)^2 - b^2 = db (2b + db)
+  template <class R>
+  static GS_HD void rhs_delta(const R* y, const R* p, const R* d, R* df) {
+    const R k1 = p[0], k2 = p[1], k3 = p[2];
+    const R e = y[1] * d[2] + d[1] * (y[2] + d[2]);
+    const R q = d[1] * (R(2.0) * y[1] + d[1]);
+    df[0] = -k1 * d[0] + k3 * e;
+    df[1] = k1 * d[0] - k3 * e - k2 * q;
+    df[2] = k2 * q;
   }
   template <class R>
   static GS_HD void vjp(const R* y, const R* p, const R* w, R* gy, R* gp) {

@@ -1,0 +1,398 @@
+// gs_mixed.cuh -- Tsit5 forward/replay/adjoint with float32 stages (GS_PREC_MIXED).
+//
+// Float64 is kept for the time, the state y (updated with compensated summation), the
+// base right-hand side k1 = f(y) (the FSAL stage, once per attempt), the error norm and the
+// step-size controller.  Everything else runs in float32 in increment form:
+//
+//   k_i = k1 + dk_i,  dk_i = f(y + d_i) - f(y)  (F::rhs_delta: expanded, no cancellation)
+//   d_i = h (c_i k1 + sum_{j=2}^{i-1} a_ij dk_j)          (c_i = sum_j a_ij)
+//   y5  = y + h k1 + h sum_{i>=2} b_i dk_i                (sum_i b_i = 1)
+//   e   = h sum_{i>=2} E_i dk_i                           (sum_i E_i = 0)
+//
+// This is the same Tsit5 step (gradsolve/solvers/tsit5_step.py:80-102) regrouped, so the
+// float32 roundings act only on the increments dk_i and d_i, which are smaller than k and
+// y by the factor h|J|; the embedded error estimate, whose terms cancel in float64 form,
+// is computed from the increments directly.  The reverse pass applies the float32 stage
+// VJPs at the stage states y + d_i and accumulates the cotangent lambda and the parameter
+// gradient in float64.
+#pragma once
+#include "gs_fields.cuh"
+#include "gs_tableau.cuh"
+#include "gs_tsit5.cuh"
+
+namespace gs {
+
+struct Tsit5f {
+  static constexpr float C2 = (float)Tsit5::C2, C3 = (float)Tsit5::C3, C4 = (float)Tsit5::C4,
+                         C5 = (float)Tsit5::C5, C6 = 1.0f;
+  static constexpr float A21 = (float)Tsit5::A21, A31 = (float)Tsit5::A31,
+                         A32 = (float)Tsit5::A32, A41 = (float)Tsit5::A41,
+                         A42 = (float)Tsit5::A42, A43 = (float)Tsit5::A43,
+                         A51 = (float)Tsit5::A51, A52 = (float)Tsit5::A52,
+                         A53 = (float)Tsit5::A53, A54 = (float)Tsit5::A54,
+                         A61 = (float)Tsit5::A61, A62 = (float)Tsit5::A62,
+                         A63 = (float)Tsit5::A63, A64 = (float)Tsit5::A64,
+                         A65 = (float)Tsit5::A65;
+  static constexpr float B1 = (float)Tsit5::B1, B2 = (float)Tsit5::B2, B3 = (float)Tsit5::B3,
+                         B4 = (float)Tsit5::B4, B5 = (float)Tsit5::B5, B6 = (float)Tsit5::B6;
+  static constexpr float E2 = (float)Tsit5::E2, E3 = (float)Tsit5::E3, E4 = (float)Tsit5::E4,
+                         E5 = (float)Tsit5::E5, E6 = (float)Tsit5::E6, E7 = (float)Tsit5::E7;
+};
+
+template <class F>
+struct MixedStages {
+  static constexpr int D = F::D;
+  float dk2[D], dk3[D], dk4[D], dk5[D], dk6[D];
+};
+
+// Increments dk2..dk6 for step h from (y, k1); yf/pf/k1f are the float copies.
+template <class F>
+__device__ __forceinline__ void mixed_dk2_to_dk6(const float* yf, const float* pf,
+                                                 const float* k1f, float hf,
+                                                 MixedStages<F>& S) {
+  constexpr int D = F::D;
+  using T = Tsit5f;
+  float d[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) d[i] = hf * (T::C2 * k1f[i]);
+  F::rhs_delta(yf, pf, d, S.dk2);
+#pragma unroll
+  for (int i = 0; i < D; ++i) d[i] = hf * (T::C3 * k1f[i] + T::A32 * S.dk2[i]);
+  F::rhs_delta(yf, pf, d, S.dk3);
+#pragma unroll
+  for (int i = 0; i < D; ++i) d[i] = hf * (T::C4 * k1f[i] + T::A42 * S.dk2[i] + T::A43 * S.dk3[i]);
+  F::rhs_delta(yf, pf, d, S.dk4);
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+    d[i] = hf * (T::C5 * k1f[i] + T::A52 * S.dk2[i] + T::A53 * S.dk3[i] + T::A54 * S.dk4[i]);
+  F::rhs_delta(yf, pf, d, S.dk5);
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+    d[i] = hf * (T::C6 * k1f[i] + T::A62 * S.dk2[i] + T::A63 * S.dk3[i] + T::A64 * S.dk4[i] +
+                 T::A65 * S.dk5[i]);
+  F::rhs_delta(yf, pf, d, S.dk6);
+}
+
+// Full float64 increment of the step: h k1 + h sum b_i dk_i.
+template <class F>
+__device__ __forceinline__ void mixed_increment(const double* k1, const MixedStages<F>& S,
+                                                double h, float hf, double* inc) {
+  using T = Tsit5f;
+#pragma unroll
+  for (int i = 0; i < F::D; ++i) {
+    const float s = hf * (T::B2 * S.dk2[i] + T::B3 * S.dk3[i] + T::B4 * S.dk4[i] +
+                          T::B5 * S.dk5[i] + T::B6 * S.dk6[i]);
+    inc[i] = fma(h, k1[i], (double)s);
+  }
+}
+
+// y <- y + inc with Kahan compensation c (both float64).
+template <int D>
+__device__ __forceinline__ void kahan_add(double* y, double* c, const double* inc) {
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    const double yk = inc[i] - c[i];
+    const double tt = y[i] + yk;
+    c[i] = (tt - y[i]) - yk;
+    y[i] = tt;
+  }
+}
+
+template <class F>
+__device__ __forceinline__ void to_float(const double* a, float* b) {
+#pragma unroll
+  for (int i = 0; i < F::D; ++i) b[i] = (float)a[i];
+}
+
+// One replay step (values), float32 stages.
+template <class F>
+__device__ __forceinline__ void mixed_replay_step(double* y, double* c, const double* p,
+                                                  const float* pf, double dt) {
+  constexpr int D = F::D;
+  double k1[D], inc[D];
+  float yf[D], k1f[D];
+  F::rhs(y, p, k1);
+  to_float<F>(y, yf);
+  to_float<F>(k1, k1f);
+  MixedStages<F> S;
+  const float hf = (float)dt;
+  mixed_dk2_to_dk6<F>(yf, pf, k1f, hf, S);
+  mixed_increment<F>(k1, S, dt, hf, inc);
+  kahan_add<D>(y, c, inc);
+}
+
+// Reverse of one step at (y, dt): lam (float64) <- (dy'/dy)^T lam; gp += (dy'/dp)^T lam.
+template <class F>
+__device__ __forceinline__ void mixed_step_vjp(const double* y, const double* p, const float* pf,
+                                               double dt, double* lam, double* gp) {
+  constexpr int D = F::D, P = F::P;
+  using T = Tsit5f;
+  double k1[D];
+  float yf[D], k1f[D];
+  F::rhs(y, p, k1);
+  to_float<F>(y, yf);
+  to_float<F>(k1, k1f);
+  const float hf = (float)dt;
+  // stage states s_m = y + d_m (m = 2..6), float32
+  float s2[D], s3[D], s4[D], s5[D], s6[D];
+  {
+    float d[D], dk2[D], dk3[D], dk4[D], dk5[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) { d[i] = hf * (T::C2 * k1f[i]); s2[i] = yf[i] + d[i]; }
+    F::rhs_delta(yf, pf, d, dk2);
+#pragma unroll
+    for (int i = 0; i < D; ++i) { d[i] = hf * (T::C3 * k1f[i] + T::A32 * dk2[i]); s3[i] = yf[i] + d[i]; }
+    F::rhs_delta(yf, pf, d, dk3);
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      d[i] = hf * (T::C4 * k1f[i] + T::A42 * dk2[i] + T::A43 * dk3[i]);
+      s4[i] = yf[i] + d[i];
+    }
+    F::rhs_delta(yf, pf, d, dk4);
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      d[i] = hf * (T::C5 * k1f[i] + T::A52 * dk2[i] + T::A53 * dk3[i] + T::A54 * dk4[i]);
+      s5[i] = yf[i] + d[i];
+    }
+    F::rhs_delta(yf, pf, d, dk5);
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      d[i] = hf * (T::C6 * k1f[i] + T::A62 * dk2[i] + T::A63 * dk3[i] + T::A64 * dk4[i] +
+                   T::A65 * dk5[i]);
+      s6[i] = yf[i] + d[i];
+    }
+  }
+  float g[D], kb1[D], kb2[D], kb3[D], kb4[D], kb5[D], kb6[D], sb[D], acc[D], gpf[P];
+#pragma unroll
+  for (int k = 0; k < P; ++k) gpf[k] = 0.0f;
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    g[i] = hf * (float)lam[i];
+    acc[i] = 0.0f;
+    kb1[i] = T::B1 * g[i];
+    kb2[i] = T::B2 * g[i];
+    kb3[i] = T::B3 * g[i];
+    kb4[i] = T::B4 * g[i];
+    kb5[i] = T::B5 * g[i];
+    kb6[i] = T::B6 * g[i];
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) sb[i] = 0.0f;
+  F::vjp(s6, pf, kb6, sb, gpf);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    acc[i] += sb[i];
+    const float u = hf * sb[i];
+    kb1[i] += T::A61 * u; kb2[i] += T::A62 * u; kb3[i] += T::A63 * u;
+    kb4[i] += T::A64 * u; kb5[i] += T::A65 * u;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) sb[i] = 0.0f;
+  F::vjp(s5, pf, kb5, sb, gpf);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    acc[i] += sb[i];
+    const float u = hf * sb[i];
+    kb1[i] += T::A51 * u; kb2[i] += T::A52 * u; kb3[i] += T::A53 * u; kb4[i] += T::A54 * u;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) sb[i] = 0.0f;
+  F::vjp(s4, pf, kb4, sb, gpf);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    acc[i] += sb[i];
+    const float u = hf * sb[i];
+    kb1[i] += T::A41 * u; kb2[i] += T::A42 * u; kb3[i] += T::A43 * u;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) sb[i] = 0.0f;
+  F::vjp(s3, pf, kb3, sb, gpf);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    acc[i] += sb[i];
+    const float u = hf * sb[i];
+    kb1[i] += T::A31 * u; kb2[i] += T::A32 * u;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) sb[i] = 0.0f;
+  F::vjp(s2, pf, kb2, sb, gpf);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    acc[i] += sb[i];
+    kb1[i] += T::A21 * (hf * sb[i]);
+  }
+  F::vjp(yf, pf, kb1, acc, gpf);
+#pragma unroll
+  for (int i = 0; i < D; ++i) lam[i] += (double)acc[i];
+#pragma unroll
+  for (int k = 0; k < P; ++k) gp[k] += (double)gpf[k];
+}
+
+// --- forward adaptive solve with record, float32 stages ----------------------------------
+template <class F>
+__global__ void __launch_bounds__(128) tsit5_mixed_record_kernel(const RecordArgs a) {
+  constexpr int D = F::D, P = F::P;
+  using T = Tsit5f;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  double y[D], c[D], p[P], k1[D], y5[D], c5[D], k7[D], ed[D], inc[D];
+  float pf[P];
+#pragma unroll
+  for (int i = 0; i < D; ++i) { y[i] = a.y0[j * D + i]; c[i] = 0.0; }
+#pragma unroll
+  for (int i = 0; i < P; ++i) { p[i] = a.p[j * P + i]; pf[i] = (float)p[i]; }
+  double t = a.t0;
+  const double t1 = a.t1v ? a.t1v[j] : a.t1;
+  double dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
+  const bool rec_on = a.rec != nullptr;
+  const bool ck_on = a.ckpt != nullptr;
+  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
+  F::rhs(y, p, k1);
+  int acc = 0, rej = 0, st = 0, ck_cnt = 0, ck_slot = 0;
+  double b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
+  for (int it = 0; it < a.max_steps; ++it) {
+    if (t >= t1) break;
+    const double h = (t1 - t < dt) ? (t1 - t) : dt;
+    const float hf = (float)h;
+    float yf[D], k1f[D];
+    to_float<F>(y, yf);
+    to_float<F>(k1, k1f);
+    MixedStages<F> S;
+    mixed_dk2_to_dk6<F>(yf, pf, k1f, hf, S);
+    mixed_increment<F>(k1, S, h, hf, inc);
+#pragma unroll
+    for (int i = 0; i < D; ++i) { y5[i] = y[i]; c5[i] = c[i]; }
+    kahan_add<D>(y5, c5, inc);
+    F::rhs(y5, p, k7);
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      const float dk7 = (float)(k7[i] - k1[i]);
+      ed[i] = (double)(hf * (T::E2 * S.dk2[i] + T::E3 * S.dk3[i] + T::E4 * S.dk4[i] +
+                             T::E5 * S.dk5[i] + T::E6 * S.dk6[i] + T::E7 * dk7));
+    }
+    const double err = wrms_norm<D>(ed, y, y5, a.rtol, a.atol);
+    if (!(err == err)) {
+      st = 1;
+      break;
+    }
+    if (err <= 1.0) {
+      if ((rec_on || ck_on) && acc >= a.cap) {
+        st = 3;
+        break;
+      }
+      t = t + h;
+#pragma unroll
+      for (int i = 0; i < D; ++i) { y[i] = y5[i]; c[i] = c5[i]; k1[i] = k7[i]; }
+      if (rec_on) {
+        b0 = b1; b1 = b2; b2 = b3; b3 = h;
+        if ((acc & 3) == 3) store_rec_chunk(a.rec, a.n, j, acc >> 2, b0, b1, b2, b3);
+      }
+      ++acc;
+      if (ck_on && ++ck_cnt == a.ck_every) {
+        ck_cnt = 0;
+        if (++ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, ck_slot, y, t);
+      }
+    } else {
+      ++rej;
+    }
+    dt = step_controller(err, h, Tsit5::ORDER_EXP);
+  }
+  if (st == 0 && !(t >= t1)) st = 1;
+  if (rec_on) {
+    switch (acc & 3) {
+      case 1: store_rec_chunk(a.rec, a.n, j, acc >> 2, b3, 0.0, 0.0, 0.0); break;
+      case 2: store_rec_chunk(a.rec, a.n, j, acc >> 2, b2, b3, 0.0, 0.0); break;
+      case 3: store_rec_chunk(a.rec, a.n, j, acc >> 2, b1, b2, b3, 0.0); break;
+      default: break;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
+  a.n_acc[j] = acc;
+  a.n_rej[j] = rej;
+  a.status[j] = st;
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) tsit5_mixed_replay_kernel(const ReplayArgs a) {
+  constexpr int D = F::D, P = F::P;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  double y[D], c[D], p[P];
+  float pf[P];
+#pragma unroll
+  for (int i = 0; i < D; ++i) { y[i] = a.y0[j * D + i]; c[i] = 0.0; }
+#pragma unroll
+  for (int i = 0; i < P; ++i) { p[i] = a.p[j * P + i]; pf[i] = (float)p[i]; }
+  const int na = a.n_acc[j];
+  double t = a.t0;
+  const bool ck_on = a.ckpt != nullptr;
+  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
+  int ck_cnt = 0, ck_slot = 0;
+  for (int s = 0; s < na; ++s) {
+    const double dt = load_rec(a.rec, a.n, j, s);
+    mixed_replay_step<F>(y, c, p, pf, dt);
+    t = t + dt;
+    if (ck_on && ++ck_cnt == a.ck_every) {
+      ck_cnt = 0;
+      if (++ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, ck_slot, y, t);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) tsit5_mixed_adjoint_kernel(const AdjointArgs a) {
+  constexpr int D = F::D, P = F::P;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  double p[P], lam[D], gp[P];
+  float pf[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    p[i] = a.p[j * P + i];
+    pf[i] = (float)p[i];
+    gp[i] = 0.0;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
+  const int na = a.n_acc[j];
+  const int K = a.ck_every;
+  const int nseg = (na + K - 1) / K;
+  double seg[KMAX][D];
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int start = sg * K;
+    double y[D], c[D];
+    load_ckpt<D>(a.ckpt, a.n, j, sg, y);
+#pragma unroll
+    for (int i = 0; i < D; ++i) { seg[0][i] = y[i]; c[i] = 0.0; }
+    for (int q = 1; q < K; ++q) {
+      const int s = start + q - 1;
+      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      if (dt != 0.0) mixed_replay_step<F>(y, c, p, pf, dt);
+#pragma unroll
+      for (int i = 0; i < D; ++i) seg[q][i] = y[i];
+    }
+    for (int q = K - 1; q >= 0; --q) {
+      const int s = start + q;
+      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      if (dt != 0.0) {
+        double ys[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) ys[i] = seg[q][i];
+        mixed_step_vjp<F>(ys, p, pf, dt, lam, gp);
+      }
+    }
+  }
+  if (a.gy0) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) a.gy0[j * D + i] = lam[i];
+  }
+  if (a.gp) {
+#pragma unroll
+    for (int i = 0; i < P; ++i) a.gp[j * P + i] = gp[i];
+  }
+}
+
+}  // namespace gs

@@ -1,0 +1,95 @@
+"""The float32-stage mode (GS_PREC_MIXED) against the float64 oracle.
+
+Reported two ways, as the precision question needs (the reference's own f32 checks are
+tests/test_f32_replay.py:88-94, 208-270, 278-369):
+  * same mesh -- the reference's recorded dts replayed in mixed precision: isolates the
+    arithmetic error of float32 stages from mesh differences;
+  * own mesh -- the mixed forward records its own mesh (its controller reads a float32-built
+    error estimate), compared end to end; step counts may differ by a few.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+CASES = [("lv_mixed", "lv"), ("lorenz_small", "lorenz"), ("vdp_batch", "vdp"),
+         ("lorenz_scale", "lorenz")]
+# measured bounds (B200): same-mesh relative error of y_final and of the gradients
+SAME_MESH_Y = {"lv": 1e-7, "lorenz": 1e-6, "vdp": 1e-7}
+SAME_MESH_G = {"lv": 1e-6, "lorenz": 1e-5, "vdp": 1e-6}
+
+
+def relmax(a, b, floor=1e-8):
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
+
+
+@pytest.mark.parametrize("case,field", CASES)
+def test_same_mesh_mixed_vs_f64(gslib, oracle, cuda, case, field):
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    g = load_golden(case)
+    spec = field_spec(field)
+    dts = torch.tensor(g["dts"], device=cuda)
+    y0 = torch.tensor(g["y0"], device=cuda)
+    p = torch.tensor(g["params"][:, : spec.nparam], device=cuda).contiguous()
+    r = engine.record_from_padded("tsit5", spec, dts, 0.0, checkpoint="sqrt")
+    yf = engine.replay(r, y0, p, precision="mixed")
+    ybar = 2.0 * yf
+    gy0, gp = engine.adjoint(r, p, ybar, precision="mixed")
+    ry = oracle.replay("tsit5", field, g["y0"], g["params"], g["dts"])
+    oy, op = oracle.replay_vjp("tsit5", field, g["y0"], g["params"], g["dts"], ybar.cpu().numpy())
+    ey = relmax(yf.cpu().numpy(), ry)
+    eg = max(relmax(gy0.cpu().numpy(), oy), relmax(gp.cpu().numpy(), op[:, : spec.nparam]))
+    print(f"{case}: same-mesh mixed rel err y_final {ey:.2e} grad {eg:.2e}")
+    bound_y = SAME_MESH_Y[field] * (100 if case == "lorenz_scale" else 1)
+    bound_g = SAME_MESH_G[field] * (1000 if case == "lorenz_scale" else 1)
+    assert ey <= bound_y
+    assert eg <= bound_g
+
+
+@pytest.mark.parametrize("case,field", CASES[:3])
+def test_own_mesh_mixed_forward(gslib, cuda, case, field):
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    g = load_golden(case)
+    spec = field_spec(field)
+    y0 = torch.tensor(g["y0"], device=cuda)
+    p = torch.tensor(g["params"][:, : spec.nparam], device=cuda).contiguous()
+    r = engine.forward_record("tsit5", spec, y0, p, t0=0.0, t1=float(g["t1"]),
+                              rtol=float(g["rtol"]), atol=float(g["atol"]), precision="mixed")
+    assert (r.status.cpu().numpy() == 0).all()
+    dn = np.abs(r.n_acc.cpu().numpy() - g["n_acc"])
+    ey = relmax(r.y_final.cpu().numpy(), g["y_final"])
+    print(f"{case}: own-mesh mixed: max |n_acc diff| {dn.max()}, rel err y_final {ey:.2e}")
+    assert dn.max() <= 2
+    # the recorded mesh replays (mixed) to the recording pass's value
+    yr = engine.replay(r, y0, p, precision="mixed")
+    assert relmax(yr.cpu().numpy(), r.y_final.cpu().numpy()) <= 1e-13
+    assert ey <= 1e-5
+
+
+def test_grad_closure_mixed_and_float32_route(gslib, oracle, cuda):
+    import gradsolve_b200 as gsb
+
+    class LV:
+        name = "lotka_volterra"
+        dim = 2
+        t0 = 0.0
+        t1 = 20.0
+        is_stiff = False
+
+    g = load_golden("lv_mixed")
+    for prec in ("mixed", "float32"):
+        clo = gsb.grad_closure(LV(), g["y0"], g["params"], rtol=1e-6, atol=1e-8, precision=prec)
+        if prec == "float32":
+            assert "float32-served-by-mixed" in clo.route.reason
+        p = torch.tensor(g["params"], device="cuda", requires_grad=True)
+        (clo(p) ** 2).sum().backward()
+        assert torch.isfinite(p.grad).all()
+    with pytest.raises(ValueError, match="unknown precision"):
+        gsb.grad_closure(LV(), g["y0"], g["params"], precision="float16")

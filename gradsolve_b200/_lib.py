@@ -48,6 +48,12 @@ _SIGS = {
     "gs_record_from_padded": (c_int, [c_ll, c_ll, c_void_p, c_ll, c_void_p, c_int, c_void_p,
                                       c_void_p]),
     "gs_record_to_padded": (c_int, [c_ll, c_int, c_void_p, c_void_p, c_ll, c_void_p, c_void_p]),
+    "gs_replay_saveat": (c_int, [c_int, c_int, c_int, c_ll, c_void_p, c_void_p, c_double,
+                                 c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p, c_ll,
+                                 c_int, c_void_p, c_void_p, c_void_p]),
+    "gs_adjoint_saveat": (c_int, [c_int, c_int, c_int, c_ll, c_void_p, c_void_p, c_void_p,
+                                  c_int, c_void_p, c_int, c_void_p, c_ll, c_int, c_void_p,
+                                  c_void_p, c_void_p, c_void_p, c_void_p]),
     "gs_tsit5_vjp_static": (c_int, [c_int, c_ll, c_void_p, c_void_p, c_double, c_void_p, c_ll,
                                     c_ll, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
 }

@@ -31,7 +31,7 @@ from . import engine
 from . import engine as engine_mod
 from .base import Route, SolveResult
 from .fields import FieldSpec, field_for, kernel_params
-from .torch_adapter import ReplayState, replay_apply
+from .torch_adapter import ReplayState, replay_apply, saveat_apply
 
 ENGINE_TSIT5 = "b200_tsit5"
 ENGINE_ROS23 = "b200_rosenbrock23"
@@ -164,19 +164,67 @@ def solve(problem, y0, params, *, saveat=None, engine: str = "auto", rtol: float
     """Forward ensemble solve (gradsolve/api.py:291-400).  Routes like the reference and
     returns a host ``SolveResult`` with true per-trajectory accepted/rejected counts.
     ``t1`` (optional) overrides ``problem.t1`` with a scalar or per-trajectory end times."""
-    if saveat is not None:
-        raise NotImplementedError("saveat is not available on the B200 engines yet")
     reasons: list[str] = []
     _require_field(problem)
     name = _resolve(problem, engine, reasons)
     spec = ENGINE_REGISTRY[name]
     if not spec.supports(problem):
         raise ValueError(f"engine {name!r} does not support problem {problem.name!r}")
+    if saveat is not None:
+        res = _solve_saveat(name, problem, y0, params, saveat, rtol=rtol, atol=atol,
+                            device=device, max_steps=max_steps, t1=t1)
+        res.route = Route(requested=engine, actual=name, reason="; ".join(reasons) or None)
+        return res
     res = spec.solve(problem, y0, params, rtol=rtol, atol=atol, device=device,
                      max_steps=max_steps, t1=t1)
     res.solver = name
     res.route = Route(requested=engine, actual=name, reason="; ".join(reasons) or None)
     return res
+
+
+def validate_saveat(saveat, t0: float, t1: float, t1v=None, n: Optional[int] = None):
+    """Validate requested output times (gradsolve/solvers/dense.py:81-103): finite, sorted
+    non-decreasing, inside [t0, t1].  A (k,) grid is shared by every trajectory; an (n, k)
+    array gives each trajectory its own row (checked against its own end time when
+    per-trajectory end times are given).  Returns float64 numpy."""
+    ts = np.asarray(saveat.detach().cpu() if isinstance(saveat, torch.Tensor) else saveat,
+                    dtype=np.float64)
+    if ts.ndim not in (1, 2):
+        raise ValueError(f"saveat must be (k,) or (n, k); got shape {ts.shape}")
+    if ts.shape[-1] == 0:
+        raise ValueError("saveat must contain at least one time")
+    if not np.all(np.isfinite(ts)):
+        raise ValueError("saveat contains non-finite times")
+    if np.any(np.diff(ts, axis=-1) < 0):
+        raise ValueError("saveat must be sorted non-decreasing")
+    if ts.ndim == 2 and n is not None and ts.shape[0] != n:
+        raise ValueError(f"per-trajectory saveat has {ts.shape[0]} rows for {n} trajectories")
+    hi = np.asarray(t1v, dtype=np.float64) if t1v is not None else np.float64(t1)
+    last = ts[..., -1]
+    if np.any(ts[..., 0] < t0) or np.any(last > (hi if ts.ndim == 2 else np.min(hi))):
+        raise ValueError(f"saveat times must lie within the problem domain [t0, t1] "
+                         f"(t0={t0}); got [{ts.min()}, {ts.max()}]")
+    return ts
+
+
+def _solve_saveat(name, problem, y0, params, saveat, *, rtol, atol, device, max_steps, t1):
+    """solve(..., saveat=ts): record the mesh, replay it with dense output
+    (gradsolve/api.py:438-536)."""
+    method = ENGINE_REGISTRY[name].method
+    dev = _device(device)
+    spec, y0_t, _p, pk = _prepare(problem, y0, params, dev)
+    t1s, t1v = _t1_arg(problem, t1, dev)
+    ts = validate_saveat(saveat, float(problem.t0), t1s,
+                         None if t1v is None else t1v.cpu().numpy(), y0_t.shape[0])
+    ms = int(max_steps or DEFAULT_MAX_STEPS[name])
+    r = engine.forward_record(method, spec, y0_t, pk, t0=float(problem.t0), t1=t1s, t1v=t1v,
+                              rtol=rtol, atol=atol, max_steps=ms, checkpoint="sqrt")
+    engine.raise_on_failed(r, ms, t1s)
+    yf, ys = engine.replay_saveat(r, y0_t, pk, torch.as_tensor(ts, device=dev),
+                                  write_ckpt=False)
+    return SolveResult(y_final=yf.cpu().numpy(), y_saved=ys.cpu().numpy(), ts_saved=ts,
+                       accepted_steps=r.n_acc.cpu().numpy().astype(np.int64),
+                       rejected_steps=r.n_rej.cpu().numpy().astype(np.int64), solver=name)
 
 
 _VALID_WRT = "'params', 'y0', or ('y0', 'params')"
@@ -212,7 +260,7 @@ def _make_reverse(name):
     method = ENGINE_REGISTRY[name].method
 
     def reverse(problem, y0, params, *, rtol, atol, device="cuda", remat=None, wrt=("params",),
-                max_steps=None, checkpoint=None, t1=None, precision="float64"):
+                max_steps=None, checkpoint=None, t1=None, precision="float64", saveat=None):
         if checkpoint is None:
             checkpoint = "auto" if remat is None else ("sqrt" if remat else "all")
         ms = max_steps or DEFAULT_MAX_STEPS[name]
@@ -221,9 +269,18 @@ def _make_reverse(name):
                                               checkpoint=checkpoint, t1=t1,
                                               precision=precision)
         dev = y0_t.device
+        if saveat is not None:
+            t1s, t1v = _t1_arg(problem, t1, dev)
+            ts = torch.as_tensor(
+                validate_saveat(saveat, float(problem.t0), t1s,
+                                None if t1v is None else t1v.cpu().numpy(), y0_t.shape[0]),
+                device=dev)
 
-        def kernel(z, p):
-            return replay_apply(state, _as_tensor(z, dev), _as_tensor(p, dev))
+            def kernel(z, p):  # the dense time series (n, k, dim), gradsolve/api.py:748-752
+                return saveat_apply(state, _as_tensor(z, dev), _as_tensor(p, dev), ts)
+        else:
+            def kernel(z, p):
+                return replay_apply(state, _as_tensor(z, dev), _as_tensor(p, dev))
 
         if wrt == ("y0",):
             fn = lambda z: kernel(z, p_t)  # noqa: E731
@@ -245,8 +302,6 @@ def grad_closure(problem, y0, params, *, wrt="params", saveat=None, precision: s
     ``wrt="params"``; ``closure(y0)`` for ``wrt="y0"``; ``closure(y0, params)`` for both.
     The closure carries ``.route`` and ``.state`` (the device record)."""
     wrt_t = _normalize_wrt(wrt)
-    if saveat is not None:
-        raise NotImplementedError("saveat is not available on the B200 engines yet")
     reasons: list[str] = []
     if precision == "float32":
         # the reference's f32 route (record and replay all in float32, gradsolve/api.py:
@@ -265,7 +320,7 @@ def grad_closure(problem, y0, params, *, wrt="params", saveat=None, precision: s
         raise ValueError("precision='mixed' is available on the Tsit5 engine only")
     fn = spec.reverse(problem, y0, params, rtol=rtol, atol=atol, device=device, remat=remat,
                       wrt=wrt_t, max_steps=max_steps, checkpoint=checkpoint, t1=t1,
-                      precision=precision)
+                      precision=precision, saveat=saveat)
     fn.route = Route(requested=engine, actual=name, reason="; ".join(reasons) or None)
     return fn
 

@@ -14,6 +14,7 @@
 #include "gs_fields.cuh"
 #include "gs_mixed.cuh"
 #include "gs_ros23.cuh"
+#include "gs_saveat.cuh"
 #include "gs_tableau.cuh"
 #include "gs_tsit5.cuh"
 
@@ -75,6 +76,7 @@ int field_dims(int field, int* D, int* P) {
 #define GS_ROS23_DISPATCH(field, FN, ...)                                                   \
   switch (field) {                                                                          \
     case gs::FIELD_ROBERTSON: return FN<gs::Robertson>(__VA_ARGS__);                        \
+    case gs::FIELD_VDP: return FN<gs::VdP>(__VA_ARGS__);                                    \
     case 4001: return FN<gs::Linear<1>>(__VA_ARGS__);                                       \
     case 4002: return FN<gs::Linear<2>>(__VA_ARGS__);                                       \
     case 4003: return FN<gs::Linear<3>>(__VA_ARGS__);                                       \
@@ -498,4 +500,98 @@ extern "C" int gs_tsit5_vjp_static(int field, long long n, const double* y0, con
   GS_TSIT5_DISPATCH(field, launch_tsit5_vjp_static, n, S, ld, y0, p, t0, dts, ybar, y_final,
                     gy0, gp, static_cast<unsigned char*>(base), cap, K, b_steps,
                     b_steps + b_rec, (cudaStream_t)stream)
+}
+
+// ---------------------------------------------------------------------------------------
+// Dense output (saveat) on the replay, and its adjoint (gs_saveat.cuh).
+// ---------------------------------------------------------------------------------------
+namespace {
+
+template <class F, class M>
+int launch_saveat(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint) {
+  if (adjoint) {
+    gs::adjoint_saveat_kernel<F, M><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    return cuda_check("adjoint_saveat_kernel");
+  }
+  gs::replay_saveat_kernel<F, M><<<grid_for(a.n), kBlock, 0, s>>>(a);
+  return cuda_check("replay_saveat_kernel");
+}
+
+template <class F>
+int launch_saveat_tsit5(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint, bool mixed) {
+  return mixed ? launch_saveat<F, gs::Tsit5MixedStep>(a, s, adjoint)
+               : launch_saveat<F, gs::Tsit5F64Step>(a, s, adjoint);
+}
+
+template <class F>
+int launch_saveat_ros23(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint) {
+  return launch_saveat<F, gs::Ros23Step>(a, s, adjoint);
+}
+
+int saveat_dispatch(int method, int field, int precision, const gs::SaveatArgs& a, void* stream,
+                    bool adjoint) {
+  const cudaStream_t s = (cudaStream_t)stream;
+  if (method == GS_METHOD_TSIT5) {
+    if (precision != GS_PREC_F64 && precision != GS_PREC_MIXED)
+      return fail(GS_ERR_PRECISION, "saveat: unknown precision mode " + std::to_string(precision));
+    GS_TSIT5_DISPATCH(field, launch_saveat_tsit5, a, s, adjoint, precision == GS_PREC_MIXED)
+  }
+  if (method == GS_METHOD_ROS23) {
+    if (precision != GS_PREC_F64)
+      return fail(GS_ERR_PRECISION, "saveat: Rosenbrock23 runs in float64 only");
+    GS_ROS23_DISPATCH(field, launch_saveat_ros23, a, s, adjoint)
+  }
+  return fail(GS_ERR_ARG, "saveat: unknown method " + std::to_string(method));
+}
+
+int check_saveat(const char* who, long long n, const double* p, const double* rec,
+                 const int* n_acc, int cap, const double* ckpt, int ckpt_every,
+                 const double* ts, long long ts_ld, int K) {
+  const std::string w(who);
+  if (n < 0 || K < 0 || ts_ld < 0) return fail(GS_ERR_ARG, w + ": bad sizes");
+  if (n == 0) return GS_OK;
+  if (!p || !rec || !n_acc || (K > 0 && !ts))
+    return fail(GS_ERR_ARG, w + ": p, rec, n_acc and ts are required");
+  if (ts_ld != 0 && ts_ld < K) return fail(GS_ERR_ARG, w + ": ts row stride < K");
+  if (cap < 1 || !aligned16(rec)) return fail(GS_ERR_ARG, w + ": bad record");
+  if (ckpt && (!aligned16(ckpt) || ckpt_every < 1 || ckpt_every > gs::KMAX))
+    return fail(GS_ERR_ARG, w + ": bad checkpoint buffer or interval");
+  return GS_OK;
+}
+
+}  // namespace
+
+extern "C" int gs_replay_saveat(int method, int field, int precision, long long n,
+                                const double* y0, const double* p, double t0, const double* rec,
+                                const int* n_acc, int cap, int ckpt_every, double* ckpt,
+                                const double* ts, long long ts_ld, int K, double* ys,
+                                double* y_final, void* stream) {
+  int rc = check_saveat("gs_replay_saveat", n, p, rec, n_acc, cap, ckpt, ckpt_every, ts, ts_ld, K);
+  if (rc) return rc;
+  int D, P;
+  if ((rc = field_dims(field, &D, &P))) return rc;
+  if (n == 0) return GS_OK;
+  if (!y0 || !y_final || (K > 0 && !ys))
+    return fail(GS_ERR_ARG, "gs_replay_saveat: y0, ys and y_final are required");
+  gs::SaveatArgs a{n, y0, p, t0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every), ckpt,
+                   ts, ts_ld, K, ys, y_final, nullptr, nullptr, nullptr, nullptr};
+  return saveat_dispatch(method, field, precision, a, stream, false);
+}
+
+extern "C" int gs_adjoint_saveat(int method, int field, int precision, long long n,
+                                 const double* p, const double* rec, const int* n_acc, int cap,
+                                 const double* ckpt, int ckpt_every, const double* ts,
+                                 long long ts_ld, int K, const double* ysbar, const double* ybar,
+                                 double* gy0, double* gp, void* stream) {
+  int rc = check_saveat("gs_adjoint_saveat", n, p, rec, n_acc, cap, ckpt, ckpt_every, ts, ts_ld, K);
+  if (rc) return rc;
+  int D, P;
+  if ((rc = field_dims(field, &D, &P))) return rc;
+  if (n == 0) return GS_OK;
+  if (!ckpt || (K > 0 && !ysbar))
+    return fail(GS_ERR_ARG, "gs_adjoint_saveat: ckpt and ysbar are required");
+  gs::SaveatArgs a{n, nullptr, p, 0.0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every),
+                   const_cast<double*>(ckpt), ts, ts_ld, K, nullptr, nullptr, ysbar, ybar, gy0,
+                   gp};
+  return saveat_dispatch(method, field, precision, a, stream, true);
 }

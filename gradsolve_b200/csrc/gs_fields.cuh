@@ -120,6 +120,22 @@ struct VdP {
     gy[1] += w[0] + w[1] * mu * (R(1.0) - x * x);
     gp[0] += w[1] * ((R(1.0) - x * x) * v - x);
   }
+  // J = [[0, 1], [mu (-2 x v - 1), mu (1 - x^2)]]  (for Rosenbrock23 at large mu)
+  template <class R>
+  static GS_HD void jac(const R* y, const R* p, R* J) {
+    const R x = y[0], v = y[1], mu = p[0];
+    J[0] = R(0.0);
+    J[1] = R(1.0);
+    J[2] = mu * (R(-2.0) * x * v - R(1.0));
+    J[3] = mu * (R(1.0) - x * x);
+  }
+  template <class R>
+  static GS_HD void jac_contract_grad(const R* y, const R* p, const R* G, R* gy, R* gp) {
+    const R x = y[0], v = y[1], mu = p[0];
+    gy[0] += R(-2.0) * mu * (G[2] * v + G[3] * x);
+    gy[1] += R(-2.0) * mu * x * G[2];
+    gp[0] += G[2] * (R(-2.0) * x * v - R(1.0)) + G[3] * (R(1.0) - x * x);
+  }
 };
 
 struct LotkaVolterra {

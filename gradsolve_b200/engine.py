@@ -208,3 +208,46 @@ def record_from_padded(method: str, spec: FieldSpec, dts: torch.Tensor, t0: floa
     yf = torch.empty((n, spec.dim), dtype=torch.float64, device=dts.device)
     return Record(method, spec, n, float(t0), cap, K, rec, ckpt, yf, n_steps, zeros,
                   zeros.clone())
+
+
+_METHOD_CODE = {METHOD_TSIT5: 0, METHOD_ROS23: 1}
+
+
+def _ts_arg(ts: torch.Tensor, n: int):
+    ts = ts.to(dtype=torch.float64).contiguous()
+    if ts.ndim == 1:
+        return ts, 0, ts.shape[0]
+    if ts.ndim != 2 or ts.shape[0] != n:
+        raise ValueError(f"saveat times must be (K,) or (n, K); got {tuple(ts.shape)}")
+    return ts, ts.shape[1], ts.shape[1]
+
+
+def replay_saveat(r: Record, y0: torch.Tensor, p: torch.Tensor, ts: torch.Tensor, *,
+                  write_ckpt: bool = True, precision: str = "float64"):
+    """Frozen-mesh replay with dense output at ``ts`` ((K,) shared or (n, K) per trajectory).
+    Returns (y_final (n, D), ys (n, K, D)); refreshes the checkpoints for the adjoint."""
+    ts, ld, K = _ts_arg(ts, r.n)
+    yf = torch.empty_like(y0)
+    ys = torch.empty((r.n, K, r.spec.dim), dtype=torch.float64, device=y0.device)
+    _lib.check(_lib.lib().gs_replay_saveat(
+        _METHOD_CODE[r.method], r.spec.code, _PREC[precision], r.n, _ptr(y0), _ptr(p),
+        float(r.t0), _ptr(r.rec), _ptr(r.n_acc), max(r.cap, 1), r.ckpt_every,
+        _ptr(r.ckpt) if write_ckpt else None, _ptr(ts), ld, K, _ptr(ys), _ptr(yf), _stream()),
+        "gs_replay_saveat")
+    return yf, ys
+
+
+def adjoint_saveat(r: Record, p: torch.Tensor, ts: torch.Tensor, ysbar: torch.Tensor,
+                   ybar: Optional[torch.Tensor] = None, *, want_y0: bool = True,
+                   want_p: bool = True, precision: str = "float64"):
+    """(dL/dy0, dL/dp) for cotangents ysbar = dL/dys (n, K, D) and ybar = dL/dy_final."""
+    ts, ld, K = _ts_arg(ts, r.n)
+    gy0 = torch.empty((r.n, r.spec.dim), dtype=torch.float64, device=p.device) if want_y0 else None
+    gp = torch.empty((r.n, p.shape[1]), dtype=torch.float64, device=p.device) if want_p else None
+    ysbar = ysbar.to(torch.float64).contiguous()
+    ybar = None if ybar is None else ybar.to(torch.float64).contiguous()
+    _lib.check(_lib.lib().gs_adjoint_saveat(
+        _METHOD_CODE[r.method], r.spec.code, _PREC[precision], r.n, _ptr(p), _ptr(r.rec),
+        _ptr(r.n_acc), max(r.cap, 1), _ptr(r.ckpt), r.ckpt_every, _ptr(ts), ld, K, _ptr(ysbar),
+        _ptr(ybar), _ptr(gy0), _ptr(gp), _stream()), "gs_adjoint_saveat")
+    return gy0, gp

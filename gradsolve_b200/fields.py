@@ -45,7 +45,7 @@ class FieldSpec:
 _STATIC = {
     "lorenz": FieldSpec("lorenz", FIELD_LORENZ, 3, 1, False),
     "lorenz3": FieldSpec("lorenz3", FIELD_LORENZ3, 3, 3, False),
-    "vdp": FieldSpec("vdp", FIELD_VDP, 2, 1, False),
+    "vdp": FieldSpec("vdp", FIELD_VDP, 2, 1, True),
     "lv": FieldSpec("lv", FIELD_LOTKA_VOLTERRA, 2, 4, False),
     "robertson": FieldSpec("robertson", FIELD_ROBERTSON, 3, 3, True),
 }

@@ -86,3 +86,47 @@ class _ReplayFn(torch.autograd.Function):
 
 def replay_apply(state: ReplayState, y0: torch.Tensor, p: torch.Tensor) -> torch.Tensor:
     return _ReplayFn.apply(y0, p, state)
+
+
+class _SaveatFn(torch.autograd.Function):
+    """Dense-output closure: (y0, p) -> ys (n, K, D) on the frozen mesh
+    (gradsolve/warp/warp_replay.py:58-84); backward = the saveat adjoint kernel."""
+
+    @staticmethod
+    def forward(ctx, y0, p, state, ts):
+        y0 = y0.contiguous()
+        p = p.contiguous()
+        pk = state.kernel_p(p)
+        _yf, ys = engine.replay_saveat(state.record, y0, pk, ts, write_ckpt=True,
+                                       precision=state.precision)
+        state.ckpt_point = (y0.detach().clone(), pk.detach().clone())
+        state.version += 1
+        ctx.state, ctx.ts, ctx.version = state, ts, state.version
+        ctx.save_for_backward(y0, p)
+        return ys
+
+    @staticmethod
+    def backward(ctx, ysbar):
+        state: ReplayState = ctx.state
+        y0, p = ctx.saved_tensors
+        pk = state.kernel_p(p)
+        if state.version != ctx.version:
+            engine.replay_saveat(state.record, y0, pk, ctx.ts, write_ckpt=True,
+                                 precision=state.precision)
+            state.ckpt_point = (y0.detach().clone(), pk.detach().clone())
+            state.version += 1
+        need_y0, need_p = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        gy0, gpk = engine.adjoint_saveat(state.record, pk, ctx.ts, ysbar, None,
+                                         want_y0=need_y0, want_p=need_p,
+                                         precision=state.precision)
+        gp = None
+        if need_p:
+            gp = gpk if p.shape[1] == state.nparam else torch.zeros_like(p)
+            if p.shape[1] != state.nparam:
+                gp[:, : state.nparam] = gpk
+        return gy0, gp, None, None
+
+
+def saveat_apply(state: ReplayState, y0: torch.Tensor, p: torch.Tensor,
+                 ts: torch.Tensor) -> torch.Tensor:
+    return _SaveatFn.apply(y0, p, state, ts)

@@ -157,6 +157,37 @@ int gs_ros23_adjoint(int field, int precision, long long n, const double* p, con
                      const int* n_acc, int cap, const double* ckpt, int ckpt_every,
                      const double* ybar, double* gy0, double* gp, void* stream);
 
+#define GS_METHOD_TSIT5 0
+#define GS_METHOD_ROS23 1
+
+/*
+ * Dense output on the frozen-mesh replay: the states at requested times ts (sorted, within
+ * [t0, t1_j]; row j at ts + j*ts_ld, ts_ld = 0 shares one row) by bracket-and-re-step:
+ * one step of the method, of size ts_k - t, from the start of the step bracketing ts_k;
+ * times <= t0 give y0 and times >= the final accumulated time give y_final bitwise.
+ * Replaces gradsolve/warp/warp_replay.py:58-94 (replay_solve_saveat_jax and its Rosenbrock
+ * twin) over gradsolve/solvers/dense.py:106-163,318-335 (scan_saveat_one / vmap_saveat);
+ * per-trajectory rows of times are an extension (the reference shares one grid).
+ * ys: (n, K, D).  Writes checkpoints for gs_adjoint_saveat when ckpt != NULL.
+ * method: GS_METHOD_TSIT5 (float64 or mixed) or GS_METHOD_ROS23 (float64).
+ */
+int gs_replay_saveat(int method, int field, int precision, long long n, const double* y0,
+                     const double* p, double t0, const double* rec, const int* n_acc, int cap,
+                     int ckpt_every, double* ckpt, const double* ts, long long ts_ld, int K,
+                     double* ys, double* y_final, void* stream);
+
+/*
+ * Adjoint of gs_replay_saveat for a loss of the saved states (and optionally y_final):
+ * ysbar (n, K, D) = dL/dys, ybar (n, D) = dL/dy_final or NULL -> gy0, gp (either may be
+ * NULL).  The gradient jax.grad takes through replay_solve_saveat_jax
+ * (gradsolve/warp/warp_replay.py:58-84, gradsolve/api.py:748-752).
+ */
+int gs_adjoint_saveat(int method, int field, int precision, long long n, const double* p,
+                      const double* rec, const int* n_acc, int cap, const double* ckpt,
+                      int ckpt_every, const double* ts, long long ts_ld, int K,
+                      const double* ysbar, const double* ybar, double* gy0, double* gp,
+                      void* stream);
+
 /*
  * Record conversion between the reference's padded (n, S) layout (row j = trajectory j's
  * accepted dts, zero padded; gradsolve/warp/warp_replay.py:181-182) and the chunked record.

@@ -276,6 +276,12 @@ static void jac_contract_grad(const field_t* f, const double* y, const double* p
       gp[1] += -2.0 * b * G[4] + 2.0 * b * G[7];
       gp[2] += c * G[1] + b * G[2] - c * G[4] - b * G[5];
     } break;
+    case F_VDP: {
+      const double x = y[0], v = y[1], mu = p[0];
+      gy[0] += -2.0 * mu * (G[2] * v + G[3] * x);
+      gy[1] += -2.0 * mu * x * G[2];
+      gp[0] += G[2] * (-2.0 * x * v - 1.0) + G[3] * (1.0 - x * x);
+    } break;
     default: break; /* constant Jacobian (linear) */
   }
 }

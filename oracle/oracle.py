@@ -303,3 +303,67 @@ def fd_grad(loss, x0, h_scale=1e-6):
         xm[i] -= h
         gf[i] = (loss(xp.reshape(x0.shape)) - loss(xm.reshape(x0.shape))) / (2.0 * h)
     return g
+
+
+# ------------------------------------------------------------------------------------
+# saveat: restatement of gradsolve/solvers/dense.py:106-163 (bracket-and-re-step)
+# ------------------------------------------------------------------------------------
+
+def _saveat_rows(y0, dts, ts, t0):
+    """For each (trajectory, requested time): the dt row whose replay gives that saved state,
+    following scan_saveat_one's rules.  Returns rows (n*K, S+1) and their kinds."""
+    n, S = dts.shape
+    ts = np.asarray(ts, np.float64)
+    if ts.ndim == 1:
+        ts = np.broadcast_to(ts, (n, ts.shape[0]))
+    K = ts.shape[1]
+    rows = np.zeros((n * K, S + 1))
+    for j in range(n):
+        t = float(t0)
+        starts = []
+        for s in range(S):
+            starts.append(t)
+            t = t + dts[j, s]
+        t_fin = t
+        for k in range(K):
+            tk = float(ts[j, k])
+            r = rows[j * K + k]
+            if tk >= t_fin:            # at or past the final accumulated time: y_final
+                r[:S] = dts[j]
+                continue
+            hit = [s for s in range(S) if dts[j, s] > 0 and tk > starts[s]
+                   and tk <= starts[s] + dts[j, s]]
+            if not hit:               # never bracketed: y0
+                continue
+            s = hit[-1]
+            r[:s] = dts[j, :s]
+            r[s] = tk - starts[s]
+    return rows, K
+
+
+def replay_saveat(method, field, y0, params, dts, ts, t0=0.0, nthreads=4):
+    """(y_final (n, D), ys (n, K, D)) of the frozen-mesh replay with dense output."""
+    y0, params, n, D, P = _prep(field, y0, params)
+    dts = np.ascontiguousarray(np.asarray(dts, np.float64).reshape(n, -1))
+    rows, K = _saveat_rows(y0, dts, ts, t0)
+    ys = replay(method, field, np.repeat(y0, K, axis=0), np.repeat(params, K, axis=0), rows,
+                t0, nthreads)
+    return replay(method, field, y0, params, dts, t0, nthreads), ys.reshape(n, K, D)
+
+
+def replay_saveat_vjp(method, field, y0, params, dts, ts, ysbar, ybar=None, t0=0.0,
+                      nthreads=4):
+    """Gradient of sum(ysbar * ys) + sum(ybar * y_final) w.r.t. (y0, params)."""
+    y0, params, n, D, P = _prep(field, y0, params)
+    dts = np.ascontiguousarray(np.asarray(dts, np.float64).reshape(n, -1))
+    rows, K = _saveat_rows(y0, dts, ts, t0)
+    ysbar = np.asarray(ysbar, np.float64).reshape(n * K, D)
+    gy, gp = replay_vjp(method, field, np.repeat(y0, K, axis=0), np.repeat(params, K, axis=0),
+                        rows, ysbar, t0, nthreads)
+    gy0 = gy.reshape(n, K, D).sum(axis=1)
+    gpp = gp.reshape(n, K, P).sum(axis=1)
+    if ybar is not None:
+        a, b = replay_vjp(method, field, y0, params, dts, ybar, t0, nthreads)
+        gy0 = gy0 + a
+        gpp = gpp + b
+    return gy0, gpp

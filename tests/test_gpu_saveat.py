@@ -1,0 +1,163 @@
+"""Dense output (saveat) on the replay and its adjoint, against the oracle's restatement of
+gradsolve/solvers/dense.py:106-163 (bracket-and-re-step), including the reference's own
+saveat contracts (tests/test_saveat.py:271-312: ys[:, -1] == y_final bitwise) and the
+per-trajectory end times / time rows of the uneven-batch workload (an extension)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def rowrel(a, b):
+    return float(np.max(np.abs(a - b).max(axis=-1) / np.maximum(np.abs(b).max(axis=-1), 1e-300)))
+
+
+def _ref_record(cuda, method, field, g):
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    spec = field_spec(field)
+    r = engine.record_from_padded(method, spec, torch.tensor(g["dts"], device=cuda), 0.0,
+                                  checkpoint="sqrt")
+    y0 = torch.tensor(g["y0"], device=cuda)
+    p = torch.tensor(g["params"][:, : spec.nparam], device=cuda).contiguous()
+    return spec, r, y0, p
+
+
+CASES = [("tsit5", "vdp_batch", "vdp", [0.0, 0.0, 0.05, 0.3, 0.3, 0.7654321, 0.999, 1.0]),
+         ("tsit5", "lorenz_small", "lorenz", [0.0, 0.1, 0.5, 0.95, 1.0]),
+         ("tsit5", "lv_mixed", "lv", list(np.linspace(0.0, 20.0, 64))),
+         ("rosenbrock23", "robertson_toy", "robertson", [0.0, 0.01, 0.2, 0.49, 0.5])]
+
+
+@pytest.mark.parametrize("method,case,field,ts", CASES)
+def test_saveat_values_and_gradients_vs_oracle(gslib, oracle, cuda, method, case, field, ts):
+    from gradsolve_b200 import engine
+    g = load_golden(case)
+    spec, r, y0, p = _ref_record(cuda, method, field, g)
+    ts_t = torch.tensor(ts, dtype=torch.float64, device=cuda)
+    yf, ys = engine.replay_saveat(r, y0, p, ts_t)
+    ryf, rys = oracle.replay_saveat(method, field, g["y0"], g["params"], g["dts"], np.array(ts))
+    assert rowrel(ys.cpu().numpy(), rys) <= 1e-10
+    assert rowrel(yf.cpu().numpy(), ryf) <= 1e-10
+    # the reference's contracts: last saved state IS y_final, times at t0 ARE y0 (bitwise)
+    assert torch.equal(ys[:, -1], yf)
+    assert torch.equal(ys[:, 0], y0)
+    rng = np.random.default_rng(7)
+    ysbar = rng.normal(size=tuple(ys.shape))
+    ybar = rng.normal(size=tuple(yf.shape))
+    gy0, gp = engine.adjoint_saveat(r, p, ts_t, torch.tensor(ysbar, device=cuda),
+                                    torch.tensor(ybar, device=cuda))
+    oy, op = oracle.replay_saveat_vjp(method, field, g["y0"], g["params"], g["dts"],
+                                      np.array(ts), ysbar, ybar)
+    assert rowrel(gy0.cpu().numpy(), oy) <= 1e-9
+    assert rowrel(gp.cpu().numpy(), op[:, : spec.nparam]) <= 1e-9
+
+
+def test_per_trajectory_end_times_and_rows(gslib, oracle, cuda):
+    """Uneven batch: VdP, mu log-uniform, per-trajectory t1 and 64 saved times per row."""
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    rng = np.random.default_rng(5)
+    n = 48
+    mu = 10 ** rng.uniform(-1, np.log10(9.0), (n, 1))
+    t1v = 10 ** rng.uniform(-1, np.log10(20.0), n)
+    y0 = rng.uniform(-2, 2, (n, 2))
+    ts = np.stack([np.linspace(0.0, t, 64) for t in t1v])
+    spec = field_spec("vdp")
+    r = engine.forward_record("tsit5", spec, torch.tensor(y0, device=cuda),
+                              torch.tensor(mu, device=cuda), t0=0.0, t1=float(t1v.max()),
+                              t1v=torch.tensor(t1v, device=cuda), rtol=1e-6, atol=1e-8,
+                              checkpoint="sqrt")
+    assert (r.status.cpu().numpy() == 0).all()
+    dts = r.padded_dts().cpu().numpy()
+    y0_t = torch.tensor(y0, device=cuda)
+    mu_t = torch.tensor(mu, device=cuda)
+    ts_t = torch.tensor(ts, device=cuda)
+    yf, ys = engine.replay_saveat(r, y0_t, mu_t, ts_t)
+    ryf, rys = oracle.replay_saveat("tsit5", "vdp", y0, mu, dts, ts)
+    assert rowrel(ys.cpu().numpy(), rys) <= 1e-10
+    assert torch.equal(ys[:, -1], yf)
+    ysbar = rng.normal(size=tuple(ys.shape))
+    gy0, gp = engine.adjoint_saveat(r, mu_t, ts_t, torch.tensor(ysbar, device=cuda))
+    oy, op = oracle.replay_saveat_vjp("tsit5", "vdp", y0, mu, dts, ts, ysbar)
+    assert rowrel(gy0.cpu().numpy(), oy) <= 1e-9
+    assert rowrel(gp.cpu().numpy(), op) <= 1e-9
+
+
+def test_stiff_vdp_saveat(gslib, oracle, cuda):
+    """VdP at mu >= 10 through Rosenbrock23 (the stiff half of the uneven workload)."""
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    rng = np.random.default_rng(6)
+    n = 16
+    mu = 10 ** rng.uniform(1, 2, (n, 1))
+    y0 = rng.uniform(-2, 2, (n, 2))
+    ts = np.linspace(0.0, 3.0, 16)
+    spec = field_spec("vdp")
+    r = engine.forward_record("rosenbrock23", spec, torch.tensor(y0, device=cuda),
+                              torch.tensor(mu, device=cuda), t0=0.0, t1=3.0, rtol=1e-6,
+                              atol=1e-8, max_steps=50000, checkpoint="sqrt")
+    assert (r.status.cpu().numpy() == 0).all()
+    o = oracle.record("rosenbrock23", "vdp", y0, mu, 0.0, 3.0, 1e-6, 1e-8, max_steps=50000)
+    np.testing.assert_array_equal(r.n_acc.cpu().numpy(), o["n_acc"])
+    dts = r.padded_dts().cpu().numpy()
+    mu_t = torch.tensor(mu, device=cuda)
+    ts_t = torch.tensor(ts, device=cuda)
+    yf, ys = engine.replay_saveat(r, torch.tensor(y0, device=cuda), mu_t, ts_t)
+    ryf, rys = oracle.replay_saveat("rosenbrock23", "vdp", y0, mu, dts, ts)
+    assert rowrel(ys.cpu().numpy(), rys) <= 1e-9
+    ysbar = rng.normal(size=tuple(ys.shape))
+    gy0, gp = engine.adjoint_saveat(r, mu_t, ts_t, torch.tensor(ysbar, device=cuda))
+    oy, op = oracle.replay_saveat_vjp("rosenbrock23", "vdp", y0, mu, dts, ts, ysbar)
+    assert rowrel(gy0.cpu().numpy(), oy) <= 1e-8
+    assert rowrel(gp.cpu().numpy(), op) <= 1e-8
+
+
+def test_api_solve_and_grad_closure_saveat(gslib, oracle, cuda):
+    import gradsolve_b200 as gsb
+
+    class VdP:
+        name = "vdp"
+        dim = 2
+        t0 = 0.0
+        t1 = 1.0
+        is_stiff = False
+
+    g = load_golden("vdp_batch")
+    ts = np.array([0.0, 0.25, 0.5, 1.0])
+    res = gsb.solve(VdP(), g["y0"], g["params"], saveat=ts)
+    assert res.y_saved.shape == (3, 4, 2) and np.array_equal(res.ts_saved, ts)
+    np.testing.assert_array_equal(res.y_saved[:, -1], res.y_final)
+    clo = gsb.grad_closure(VdP(), g["y0"], g["params"], saveat=ts)
+    p = torch.tensor(g["params"], device="cuda", requires_grad=True)
+    ys = clo(p)
+    assert ys.shape == (3, 4, 2)
+    (ys ** 2).sum().backward()
+    dts = clo.state.record.padded_dts().cpu().numpy()
+    _, rys = oracle.replay_saveat("tsit5", "vdp", g["y0"], g["params"], dts, ts)
+    _, op = oracle.replay_saveat_vjp("tsit5", "vdp", g["y0"], g["params"], dts, ts, 2 * rys)
+    assert rowrel(p.grad.cpu().numpy(), op) <= 1e-9
+    with pytest.raises(ValueError, match="sorted"):
+        gsb.grad_closure(VdP(), g["y0"], g["params"], saveat=[0.5, 0.1])
+    with pytest.raises(ValueError, match="within the problem domain"):
+        gsb.solve(VdP(), g["y0"], g["params"], saveat=[0.0, 1.5])
+
+
+def test_mixed_saveat_close_to_f64(gslib, cuda):
+    from gradsolve_b200 import engine
+    g = load_golden("lv_mixed")
+    spec, r, y0, p = _ref_record(cuda, "tsit5", "lv", g)
+    ts_t = torch.linspace(0.0, 20.0, 32, dtype=torch.float64, device=cuda)
+    _, ys64 = engine.replay_saveat(r, y0, p, ts_t)
+    _, ysm = engine.replay_saveat(r, y0, p, ts_t, precision="mixed")
+    assert rowrel(ysm.cpu().numpy(), ys64.cpu().numpy()) <= 1e-5
+    ysbar = torch.ones_like(ysm)
+    g64 = engine.adjoint_saveat(r, p, ts_t, ysbar)[1]
+    _, ysm = engine.replay_saveat(r, y0, p, ts_t, precision="mixed")
+    gm = engine.adjoint_saveat(r, p, ts_t, ysbar, precision="mixed")[1]
+    assert rowrel(gm.cpu().numpy(), g64.cpu().numpy()) <= 1e-3

@@ -1,0 +1,88 @@
+"""Host-side API logic that needs no GPU: saveat validation, field routing, parameter
+mapping, checkpoint policy."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from gradsolve_b200 import api
+from gradsolve_b200.fields import field_for, field_spec, kernel_params
+
+
+class P:
+    def __init__(self, name):
+        self.name = name
+
+
+def test_validate_saveat_rules():
+    ts = api.validate_saveat([0.0, 0.5, 0.5, 1.0], 0.0, 1.0)
+    assert ts.dtype == np.float64 and ts.shape == (4,)
+    with pytest.raises(ValueError, match="sorted"):
+        api.validate_saveat([0.5, 0.1], 0.0, 1.0)
+    with pytest.raises(ValueError, match="within the problem domain"):
+        api.validate_saveat([0.0, 1.5], 0.0, 1.0)
+    with pytest.raises(ValueError, match="non-finite"):
+        api.validate_saveat([0.0, np.nan], 0.0, 1.0)
+    with pytest.raises(ValueError, match="at least one"):
+        api.validate_saveat([], 0.0, 1.0)
+    # per-trajectory rows against per-trajectory end times
+    rows = np.array([[0.0, 0.5], [0.0, 2.0]])
+    api.validate_saveat(rows, 0.0, 2.0, t1v=np.array([1.0, 2.0]), n=2)
+    with pytest.raises(ValueError, match="within the problem domain"):
+        api.validate_saveat(rows, 0.0, 2.0, t1v=np.array([0.4, 2.0]), n=2)
+    with pytest.raises(ValueError, match="rows"):
+        api.validate_saveat(rows, 0.0, 2.0, n=3)
+
+
+def test_field_routing_mirrors_reference_names():
+    assert field_for(P("diffeqgpu_lorenz")).key == "lorenz"
+    assert field_for(P("lorenz")).key == "lorenz3"
+    assert field_for(P("vdp")).key == "vdp"
+    assert field_for(P("lotka_volterra")).key == "lv"
+    assert field_for(P("robertson")).stiff_ok
+    assert field_for(P("linear_ladder_3")).dim == 3
+    assert field_for(P("linear_ladder_5")) is None  # not built for D = 5
+    assert field_for(P("hires")) is None
+    assert field_for(P("my_rhs")) is None
+
+
+def test_kernel_params_leading_columns_and_errors():
+    spec = field_spec("lv")
+    p = np.arange(10.0).reshape(2, 5)
+    np.testing.assert_array_equal(kernel_params(spec, p), p[:, :4])
+    with pytest.raises(ValueError, match="reads 4 parameter"):
+        kernel_params(spec, p[:, :2])
+    np.testing.assert_array_equal(kernel_params(field_spec("linear_2"), np.zeros((3, 0))),
+                                  np.zeros((3, 1)))
+
+
+def test_wrt_normalisation():
+    assert api._normalize_wrt("params") == ("params",)
+    assert api._normalize_wrt(["params", "y0"]) == ("y0", "params")
+    with pytest.raises(ValueError, match="invalid wrt"):
+        api._normalize_wrt("p")
+
+
+def test_engine_resolution_and_aliases():
+    reasons = []
+
+    class S:
+        name = "robertson"
+        is_stiff = True
+
+    assert api._resolve(S(), "auto", reasons) == "b200_rosenbrock23"
+    assert api._resolve(S(), "warp_rosenbrock", reasons) == "b200_rosenbrock23"
+    assert reasons == ["served-by-b200_rosenbrock23"]
+    with pytest.raises(ValueError, match="unknown engine"):
+        api._resolve(S(), "diffrax", [])
+
+
+def test_checkpoint_policy(gslib):
+    from gradsolve_b200.engine import choose_ckpt_every
+    assert choose_ckpt_every("all", 3, 10, 700, None) == 1
+    assert choose_ckpt_every("sqrt", 3, 10, 700, None) == 27
+    assert choose_ckpt_every(5, 3, 10, 700, None) == 5
+    assert choose_ckpt_every("auto", 3, 10, 700, budget_bytes=10**9) == 1
+    assert choose_ckpt_every("auto", 3, 1 << 20, 700, budget_bytes=10**9) == 27
+    with pytest.raises(ValueError):
+        choose_ckpt_every(65, 3, 10, 700, None)

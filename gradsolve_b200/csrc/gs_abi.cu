@@ -87,6 +87,34 @@ int field_dims(int field, int* D, int* P) {
                   "field " + std::to_string(field) + " has no analytic Jacobian for Rosenbrock23"); \
   }
 
+// Launch shape of the adjoint kernels: each thread keeps its segment of K states (W doubles
+// each) in shared memory, so the block shrinks (by powers of two, at least one warp) until the
+// block's buffer fits the per-block budget.
+struct SegCfg {
+  unsigned block;
+  size_t smem;
+};
+
+SegCfg seg_cfg(int K, int W) {
+  const size_t per_thread = (size_t)K * (size_t)W * sizeof(double);
+  const size_t budget = 200u * 1024u;
+  unsigned block = kBlock;
+  while (block > 32 && per_thread * block > budget) block /= 2;
+  return {block, per_thread * block};
+}
+
+template <class Kern>
+int allow_smem(Kern kernel, size_t smem) {
+  if (smem <= 48u * 1024u) return GS_OK;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess)
+    return fail(GS_ERR_CUDA, std::string("CUDA: cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  return GS_OK;
+}
+
+unsigned grid_for_block(long long n, unsigned block) { return (unsigned)((n + block - 1) / block); }
+
 // mixed = float32 stages (GS_PREC_MIXED, gs_mixed.cuh), else float64 throughout.
 template <class F>
 int launch_tsit5_record(const gs::RecordArgs& a, cudaStream_t s, bool mixed) {
@@ -108,11 +136,15 @@ int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed) {
 }
 template <class F>
 int launch_tsit5_adjoint(const gs::AdjointArgs& a, cudaStream_t s, bool mixed) {
+  const SegCfg c = seg_cfg(a.ck_every, F::D);
+  int rc;
   if (mixed) {
-    gs::tsit5_mixed_adjoint_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    if ((rc = allow_smem(gs::tsit5_mixed_adjoint_kernel<F>, c.smem))) return rc;
+    gs::tsit5_mixed_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
     return cuda_check("tsit5_mixed_adjoint_kernel");
   }
-  gs::tsit5_adjoint_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+  if ((rc = allow_smem(gs::tsit5_adjoint_kernel<F>, c.smem))) return rc;
+  gs::tsit5_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
   return cuda_check("tsit5_adjoint_kernel");
 }
 template <class F>
@@ -127,7 +159,10 @@ int launch_ros23_replay(const gs::ReplayArgs& a, cudaStream_t s) {
 }
 template <class F>
 int launch_ros23_adjoint(const gs::AdjointArgs& a, cudaStream_t s) {
-  gs::ros23_adjoint_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+  const SegCfg c = seg_cfg(a.ck_every, F::D);
+  int rc;
+  if ((rc = allow_smem(gs::ros23_adjoint_kernel<F>, c.smem))) return rc;
+  gs::ros23_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
   return cuda_check("ros23_adjoint_kernel");
 }
 
@@ -460,7 +495,9 @@ int launch_tsit5_vjp_static(long long n, long long S, long long ld, const double
   gs::tsit5_replay_kernel<F><<<grid_for(n), kBlock, 0, s>>>(ra);
   if ((rc = cuda_check("tsit5_replay_kernel"))) return rc;
   gs::AdjointArgs aa{n, p, rec, n_steps, ckpt, K, ybar, gy0, gp};
-  gs::tsit5_adjoint_kernel<F><<<grid_for(n), kBlock, 0, s>>>(aa);
+  const SegCfg c = seg_cfg(K, F::D);
+  if ((rc = allow_smem(gs::tsit5_adjoint_kernel<F>, c.smem))) return rc;
+  gs::tsit5_adjoint_kernel<F><<<grid_for_block(n, c.block), c.block, c.smem, s>>>(aa);
   return cuda_check("tsit5_adjoint_kernel");
 }
 
@@ -510,7 +547,10 @@ namespace {
 template <class F, class M>
 int launch_saveat(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint) {
   if (adjoint) {
-    gs::adjoint_saveat_kernel<F, M><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    const SegCfg c = seg_cfg(a.ck_every, F::D + 1);
+    int rc;
+    if ((rc = allow_smem(gs::adjoint_saveat_kernel<F, M>, c.smem))) return rc;
+    gs::adjoint_saveat_kernel<F, M><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
     return cuda_check("adjoint_saveat_kernel");
   }
   gs::replay_saveat_kernel<F, M><<<grid_for(a.n), kBlock, 0, s>>>(a);

@@ -29,3 +29,31 @@ int gs_probe_fp32(float* out, int blocks, int iters, void* stream) {
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 }
+
+// ---- controller check: the solver's pow-free step factor vs CUDA's pow --------------------
+#include "gs_tsit5.cuh"
+
+__global__ void step_factor_probe(const double* m, long long n, int order, double* fast,
+                                  double* ref, int* accept_fast, int* accept_ref) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x = m[i];
+  fast[i] = order == 5 ? gs::step_from_mean<10>(x, 1.0) : gs::step_from_mean<6>(x, 1.0);
+  const double err = sqrt(x);
+  const double e = err > 1e-10 ? err : 1e-10;
+  double fac = 0.9 * pow(e, order == 5 ? -0.2 : -1.0 / 3.0);
+  fac = fac > 0.2 ? fac : 0.2;
+  fac = 5.0 < fac ? 5.0 : fac;
+  ref[i] = fac;
+  accept_fast[i] = x <= gs::kAcceptMax;
+  accept_ref[i] = err <= 1.0;
+}
+
+extern "C" int gs_probe_step_factor(const double* m, long long n, int order, double* fast,
+                                    double* ref, int* accept_fast, int* accept_ref,
+                                    void* stream) {
+  if (n <= 0) return 0;
+  step_factor_probe<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+      m, n, order, fast, ref, accept_fast, accept_ref);
+  return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}

@@ -263,12 +263,12 @@ __global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
     lu_solve<D>(c.W, r3, k3);
 #pragma unroll
     for (int i = 0; i < D; ++i) ev[i] = (h / 6.0) * (c.k1[i] - 2.0 * c.k2[i] + k3[i]);
-    const double err = wrms_norm<D>(ev, y, ynew, a.rtol, a.atol);
-    if (!(err == err)) {
+    const double m = wrms_mean<D>(ev, y, ynew, a.rtol, a.atol);
+    if (!(m == m)) {
       st = 1;
       break;
     }
-    if (err <= 1.0) {
+    if (m <= kAcceptMax) {
       if ((rec_on || ck_on) && acc >= a.cap) {
         st = 3;
         break;
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
     } else {
       ++rej;
     }
-    dt = step_controller(err, h, Ros23::ORDER_EXP);
+    dt = step_from_mean<6>(m, h);
   }
   if (st == 0 && !(t >= t1)) st = 1;
   if (rec_on) {
@@ -353,19 +353,19 @@ __global__ void __launch_bounds__(128) ros23_adjoint_kernel(const AdjointArgs a)
   const int na = a.n_acc[j];
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
-  double seg[KMAX][D];
+  SegBuf<D> seg;
   for (int sg = nseg - 1; sg >= 0; --sg) {
     const int start = sg * K;
     double y[D];
     load_ckpt<D>(a.ckpt, a.n, j, sg, y);
 #pragma unroll
-    for (int i = 0; i < D; ++i) seg[0][i] = y[i];
+    for (int i = 0; i < D; ++i) seg.at(0, i) = y[i];
     for (int q = 1; q < K; ++q) {
       const int s = start + q - 1;
       const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
       if (dt != 0.0) ros23_replay_step<F>(y, p, dt);
 #pragma unroll
-      for (int i = 0; i < D; ++i) seg[q][i] = y[i];
+      for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
     }
     for (int q = K - 1; q >= 0; --q) {
       const int s = start + q;
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(128) ros23_adjoint_kernel(const AdjointArgs a)
       if (dt != 0.0) {
         double ys[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) ys[i] = seg[q][i];
+        for (int i = 0; i < D; ++i) ys[i] = seg.at(q, i);
         ros23_step_vjp<F>(ys, p, dt, lam, gp);
       }
     }

@@ -160,8 +160,7 @@ __global__ void __launch_bounds__(128) adjoint_saveat_kernel(const SaveatArgs a)
   const int na = a.n_acc[j];
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
-  double seg[KMAX][D];
-  double segt[KMAX];
+  SegBuf<D + 1> seg;  // states and step start times (index D)
   int kk = a.K;           // times [0, kk) not yet assigned to a step
   bool fin_done = false;  // cotangents of times >= t_fin joined lam
   if (nseg == 0) {
@@ -177,8 +176,8 @@ __global__ void __launch_bounds__(128) adjoint_saveat_kernel(const SaveatArgs a)
     double y[D], c[D];
     double t = load_ckpt<D>(a.ckpt, a.n, j, sg, y);
 #pragma unroll
-    for (int i = 0; i < D; ++i) { seg[0][i] = y[i]; c[i] = 0.0; }
-    segt[0] = t;
+    for (int i = 0; i < D; ++i) { seg.at(0, i) = y[i]; c[i] = 0.0; }
+    seg.at(0, D) = t;
     for (int q = 1; q <= K; ++q) {  // states y_{start+q} and times (q = K: segment end)
       const int s = start + q - 1;
       const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
@@ -188,8 +187,8 @@ __global__ void __launch_bounds__(128) adjoint_saveat_kernel(const SaveatArgs a)
       }
       if (q < K) {
 #pragma unroll
-        for (int i = 0; i < D; ++i) seg[q][i] = y[i];
-        segt[q] = t;
+        for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
+        seg.at(q, D) = t;
       }
     }
     if (!fin_done) {  // first processed segment: t is t_fin
@@ -206,8 +205,8 @@ __global__ void __launch_bounds__(128) adjoint_saveat_kernel(const SaveatArgs a)
       if (dt > 0.0) {
         double ys[D], add[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) { ys[i] = seg[q][i]; add[i] = 0.0; }
-        const double ts0 = segt[q];
+        for (int i = 0; i < D; ++i) { ys[i] = seg.at(q, i); add[i] = 0.0; }
+        const double ts0 = seg.at(q, D);
         while (kk > 0 && ts[kk - 1] > ts0) {  // re-steps bracketed by this step
           --kk;
           double w[D];

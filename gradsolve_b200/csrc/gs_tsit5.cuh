@@ -36,6 +36,20 @@ namespace gs {
 
 constexpr int KMAX = 64;  // largest checkpoint interval the adjoint supports
 
+// Per-thread segment buffer of the adjoint kernels, in dynamic shared memory (launched with
+// K * W * 8 * blockDim bytes): element (q, i) of thread t lives at
+// smem[(q * W + i) * blockDim + t], so a warp's accesses to one element are consecutive
+// 8-byte words (no bank conflicts).  W = D (states) or D + 1 (states and step start time).
+extern __shared__ double gs_seg_smem[];
+
+template <int W>
+struct SegBuf {
+  double* base;
+  int stride;
+  __device__ __forceinline__ SegBuf() : base(gs_seg_smem + threadIdx.x), stride(blockDim.x) {}
+  __device__ __forceinline__ double& at(int q, int i) { return base[(q * W + i) * stride]; }
+};
+
 GS_HD int ckpt_width(int D) { return (D + 2) & ~1; }
 
 GS_HD size_t rec_index(long long j, long long s, long long n) {
@@ -67,8 +81,63 @@ __device__ __forceinline__ double wrms_sum(const double* q) {
   }
 }
 
+// ---- the controller from the mean of squares, without pow and sqrt ----------------------
+// The reference computes err = sqrt(m) (m = mean((e/sc)^2)), accepts iff err <= 1 and sets
+// dt = h * clip(0.9 * max(err, 1e-10)^(-1/q), 0.2, 5) with q = 5 (Tsit5) or 3 (Rosenbrock23).
+//  * err <= 1  <=>  m <= 1 + 2^-52: sqrt is correctly rounded, and sqrt(1 + 2^-52) rounds to
+//    1 while sqrt(1 + 2^-51) does not, so the accept test is unchanged bit for bit.
+//  * 0.9 * err^(-1/q) = 0.9 * m^(-1/(2q)); the clip at 5 (resp. 0.2) is reached for
+//    m <= (0.9/5)^(2q) (resp. m >= (0.9/0.2)^(2q)), which also covers the 1e-10 floor.
+//  * in between, y = m^(-1/k), k = 2q, is computed by Newton-Raphson on y^-k - m = 0,
+//    y <- y (k + 1 - m y^k) / k, from a single-precision first guess (exp2(-log2(m)/k),
+//    ~2^-21 relative); two iterations reach double precision (quadratic convergence).
+// The result agrees with 0.9 * pow(sqrt(m), -1/q) to a few ulp (checked against CUDA's pow
+// by tests/test_gpu_controller.py); the reference's own Warp and numpy paths already differ
+// at that level.
+constexpr double kAcceptMax = 1.0000000000000002;  // 1 + 2^-52
+
+template <int K>
+__device__ __forceinline__ double pow_k(double y) {
+  static_assert(K == 6 || K == 10, "inverse root order");
+  const double y2 = y * y;
+  const double y4 = y2 * y2;
+  if constexpr (K == 6) {
+    return y4 * y2;
+  } else {
+    return (y4 * y4) * y2;
+  }
+}
+
+template <int K>
+__device__ __forceinline__ double inv_root(double m) {
+  double y = (double)exp2f(__log2f((float)m) * (-1.0f / (float)K));
+  constexpr double kp1 = K + 1.0, rk = 1.0 / K;
+#pragma unroll
+  for (int it = 0; it < 2; ++it) y = (y * fma(-m, pow_k<K>(y), kp1)) * rk;
+  return y;
+}
+
+// K = 10 for Tsit5 (q = 5), K = 6 for Rosenbrock23 (q = 3).  Returns the new dt.
+template <int K>
+__device__ __forceinline__ double step_from_mean(double m, double h) {
+  constexpr double lo = K == 10 ? 3.570467226623999e-08 : 3.401222399999999e-05;  // 0.18^K
+  constexpr double hi = K == 10 ? 3405062.8916015625 : 8303.765625;                   // 4.5^K
+  double fac;
+  if (m <= lo) {
+    fac = Ctrl::FAC_MAX;
+  } else if (m >= hi) {
+    fac = Ctrl::FAC_MIN;
+  } else {
+    fac = Ctrl::SAFETY * inv_root<K>(m);
+    fac = fac > Ctrl::FAC_MIN ? fac : Ctrl::FAC_MIN;
+    fac = Ctrl::FAC_MAX < fac ? Ctrl::FAC_MAX : fac;
+  }
+  return h * fac;
+}
+
+// mean of squares (e_i / sc_i)^2 in numpy's summation order (the reference's np.mean)
 template <int D>
-__device__ __forceinline__ double wrms_norm(const double* e, const double* y, const double* yn,
+__device__ __forceinline__ double wrms_mean(const double* e, const double* y, const double* yn,
                                             double rtol, double atol) {
   double q[D];
 #pragma unroll
@@ -77,15 +146,7 @@ __device__ __forceinline__ double wrms_norm(const double* e, const double* y, co
     const double c = e[i] / sc;
     q[i] = c * c;
   }
-  return sqrt(wrms_sum<D>(q) / (double)D);
-}
-
-__device__ __forceinline__ double step_controller(double err, double h, double order_exp) {
-  const double e = err > Ctrl::ERR_FLOOR ? err : Ctrl::ERR_FLOOR;
-  double fac = Ctrl::SAFETY * pow(e, order_exp);
-  fac = fac > Ctrl::FAC_MIN ? fac : Ctrl::FAC_MIN;
-  fac = Ctrl::FAC_MAX < fac ? Ctrl::FAC_MAX : fac;
-  return h * fac;
+  return wrms_sum<D>(q) / (double)D;
 }
 
 // --- the shared stage arithmetic ------------------------------------------------------
@@ -372,12 +433,12 @@ __global__ void __launch_bounds__(128) tsit5_record_kernel(const RecordArgs a) {
     for (int i = 0; i < D; ++i)
       e[i] = h * (T::E1 * k1[i] + T::E2 * S.k2[i] + T::E3 * S.k3[i] + T::E4 * S.k4[i] +
                   T::E5 * S.k5[i] + T::E6 * S.k6[i] + T::E7 * k7[i]);
-    const double err = wrms_norm<D>(e, y, y5, a.rtol, a.atol);
-    if (!(err == err)) {  // NaN error: dt would turn NaN and the loop could never finish
+    const double m = wrms_mean<D>(e, y, y5, a.rtol, a.atol);
+    if (!(m == m)) {  // NaN error: dt would turn NaN and the loop could never finish
       st = 1;
       break;
     }
-    if (err <= 1.0) {
+    if (m <= kAcceptMax) {  // err = sqrt(m) <= 1
       if ((rec_on || ck_on) && acc >= a.cap) {
         st = 3;
         break;
@@ -403,7 +464,7 @@ __global__ void __launch_bounds__(128) tsit5_record_kernel(const RecordArgs a) {
     } else {
       ++rej;
     }
-    dt = step_controller(err, h, T::ORDER_EXP);
+    dt = step_from_mean<10>(m, h);
   }
   if (st == 0 && !(t >= t1)) st = 1;
   if (rec_on) {
@@ -467,19 +528,19 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a)
   const int na = a.n_acc[j];
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
-  double seg[KMAX][D];  // interior states of the current segment (per-thread local memory)
+  SegBuf<D> seg;
   for (int sg = nseg - 1; sg >= 0; --sg) {
     const int start = sg * K;
     double y[D];
     load_ckpt<D>(a.ckpt, a.n, j, sg, y);
 #pragma unroll
-    for (int i = 0; i < D; ++i) seg[0][i] = y[i];
+    for (int i = 0; i < D; ++i) seg.at(0, i) = y[i];
     for (int q = 1; q < K; ++q) {
       const int s = start + q - 1;
       const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
       if (dt != 0.0) tsit5_replay_step<F>(y, p, dt);
 #pragma unroll
-      for (int i = 0; i < D; ++i) seg[q][i] = y[i];
+      for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
     }
     for (int q = K - 1; q >= 0; --q) {
       const int s = start + q;
@@ -487,7 +548,7 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a)
       if (dt != 0.0) {
         double ys[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) ys[i] = seg[q][i];
+        for (int i = 0; i < D; ++i) ys[i] = seg.at(q, i);
         tsit5_step_vjp<F>(ys, p, dt, lam, gp);
       }
     }

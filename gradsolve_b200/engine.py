@@ -41,13 +41,15 @@ def ckpt_width(dim: int) -> int:
     return (dim + 2) & ~1
 
 
-def choose_ckpt_every(policy, dim: int, n: int, cap: int, budget_bytes: Optional[int]) -> int:
-    """Checkpoint interval K.
+def choose_ckpt_every(policy, dim: int, n: int, cap: int, budget_bytes: Optional[int],
+                      tuned: Optional[int] = None) -> int:
+    """Checkpoint interval K (the segment length of the reverse pass).
 
     ``policy``: an int K; ``"all"`` (K = 1, every state stored, no recomputation);
-    ``"sqrt"`` (K = ceil(sqrt(cap)), the sqrt(N) segment scheme); ``"auto"``: K = 1 when the
-    full state record fits ``budget_bytes`` (default: a quarter of the free device memory),
-    else the sqrt(N) scheme."""
+    ``"sqrt"`` (K = ceil(sqrt(cap)), the classic sqrt(N) segment scheme); ``"auto"``: the
+    segment length the autotuner measured fastest for this (method, field, precision)
+    (``tuned``; 8 before tuning), raised until the checkpoints fit ``budget_bytes``
+    (default: a quarter of the free device memory)."""
     kmax = _lib.lib().gs_max_ckpt_every()
     if isinstance(policy, int):
         if not 1 <= policy <= kmax:
@@ -63,8 +65,51 @@ def choose_ckpt_every(policy, dim: int, n: int, cap: int, budget_bytes: Optional
     if budget_bytes is None:
         free, _total = torch.cuda.mem_get_info()
         budget_bytes = free // 4
-    full = (cap + 1) * n * ckpt_width(dim) * 8
-    return 1 if full <= budget_bytes else sq
+    K = tuned or 8
+    while K < kmax and (cap // K + 2) * n * ckpt_width(dim) * 8 > budget_bytes:
+        K *= 2
+    return min(K, kmax)
+
+
+# ---- checkpoint-interval autotuner ---------------------------------------------------------
+# The reverse pass keeps each thread's K segment states in shared memory, so K trades
+# recomputation (none at K = 1) against occupancy (the buffer is K*D*8 bytes per thread).
+# The best K depends on the field, the method and the precision; it is measured once per
+# process on a sample of the caller's own trajectories and cached.
+_TUNED: dict = {}
+TUNE_CANDIDATES = (4, 6, 8, 12, 16)
+
+
+def tuned_ckpt_every(method: str, spec: FieldSpec, precision: str) -> Optional[int]:
+    return _TUNED.get((method, spec.key, precision))
+
+
+def autotune_ckpt_every(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tensor, *,
+                        t0: float, t1: float, rtol: float, atol: float,
+                        t1v: Optional[torch.Tensor] = None, max_steps: int = 100000,
+                        precision: str = "float64", sample: int = 1 << 17,
+                        candidates=TUNE_CANDIDATES) -> int:
+    """Time the reverse pass for each candidate K on up to ``sample`` trajectories (about two
+    waves of the GPU) and cache the fastest."""
+    m = min(y0.shape[0], sample)
+    ys, ps = y0[:m].contiguous(), p[:m].contiguous()
+    tv = None if t1v is None else t1v[:m].contiguous()
+    best, best_ms = None, float("inf")
+    for K in candidates:
+        r = forward_record(method, spec, ys, ps, t0=t0, t1=t1, t1v=tv, rtol=rtol, atol=atol,
+                           max_steps=max_steps, checkpoint=K, precision=precision)
+        ybar = torch.ones_like(r.y_final)
+        adjoint(r, ps, ybar, precision=precision)  # warm
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        adjoint(r, ps, ybar, precision=precision)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        if ms < best_ms:
+            best, best_ms = K, ms
+    _TUNED[(method, spec.key, precision)] = best
+    return best
 
 
 @dataclass
@@ -108,18 +153,22 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
                    t1v: Optional[torch.Tensor] = None, max_steps: int = 100000,
                    cap0: int = DEFAULT_CAP0, checkpoint="auto",
                    budget_bytes: Optional[int] = None, precision: str = "float64",
-                   record: bool = True) -> Record:
+                   record: bool = True, workspace: Optional[Record] = None) -> Record:
     """Adaptive solve on the device; with ``record`` the dts and checkpoints are kept.
 
-    ``y0`` (n, D) and ``p`` (n, P) float64 contiguous device tensors."""
+    ``y0`` (n, D) and ``p`` (n, P) float64 contiguous device tensors.  ``workspace``: a Record
+    from an earlier call of the same shape whose buffers are reused (overwritten) instead of
+    allocating new ones -- the steady-state pattern of a training loop."""
     n = y0.shape[0]
     device = y0.device
     L = _lib.lib()
     fn = L.gs_tsit5_fwd_record if method == METHOD_TSIT5 else L.gs_ros23_fwd_record
-    yf = torch.empty_like(y0)
-    n_acc = torch.empty(n, dtype=torch.int32, device=device)
-    n_rej = torch.empty(n, dtype=torch.int32, device=device)
-    status = torch.empty(n, dtype=torch.int32, device=device)
+    ws = workspace if (workspace is not None and workspace.n == n and
+                       workspace.spec.dim == spec.dim) else None
+    yf = ws.y_final if ws is not None else torch.empty_like(y0)
+    n_acc = ws.n_acc if ws is not None else torch.empty(n, dtype=torch.int32, device=device)
+    n_rej = ws.n_rej if ws is not None else torch.empty(n, dtype=torch.int32, device=device)
+    status = ws.status if ws is not None else torch.empty(n, dtype=torch.int32, device=device)
     dt0_arg = -1.0 if dt0 is None else float(dt0)
     if not record:
         _lib.check(fn(spec.code, _PREC[precision], n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
@@ -129,9 +178,18 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
         empty = torch.empty(0, dtype=torch.float64, device=device)
         return Record(method, spec, n, float(t0), 0, 1, empty, empty, yf, n_acc, n_rej, status)
     cap = max(1, min(int(cap0), int(max_steps)))
+    if ws is not None and ws.cap > cap:
+        cap = ws.cap
+    if checkpoint == "auto" and tuned_ckpt_every(method, spec, precision) is None and n >= 4096:
+        autotune_ckpt_every(method, spec, y0, p, t0=t0, t1=t1, t1v=t1v, rtol=rtol, atol=atol,
+                            max_steps=max_steps, precision=precision)
     while True:
-        K = choose_ckpt_every(checkpoint, spec.dim, n, cap, budget_bytes)
-        rec, ckpt = _alloc_record(n, cap, spec.dim, K, device)
+        K = choose_ckpt_every(checkpoint, spec.dim, n, cap, budget_bytes,
+                              tuned_ckpt_every(method, spec, precision))
+        if ws is not None and ws.cap == cap and ws.ckpt_every == K and ws.rec.numel() > 2:
+            rec, ckpt = ws.rec, ws.ckpt
+        else:
+            rec, ckpt = _alloc_record(n, cap, spec.dim, K, device)
         _lib.check(fn(spec.code, _PREC[precision], n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
                       float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), cap, K,
                       _ptr(rec), _ptr(ckpt), _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status),

@@ -82,7 +82,9 @@ def test_checkpoint_policy(gslib):
     assert choose_ckpt_every("all", 3, 10, 700, None) == 1
     assert choose_ckpt_every("sqrt", 3, 10, 700, None) == 27
     assert choose_ckpt_every(5, 3, 10, 700, None) == 5
-    assert choose_ckpt_every("auto", 3, 10, 700, budget_bytes=10**9) == 1
-    assert choose_ckpt_every("auto", 3, 1 << 20, 700, budget_bytes=10**9) == 27
+    # auto: the tuned segment length (8 before tuning), raised until the checkpoints fit
+    assert choose_ckpt_every("auto", 3, 10, 700, budget_bytes=10**9) == 8
+    assert choose_ckpt_every("auto", 3, 10, 700, budget_bytes=10**9, tuned=12) == 12
+    assert choose_ckpt_every("auto", 3, 1 << 20, 700, budget_bytes=10**9) == 32
     with pytest.raises(ValueError):
         choose_ckpt_every(65, 3, 10, 700, None)

@@ -14,6 +14,7 @@
 #include "gs_fields.cuh"
 #include "gs_mixed.cuh"
 #include "gs_ros23.cuh"
+#include "gs_persistent.cuh"
 #include "gs_saveat.cuh"
 #include "gs_tableau.cuh"
 #include "gs_tsit5.cuh"
@@ -115,15 +116,68 @@ int allow_smem(Kern kernel, size_t smem) {
 
 unsigned grid_for_block(long long n, unsigned block) { return (unsigned)((n + block - 1) / block); }
 
+// ---- persistent launches (gs_persistent.cuh) ------------------------------------------------
+// One wave of resident blocks; the work counter lives in the control block that follows the
+// checkpoint slots (gs_ckpt_bytes includes it) and is zeroed on the stream before the launch.
+unsigned long long* ctrl_counter(double* ckpt, long long n, int slots, int D, int which) {
+  if (!ckpt) return nullptr;
+  double* end = ckpt + (size_t)slots * (size_t)n * (size_t)gs::ckpt_width(D);
+  return reinterpret_cast<unsigned long long*>(end) + which;
+}
+
+template <class Kern>
+int persistent_grid(Kern kernel, unsigned block, size_t smem, long long n, unsigned* grid) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem);
+  if (e != cudaSuccess)
+    return fail(GS_ERR_CUDA, std::string("CUDA: occupancy query: ") + cudaGetErrorString(e));
+  const long long resident = (long long)sms * (per_sm > 0 ? per_sm : 1);
+  const long long needed = (n + block - 1) / block;
+  *grid = (unsigned)(needed < resident ? needed : resident);
+  return GS_OK;
+}
+
+int zero_counter(unsigned long long* c, cudaStream_t s) {
+  if (!c) return GS_OK;
+  cudaError_t e = cudaMemsetAsync(c, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess)
+    return fail(GS_ERR_CUDA, std::string("CUDA: cudaMemsetAsync: ") + cudaGetErrorString(e));
+  return GS_OK;
+}
+
+template <class F, class L>
+int launch_record_persistent(const gs::RecordArgs& a, cudaStream_t s) {
+  unsigned long long* counter = ctrl_counter(a.ckpt, a.n, a.ck_slots, F::D, gs::kCtrlFwd);
+  unsigned grid = 0;
+  int rc;
+  if ((rc = persistent_grid(gs::record_persistent_kernel<F, L>, kBlock, 0, a.n, &grid))) return rc;
+  if ((rc = zero_counter(counter, s))) return rc;
+  gs::record_persistent_kernel<F, L><<<grid, kBlock, 0, s>>>(a, counter);
+  return cuda_check("record_persistent_kernel");
+}
+
+template <class F, class M>
+int launch_adjoint_persistent(const gs::AdjointArgs& a, int cap, cudaStream_t s) {
+  const SegCfg c = seg_cfg(a.ck_every, F::D);
+  unsigned long long* counter = ctrl_counter(const_cast<double*>(a.ckpt), a.n,
+                                             gs_ckpt_slots(cap, a.ck_every), F::D, gs::kCtrlAdj);
+  unsigned grid = 0;
+  int rc;
+  if ((rc = allow_smem(gs::adjoint_persistent_kernel<F, M>, c.smem))) return rc;
+  if ((rc = persistent_grid(gs::adjoint_persistent_kernel<F, M>, c.block, c.smem, a.n, &grid)))
+    return rc;
+  if ((rc = zero_counter(counter, s))) return rc;
+  gs::adjoint_persistent_kernel<F, M><<<grid, c.block, c.smem, s>>>(a, counter);
+  return cuda_check("adjoint_persistent_kernel");
+}
+
 // mixed = float32 stages (GS_PREC_MIXED, gs_mixed.cuh), else float64 throughout.
 template <class F>
 int launch_tsit5_record(const gs::RecordArgs& a, cudaStream_t s, bool mixed) {
-  if (mixed) {
-    gs::tsit5_mixed_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
-    return cuda_check("tsit5_mixed_record_kernel");
-  }
-  gs::tsit5_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
-  return cuda_check("tsit5_record_kernel");
+  return mixed ? launch_record_persistent<F, gs::LaneTsit5Mixed<F>>(a, s)
+               : launch_record_persistent<F, gs::LaneTsit5F64<F>>(a, s);
 }
 template <class F>
 int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed) {
@@ -135,22 +189,13 @@ int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed) {
   return cuda_check("tsit5_replay_kernel");
 }
 template <class F>
-int launch_tsit5_adjoint(const gs::AdjointArgs& a, cudaStream_t s, bool mixed) {
-  const SegCfg c = seg_cfg(a.ck_every, F::D);
-  int rc;
-  if (mixed) {
-    if ((rc = allow_smem(gs::tsit5_mixed_adjoint_kernel<F>, c.smem))) return rc;
-    gs::tsit5_mixed_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
-    return cuda_check("tsit5_mixed_adjoint_kernel");
-  }
-  if ((rc = allow_smem(gs::tsit5_adjoint_kernel<F>, c.smem))) return rc;
-  gs::tsit5_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
-  return cuda_check("tsit5_adjoint_kernel");
+int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool mixed) {
+  return mixed ? launch_adjoint_persistent<F, gs::Tsit5MixedStep>(a, cap, s)
+               : launch_adjoint_persistent<F, gs::Tsit5F64Step>(a, cap, s);
 }
 template <class F>
 int launch_ros23_record(const gs::RecordArgs& a, cudaStream_t s) {
-  gs::ros23_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
-  return cuda_check("ros23_record_kernel");
+  return launch_record_persistent<F, gs::LaneRos23<F>>(a, s);
 }
 template <class F>
 int launch_ros23_replay(const gs::ReplayArgs& a, cudaStream_t s) {
@@ -158,12 +203,8 @@ int launch_ros23_replay(const gs::ReplayArgs& a, cudaStream_t s) {
   return cuda_check("ros23_replay_kernel");
 }
 template <class F>
-int launch_ros23_adjoint(const gs::AdjointArgs& a, cudaStream_t s) {
-  const SegCfg c = seg_cfg(a.ck_every, F::D);
-  int rc;
-  if ((rc = allow_smem(gs::ros23_adjoint_kernel<F>, c.smem))) return rc;
-  gs::ros23_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
-  return cuda_check("ros23_adjoint_kernel");
+int launch_ros23_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s) {
+  return launch_adjoint_persistent<F, gs::Ros23Step>(a, cap, s);
 }
 
 __global__ void device_tableau_kernel(double* out) {
@@ -294,7 +335,8 @@ size_t gs_ckpt_bytes(int field, long long n, int cap, int ckpt_every) {
   int D, P;
   if (field_dims(field, &D, &P) != GS_OK || n <= 0) return 0;
   return (size_t)gs_ckpt_slots(cap, ckpt_every) * (size_t)n * (size_t)gs::ckpt_width(D) *
-         sizeof(double);
+             sizeof(double) +
+         gs::kCtrlBytes;  // control block of the persistent kernels (work counters)
 }
 
 int gs_max_ckpt_every(void) { return gs::KMAX; }
@@ -350,7 +392,7 @@ int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, con
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (n == 0) return GS_OK;
   gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp};
-  GS_TSIT5_DISPATCH(field, launch_tsit5_adjoint, a, (cudaStream_t)stream,
+  GS_TSIT5_DISPATCH(field, launch_tsit5_adjoint, a, cap, (cudaStream_t)stream,
                     precision == GS_PREC_MIXED)
 }
 
@@ -403,7 +445,7 @@ int gs_ros23_adjoint(int field, int precision, long long n, const double* p, con
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (n == 0) return GS_OK;
   gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp};
-  GS_ROS23_DISPATCH(field, launch_ros23_adjoint, a, (cudaStream_t)stream)
+  GS_ROS23_DISPATCH(field, launch_ros23_adjoint, a, cap, (cudaStream_t)stream)
 }
 
 int gs_record_from_padded(long long n, long long S, const double* dts, long long ld,

@@ -1,0 +1,298 @@
+// gs_persistent.cuh -- persistent, work-stealing forward and reverse kernels.
+//
+// The grid holds one wave of resident blocks.  Every lane (thread) takes a trajectory index
+// from a global counter (atomicAdd), integrates it, writes its outputs, and takes the next
+// one, until the counter passes n.  Each loop iteration is one attempt (forward) or one whole
+// segment (reverse) for every active lane, so the lanes of a warp execute the same code every
+// iteration: a lane whose trajectory finishes refills itself with a fresh trajectory instead
+// of idling until its warp's slowest trajectory ends.  This removes both the last partial
+// wave of a one-thread-per-trajectory launch and the idle lanes of warps whose trajectories
+// take very different numbers of steps (the uneven-batch workload: 4 to 7841 steps).
+//
+// The counter lives in a 256-byte control block after the checkpoint slots of the caller's
+// checkpoint buffer (gs_ckpt_bytes includes it) and is zeroed on the stream before each
+// launch.  Without a counter (a forward solve with neither record nor checkpoints) lanes take
+// trajectories j, j + G, j + 2G, ... (G = resident threads) instead.
+//
+// Per-trajectory arithmetic is exactly that of gs_tsit5.cuh / gs_mixed.cuh / gs_ros23.cuh:
+// results do not depend on which lane integrates which trajectory.
+#pragma once
+#include "gs_mixed.cuh"
+#include "gs_ros23.cuh"
+#include "gs_saveat.cuh"
+#include "gs_tsit5.cuh"
+
+namespace gs {
+
+constexpr int kCtrlBytes = 256;
+constexpr int kCtrlFwd = 0;  // counter slots (unsigned long long) in the control block
+constexpr int kCtrlAdj = 1;
+
+struct Fetch {
+  unsigned long long* counter;  // null: static striding
+  long long next;
+  long long stride;
+  __device__ __forceinline__ Fetch(unsigned long long* c) : counter(c) {
+    next = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    stride = (long long)gridDim.x * blockDim.x;
+  }
+  __device__ __forceinline__ long long get() {
+    if (counter) return (long long)atomicAdd(counter, 1ull);
+    const long long j = next;
+    next += stride;
+    return j;
+  }
+};
+
+// ---- forward method policies: per-lane state carried between attempts -----------------
+template <class F>
+struct LaneTsit5F64 {
+  static constexpr int D = F::D, QK = 10;
+  double k1[D], k7[D];
+  __device__ __forceinline__ void start(const double* y, const double* p, const float*) {
+    F::rhs(y, p, k1);
+  }
+  // candidate y5 for step h; returns the mean of squares of the scaled error
+  __device__ __forceinline__ double trial(const double* y, const double* p, const float*, double h,
+                                          double rtol, double atol, double* y5) {
+    using T = Tsit5;
+    Stages<F> S;
+    double e[D];
+    tsit5_k2_to_k6<F>(y, p, k1, h, S);
+    tsit5_y5<F>(y, k1, S, h, y5);
+    F::rhs(y5, p, k7);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      e[i] = h * (T::E1 * k1[i] + T::E2 * S.k2[i] + T::E3 * S.k3[i] + T::E4 * S.k4[i] +
+                  T::E5 * S.k5[i] + T::E6 * S.k6[i] + T::E7 * k7[i]);
+    return wrms_mean<D>(e, y, y5, rtol, atol);
+  }
+  __device__ __forceinline__ void commit() {
+#pragma unroll
+    for (int i = 0; i < D; ++i) k1[i] = k7[i];
+  }
+  __device__ __forceinline__ bool degenerate(double, double) const { return false; }
+};
+
+template <class F>
+struct LaneTsit5Mixed {
+  static constexpr int D = F::D, QK = 10;
+  double k1[D], k7[D], c[D], c5[D];
+  __device__ __forceinline__ void start(const double* y, const double* p, const float*) {
+    F::rhs(y, p, k1);
+#pragma unroll
+    for (int i = 0; i < D; ++i) c[i] = 0.0;
+  }
+  __device__ __forceinline__ double trial(const double* y, const double* p, const float* pf,
+                                          double h, double rtol, double atol, double* y5) {
+    using T = Tsit5f;
+    const float hf = (float)h;
+    float yf[D], k1f[D];
+    double inc[D], ed[D];
+    to_float<F>(y, yf);
+    to_float<F>(k1, k1f);
+    MixedStages<F> S;
+    mixed_dk2_to_dk6<F>(yf, pf, k1f, hf, S);
+    mixed_increment<F>(k1, S, h, hf, inc);
+#pragma unroll
+    for (int i = 0; i < D; ++i) { y5[i] = y[i]; c5[i] = c[i]; }
+    kahan_add<D>(y5, c5, inc);
+    F::rhs(y5, p, k7);
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      const float dk7 = (float)(k7[i] - k1[i]);
+      ed[i] = (double)(hf * (T::E2 * S.dk2[i] + T::E3 * S.dk3[i] + T::E4 * S.dk4[i] +
+                             T::E5 * S.dk5[i] + T::E6 * S.dk6[i] + T::E7 * dk7));
+    }
+    return wrms_mean<D>(ed, y, y5, rtol, atol);
+  }
+  __device__ __forceinline__ void commit() {
+#pragma unroll
+    for (int i = 0; i < D; ++i) { k1[i] = k7[i]; c[i] = c5[i]; }
+  }
+  __device__ __forceinline__ bool degenerate(double, double) const { return false; }
+};
+
+template <class F>
+struct LaneRos23 {
+  static constexpr int D = F::D, QK = 6;
+  __device__ __forceinline__ void start(const double*, const double*, const float*) {}
+  __device__ __forceinline__ double trial(const double* y, const double* p, const float*, double h,
+                                          double rtol, double atol, double* ynew) {
+    RosCore<F> c;
+    ros23_core<F>(y, p, h, c, ynew);
+    double F2[D], r3[D], k3[D], ev[D];
+    F::rhs(ynew, p, F2);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      r3[i] = F2[i] - Ros23::E32 * (c.k2[i] - c.F1[i]) - 2.0 * (c.k1[i] - c.F0[i]);
+    lu_solve<D>(c.W, r3, k3);
+#pragma unroll
+    for (int i = 0; i < D; ++i) ev[i] = (h / 6.0) * (c.k1[i] - 2.0 * c.k2[i] + k3[i]);
+    return wrms_mean<D>(ev, y, ynew, rtol, atol);
+  }
+  __device__ __forceinline__ void commit() {}
+  // the step no longer advances time: status 2 (gradsolve/solvers/record_jax.py:109)
+  __device__ __forceinline__ bool degenerate(double t, double h) const { return t + h == t; }
+};
+
+// ---- persistent forward with record ---------------------------------------------------------
+template <class F, class L>
+__global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs a,
+                                                                unsigned long long* counter) {
+  constexpr int D = F::D, P = F::P;
+  Fetch fetch(counter);
+  const bool rec_on = a.rec != nullptr;
+  const bool ck_on = a.ckpt != nullptr;
+  long long j = fetch.get();
+  double y[D], ynew[D], p[P], t = 0.0, t1 = 0.0, dt = 0.0;
+  float pf[P];
+  int acc = 0, rej = 0, it = 0, ck_cnt = 0, ck_slot = 0;
+  double b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
+  L lane;
+  auto begin = [&](long long jj) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) y[i] = a.y0[jj * D + i];
+#pragma unroll
+    for (int i = 0; i < P; ++i) { p[i] = a.p[jj * P + i]; pf[i] = (float)p[i]; }
+    t = a.t0;
+    t1 = a.t1v ? a.t1v[jj] : a.t1;
+    dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
+    acc = rej = it = ck_cnt = ck_slot = 0;
+    b0 = b1 = b2 = b3 = 0.0;
+    if (ck_on) store_ckpt<D>(a.ckpt, a.n, jj, 0, y, t);
+    lane.start(y, p, pf);
+  };
+  if (j < a.n) begin(j);
+  while (j < a.n) {
+    int st = -1;  // stays -1 while the trajectory is running
+    if (t >= t1) {
+      st = 0;
+    } else if (it >= a.max_steps) {
+      st = 1;
+    } else {
+      const double h = (t1 - t < dt) ? (t1 - t) : dt;
+      if (lane.degenerate(t, h)) {
+        st = 2;
+      } else {
+        const double m = lane.trial(y, p, pf, h, a.rtol, a.atol, ynew);
+        ++it;
+        if (!(m == m)) {
+          st = 1;
+        } else if (m <= kAcceptMax) {
+          if ((rec_on || ck_on) && acc >= a.cap) {
+            st = 3;
+          } else {
+            t = t + h;
+#pragma unroll
+            for (int i = 0; i < D; ++i) y[i] = ynew[i];
+            lane.commit();
+            if (rec_on) {
+              b0 = b1; b1 = b2; b2 = b3; b3 = h;
+              if ((acc & 3) == 3) store_rec_chunk(a.rec, a.n, j, acc >> 2, b0, b1, b2, b3);
+            }
+            ++acc;
+            if (ck_on && ++ck_cnt == a.ck_every) {
+              ck_cnt = 0;
+              if (++ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, ck_slot, y, t);
+            }
+          }
+        } else {
+          ++rej;
+        }
+        if (st < 0) dt = step_from_mean<L::QK>(m, h);
+      }
+    }
+    if (st >= 0) {  // finished: write this trajectory's outputs, take the next one
+      if (rec_on) {
+        switch (acc & 3) {
+          case 1: store_rec_chunk(a.rec, a.n, j, acc >> 2, b3, 0.0, 0.0, 0.0); break;
+          case 2: store_rec_chunk(a.rec, a.n, j, acc >> 2, b2, b3, 0.0, 0.0); break;
+          case 3: store_rec_chunk(a.rec, a.n, j, acc >> 2, b1, b2, b3, 0.0); break;
+          default: break;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
+      a.n_acc[j] = acc;
+      a.n_rej[j] = rej;
+      a.status[j] = st;
+      j = fetch.get();
+      if (j < a.n) begin(j);
+    }
+  }
+}
+
+// ---- persistent reverse pass (one segment of K steps per iteration) --------------------------
+template <class F, class M>
+__global__ void __launch_bounds__(128) adjoint_persistent_kernel(const AdjointArgs a,
+                                                                 unsigned long long* counter) {
+  constexpr int D = F::D, P = F::P;
+  Fetch fetch(counter);
+  const int K = a.ck_every;
+  SegBuf<D> seg;
+  double p[P], lam[D], gp[P];
+  float pf[P];
+  int na = 0, sg = -1;
+  long long j;
+  // take trajectories until one has work (n_acc = 0 ones finish at once: gy0 = ybar)
+  auto take = [&]() {
+    for (;;) {
+      j = fetch.get();
+      if (j >= a.n) return;
+#pragma unroll
+      for (int i = 0; i < P; ++i) { p[i] = a.p[j * P + i]; pf[i] = (float)p[i]; gp[i] = 0.0; }
+#pragma unroll
+      for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
+      na = a.n_acc[j];
+      sg = (na + K - 1) / K - 1;
+      if (sg >= 0) return;
+      if (a.gy0) {
+#pragma unroll
+        for (int i = 0; i < D; ++i) a.gy0[j * D + i] = lam[i];
+      }
+      if (a.gp) {
+#pragma unroll
+        for (int i = 0; i < P; ++i) a.gp[j * P + i] = 0.0;
+      }
+    }
+  };
+  take();
+  while (j < a.n) {
+    const int start = sg * K;
+    double y[D], c[D];
+    load_ckpt<D>(a.ckpt, a.n, j, sg, y);
+#pragma unroll
+    for (int i = 0; i < D; ++i) { seg.at(0, i) = y[i]; c[i] = 0.0; }
+    for (int q = 1; q < K; ++q) {
+      const int s = start + q - 1;
+      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      if (dt != 0.0) M::template step<F>(y, c, p, pf, dt);
+#pragma unroll
+      for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
+    }
+    for (int q = K - 1; q >= 0; --q) {
+      const int s = start + q;
+      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      if (dt != 0.0) {
+        double ys[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) ys[i] = seg.at(q, i);
+        M::template vjp<F>(ys, p, pf, dt, lam, gp);
+      }
+    }
+    if (--sg < 0) {
+      if (a.gy0) {
+#pragma unroll
+        for (int i = 0; i < D; ++i) a.gy0[j * D + i] = lam[i];
+      }
+      if (a.gp) {
+#pragma unroll
+        for (int i = 0; i < P; ++i) a.gp[j * P + i] = gp[i];
+      }
+      take();
+    }
+  }
+}
+
+}  // namespace gs

@@ -27,6 +27,7 @@ _PREC = {"float64": _lib.GS_PREC_F64, "mixed": _lib.GS_PREC_MIXED}
 
 # default record capacity before growth (the reference's device recorder starts at 1024)
 DEFAULT_CAP0 = 1024
+CTRL_DOUBLES = 256 // 8  # control block after the checkpoint slots (work counters)
 
 
 def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
@@ -144,7 +145,9 @@ def _alloc_record(n: int, cap: int, dim: int, K: int, device) -> tuple:
     rec_elems = L.gs_record_bytes(n, cap) // 8
     slots = L.gs_ckpt_slots(cap, K)
     rec = torch.empty(max(rec_elems, 2), dtype=torch.float64, device=device)
-    ckpt = torch.empty(max(slots * n * ckpt_width(dim), 2), dtype=torch.float64, device=device)
+    # checkpoint slots + the persistent kernels' 256-byte control block (gs_ckpt_bytes)
+    ckpt = torch.empty(slots * n * ckpt_width(dim) + CTRL_DOUBLES, dtype=torch.float64,
+                       device=device)
     return rec, ckpt
 
 

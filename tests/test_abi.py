@@ -65,9 +65,10 @@ def test_workspace_sizes(gslib):
     assert L.gs_record_bytes(0, 5) == 0
     assert L.gs_ckpt_slots(100, 10) == 11
     assert L.gs_ckpt_slots(101, 10) == 12
-    assert L.gs_ckpt_bytes(1, 7, 100, 10) == 11 * 7 * 4 * 8     # lorenz: CW = 4
-    assert L.gs_ckpt_bytes(2, 7, 100, 1) == 101 * 7 * 4 * 8     # vdp: CW = 4
-    assert L.gs_ckpt_bytes(4008, 7, 100, 1) == 101 * 7 * 10 * 8  # linear_8: CW = 10
+    ctrl = 256  # control block of the persistent kernels after the slots
+    assert L.gs_ckpt_bytes(1, 7, 100, 10) == 11 * 7 * 4 * 8 + ctrl     # lorenz: CW = 4
+    assert L.gs_ckpt_bytes(2, 7, 100, 1) == 101 * 7 * 4 * 8 + ctrl     # vdp: CW = 4
+    assert L.gs_ckpt_bytes(4008, 7, 100, 1) == 101 * 7 * 10 * 8 + ctrl  # linear_8: CW = 10
     assert L.gs_max_ckpt_every() == 64
 
 

@@ -310,14 +310,15 @@ def run_b200(args) -> None:
             r = engine.forward_record("tsit5", spec, y0, rho, t0=T0, t1=T1, rtol=RTOL,
                                       atol=ATOL, max_steps=100000, cap0=args.cap,
                                       checkpoint=args.checkpoint, precision=precision,
-                                      workspace=ws["r"])
+                                      workspace=ws["r"], schedule=args.schedule)
             ws["r"] = r
             if events:
                 events[1].record(stream)
             ybar = (2.0 * inv) * r.y_final
             if events:
                 events[2].record(stream)
-            _gy0, gp = engine.adjoint(r, rho, ybar, want_y0=False, precision=precision)
+            _gy0, gp = engine.adjoint(r, rho, ybar, want_y0=False, precision=precision,
+                                      schedule=args.schedule)
             if events:
                 events[3].record(stream)
             return r, gp
@@ -487,6 +488,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--schedule", default="auto", choices=["auto", "static", "refill", "strided"])
     args = ap.parse_args()
     if args.checkpoint not in ("sqrt", "all", "auto"):
         args.checkpoint = int(args.checkpoint)

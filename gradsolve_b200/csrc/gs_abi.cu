@@ -116,6 +116,23 @@ int allow_smem(Kern kernel, size_t smem) {
 
 unsigned grid_for_block(long long n, unsigned block) { return (unsigned)((n + block - 1) / block); }
 
+// ---- scheduling ------------------------------------------------------------------------------
+// GS_SCHED_* flags ride in the high bits of the precision argument.  AUTO: one thread per
+// trajectory (hardware block scheduling) for a shared end time, lane refill with a work
+// counter when trajectories have their own end times (uneven batches); the reverse pass runs
+// one thread per trajectory unless the caller asks for refill.
+int forward_schedule(int precision, const double* t1v, const double* ckpt) {
+  int s = precision & GS_SCHED_MASK;
+  if (s == GS_SCHED_AUTO) s = t1v ? GS_SCHED_REFILL : GS_SCHED_STATIC;
+  if (s == GS_SCHED_REFILL && !ckpt) s = GS_SCHED_STRIDED;  // no control block to count in
+  return s;
+}
+
+int adjoint_schedule(int precision) {
+  const int s = precision & GS_SCHED_MASK;
+  return s == GS_SCHED_AUTO ? GS_SCHED_STATIC : s;
+}
+
 // ---- persistent launches (gs_persistent.cuh) ------------------------------------------------
 // One wave of resident blocks; the work counter lives in the control block that follows the
 // checkpoint slots (gs_ckpt_bytes includes it) and is zeroed on the stream before the launch.
@@ -148,8 +165,9 @@ int zero_counter(unsigned long long* c, cudaStream_t s) {
 }
 
 template <class F, class L>
-int launch_record_persistent(const gs::RecordArgs& a, cudaStream_t s) {
-  unsigned long long* counter = ctrl_counter(a.ckpt, a.n, a.ck_slots, F::D, gs::kCtrlFwd);
+int launch_record_persistent(const gs::RecordArgs& a, cudaStream_t s, bool use_counter) {
+  unsigned long long* counter =
+      use_counter ? ctrl_counter(a.ckpt, a.n, a.ck_slots, F::D, gs::kCtrlFwd) : nullptr;
   unsigned grid = 0;
   int rc;
   if ((rc = persistent_grid(gs::record_persistent_kernel<F, L>, kBlock, 0, a.n, &grid))) return rc;
@@ -159,10 +177,13 @@ int launch_record_persistent(const gs::RecordArgs& a, cudaStream_t s) {
 }
 
 template <class F, class M>
-int launch_adjoint_persistent(const gs::AdjointArgs& a, int cap, cudaStream_t s) {
+int launch_adjoint_persistent(const gs::AdjointArgs& a, int cap, cudaStream_t s,
+                              bool use_counter) {
   const SegCfg c = seg_cfg(a.ck_every, F::D);
-  unsigned long long* counter = ctrl_counter(const_cast<double*>(a.ckpt), a.n,
-                                             gs_ckpt_slots(cap, a.ck_every), F::D, gs::kCtrlAdj);
+  unsigned long long* counter =
+      use_counter ? ctrl_counter(const_cast<double*>(a.ckpt), a.n,
+                                 gs_ckpt_slots(cap, a.ck_every), F::D, gs::kCtrlAdj)
+                  : nullptr;
   unsigned grid = 0;
   int rc;
   if ((rc = allow_smem(gs::adjoint_persistent_kernel<F, M>, c.smem))) return rc;
@@ -175,9 +196,18 @@ int launch_adjoint_persistent(const gs::AdjointArgs& a, int cap, cudaStream_t s)
 
 // mixed = float32 stages (GS_PREC_MIXED, gs_mixed.cuh), else float64 throughout.
 template <class F>
-int launch_tsit5_record(const gs::RecordArgs& a, cudaStream_t s, bool mixed) {
-  return mixed ? launch_record_persistent<F, gs::LaneTsit5Mixed<F>>(a, s)
-               : launch_record_persistent<F, gs::LaneTsit5F64<F>>(a, s);
+int launch_tsit5_record(const gs::RecordArgs& a, cudaStream_t s, bool mixed, int sched) {
+  if (sched == GS_SCHED_STATIC) {
+    if (mixed) {
+      gs::tsit5_mixed_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+      return cuda_check("tsit5_mixed_record_kernel");
+    }
+    gs::tsit5_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    return cuda_check("tsit5_record_kernel");
+  }
+  const bool counter = sched == GS_SCHED_REFILL;
+  return mixed ? launch_record_persistent<F, gs::LaneTsit5Mixed<F>>(a, s, counter)
+               : launch_record_persistent<F, gs::LaneTsit5F64<F>>(a, s, counter);
 }
 template <class F>
 int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed) {
@@ -189,13 +219,31 @@ int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed) {
   return cuda_check("tsit5_replay_kernel");
 }
 template <class F>
-int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool mixed) {
-  return mixed ? launch_adjoint_persistent<F, gs::Tsit5MixedStep>(a, cap, s)
-               : launch_adjoint_persistent<F, gs::Tsit5F64Step>(a, cap, s);
+int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool mixed,
+                         int sched) {
+  if (sched == GS_SCHED_STATIC) {
+    const SegCfg c = seg_cfg(a.ck_every, F::D);
+    int rc;
+    if (mixed) {
+      if ((rc = allow_smem(gs::tsit5_mixed_adjoint_kernel<F>, c.smem))) return rc;
+      gs::tsit5_mixed_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+      return cuda_check("tsit5_mixed_adjoint_kernel");
+    }
+    if ((rc = allow_smem(gs::tsit5_adjoint_kernel<F>, c.smem))) return rc;
+    gs::tsit5_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+    return cuda_check("tsit5_adjoint_kernel");
+  }
+  const bool counter = sched == GS_SCHED_REFILL;
+  return mixed ? launch_adjoint_persistent<F, gs::Tsit5MixedStep>(a, cap, s, counter)
+               : launch_adjoint_persistent<F, gs::Tsit5F64Step>(a, cap, s, counter);
 }
 template <class F>
-int launch_ros23_record(const gs::RecordArgs& a, cudaStream_t s) {
-  return launch_record_persistent<F, gs::LaneRos23<F>>(a, s);
+int launch_ros23_record(const gs::RecordArgs& a, cudaStream_t s, int sched) {
+  if (sched == GS_SCHED_STATIC) {
+    gs::ros23_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    return cuda_check("ros23_record_kernel");
+  }
+  return launch_record_persistent<F, gs::LaneRos23<F>>(a, s, sched == GS_SCHED_REFILL);
 }
 template <class F>
 int launch_ros23_replay(const gs::ReplayArgs& a, cudaStream_t s) {
@@ -203,8 +251,15 @@ int launch_ros23_replay(const gs::ReplayArgs& a, cudaStream_t s) {
   return cuda_check("ros23_replay_kernel");
 }
 template <class F>
-int launch_ros23_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s) {
-  return launch_adjoint_persistent<F, gs::Ros23Step>(a, cap, s);
+int launch_ros23_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, int sched) {
+  if (sched == GS_SCHED_STATIC) {
+    const SegCfg c = seg_cfg(a.ck_every, F::D);
+    int rc;
+    if ((rc = allow_smem(gs::ros23_adjoint_kernel<F>, c.smem))) return rc;
+    gs::ros23_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+    return cuda_check("ros23_adjoint_kernel");
+  }
+  return launch_adjoint_persistent<F, gs::Ros23Step>(a, cap, s, sched == GS_SCHED_REFILL);
 }
 
 __global__ void device_tableau_kernel(double* out) {
@@ -346,8 +401,9 @@ int gs_tsit5_fwd_record(int field, int precision, long long n, const double* y0,
                         double atol, double dt0, int max_steps, int cap, int ckpt_every,
                         double* rec, double* ckpt, double* y_final, int* n_acc, int* n_rej,
                         int* status, void* stream) {
-  if (precision != GS_PREC_F64 && precision != GS_PREC_MIXED)
-    return fail(GS_ERR_PRECISION, "gs_tsit5_fwd_record: unknown precision mode " + std::to_string(precision));
+  const int prec = precision & GS_PREC_MASK;
+  if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED)
+    return fail(GS_ERR_PRECISION, "gs_tsit5_fwd_record: unknown precision mode " + std::to_string(prec));
   int rc = check_record_args("gs_tsit5_fwd_record", n, y0, p, rtol, atol, max_steps, cap,
                              ckpt_every, rec, ckpt, y_final, n_acc, n_rej, status);
   if (rc) return rc;
@@ -357,7 +413,7 @@ int gs_tsit5_fwd_record(int field, int precision, long long n, const double* y0,
   gs::RecordArgs a{n, y0, p, t0, t1, rtol, atol, dt0, t1v, max_steps, cap, ckpt_every,
                    gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status};
   GS_TSIT5_DISPATCH(field, launch_tsit5_record, a, (cudaStream_t)stream,
-                    precision == GS_PREC_MIXED)
+                    prec == GS_PREC_MIXED, forward_schedule(precision, t1v, ckpt))
 }
 
 int gs_tsit5_replay(int field, int precision, long long n, const double* y0, const double* p,
@@ -384,8 +440,9 @@ int gs_tsit5_replay(int field, int precision, long long n, const double* y0, con
 int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, const double* rec,
                      const int* n_acc, int cap, const double* ckpt, int ckpt_every,
                      const double* ybar, double* gy0, double* gp, void* stream) {
-  if (precision != GS_PREC_F64 && precision != GS_PREC_MIXED)
-    return fail(GS_ERR_PRECISION, "gs_tsit5_adjoint: unknown precision mode " + std::to_string(precision));
+  const int prec = precision & GS_PREC_MASK;
+  if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED)
+    return fail(GS_ERR_PRECISION, "gs_tsit5_adjoint: unknown precision mode " + std::to_string(prec));
   int rc = check_adjoint_args("gs_tsit5_adjoint", n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar);
   if (rc) return rc;
   int D, P;
@@ -393,7 +450,7 @@ int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, con
   if (n == 0) return GS_OK;
   gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp};
   GS_TSIT5_DISPATCH(field, launch_tsit5_adjoint, a, cap, (cudaStream_t)stream,
-                    precision == GS_PREC_MIXED)
+                    prec == GS_PREC_MIXED, adjoint_schedule(precision))
 }
 
 int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,
@@ -401,8 +458,8 @@ int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,
                         double atol, double dt0, int max_steps, int cap, int ckpt_every,
                         double* rec, double* ckpt, double* y_final, int* n_acc, int* n_rej,
                         int* status, void* stream) {
-  if (precision != GS_PREC_F64)
-    return fail(GS_ERR_PRECISION, "gs_ros23_fwd_record: precision mode not built");
+  if ((precision & GS_PREC_MASK) != GS_PREC_F64)
+    return fail(GS_ERR_PRECISION, "gs_ros23_fwd_record: Rosenbrock23 runs in float64 only");
   int rc = check_record_args("gs_ros23_fwd_record", n, y0, p, rtol, atol, max_steps, cap,
                              ckpt_every, rec, ckpt, y_final, n_acc, n_rej, status);
   if (rc) return rc;
@@ -411,7 +468,8 @@ int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,
   if (n == 0) return GS_OK;
   gs::RecordArgs a{n, y0, p, t0, t1, rtol, atol, dt0, t1v, max_steps, cap, ckpt_every,
                    gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status};
-  GS_ROS23_DISPATCH(field, launch_ros23_record, a, (cudaStream_t)stream)
+  GS_ROS23_DISPATCH(field, launch_ros23_record, a, (cudaStream_t)stream,
+                    forward_schedule(precision, t1v, ckpt))
 }
 
 int gs_ros23_replay(int field, int precision, long long n, const double* y0, const double* p,
@@ -437,15 +495,16 @@ int gs_ros23_replay(int field, int precision, long long n, const double* y0, con
 int gs_ros23_adjoint(int field, int precision, long long n, const double* p, const double* rec,
                      const int* n_acc, int cap, const double* ckpt, int ckpt_every,
                      const double* ybar, double* gy0, double* gp, void* stream) {
-  if (precision != GS_PREC_F64)
-    return fail(GS_ERR_PRECISION, "gs_ros23_adjoint: precision mode not built");
+  if ((precision & GS_PREC_MASK) != GS_PREC_F64)
+    return fail(GS_ERR_PRECISION, "gs_ros23_adjoint: Rosenbrock23 runs in float64 only");
   int rc = check_adjoint_args("gs_ros23_adjoint", n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar);
   if (rc) return rc;
   int D, P;
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (n == 0) return GS_OK;
   gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp};
-  GS_ROS23_DISPATCH(field, launch_ros23_adjoint, a, cap, (cudaStream_t)stream)
+  GS_ROS23_DISPATCH(field, launch_ros23_adjoint, a, cap, (cudaStream_t)stream,
+                    adjoint_schedule(precision))
 }
 
 int gs_record_from_padded(long long n, long long S, const double* dts, long long ld,

@@ -24,6 +24,9 @@ from .fields import FieldSpec
 METHOD_TSIT5 = "tsit5"
 METHOD_ROS23 = "rosenbrock23"
 _PREC = {"float64": _lib.GS_PREC_F64, "mixed": _lib.GS_PREC_MIXED}
+# scheduling flags (include/gsolve.h GS_SCHED_*): one thread per trajectory, persistent lanes
+# refilled from a work counter, or persistent lanes with strided assignment
+_SCHED = {"auto": 0x000, "static": 0x100, "refill": 0x200, "strided": 0x300}
 
 # default record capacity before growth (the reference's device recorder starts at 1024)
 DEFAULT_CAP0 = 1024
@@ -128,6 +131,7 @@ class Record:
     n_acc: torch.Tensor      # (n,) int32
     n_rej: torch.Tensor      # (n,) int32
     status: torch.Tensor     # (n,) int32
+    uneven: bool = False     # per-trajectory end times: the reverse pass refills lanes
 
     def padded_dts(self, S: Optional[int] = None) -> torch.Tensor:
         """The record in the reference's (n, S) zero-padded layout."""
@@ -156,7 +160,8 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
                    t1v: Optional[torch.Tensor] = None, max_steps: int = 100000,
                    cap0: int = DEFAULT_CAP0, checkpoint="auto",
                    budget_bytes: Optional[int] = None, precision: str = "float64",
-                   record: bool = True, workspace: Optional[Record] = None) -> Record:
+                   record: bool = True, workspace: Optional[Record] = None,
+                   schedule: str = "auto") -> Record:
     """Adaptive solve on the device; with ``record`` the dts and checkpoints are kept.
 
     ``y0`` (n, D) and ``p`` (n, P) float64 contiguous device tensors.  ``workspace``: a Record
@@ -173,13 +178,15 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
     n_rej = ws.n_rej if ws is not None else torch.empty(n, dtype=torch.int32, device=device)
     status = ws.status if ws is not None else torch.empty(n, dtype=torch.int32, device=device)
     dt0_arg = -1.0 if dt0 is None else float(dt0)
+    mode = _PREC[precision] | _SCHED[schedule]
     if not record:
-        _lib.check(fn(spec.code, _PREC[precision], n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
+        _lib.check(fn(spec.code, mode, n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
                       float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), 0, 1, None,
                       None, _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status), _stream()),
                    fn.__name__)
         empty = torch.empty(0, dtype=torch.float64, device=device)
-        return Record(method, spec, n, float(t0), 0, 1, empty, empty, yf, n_acc, n_rej, status)
+        return Record(method, spec, n, float(t0), 0, 1, empty, empty, yf, n_acc, n_rej, status,
+                      uneven=t1v is not None)
     cap = max(1, min(int(cap0), int(max_steps)))
     if ws is not None and ws.cap > cap:
         cap = ws.cap
@@ -193,14 +200,15 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
             rec, ckpt = ws.rec, ws.ckpt
         else:
             rec, ckpt = _alloc_record(n, cap, spec.dim, K, device)
-        _lib.check(fn(spec.code, _PREC[precision], n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
+        _lib.check(fn(spec.code, mode, n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
                       float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), cap, K,
                       _ptr(rec), _ptr(ckpt), _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status),
                       _stream()), fn.__name__)
         if n == 0 or cap >= max_steps or not bool((status == 3).any().item()):
             break
         cap = min(2 * cap, int(max_steps))
-    return Record(method, spec, n, float(t0), cap, K, rec, ckpt, yf, n_acc, n_rej, status)
+    return Record(method, spec, n, float(t0), cap, K, rec, ckpt, yf, n_acc, n_rej, status,
+                  uneven=t1v is not None)
 
 
 def raise_on_failed(r: Record, max_steps: int, t1) -> None:
@@ -239,14 +247,19 @@ def replay(r: Record, y0: torch.Tensor, p: torch.Tensor, *, write_ckpt: bool = T
 
 
 def adjoint(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
-            want_p: bool = True, precision: str = "float64"):
-    """(dL/dy0, dL/dp) for cotangent ybar = dL/dy_final, using the record's checkpoints."""
+            want_p: bool = True, precision: str = "float64", schedule: str = "auto"):
+    """(dL/dy0, dL/dp) for cotangent ybar = dL/dy_final, using the record's checkpoints.
+    ``schedule="auto"`` refills lanes from a work counter when the record came from an
+    uneven batch (per-trajectory end times), else runs one thread per trajectory."""
     L = _lib.lib()
     fn = L.gs_tsit5_adjoint if r.method == METHOD_TSIT5 else L.gs_ros23_adjoint
     gy0 = torch.empty((r.n, r.spec.dim), dtype=torch.float64, device=p.device) if want_y0 else None
     gp = torch.empty((r.n, p.shape[1]), dtype=torch.float64, device=p.device) if want_p else None
     ybar = ybar.contiguous()
-    _lib.check(fn(r.spec.code, _PREC[precision], r.n, _ptr(p), _ptr(r.rec), _ptr(r.n_acc),
+    if schedule == "auto" and r.uneven:
+        schedule = "refill"
+    _lib.check(fn(r.spec.code, _PREC[precision] | _SCHED[schedule], r.n, _ptr(p), _ptr(r.rec),
+                  _ptr(r.n_acc),
                   max(r.cap, 1), _ptr(r.ckpt), r.ckpt_every, _ptr(ybar), _ptr(gy0), _ptr(gp),
                   _stream()), fn.__name__)
     return gy0, gp

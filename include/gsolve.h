@@ -50,6 +50,19 @@ extern "C" {
 
 #define GS_PREC_F64 0   /* everything float64 */
 #define GS_PREC_MIXED 1 /* float32 stages/RHS; float64 time, controller, error norm, state */
+#define GS_PREC_MASK 0xff
+
+/* Scheduling flags, OR-ed into the precision argument of the forward and adjoint entry
+ * points.  STATIC: one thread per trajectory.  REFILL: a persistent grid whose lanes take
+ * the next trajectory from a work counter when theirs finishes (uneven batches; the counter
+ * lives in the checkpoint buffer's control block).  STRIDED: persistent lanes taking
+ * trajectories j, j+G, ...  AUTO (0): STATIC, except REFILL for a forward with per-trajectory
+ * end times. */
+#define GS_SCHED_AUTO 0x000
+#define GS_SCHED_STATIC 0x100
+#define GS_SCHED_REFILL 0x200
+#define GS_SCHED_STRIDED 0x300
+#define GS_SCHED_MASK 0x300
 
 /* per-trajectory status values written to status[] */
 #define GS_TRAJ_OK 0          /* reached t1 */

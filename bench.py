@@ -282,6 +282,7 @@ def run_b200(args) -> None:
 
     from gradsolve_b200 import engine, flops
     from gradsolve_b200.fields import field_spec
+    from gradsolve_b200.sharding import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -343,10 +344,7 @@ def run_b200(args) -> None:
     if world > 1:
         dist.barrier()
     ms_per_step = float(np.mean(step_ms))
-    if world > 1:
-        t = torch.tensor([ms_per_step], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_per_step = float(t.item())
+    ms_per_step = max_over_ranks(ms_per_step, dev)
     value = n * world / (ms_per_step * 1e-3)
     assert torch.isfinite(gp).all()
 
@@ -358,10 +356,7 @@ def run_b200(args) -> None:
             rm, gpm = mstep()
         m_fwd, m_adj, m_step, (rm, gpm) = _time_steps(torch, mstep, args.steps, flush, stream)
         m_ms = float(np.mean(m_step))
-        if world > 1:
-            t = torch.tensor([m_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            m_ms = float(t.item())
+        m_ms = max_over_ranks(m_ms, dev)
         # same mesh: the float64 record replayed and differentiated with float32 stages
         ybar64 = (2.0 * inv) * r.y_final
         yf_sm = engine.replay(r, y0, rho, write_ckpt=True, precision="mixed")
@@ -377,6 +372,30 @@ def run_b200(args) -> None:
                  "y_final_rel_err_same_mesh_median": float(yrel.median().item()),
                  "n_acc_diff_max": int(n_acc_diff.max().item()),
                  "meets_1e-6": _grad_err(gp_sm, gp)["max"] <= 1e-6}
+    # ---- forward-only solve lane (no record, no checkpoints): trajectory-solves/s ------
+    solve = {}
+    if not args.no_solve:
+        for prec in ("float64",) + (() if args.no_mixed else ("mixed",)):
+            def fwd_only():
+                return engine.forward_record("tsit5", spec, y0, rho, t0=T0, t1=T1, rtol=RTOL,
+                                             atol=ATOL, max_steps=100000, record=False,
+                                             precision=prec, schedule=args.schedule)
+            for _ in range(args.warmup):
+                fwd_only()
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(args.steps)]
+            for e0, e1 in evs:
+                flush.zero_()
+                e0.record(stream)
+                rs = fwd_only()
+                e1.record(stream)
+            torch.cuda.synchronize()
+            s_ms = float(np.mean([e0.elapsed_time(e1) for e0, e1 in evs]))
+            s_ms = max_over_ranks(s_ms, dev)
+            s_att = int((rs.n_acc.to(torch.int64) + rs.n_rej.to(torch.int64)).sum().item())
+            solve[prec] = {"value": n * world / (s_ms * 1e-3), "unit": "trajectory-solves/s",
+                           "ms_per_step": s_ms, "attempts": s_att,
+                           "tflops": flops.solve_flops("tsit5", "lorenz", s_att) / (s_ms * 1e-3) / 1e12}
     clk = clocks.stop()
 
     # ---- e2e through the public API, host buffers, H2D + D2H inside the timed region ----
@@ -407,10 +426,7 @@ def run_b200(args) -> None:
             e2e_step()
         torch.cuda.synchronize()
         el = (time.perf_counter() - t0) / ke
-        if world > 1:
-            t = torch.tensor([el], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(el, dev)
         e2e = {"value": n * world / el, "unit": UNIT,
                "h2d_bytes_per_step": int(y0_h.numel() * 8 + rho_h.numel() * 8),
                "d2h_bytes_per_step": int(grad_h.numel() * 8 + 8),
@@ -423,6 +439,8 @@ def run_b200(args) -> None:
 
     # ---- roofline of the dominant kernel -------------------------------------------
     fp64_peak = probe_fp64_tflops(torch, stream)
+    for v in solve.values():
+        v["frac_of_fp64_peak"] = v["tflops"] / fp64_peak
     peaks = measured_peaks()
     f_fwd = flops.solve_flops("tsit5", "lorenz", att)
     f_adj = flops.adjoint_flops("tsit5", "lorenz", acc)
@@ -468,11 +486,275 @@ def run_b200(args) -> None:
                    "l2": "flushed between timed steps (record traffic also >> L2)"},
         "gpu_launches": 2 * args.steps,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-        "fwd_ms": fwd_avg, "adj_ms": adj_avg, "mixed": mixed,
+        "fwd_ms": fwd_avg, "adj_ms": adj_avg, "mixed": mixed, "solve": solve or None,
     }
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+# ------------------------------------------------------------------------------------
+# the other workloads of the path: one JSON line each (the default run is the headline)
+# ------------------------------------------------------------------------------------
+class Group:
+    """One homogeneous sub-batch: a method, a field and its inputs (numpy, host)."""
+
+    def __init__(self, name, method, field, y0, p, t1, rtol, atol, *, t1v=None, ts=None,
+                 dt0=None, cap=1024, loss="mean_sq", pilot_p=None):
+        self.name, self.method, self.field = name, method, field
+        self.y0, self.p, self.t1, self.rtol, self.atol = y0, p, t1, rtol, atol
+        self.t1v, self.ts, self.dt0, self.cap, self.loss = t1v, ts, dt0, cap, loss
+        self.pilot_p = pilot_p  # saveat target: the float64 solution at these parameters
+
+
+def workload_groups(name: str, n: int, seed_shift: int):
+    """Seeded inputs of each workload (numpy default_rng; seed + seed_shift per rank)."""
+    if name == "lv_2e22":
+        rng = np.random.default_rng(2 + seed_shift)
+        prm = rng.uniform(0.5, 1.5, (n, 4))            # [alpha, beta, gamma, delta]
+        y0 = rng.uniform(0.5, 2.0, (n, 2))
+        return [Group("lv", "tsit5", "lv", y0, prm, 20.0, 1e-6, 1e-8, cap=256)]
+    if name == "lorenz_2e22":
+        y0, rho = make_inputs(n, 3 + seed_shift)
+        return [Group("lorenz", "tsit5", "lorenz", y0, rho, 20.0, 1e-6, 1e-8, cap=1024)]
+    if name == "robertson_2e18":
+        rng = np.random.default_rng(4 + seed_shift)
+        k = np.array([0.04, 3e7, 1e4]) * 10.0 ** rng.uniform(-0.5, 0.5, (n, 3))
+        y0 = np.tile(np.array([1.0, 0.0, 0.0]), (n, 1))
+        return [Group("robertson", "rosenbrock23", "robertson", y0, k, 1e4, 1e-6, 1e-10,
+                      dt0=100.0, cap=1024, loss="last")]
+    if name == "vdp_uneven_saveat":
+        rng = np.random.default_rng(5 + seed_shift)
+        mu = 10.0 ** rng.uniform(-1.0, 2.0, n)
+        t1 = 10.0 ** rng.uniform(-1.0, math.log10(20.0), n)
+        y0 = rng.uniform(-2.0, 2.0, (n, 2))
+        mu_t = mu * (1.0 + 0.05 * np.random.default_rng(6 + seed_shift).normal(0.0, 1.0, n))
+        ts = t1[:, None] * np.linspace(0.0, 1.0, 64)[None, :]
+        out = []
+        for gname, method, sel in (("vdp_tsit5", "tsit5", mu < 10.0),
+                                   ("vdp_ros23", "rosenbrock23", mu >= 10.0)):
+            out.append(Group(gname, method, "vdp", y0[sel], mu[sel, None], float(t1[sel].max()),
+                             1e-6, 1e-9, t1v=t1[sel], ts=ts[sel],
+                             cap=1024 if method == "tsit5" else 8192, loss="mse",
+                             pilot_p=mu_t[sel, None]))
+        return out
+    raise ValueError(f"unknown workload {name!r}")
+
+
+WORKLOAD_N = {"lv_2e22": 1 << 22, "lorenz_2e22": 1 << 22, "robertson_2e18": 1 << 18,
+              "vdp_uneven_saveat": 1 << 20}
+
+
+def run_workload(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from gradsolve_b200 import engine, flops
+    from gradsolve_b200.fields import field_spec
+    from gradsolve_b200.sharding import max_over_ranks
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    n = args.n if args.n != N_DEFAULT else WORKLOAD_N[args.workload]
+    groups = workload_groups(args.workload, n, 1000 * rank)
+    n_tot = n * world
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    D = field_spec(groups[0].field).dim
+    for g in groups:
+        g.spec = field_spec(g.field)
+        g.y0_d = torch.tensor(g.y0, device=dev)
+        g.p_d = torch.tensor(g.p, device=dev)
+        g.t1v_d = None if g.t1v is None else torch.tensor(g.t1v, device=dev)
+        g.ts_d = None if g.ts is None else torch.tensor(g.ts, device=dev)
+        g.target = None
+        if g.pilot_p is not None:  # the float64 solution at the perturbed parameters
+            pt = torch.tensor(g.pilot_p, device=dev)
+            r = engine.forward_record(g.method, g.spec, g.y0_d, pt, t0=0.0, t1=g.t1,
+                                      t1v=g.t1v_d, rtol=g.rtol, atol=g.atol, dt0=g.dt0,
+                                      cap0=g.cap, checkpoint="auto")
+            engine.raise_on_failed(r, 100000, g.t1)
+            g.target = engine.replay_saveat(r, g.y0_d, pt, g.ts_d, write_ckpt=False)[1]
+            del r
+            torch.cuda.empty_cache()
+        g.ws = None
+
+    def cotangent(g, r, prec, ys=None):
+        if g.loss == "mean_sq":
+            return (2.0 / (n_tot * D)) * r.y_final
+        if g.loss == "last":
+            yb = torch.zeros_like(r.y_final)
+            yb[:, 2] = 1.0
+            return yb
+        return (2.0 / (n_tot * ys.shape[1] * D)) * (ys - g.target)
+
+    def group_step(g, prec, r=None):
+        """forward (record) + loss cotangent + reverse pass; with ``r`` given, the record is
+        replayed instead (same mesh) in precision ``prec``."""
+        if r is None:
+            r = engine.forward_record(g.method, g.spec, g.y0_d, g.p_d, t0=0.0, t1=g.t1,
+                                      t1v=g.t1v_d, rtol=g.rtol, atol=g.atol, dt0=g.dt0,
+                                      max_steps=100000, cap0=g.cap, checkpoint=args.checkpoint,
+                                      precision=prec, workspace=g.ws, schedule=args.schedule)
+            g.ws = r
+            replay_ck = False
+        else:
+            replay_ck = True
+        if g.ts_d is None:
+            if replay_ck:
+                engine.replay(r, g.y0_d, g.p_d, write_ckpt=True, precision=prec)
+            gy0, gp = engine.adjoint(r, g.p_d, cotangent(g, r, prec), want_y0=False,
+                                     precision=prec, schedule=args.schedule)
+        else:
+            _yf, ys = engine.replay_saveat(r, g.y0_d, g.p_d, g.ts_d, write_ckpt=replay_ck,
+                                           precision=prec)
+            gy0, gp = engine.adjoint_saveat(r, g.p_d, g.ts_d, cotangent(g, r, prec, ys),
+                                            want_y0=False, precision=prec)
+        return r, gp
+
+    def prec_of(g, variant):
+        return "mixed" if (variant == "mixed" and g.method == "tsit5") else "float64"
+
+    def time_variant(variant):
+        for _ in range(args.warmup):
+            for g in groups:
+                group_step(g, prec_of(g, variant))
+        torch.cuda.synchronize()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(len(groups) + 1)]
+               for _ in range(args.steps)]
+        outs = None
+        for e in evs:
+            flush.zero_()
+            e[0].record(stream)
+            outs = []
+            for k, g in enumerate(groups):
+                outs.append(group_step(g, prec_of(g, variant)))
+                e[k + 1].record(stream)
+        torch.cuda.synchronize()
+        per_group = [float(np.mean([e[k].elapsed_time(e[k + 1]) for e in evs]))
+                     for k in range(len(groups))]
+        whole = max_over_ranks(float(np.mean([e[0].elapsed_time(e[-1]) for e in evs])), dev)
+        return whole, per_group, outs
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, per_group, outs = time_variant("float64")
+    infos = []
+    for g, t_ms, (r, gp) in zip(groups, per_group, outs):
+        assert int((r.status != 0).sum().item()) == 0, f"{g.name}: solve failed"
+        att = int((r.n_acc.to(torch.int64) + r.n_rej.to(torch.int64)).sum().item())
+        acc = int(r.n_acc.to(torch.int64).sum().item())
+        fl = flops.gradient_flops(g.method, g.field, att, acc)
+        infos.append({"group": g.name, "method": g.method, "field": g.field, "n": r.n,
+                      "attempts": att, "accepted": acc, "record_len_max": int(r.n_acc.max()),
+                      "checkpoint_every": r.ckpt_every, "ms": t_ms,
+                      "tflops": fl / (t_ms * 1e-3) / 1e12,
+                      "saveat_points": None if g.ts is None else int(g.ts.shape[1])})
+        g.gp64 = gp.clone()
+        g.r64 = r
+
+    # parity at scale: 32 sampled rows of each group against the oracle on the GPU's own mesh
+    from oracle import oracle as O
+    O.build()
+    parity = {}
+    for g, info in zip(groups, infos):
+        r = g.r64
+        m = min(32, r.n)
+        idx = np.sort(np.random.default_rng(1).choice(r.n, m, replace=False))
+        dts = r.dts_rows(torch.tensor(idx, device=dev)).cpu().numpy()
+        y0s, ps = g.y0[idx], g.p[idx]
+        if g.ts is None:
+            ybar = cotangent(g, r, "float64")[torch.tensor(idx, device=dev)].cpu().numpy()
+            _oy, op = O.replay_vjp(g.method, g.field, y0s, ps, dts, ybar)
+        else:
+            _yf, ys = engine.replay_saveat(r, g.y0_d, g.p_d, g.ts_d, write_ckpt=False)
+            ysbar = cotangent(g, r, "float64", ys)[torch.tensor(idx, device=dev)].cpu().numpy()
+            _oy, op = O.replay_saveat_vjp(g.method, g.field, y0s, ps, dts, g.ts[idx], ysbar)
+        got = g.gp64[torch.tensor(idx, device=dev)].cpu().numpy()
+        den = np.maximum(np.abs(op).max(axis=1), 1e-300)
+        q = np.abs(got - op).max(axis=1) / den
+        parity[g.name] = {"rows": m, "grad_rowrel_max": float(q.max()),
+                          "within_1e-9": bool(q.max() <= 1e-9)}
+
+    outs = r = gp = None  # the float64 records stay reachable through g.r64 only
+    mixed = None
+    if not args.no_mixed and any(g.method == "tsit5" for g in groups):
+        same = {}
+        for g in groups:
+            if g.method != "tsit5":
+                continue
+            _r, gp_sm = group_step(g, "mixed", r=g.r64)
+            same[g.name] = _grad_err(gp_sm, g.gp64)
+        for g in groups:  # release the float64 record before the mixed one is allocated
+            g.r64 = g.ws = None
+        torch.cuda.empty_cache()
+        m_ms, m_groups, m_outs = time_variant("mixed")
+        own = {}
+        for g, (r, gp) in zip(groups, m_outs):
+            if g.method == "tsit5":
+                own[g.name] = _grad_err(gp, g.gp64)
+        mixed = {"value": n_tot / (m_ms * 1e-3), "ms_per_step": m_ms, "group_ms": m_groups,
+                 "speedup_vs_f64": ms / m_ms, "grad_rel_err_same_mesh": same,
+                 "grad_rel_err_own_mesh": own,
+                 "note": "float32 stage increments on the tsit5 groups; rosenbrock23 groups "
+                         "stay float64"}
+    clk = clocks.stop()
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    fp64_peak = probe_fp64_tflops(torch, stream)
+    for info in infos:
+        info["frac_of_fp64_peak"] = info["tflops"] / fp64_peak
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        cpu = cpu_workload_rate(groups, args.cpu_seconds)
+    line = {
+        "workload": args.workload, "metric": "trajectory grads/s (fwd+adjoint)",
+        "value": n_tot / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "dtype": "f64", "data": "synthetic (seeded numpy default_rng)", "groups": infos,
+        "fp64_peak_tflops": fp64_peak, "oracle_parity_sample": parity, "mixed": mixed,
+        "cpu_baseline": cpu, "clocks": clk,
+        "config": {"n_per_gpu": n, "checkpoint_policy": str(args.checkpoint),
+                   "schedule": args.schedule, "l2": "flushed between timed steps"},
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def cpu_workload_rate(groups, target_s: float) -> dict:
+    """The oracle port's record + replay adjoint on a bounded sample of each group, all host
+    cores (saveat re-steps are not included: a lower bound of the CPU cost there)."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    total_t, total_n = 0.0, 0
+    for g in groups:
+        def run(m):
+            t = time.perf_counter()
+            rr = O.record(g.method, g.field, g.y0[:m], g.p[:m], 0.0, g.t1, g.rtol, g.atol,
+                          dt0=g.dt0, cap=16384, nthreads=cores,
+                          t1v=None if g.t1v is None else g.t1v[:m])
+            O.replay_vjp(g.method, g.field, g.y0[:m], g.p[:m], rr["dts"],
+                         np.ones_like(rr["y_final"]), nthreads=cores)
+            return time.perf_counter() - t
+        m = min(len(g.y0), cores * 8)
+        dt = run(m)
+        share = target_s / len(groups)
+        m2 = int(min(len(g.y0), max(m, m * share / max(dt, 1e-3))))
+        total_t += run(m2)
+        total_n += m2
+    return {"value": total_n / total_t, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{total_n} trajectories (first rows of each group), C restatement of the "
+                      f"record + replay adjoint, {cores} host threads, {total_t:.1f} s"}
+
 
 
 def main():
@@ -488,12 +770,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--schedule", default="auto", choices=["auto", "static", "refill", "strided"])
+    ap.add_argument("--workload", default="lorenz_2e20",
+                    choices=["lorenz_2e20"] + sorted(WORKLOAD_N))
     args = ap.parse_args()
     if args.checkpoint not in ("sqrt", "all", "auto"):
         args.checkpoint = int(args.checkpoint)
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload != "lorenz_2e20":
+        run_workload(args)
     else:
         run_b200(args)
 

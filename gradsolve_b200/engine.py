@@ -143,6 +143,18 @@ class Record:
                    "gs_record_to_padded")
         return out
 
+    def dts_rows(self, rows: torch.Tensor, S: Optional[int] = None) -> torch.Tensor:
+        """Padded dts of the selected trajectories only (a torch gather of the
+        chunk-interleaved record: step s of trajectory j sits at ((s//4)*n + j)*4 + s%4)."""
+        rows = rows.to(device=self.rec.device, dtype=torch.int64)
+        na = self.n_acc[rows].to(torch.int64)
+        if S is None:
+            S = int(na.max().item()) if rows.numel() else 0
+        s = torch.arange(S, device=rows.device, dtype=torch.int64)
+        idx = ((s // 4)[None, :] * self.n + rows[:, None]) * 4 + (s % 4)[None, :]
+        out = self.rec[idx.clamp_max(self.rec.numel() - 1)]
+        return torch.where(s[None, :] < na[:, None], out, torch.zeros_like(out))
+
 
 def _alloc_record(n: int, cap: int, dim: int, K: int, device) -> tuple:
     L = _lib.lib()

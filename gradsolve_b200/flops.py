@@ -16,6 +16,7 @@ COUNTS = {
     ("tsit5", "lv"): dict(F_att=193, F_step=144, F_vjp=204),
     ("tsit5", "vdp"): dict(F_att=175, F_step=126, F_vjp=186),
     ("rosenbrock23", "robertson"): dict(F_att=205, F_step=115, F_vjp=191),
+    ("rosenbrock23", "vdp"): dict(F_att=108, F_step=54, F_vjp=97),
 }
 
 

@@ -134,6 +134,22 @@ def jcg_rob(y, p, G):
     return gy, gp
 
 
+def jac_vdp(y, p):
+    x, v = y
+    mu = p[0]
+    return [[0.0, 1.0], [mu * (-2.0 * x * v - 1.0), mu * (1.0 - x * x)]]
+
+
+def jcg_vdp(y, p, G):
+    x, v = y
+    mu = p[0]
+    gy = [G[1][0] * mu * (-2.0 * v) + G[1][1] * mu * (-2.0 * x), G[1][0] * mu * (-2.0 * x)]
+    gp = [G[1][0] * (-2.0 * x * v - 1.0) + G[1][1] * (1.0 - x * x)]
+    return gy, gp
+
+
+STIFF = {"robertson": (jac_rob, jcg_rob, [0.04, 3e7, 1e4]), "vdp": (jac_vdp, jcg_vdp, [50.0])}
+
 FIELDS = {"lorenz": (f_lorenz, vjp_lorenz, 3, 1), "lv": (f_lv, vjp_lv, 2, 4),
           "vdp": (f_vdp, vjp_vdp, 2, 1), "robertson": (f_rob, vjp_rob, 3, 3)}
 
@@ -235,11 +251,12 @@ def _lu_factor_count(W, D):
 
 def count_ros23(field="robertson"):
     f, vjp, D, P = FIELDS[field]
-    y, p, h = _y(D), [Num(0.04), Num(3e7), Num(1e4)], Num(0.01)
+    jac, jcg, pv = STIFF[field]
+    y, p, h = _y(D), [Num(v) for v in pv], Num(0.01)
     d, e32 = 0.2928932188134525, 7.414213562373095
 
     def core(y, p, h):
-        J = [[v if isinstance(v, Num) else Num(v) for v in row] for row in jac_rob(y, p)]
+        J = [[v if isinstance(v, Num) else Num(v) for v in row] for row in jac(y, p)]
         dh = h * (-d)                                   # W = I - d h J: 1 + 9 + 3 ops
         W = [[dh * J[i][c] for c in range(D)] for i in range(D)]
         for i in range(D):
@@ -293,7 +310,7 @@ def count_ros23(field="robertson"):
     G = [[G[i][c] + scale * (r1b[i] * k1[c]) for c in range(D)] for i in range(D)]
     gyb, _ = vjp(y, p, r1b)
     yb = [yb[i] + gyb[i] for i in range(D)]
-    jy, _ = jcg_rob(y, p, G)
+    jy, _ = jcg(y, p, G)
     yb = [yb[i] + jy[i] for i in range(D)]
     f_vjp = Counter.n
     return dict(F_att=f_att, F_step=f_step, F_vjp=f_vjp)
@@ -302,6 +319,7 @@ def count_ros23(field="robertson"):
 def all_counts():
     out = {("tsit5", k): count_tsit5(k) for k in ("lorenz", "lv", "vdp")}
     out[("rosenbrock23", "robertson")] = count_ros23("robertson")
+    out[("rosenbrock23", "vdp")] = count_ros23("vdp")
     return out
 
 

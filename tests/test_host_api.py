@@ -88,3 +88,29 @@ def test_checkpoint_policy(gslib):
     assert choose_ckpt_every("auto", 3, 1 << 20, 700, budget_bytes=10**9) == 32
     with pytest.raises(ValueError):
         choose_ckpt_every(65, 3, 10, 700, None)
+
+
+def test_record_row_gather_follows_the_chunked_layout():
+    """Record.dts_rows reads step s of trajectory j at ((s//4)*n + j)*4 + s%4 and zero-pads
+    past n_acc (the reference's padded layout, for a subset of rows)."""
+    import torch
+
+    from gradsolve_b200.engine import Record
+    n, cap = 5, 9
+    n_acc = np.array([0, 3, 9, 4, 7], np.int32)
+    rec = np.full(((cap + 3) // 4) * n * 4, -1.0)
+    for j in range(n):
+        for s in range(n_acc[j]):
+            rec[((s // 4) * n + j) * 4 + s % 4] = 100 * j + s + 1
+    z = torch.zeros(n, dtype=torch.int32)
+    r = Record("tsit5", field_spec("lorenz"), n, 0.0, cap, 1, torch.tensor(rec),
+               torch.zeros(1), torch.zeros(n, 3, dtype=torch.float64),
+               torch.tensor(n_acc), z, z)
+    rows = torch.tensor([4, 0, 2])
+    got = r.dts_rows(rows).numpy()
+    assert got.shape == (3, 9)
+    for k, j in enumerate([4, 0, 2]):
+        want = np.zeros(9)
+        want[: n_acc[j]] = 100 * j + np.arange(n_acc[j]) + 1
+        np.testing.assert_array_equal(got[k], want)
+    assert r.dts_rows(rows, S=12).shape == (3, 12)

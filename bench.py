@@ -319,7 +319,7 @@ def run_b200(args) -> None:
             if events:
                 events[2].record(stream)
             _gy0, gp = engine.adjoint(r, rho, ybar, want_y0=False, precision=precision,
-                                      schedule=args.schedule)
+                                      schedule=args.schedule, variant=args.adjoint_variant)
             if events:
                 events[3].record(stream)
             return r, gp
@@ -610,7 +610,8 @@ def run_workload(args) -> None:
             if replay_ck:
                 engine.replay(r, g.y0_d, g.p_d, write_ckpt=True, precision=prec)
             gy0, gp = engine.adjoint(r, g.p_d, cotangent(g, r, prec), want_y0=False,
-                                     precision=prec, schedule=args.schedule)
+                                     precision=prec, schedule=args.schedule,
+                                     variant=args.adjoint_variant)
         else:
             _yf, ys = engine.replay_saveat(r, g.y0_d, g.p_d, g.ts_d, write_ckpt=replay_ck,
                                            precision=prec)
@@ -772,6 +773,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--schedule", default="auto", choices=["auto", "static", "refill", "strided"])
+    ap.add_argument("--adjoint-variant", default="auto", choices=["auto", "stages", "recompute"])
     ap.add_argument("--workload", default="lorenz_2e20",
                     choices=["lorenz_2e20"] + sorted(WORKLOAD_N))
     args = ap.parse_args()

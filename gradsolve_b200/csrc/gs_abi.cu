@@ -96,9 +96,11 @@ struct SegCfg {
   size_t smem;
 };
 
+constexpr size_t kSegBudget = 200u * 1024u;
+
 SegCfg seg_cfg(int K, int W) {
   const size_t per_thread = (size_t)K * (size_t)W * sizeof(double);
-  const size_t budget = 200u * 1024u;
+  const size_t budget = kSegBudget;
   unsigned block = kBlock;
   while (block > 32 && per_thread * block > budget) block /= 2;
   return {block, per_thread * block};
@@ -220,10 +222,19 @@ int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed) {
 }
 template <class F>
 int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool mixed,
-                         int sched) {
+                         int sched, int variant) {
   if (sched == GS_SCHED_STATIC) {
-    const SegCfg c = seg_cfg(a.ck_every, F::D);
     int rc;
+    // the stage-keeping variant needs 6*D doubles per step of the segment; where that does not
+    // fit one warp's worth of shared memory (large K and D) the stages are recomputed instead
+    const SegCfg cs = seg_cfg(a.ck_every, 6 * F::D);
+    if (!mixed && variant != GS_ADJ_RECOMPUTE && cs.smem <= kSegBudget) {
+      const SegCfg c = cs;
+      if ((rc = allow_smem(gs::tsit5_adjoint_stages_kernel<F>, c.smem))) return rc;
+      gs::tsit5_adjoint_stages_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+      return cuda_check("tsit5_adjoint_stages_kernel");
+    }
+    const SegCfg c = seg_cfg(a.ck_every, F::D);
     if (mixed) {
       if ((rc = allow_smem(gs::tsit5_mixed_adjoint_kernel<F>, c.smem))) return rc;
       gs::tsit5_mixed_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
@@ -450,7 +461,7 @@ int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, con
   if (n == 0) return GS_OK;
   gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp};
   GS_TSIT5_DISPATCH(field, launch_tsit5_adjoint, a, cap, (cudaStream_t)stream,
-                    prec == GS_PREC_MIXED, adjoint_schedule(precision))
+                    prec == GS_PREC_MIXED, adjoint_schedule(precision), precision & GS_ADJ_MASK)
 }
 
 int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,

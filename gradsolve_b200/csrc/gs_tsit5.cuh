@@ -209,36 +209,65 @@ __device__ __forceinline__ void tsit5_replay_step(double* y, const double* p, do
   for (int i = 0; i < D; ++i) y[i] = yn[i];
 }
 
-// Reverse of one replay step at (y, dt): lam <- (dy'/dy)^T lam, gp += (dy'/dp)^T lam.
-// Stage 7 carries weight B7 == 0, so its cotangent is exactly zero and it is skipped.
+// Stage inputs s2..s6 of one step at (y, dt) -- the expressions of tsit5_k2_to_k6 -- and,
+// with kNext, the step's result (tsit5_y5), so a pass that keeps the stages for the reverse
+// sweep produces the same states as tsit5_replay_step.
 template <class F>
-__device__ __forceinline__ void tsit5_step_vjp(const double* y, const double* p, double dt,
-                                               double* lam, double* gp) {
+struct StageStates {
+  static constexpr int D = F::D;
+  double s2[D], s3[D], s4[D], s5[D], s6[D];
+  template <int M>
+  __device__ __forceinline__ void get(double* out) const {
+    const double* src = M == 2 ? s2 : M == 3 ? s3 : M == 4 ? s4 : M == 5 ? s5 : s6;
+#pragma unroll
+    for (int i = 0; i < D; ++i) out[i] = src[i];
+  }
+};
+
+template <class F, bool kNext>
+__device__ __forceinline__ void tsit5_stage_states(const double* y, const double* p, double dt,
+                                                   StageStates<F>& S, double* ynext) {
   constexpr int D = F::D;
   using T = Tsit5;
-  double k1[D], s2[D], s3[D], s4[D], s5[D], s6[D];
-  {
-    double k2[D], k3[D], k4[D], k5[D];
-    F::rhs(y, p, k1);
+  double k1[D], k2[D], k3[D], k4[D], k5[D];
+  F::rhs(y, p, k1);
 #pragma unroll
-    for (int i = 0; i < D; ++i) s2[i] = y[i] + dt * (T::A21 * k1[i]);
-    F::rhs(s2, p, k2);
+  for (int i = 0; i < D; ++i) S.s2[i] = y[i] + dt * (T::A21 * k1[i]);
+  F::rhs(S.s2, p, k2);
 #pragma unroll
-    for (int i = 0; i < D; ++i) s3[i] = y[i] + dt * (T::A31 * k1[i] + T::A32 * k2[i]);
-    F::rhs(s3, p, k3);
+  for (int i = 0; i < D; ++i) S.s3[i] = y[i] + dt * (T::A31 * k1[i] + T::A32 * k2[i]);
+  F::rhs(S.s3, p, k3);
 #pragma unroll
-    for (int i = 0; i < D; ++i)
-      s4[i] = y[i] + dt * (T::A41 * k1[i] + T::A42 * k2[i] + T::A43 * k3[i]);
-    F::rhs(s4, p, k4);
+  for (int i = 0; i < D; ++i)
+    S.s4[i] = y[i] + dt * (T::A41 * k1[i] + T::A42 * k2[i] + T::A43 * k3[i]);
+  F::rhs(S.s4, p, k4);
 #pragma unroll
-    for (int i = 0; i < D; ++i)
-      s5[i] = y[i] + dt * (T::A51 * k1[i] + T::A52 * k2[i] + T::A53 * k3[i] + T::A54 * k4[i]);
-    F::rhs(s5, p, k5);
+  for (int i = 0; i < D; ++i)
+    S.s5[i] = y[i] + dt * (T::A51 * k1[i] + T::A52 * k2[i] + T::A53 * k3[i] + T::A54 * k4[i]);
+  F::rhs(S.s5, p, k5);
 #pragma unroll
-    for (int i = 0; i < D; ++i)
-      s6[i] = y[i] + dt * (T::A61 * k1[i] + T::A62 * k2[i] + T::A63 * k3[i] + T::A64 * k4[i] +
+  for (int i = 0; i < D; ++i)
+    S.s6[i] = y[i] + dt * (T::A61 * k1[i] + T::A62 * k2[i] + T::A63 * k3[i] + T::A64 * k4[i] +
                            T::A65 * k5[i]);
+  if (kNext) {
+    double k6[D];
+    F::rhs(S.s6, p, k6);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      ynext[i] = y[i] + dt * (T::B1 * k1[i] + T::B2 * k2[i] + T::B3 * k3[i] + T::B4 * k4[i] +
+                              T::B5 * k5[i] + T::B6 * k6[i]);
   }
+}
+
+// Reverse of one replay step at (y, dt) given its stage inputs (Src::get<M> yields s_M):
+// lam <- (dy'/dy)^T lam, gp += (dy'/dp)^T lam.  Stage 7 carries weight B7 == 0, so its
+// cotangent is exactly zero and it is skipped.
+template <class F, class Src>
+__device__ __forceinline__ void tsit5_vjp_core(const double* y, const Src& src, const double* p,
+                                               double dt, double* lam, double* gp) {
+  constexpr int D = F::D;
+  using T = Tsit5;
+  double st[D];
   double g[D], kb1[D], kb2[D], kb3[D], kb4[D], kb5[D], kb6[D], sb[D], yb[D];
 #pragma unroll
   for (int i = 0; i < D; ++i) {
@@ -252,9 +281,10 @@ __device__ __forceinline__ void tsit5_step_vjp(const double* y, const double* p,
     kb6[i] = T::B6 * g[i];
   }
   // stage 6
+  src.template get<6>(st);
 #pragma unroll
   for (int i = 0; i < D; ++i) sb[i] = 0.0;
-  F::vjp(s6, p, kb6, sb, gp);
+  F::vjp(st, p, kb6, sb, gp);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     yb[i] += sb[i];
@@ -266,9 +296,10 @@ __device__ __forceinline__ void tsit5_step_vjp(const double* y, const double* p,
     kb5[i] += T::A65 * u;
   }
   // stage 5
+  src.template get<5>(st);
 #pragma unroll
   for (int i = 0; i < D; ++i) sb[i] = 0.0;
-  F::vjp(s5, p, kb5, sb, gp);
+  F::vjp(st, p, kb5, sb, gp);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     yb[i] += sb[i];
@@ -279,9 +310,10 @@ __device__ __forceinline__ void tsit5_step_vjp(const double* y, const double* p,
     kb4[i] += T::A54 * u;
   }
   // stage 4
+  src.template get<4>(st);
 #pragma unroll
   for (int i = 0; i < D; ++i) sb[i] = 0.0;
-  F::vjp(s4, p, kb4, sb, gp);
+  F::vjp(st, p, kb4, sb, gp);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     yb[i] += sb[i];
@@ -291,9 +323,10 @@ __device__ __forceinline__ void tsit5_step_vjp(const double* y, const double* p,
     kb3[i] += T::A43 * u;
   }
   // stage 3
+  src.template get<3>(st);
 #pragma unroll
   for (int i = 0; i < D; ++i) sb[i] = 0.0;
-  F::vjp(s3, p, kb3, sb, gp);
+  F::vjp(st, p, kb3, sb, gp);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     yb[i] += sb[i];
@@ -302,9 +335,10 @@ __device__ __forceinline__ void tsit5_step_vjp(const double* y, const double* p,
     kb2[i] += T::A32 * u;
   }
   // stage 2
+  src.template get<2>(st);
 #pragma unroll
   for (int i = 0; i < D; ++i) sb[i] = 0.0;
-  F::vjp(s2, p, kb2, sb, gp);
+  F::vjp(st, p, kb2, sb, gp);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     yb[i] += sb[i];
@@ -314,6 +348,15 @@ __device__ __forceinline__ void tsit5_step_vjp(const double* y, const double* p,
   F::vjp(y, p, kb1, yb, gp);
 #pragma unroll
   for (int i = 0; i < D; ++i) lam[i] = yb[i];
+}
+
+// Reverse of one replay step, recomputing its stages from y.
+template <class F>
+__device__ __forceinline__ void tsit5_step_vjp(const double* y, const double* p, double dt,
+                                               double* lam, double* gp) {
+  StageStates<F> S;
+  tsit5_stage_states<F, false>(y, p, dt, S, nullptr);
+  tsit5_vjp_core<F>(y, S, p, dt, lam, gp);
 }
 
 // --- kernel arguments -----------------------------------------------------------------
@@ -550,6 +593,92 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a)
 #pragma unroll
         for (int i = 0; i < D; ++i) ys[i] = seg.at(q, i);
         tsit5_step_vjp<F>(ys, p, dt, lam, gp);
+      }
+    }
+  }
+  if (a.gy0) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) a.gy0[j * D + i] = lam[i];
+  }
+  if (a.gp) {
+#pragma unroll
+    for (int i = 0; i < P; ++i) a.gp[j * P + i] = gp[i];
+  }
+}
+
+// --- reverse-replay adjoint that keeps the stage inputs -----------------------------------
+// The segment's forward pass stores, per step, y and the stage inputs s2..s6 (6*D doubles) in
+// the shared-memory segment buffer, so the reverse sweep runs the step VJPs without
+// recomputing the stages: one stage evaluation per step instead of two, for 6x the buffer.
+// Same states (tsit5_stage_states<F, true> evaluates tsit5_replay_step's expressions) and the
+// same VJP code (tsit5_vjp_core) as tsit5_adjoint_kernel.
+template <class F>
+struct SegStages {
+  static constexpr int D = F::D;
+  const double* base;
+  int stride, q;
+  template <int M>
+  __device__ __forceinline__ void get(double* out) const {
+#pragma unroll
+    for (int i = 0; i < D; ++i) out[i] = base[(q * 6 * D + (M - 1) * D + i) * stride];
+  }
+};
+
+template <class F>
+__global__ void __launch_bounds__(128) tsit5_adjoint_stages_kernel(const AdjointArgs a) {
+  constexpr int D = F::D, P = F::P;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  double p[P], lam[D], gp[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    p[i] = a.p[j * P + i];
+    gp[i] = 0.0;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
+  const int na = a.n_acc[j];
+  const int K = a.ck_every;
+  const int nseg = (na + K - 1) / K;
+  SegBuf<6 * D> seg;
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int start = sg * K;
+    double y[D];
+    load_ckpt<D>(a.ckpt, a.n, j, sg, y);
+    for (int q = 0; q < K; ++q) {
+      const int s = start + q;
+      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+#pragma unroll
+      for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
+      if (dt != 0.0) {
+        StageStates<F> S;
+        if (q + 1 < K) {
+          double yn[D];
+          tsit5_stage_states<F, true>(y, p, dt, S, yn);
+#pragma unroll
+          for (int i = 0; i < D; ++i) y[i] = yn[i];
+        } else {
+          tsit5_stage_states<F, false>(y, p, dt, S, nullptr);
+        }
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          seg.at(q, D + i) = S.s2[i];
+          seg.at(q, 2 * D + i) = S.s3[i];
+          seg.at(q, 3 * D + i) = S.s4[i];
+          seg.at(q, 4 * D + i) = S.s5[i];
+          seg.at(q, 5 * D + i) = S.s6[i];
+        }
+      }
+    }
+    for (int q = K - 1; q >= 0; --q) {
+      const int s = start + q;
+      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      if (dt != 0.0) {
+        double ys[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) ys[i] = seg.at(q, i);
+        const SegStages<F> src{seg.base, seg.stride, q};
+        tsit5_vjp_core<F>(ys, src, p, dt, lam, gp);
       }
     }
   }

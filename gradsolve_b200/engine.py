@@ -76,12 +76,13 @@ def choose_ckpt_every(policy, dim: int, n: int, cap: int, budget_bytes: Optional
 
 
 # ---- checkpoint-interval autotuner ---------------------------------------------------------
-# The reverse pass keeps each thread's K segment states in shared memory, so K trades
-# recomputation (none at K = 1) against occupancy (the buffer is K*D*8 bytes per thread).
+# The reverse pass keeps each thread's K segment states (and, for Tsit5 float64, their stage
+# inputs) in shared memory, so K trades recomputation and checkpoint traffic (none and the
+# most at K = 1) against occupancy (the buffer grows with K).
 # The best K depends on the field, the method and the precision; it is measured once per
 # process on a sample of the caller's own trajectories and cached.
 _TUNED: dict = {}
-TUNE_CANDIDATES = (4, 6, 8, 12, 16)
+TUNE_CANDIDATES = (2, 3, 4, 6, 8, 12, 16)
 
 
 def tuned_ckpt_every(method: str, spec: FieldSpec, precision: str) -> Optional[int]:
@@ -93,19 +94,22 @@ def autotune_ckpt_every(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch
                         t1v: Optional[torch.Tensor] = None, max_steps: int = 100000,
                         precision: str = "float64", sample: int = 1 << 17,
                         candidates=TUNE_CANDIDATES) -> int:
-    """Time the reverse pass for each candidate K on up to ``sample`` trajectories (about two
-    waves of the GPU) and cache the fastest."""
+    """Time forward + reverse pass for each candidate K on up to ``sample`` trajectories
+    (about two waves of the GPU) and cache the fastest."""
     m = min(y0.shape[0], sample)
     ys, ps = y0[:m].contiguous(), p[:m].contiguous()
     tv = None if t1v is None else t1v[:m].contiguous()
     best, best_ms = None, float("inf")
     for K in candidates:
-        r = forward_record(method, spec, ys, ps, t0=t0, t1=t1, t1v=tv, rtol=rtol, atol=atol,
-                           max_steps=max_steps, checkpoint=K, precision=precision)
+        kw = dict(t0=t0, t1=t1, t1v=tv, rtol=rtol, atol=atol, max_steps=max_steps,
+                  checkpoint=K, precision=precision)
+        r = forward_record(method, spec, ys, ps, **kw)
         ybar = torch.ones_like(r.y_final)
         adjoint(r, ps, ybar, precision=precision)  # warm
+        # forward (checkpoint writes grow as K shrinks) + reverse pass, buffers reused
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
+        r = forward_record(method, spec, ys, ps, workspace=r, **kw)
         adjoint(r, ps, ybar, precision=precision)
         e1.record()
         e1.synchronize()
@@ -258,11 +262,18 @@ def replay(r: Record, y0: torch.Tensor, p: torch.Tensor, *, write_ckpt: bool = T
     return yf
 
 
+_ADJ = {"auto": 0x000, "recompute": 0x400, "stages": 0x800}
+
+
 def adjoint(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
-            want_p: bool = True, precision: str = "float64", schedule: str = "auto"):
+            want_p: bool = True, precision: str = "float64", schedule: str = "auto",
+            variant: str = "auto"):
     """(dL/dy0, dL/dp) for cotangent ybar = dL/dy_final, using the record's checkpoints.
     ``schedule="auto"`` refills lanes from a work counter when the record came from an
-    uneven batch (per-trajectory end times), else runs one thread per trajectory."""
+    uneven batch (per-trajectory end times), else runs one thread per trajectory.
+    ``variant`` (Tsit5, float64, one thread per trajectory): "stages" keeps each step's stage
+    inputs from the segment's forward pass, "recompute" re-evaluates them in the reverse
+    sweep; "auto" is "stages"."""
     L = _lib.lib()
     fn = L.gs_tsit5_adjoint if r.method == METHOD_TSIT5 else L.gs_ros23_adjoint
     gy0 = torch.empty((r.n, r.spec.dim), dtype=torch.float64, device=p.device) if want_y0 else None
@@ -270,7 +281,8 @@ def adjoint(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = T
     ybar = ybar.contiguous()
     if schedule == "auto" and r.uneven:
         schedule = "refill"
-    _lib.check(fn(r.spec.code, _PREC[precision] | _SCHED[schedule], r.n, _ptr(p), _ptr(r.rec),
+    flags = _PREC[precision] | _SCHED[schedule] | (_ADJ[variant] if fn is L.gs_tsit5_adjoint else 0)
+    _lib.check(fn(r.spec.code, flags, r.n, _ptr(p), _ptr(r.rec),
                   _ptr(r.n_acc),
                   max(r.cap, 1), _ptr(r.ckpt), r.ckpt_every, _ptr(ybar), _ptr(gy0), _ptr(gp),
                   _stream()), fn.__name__)

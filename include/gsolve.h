@@ -64,6 +64,16 @@ extern "C" {
 #define GS_SCHED_STRIDED 0x300
 #define GS_SCHED_MASK 0x300
 
+/* Reverse-pass variant flags, OR-ed into the precision argument of gs_tsit5_adjoint (float64,
+ * one thread per trajectory).  RECOMPUTE: the reverse sweep re-evaluates each step's stages
+ * from the segment's states.  STAGES: the segment's forward pass keeps the stage inputs in
+ * shared memory (6x the segment buffer), so each step's stages are evaluated once.  AUTO (0):
+ * STAGES. */
+#define GS_ADJ_AUTO 0x000
+#define GS_ADJ_RECOMPUTE 0x400
+#define GS_ADJ_STAGES 0x800
+#define GS_ADJ_MASK 0xC00
+
 /* per-trajectory status values written to status[] */
 #define GS_TRAJ_OK 0          /* reached t1 */
 #define GS_TRAJ_MAX_STEPS 1   /* max_steps attempts exhausted (or non-finite error) */

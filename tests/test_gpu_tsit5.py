@@ -282,6 +282,9 @@ def test_schedules_give_identical_results(gslib, cuda, precision):
 
 
 def test_schedules_rosenbrock(gslib, cuda):
+    """Rosenbrock23 lanes: the persistent kernel evaluates the same expressions as the
+    one-thread-per-trajectory kernel, but the compiler contracts multiply-adds differently
+    in the two kernels, so results agree to rounding (counts exactly), not bit for bit."""
     from gradsolve_b200 import engine
     from gradsolve_b200.fields import field_spec
     g = load_golden("robertson_stiff")
@@ -294,6 +297,29 @@ def test_schedules_rosenbrock(gslib, cuda):
                                   atol=1e-10, max_steps=50000, checkpoint=8, schedule=sched)
         gy0, gp = engine.adjoint(r, p, torch.ones_like(r.y_final), schedule=sched)
         torch.cuda.synchronize()
-        outs[sched] = [r.y_final.cpu(), r.n_acc.cpu(), gy0.cpu(), gp.cpu()]
-    for a, b in zip(outs["refill"], outs["static"]):
-        assert torch.equal(a, b)
+        outs[sched] = [r.n_acc.cpu(), r.y_final.cpu(), gy0.cpu(), gp.cpu()]
+    assert torch.equal(outs["refill"][0], outs["static"][0])
+    for a, b in zip(outs["refill"][1:], outs["static"][1:]):
+        a, b = a.numpy(), b.numpy()
+        den = np.maximum(np.abs(b).max(axis=1, keepdims=True), 1e-300)
+        assert float((np.abs(a - b) / den).max()) <= 1e-10
+
+
+@pytest.mark.parametrize("case,field", CASES)
+def test_adjoint_variants_agree(gslib, cuda, case, field):
+    """The reverse pass that keeps each step's stage inputs from the segment's forward pass
+    and the one that recomputes them evaluate the same expressions: the gradients agree to
+    rounding (bitwise where the compiler contracts both the same way).  K = 64 exceeds the
+    stage buffer's shared memory for D = 3 and exercises the fallback to recomputation."""
+    from gradsolve_b200 import engine
+    g = load_golden(case)
+    for K in (1, 4, 7, 64):
+        spec, y0, p, r = _record(gslib, cuda, field, g, checkpoint=K)
+        ybar = 2.0 * r.y_final
+        a = engine.adjoint(r, p, ybar, variant="stages")
+        b = engine.adjoint(r, p, ybar, variant="recompute")
+        torch.cuda.synchronize()
+        for x, y in zip(a, b):
+            x, y = x.cpu().numpy(), y.cpu().numpy()
+            den = np.maximum(np.abs(y).max(axis=1, keepdims=True), 1e-300)
+            assert float((np.abs(x - y) / den).max()) <= 1e-13, (case, K)

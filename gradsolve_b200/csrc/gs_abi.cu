@@ -228,7 +228,7 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
     // the stage-keeping variant needs 6*D doubles per step of the segment; where that does not
     // fit one warp's worth of shared memory (large K and D) the stages are recomputed instead
     const SegCfg cs = seg_cfg(a.ck_every, 6 * F::D);
-    if (!mixed && variant != GS_ADJ_RECOMPUTE && cs.smem <= kSegBudget) {
+    if (!mixed && variant == GS_ADJ_STAGES && cs.smem <= kSegBudget) {
       const SegCfg c = cs;
       if ((rc = allow_smem(gs::tsit5_adjoint_stages_kernel<F>, c.smem))) return rc;
       gs::tsit5_adjoint_stages_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);

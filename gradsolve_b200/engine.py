@@ -273,7 +273,8 @@ def adjoint(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = T
     uneven batch (per-trajectory end times), else runs one thread per trajectory.
     ``variant`` (Tsit5, float64, one thread per trajectory): "stages" keeps each step's stage
     inputs from the segment's forward pass, "recompute" re-evaluates them in the reverse
-    sweep; "auto" is "stages"."""
+    sweep; "auto" is "recompute" (the larger stage buffer costs more occupancy than the
+    saved stage evaluations gain for the built-in fields)."""
     L = _lib.lib()
     fn = L.gs_tsit5_adjoint if r.method == METHOD_TSIT5 else L.gs_ros23_adjoint
     gy0 = torch.empty((r.n, r.spec.dim), dtype=torch.float64, device=p.device) if want_y0 else None

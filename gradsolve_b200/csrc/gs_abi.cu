@@ -443,7 +443,7 @@ int gs_tsit5_replay(int field, int precision, long long n, const double* y0, con
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (n == 0) return GS_OK;
   gs::ReplayArgs a{n, y0, p, t0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every), ckpt,
-                   y_final};
+                   y_final, cap};
   GS_TSIT5_DISPATCH(field, launch_tsit5_replay, a, (cudaStream_t)stream,
                     precision == GS_PREC_MIXED)
 }
@@ -459,7 +459,7 @@ int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, con
   int D, P;
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (n == 0) return GS_OK;
-  gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp};
+  gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp, cap};
   GS_TSIT5_DISPATCH(field, launch_tsit5_adjoint, a, cap, (cudaStream_t)stream,
                     prec == GS_PREC_MIXED, adjoint_schedule(precision), precision & GS_ADJ_MASK)
 }
@@ -499,7 +499,7 @@ int gs_ros23_replay(int field, int precision, long long n, const double* y0, con
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (n == 0) return GS_OK;
   gs::ReplayArgs a{n, y0, p, t0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every), ckpt,
-                   y_final};
+                   y_final, cap};
   GS_ROS23_DISPATCH(field, launch_ros23_replay, a, (cudaStream_t)stream)
 }
 
@@ -513,7 +513,7 @@ int gs_ros23_adjoint(int field, int precision, long long n, const double* p, con
   int D, P;
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (n == 0) return GS_OK;
-  gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp};
+  gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp, cap};
   GS_ROS23_DISPATCH(field, launch_ros23_adjoint, a, cap, (cudaStream_t)stream,
                     adjoint_schedule(precision))
 }
@@ -603,10 +603,10 @@ int launch_tsit5_vjp_static(long long n, long long S, long long ld, const double
   record_from_padded_kernel<<<grid_for(n), kBlock, 0, s>>>(n, S, dts, ld, rec, cap, n_steps);
   int rc = cuda_check("record_from_padded_kernel");
   if (rc) return rc;
-  gs::ReplayArgs ra{n, y0, p, t0, rec, n_steps, K, gs_ckpt_slots(cap, K), ckpt, y_final};
+  gs::ReplayArgs ra{n, y0, p, t0, rec, n_steps, K, gs_ckpt_slots(cap, K), ckpt, y_final, cap};
   gs::tsit5_replay_kernel<F><<<grid_for(n), kBlock, 0, s>>>(ra);
   if ((rc = cuda_check("tsit5_replay_kernel"))) return rc;
-  gs::AdjointArgs aa{n, p, rec, n_steps, ckpt, K, ybar, gy0, gp};
+  gs::AdjointArgs aa{n, p, rec, n_steps, ckpt, K, ybar, gy0, gp, cap};
   const SegCfg c = seg_cfg(K, F::D);
   if ((rc = allow_smem(gs::tsit5_adjoint_kernel<F>, c.smem))) return rc;
   gs::tsit5_adjoint_kernel<F><<<grid_for_block(n, c.block), c.block, c.smem, s>>>(aa);
@@ -726,7 +726,7 @@ extern "C" int gs_replay_saveat(int method, int field, int precision, long long 
   if (!y0 || !y_final || (K > 0 && !ys))
     return fail(GS_ERR_ARG, "gs_replay_saveat: y0, ys and y_final are required");
   gs::SaveatArgs a{n, y0, p, t0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every), ckpt,
-                   ts, ts_ld, K, ys, y_final, nullptr, nullptr, nullptr, nullptr};
+                   ts, ts_ld, K, ys, y_final, nullptr, nullptr, nullptr, nullptr, cap};
   return saveat_dispatch(method, field, precision, a, stream, false);
 }
 
@@ -744,6 +744,6 @@ extern "C" int gs_adjoint_saveat(int method, int field, int precision, long long
     return fail(GS_ERR_ARG, "gs_adjoint_saveat: ckpt and ysbar are required");
   gs::SaveatArgs a{n, nullptr, p, 0.0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every),
                    const_cast<double*>(ckpt), ts, ts_ld, K, nullptr, nullptr, ysbar, ybar, gy0,
-                   gp};
+                   gp, cap};
   return saveat_dispatch(method, field, precision, a, stream, true);
 }

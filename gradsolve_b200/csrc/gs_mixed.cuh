@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(128) tsit5_mixed_replay_kernel(const ReplayArg
   for (int i = 0; i < D; ++i) { y[i] = a.y0[j * D + i]; c[i] = 0.0; }
 #pragma unroll
   for (int i = 0; i < P; ++i) { p[i] = a.p[j * P + i]; pf[i] = (float)p[i]; }
-  const int na = a.n_acc[j];
+  const int na = steps_in_record(a.n_acc, j, a.cap);
   double t = a.t0;
   const bool ck_on = a.ckpt != nullptr;
   if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(128) tsit5_mixed_adjoint_kernel(const AdjointA
   }
 #pragma unroll
   for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
-  const int na = a.n_acc[j];
+  const int na = steps_in_record(a.n_acc, j, a.cap);
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
   SegBuf<D> seg;

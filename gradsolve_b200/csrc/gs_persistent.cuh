@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(128) adjoint_persistent_kernel(const AdjointAr
       for (int i = 0; i < P; ++i) { p[i] = a.p[j * P + i]; pf[i] = (float)p[i]; gp[i] = 0.0; }
 #pragma unroll
       for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
-      na = a.n_acc[j];
+      na = steps_in_record(a.n_acc, j, a.cap);
       sg = (na + K - 1) / K - 1;
       if (sg >= 0) return;
       if (a.gy0) {

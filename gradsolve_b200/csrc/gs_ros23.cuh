@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(128) ros23_replay_kernel(const ReplayArgs a) {
   for (int i = 0; i < D; ++i) y[i] = a.y0[j * D + i];
 #pragma unroll
   for (int i = 0; i < P; ++i) p[i] = a.p[j * P + i];
-  const int na = a.n_acc[j];
+  const int na = steps_in_record(a.n_acc, j, a.cap);
   double t = a.t0;
   const bool ck_on = a.ckpt != nullptr;
   if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(128) ros23_adjoint_kernel(const AdjointArgs a)
   }
 #pragma unroll
   for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
-  const int na = a.n_acc[j];
+  const int na = steps_in_record(a.n_acc, j, a.cap);
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
   SegBuf<D> seg;

@@ -87,6 +87,7 @@ struct SaveatArgs {
   const double* ybar;    // (n, D) cotangent of y_final or null (adjoint)
   double* gy0;
   double* gp;
+  int cap;               // record capacity: step counts are clamped to [0, cap]
 };
 
 template <int D>
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(128) replay_saveat_kernel(const SaveatArgs a) 
   for (int i = 0; i < P; ++i) { p[i] = a.p[j * P + i]; pf[i] = (float)p[i]; }
   const double* ts = a.ts + j * a.ts_ld;
   double* ys = a.ys + j * (long long)a.K * D;
-  const int na = a.n_acc[j];
+  const int na = steps_in_record(a.n_acc, j, a.cap);
   double t = a.t0;
   int kk = 0;
   while (kk < a.K && ts[kk] <= t) {  // never bracketed: y0
@@ -157,7 +158,7 @@ __global__ void __launch_bounds__(128) adjoint_saveat_kernel(const SaveatArgs a)
   for (int i = 0; i < D; ++i) lam[i] = a.ybar ? a.ybar[j * D + i] : 0.0;
   const double* ts = a.ts + j * a.ts_ld;
   const double* ysb = a.ysbar + j * (long long)a.K * D;
-  const int na = a.n_acc[j];
+  const int na = steps_in_record(a.n_acc, j, a.cap);
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
   SegBuf<D + 1> seg;  // states and step start times (index D)

@@ -385,6 +385,7 @@ struct AdjointArgs {
   const double* ybar;
   double* gy0;
   double* gp;
+  int cap;  // record capacity: step counts are clamped to [0, cap] before any record read
 };
 
 struct ReplayArgs {
@@ -397,7 +398,16 @@ struct ReplayArgs {
   int ck_every, ck_slots;
   double* ckpt;
   double* yf;
+  int cap;  // record capacity: step counts are clamped to [0, cap] before any record read
 };
+
+// A trajectory's step count as the reverse and replay kernels use it: never outside the
+// record's capacity, whatever the caller's n_acc holds (a record read past the capacity would
+// leave the buffer).
+__device__ __forceinline__ int steps_in_record(const int* n_acc, long long j, int cap) {
+  const int na = n_acc[j];
+  return na < 0 ? 0 : (na > cap ? cap : na);
+}
 
 template <int D>
 __device__ __forceinline__ void store_ckpt(double* ckpt, long long n, long long j, int slot,
@@ -536,7 +546,7 @@ __global__ void __launch_bounds__(128) tsit5_replay_kernel(const ReplayArgs a) {
   for (int i = 0; i < D; ++i) y[i] = a.y0[j * D + i];
 #pragma unroll
   for (int i = 0; i < P; ++i) p[i] = a.p[j * P + i];
-  const int na = a.n_acc[j];
+  const int na = steps_in_record(a.n_acc, j, a.cap);
   double t = a.t0;
   const bool ck_on = a.ckpt != nullptr;
   if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
@@ -568,7 +578,7 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a)
   }
 #pragma unroll
   for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
-  const int na = a.n_acc[j];
+  const int na = steps_in_record(a.n_acc, j, a.cap);
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
   SegBuf<D> seg;
@@ -637,7 +647,7 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_stages_kernel(const Adjoint
   }
 #pragma unroll
   for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
-  const int na = a.n_acc[j];
+  const int na = steps_in_record(a.n_acc, j, a.cap);
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
   SegBuf<6 * D> seg;

@@ -5,9 +5,11 @@ CUDA device, the current stream); all arithmetic happens in libgsolve.so.  The f
 here work on device tensors and return device tensors; the public API (``api.py``) and the
 autograd adapter (``torch_adapter.py``) sit on top.
 
-Record capacity follows the reference's device recorder (gradsolve/solvers/record_jax.py:
-171-213): start with a bounded capacity, and if any trajectory reports a full record
-(status 3) double it (up to ``max_steps``) and run again.  Failures then raise with the
+Record capacity starts bounded, as in the reference's device recorder
+(gradsolve/solvers/record_jax.py:171-213).  Where the reference doubles the capacity and
+re-solves the whole batch when any trajectory reports a full record (status 3), the rows that
+overflowed are re-solved alone with a larger capacity, in further tiers (``RecordSet``), so
+memory follows the step-count distribution of ragged batches.  Failures then raise with the
 reference's messages ("exhausted max_steps", "underflow").
 """
 from __future__ import annotations
@@ -160,6 +162,89 @@ class Record:
         return torch.where(s[None, :] < na[:, None], out, torch.zeros_like(out))
 
 
+# capacity factor between the tiers of a RecordSet
+TIER_GROWTH = 4
+
+
+@dataclass
+class RecordSet:
+    """A record kept in tiers, for batches whose step counts differ widely.
+
+    The first tier holds every trajectory at the first capacity.  Trajectories whose record
+    overflowed it (status 3) are solved again, alone, with TIER_GROWTH times the capacity,
+    and so on up to ``max_steps`` -- the reference's device recorder doubles the capacity and
+    re-solves the whole batch instead (gradsolve/solvers/record_jax.py:192-199).  Memory then
+    follows the step-count distribution (the sum over tiers of rows x capacity) rather than
+    n x the longest trajectory, and each tier's launch holds trajectories of similar length.
+    ``parts`` lists (rows, Record): rows None for the first tier (all trajectories), else the
+    sorted batch indices the tier covers; a later tier's results replace the earlier ones for
+    its rows.  Per-trajectory results are bitwise those of a single record (trajectories are
+    independent and every tier runs the same kernel)."""
+    method: str
+    spec: FieldSpec
+    n: int
+    t0: float
+    parts: list
+    sub: object               # the nested result of the overflowed rows (workspace reuse)
+    y_final: torch.Tensor
+    n_acc: torch.Tensor
+    n_rej: torch.Tensor
+    status: torch.Tensor
+    uneven: bool = False
+
+    @property
+    def cap(self) -> int:
+        return max(r.cap for _, r in self.parts)
+
+    @property
+    def ckpt_every(self) -> int:
+        return self.parts[0][1].ckpt_every
+
+    @property
+    def nbytes(self) -> int:
+        return sum(r.rec.numel() * 8 + r.ckpt.numel() * 8 for _, r in self.parts)
+
+    def padded_dts(self, S: Optional[int] = None) -> torch.Tensor:
+        if S is None:
+            S = int(self.n_acc.max().item()) if self.n else 0
+        out = torch.zeros((self.n, S), dtype=torch.float64, device=self.y_final.device)
+        for rows, r in self.parts:
+            w = min(S, r.cap)  # a tier holds at most its capacity
+            part = r.padded_dts(w)
+            if rows is None:
+                out[:, :w].copy_(part)
+            else:
+                out[:, :w].index_copy_(0, rows, part)
+                out[rows, w:] = 0.0
+        return out
+
+    def dts_rows(self, rows: torch.Tensor, S: Optional[int] = None) -> torch.Tensor:
+        rows = rows.to(device=self.y_final.device, dtype=torch.int64)
+        if S is None:
+            S = int(self.n_acc[rows].max().item()) if rows.numel() else 0
+        out = torch.zeros((rows.numel(), S), dtype=torch.float64, device=rows.device)
+        for prow, r in self.parts:
+            if prow is None:
+                out.copy_(r.dts_rows(rows, S))
+                continue
+            pos = torch.searchsorted(prow, rows).clamp_max(prow.numel() - 1)
+            hit = prow[pos] == rows
+            if bool(hit.any()):
+                sel = torch.nonzero(hit).squeeze(1)
+                out.index_copy_(0, sel, r.dts_rows(pos[sel], S))
+        return out
+
+
+def _parts(r):
+    return r.parts if isinstance(r, RecordSet) else [(None, r)]
+
+
+def _take(t: Optional[torch.Tensor], rows: Optional[torch.Tensor]):
+    if t is None or rows is None:
+        return t
+    return t.index_select(0, rows).contiguous()
+
+
 def _alloc_record(n: int, cap: int, dim: int, K: int, device) -> tuple:
     L = _lib.lib()
     rec_elems = L.gs_record_bytes(n, cap) // 8
@@ -203,28 +288,51 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
         empty = torch.empty(0, dtype=torch.float64, device=device)
         return Record(method, spec, n, float(t0), 0, 1, empty, empty, yf, n_acc, n_rej, status,
                       uneven=t1v is not None)
+    ws_sub = ws.sub if isinstance(ws, RecordSet) else None
+    ws = ws.parts[0][1] if isinstance(ws, RecordSet) else ws
     cap = max(1, min(int(cap0), int(max_steps)))
-    if ws is not None and ws.cap > cap:
-        cap = ws.cap
     if checkpoint == "auto" and tuned_ckpt_every(method, spec, precision) is None and n >= 4096:
         autotune_ckpt_every(method, spec, y0, p, t0=t0, t1=t1, t1v=t1v, rtol=rtol, atol=atol,
                             max_steps=max_steps, precision=precision)
-    while True:
-        K = choose_ckpt_every(checkpoint, spec.dim, n, cap, budget_bytes,
-                              tuned_ckpt_every(method, spec, precision))
-        if ws is not None and ws.cap == cap and ws.ckpt_every == K and ws.rec.numel() > 2:
-            rec, ckpt = ws.rec, ws.ckpt
-        else:
-            rec, ckpt = _alloc_record(n, cap, spec.dim, K, device)
-        _lib.check(fn(spec.code, mode, n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
-                      float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), cap, K,
-                      _ptr(rec), _ptr(ckpt), _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status),
-                      _stream()), fn.__name__)
-        if n == 0 or cap >= max_steps or not bool((status == 3).any().item()):
-            break
-        cap = min(2 * cap, int(max_steps))
-    return Record(method, spec, n, float(t0), cap, K, rec, ckpt, yf, n_acc, n_rej, status,
-                  uneven=t1v is not None)
+    K = choose_ckpt_every(checkpoint, spec.dim, n, cap, budget_bytes,
+                          tuned_ckpt_every(method, spec, precision))
+    if ws is not None and ws.cap == cap and ws.ckpt_every == K and ws.rec.numel() > 2:
+        rec, ckpt = ws.rec, ws.ckpt
+    else:
+        rec, ckpt = _alloc_record(n, cap, spec.dim, K, device)
+    _lib.check(fn(spec.code, mode, n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
+                  float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), cap, K,
+                  _ptr(rec), _ptr(ckpt), _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status),
+                  _stream()), fn.__name__)
+    r0 = Record(method, spec, n, float(t0), cap, K, rec, ckpt, yf, n_acc, n_rej, status,
+                uneven=t1v is not None)
+    if n == 0 or cap >= max_steps:
+        return r0
+    rows = torch.nonzero(status == 3).squeeze(1)
+    if rows.numel() == 0:
+        return r0
+    # the next tier: only the trajectories whose record overflowed, with TIER_GROWTH x capacity
+    sub = forward_record(method, spec, y0.index_select(0, rows).contiguous(),
+                         p.index_select(0, rows).contiguous(), t0=t0, t1=t1, rtol=rtol,
+                         atol=atol, dt0=dt0,
+                         t1v=None if t1v is None else t1v.index_select(0, rows).contiguous(),
+                         max_steps=max_steps, cap0=min(TIER_GROWTH * cap, int(max_steps)),
+                         checkpoint=checkpoint, budget_bytes=budget_bytes,
+                         precision=precision,
+                         workspace=ws_sub if (ws_sub is not None and ws_sub.n == rows.numel())
+                         else None, schedule=schedule)
+    # the batch's results: the first tier's, with the overflowed rows replaced.  The first
+    # tier's own Record keeps its counts (at most its capacity) for its own kernels.
+    yf_all, acc_all, rej_all, st_all = yf.clone(), n_acc.clone(), n_rej.clone(), status.clone()
+    yf_all.index_copy_(0, rows, sub.y_final)
+    acc_all.index_copy_(0, rows, sub.n_acc)
+    rej_all.index_copy_(0, rows, sub.n_rej)
+    st_all.index_copy_(0, rows, sub.status)
+    parts = [(None, r0)]
+    for srows, rr in (sub.parts if isinstance(sub, RecordSet) else [(None, sub)]):
+        parts.append((rows if srows is None else rows.index_select(0, srows), rr))
+    return RecordSet(method, spec, n, float(t0), parts, sub, yf_all, acc_all, rej_all, st_all,
+                     uneven=t1v is not None)
 
 
 def raise_on_failed(r: Record, max_steps: int, t1) -> None:
@@ -250,9 +358,22 @@ def raise_on_failed(r: Record, max_steps: int, t1) -> None:
         "or shorten the horizon.")
 
 
-def replay(r: Record, y0: torch.Tensor, p: torch.Tensor, *, write_ckpt: bool = True,
+def replay(r, y0: torch.Tensor, p: torch.Tensor, *, write_ckpt: bool = True,
            precision: str = "float64") -> torch.Tensor:
     """Frozen-mesh replay at (y0, p); refreshes the checkpoints for a following adjoint."""
+    out = None
+    for rows, rr in _parts(r):
+        yf = _replay_one(rr, _take(y0, rows), _take(p, rows), write_ckpt=write_ckpt,
+                         precision=precision)
+        if rows is None:
+            out = yf
+        else:
+            out.index_copy_(0, rows, yf)
+    return out
+
+
+def _replay_one(r: Record, y0: torch.Tensor, p: torch.Tensor, *, write_ckpt: bool,
+                precision: str) -> torch.Tensor:
     L = _lib.lib()
     fn = L.gs_tsit5_replay if r.method == METHOD_TSIT5 else L.gs_ros23_replay
     yf = torch.empty_like(y0)
@@ -265,7 +386,7 @@ def replay(r: Record, y0: torch.Tensor, p: torch.Tensor, *, write_ckpt: bool = T
 _ADJ = {"auto": 0x000, "recompute": 0x400, "stages": 0x800}
 
 
-def adjoint(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
+def adjoint(r, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
             want_p: bool = True, precision: str = "float64", schedule: str = "auto",
             variant: str = "auto"):
     """(dL/dy0, dL/dp) for cotangent ybar = dL/dy_final, using the record's checkpoints.
@@ -275,6 +396,23 @@ def adjoint(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = T
     inputs from the segment's forward pass, "recompute" re-evaluates them in the reverse
     sweep; "auto" is "recompute" (the larger stage buffer costs more occupancy than the
     saved stage evaluations gain for the built-in fields)."""
+    gy0 = gp = None
+    for rows, rr in _parts(r):
+        a, b = _adjoint_one(rr, _take(p, rows), _take(ybar, rows), want_y0=want_y0,
+                            want_p=want_p, precision=precision, schedule=schedule,
+                            variant=variant)
+        if rows is None:
+            gy0, gp = a, b
+        else:
+            if a is not None:
+                gy0.index_copy_(0, rows, a)
+            if b is not None:
+                gp.index_copy_(0, rows, b)
+    return gy0, gp
+
+
+def _adjoint_one(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool,
+                 want_p: bool, precision: str, schedule: str, variant: str):
     L = _lib.lib()
     fn = L.gs_tsit5_adjoint if r.method == METHOD_TSIT5 else L.gs_ros23_adjoint
     gy0 = torch.empty((r.n, r.spec.dim), dtype=torch.float64, device=p.device) if want_y0 else None
@@ -321,10 +459,26 @@ def _ts_arg(ts: torch.Tensor, n: int):
     return ts, ts.shape[1], ts.shape[1]
 
 
-def replay_saveat(r: Record, y0: torch.Tensor, p: torch.Tensor, ts: torch.Tensor, *,
+def replay_saveat(r, y0: torch.Tensor, p: torch.Tensor, ts: torch.Tensor, *,
                   write_ckpt: bool = True, precision: str = "float64"):
     """Frozen-mesh replay with dense output at ``ts`` ((K,) shared or (n, K) per trajectory).
     Returns (y_final (n, D), ys (n, K, D)); refreshes the checkpoints for the adjoint."""
+    yf = ys = None
+    per_row = ts.ndim == 2
+    for rows, rr in _parts(r):
+        a, b = _replay_saveat_one(rr, _take(y0, rows), _take(p, rows),
+                                  _take(ts, rows) if per_row else ts, write_ckpt=write_ckpt,
+                                  precision=precision)
+        if rows is None:
+            yf, ys = a, b
+        else:
+            yf.index_copy_(0, rows, a)
+            ys.index_copy_(0, rows, b)
+    return yf, ys
+
+
+def _replay_saveat_one(r: Record, y0: torch.Tensor, p: torch.Tensor, ts: torch.Tensor, *,
+                       write_ckpt: bool, precision: str):
     ts, ld, K = _ts_arg(ts, r.n)
     yf = torch.empty_like(y0)
     ys = torch.empty((r.n, K, r.spec.dim), dtype=torch.float64, device=y0.device)
@@ -336,10 +490,29 @@ def replay_saveat(r: Record, y0: torch.Tensor, p: torch.Tensor, ts: torch.Tensor
     return yf, ys
 
 
-def adjoint_saveat(r: Record, p: torch.Tensor, ts: torch.Tensor, ysbar: torch.Tensor,
+def adjoint_saveat(r, p: torch.Tensor, ts: torch.Tensor, ysbar: torch.Tensor,
                    ybar: Optional[torch.Tensor] = None, *, want_y0: bool = True,
                    want_p: bool = True, precision: str = "float64"):
     """(dL/dy0, dL/dp) for cotangents ysbar = dL/dys (n, K, D) and ybar = dL/dy_final."""
+    gy0 = gp = None
+    per_row = ts.ndim == 2
+    for rows, rr in _parts(r):
+        a, b = _adjoint_saveat_one(rr, _take(p, rows), _take(ts, rows) if per_row else ts,
+                                   _take(ysbar, rows), _take(ybar, rows), want_y0=want_y0,
+                                   want_p=want_p, precision=precision)
+        if rows is None:
+            gy0, gp = a, b
+        else:
+            if a is not None:
+                gy0.index_copy_(0, rows, a)
+            if b is not None:
+                gp.index_copy_(0, rows, b)
+    return gy0, gp
+
+
+def _adjoint_saveat_one(r: Record, p: torch.Tensor, ts: torch.Tensor, ysbar: torch.Tensor,
+                        ybar: Optional[torch.Tensor], *, want_y0: bool, want_p: bool,
+                        precision: str):
     ts, ld, K = _ts_arg(ts, r.n)
     gy0 = torch.empty((r.n, r.spec.dim), dtype=torch.float64, device=p.device) if want_y0 else None
     gp = torch.empty((r.n, p.shape[1]), dtype=torch.float64, device=p.device) if want_p else None

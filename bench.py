@@ -487,6 +487,7 @@ def run_b200(args) -> None:
         "gpu_launches": 2 * args.steps,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
         "fwd_ms": fwd_avg, "adj_ms": adj_avg, "mixed": mixed, "solve": solve or None,
+        "fwd_ms_steps": [round(x, 3) for x in fwd_ms], "adj_ms_steps": [round(x, 3) for x in adj_ms],
     }
     print(json.dumps(line), flush=True)
     if world > 1:
@@ -640,12 +641,15 @@ def run_workload(args) -> None:
         torch.cuda.synchronize()
         per_group = [float(np.mean([e[k].elapsed_time(e[k + 1]) for e in evs]))
                      for k in range(len(groups))]
-        whole = max_over_ranks(float(np.mean([e[0].elapsed_time(e[-1]) for e in evs])), dev)
+        steps_ms = [e[0].elapsed_time(e[-1]) for e in evs]
+        whole = max_over_ranks(float(np.mean(steps_ms)), dev)
+        time_variant.steps_ms = [round(x, 3) for x in steps_ms]
         return whole, per_group, outs
 
     clocks = ClockSampler(local)
     clocks.start()
     ms, per_group, outs = time_variant("float64")
+    steps_ms = time_variant.steps_ms
     infos = []
     for g, t_ms, (r, gp) in zip(groups, per_group, outs):
         assert int((r.status != 0).sum().item()) == 0, f"{g.name}: solve failed"
@@ -722,7 +726,7 @@ def run_workload(args) -> None:
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "dtype": "f64", "data": "synthetic (seeded numpy default_rng)", "groups": infos,
         "fp64_peak_tflops": fp64_peak, "oracle_parity_sample": parity, "mixed": mixed,
-        "cpu_baseline": cpu, "clocks": clk,
+        "cpu_baseline": cpu, "clocks": clk, "ms_steps": steps_ms,
         "config": {"n_per_gpu": n, "checkpoint_policy": str(args.checkpoint),
                    "schedule": args.schedule, "l2": "flushed between timed steps"},
     }

@@ -328,6 +328,9 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
     acc_all.index_copy_(0, rows, sub.n_acc)
     rej_all.index_copy_(0, rows, sub.n_rej)
     st_all.index_copy_(0, rows, sub.status)
+    # in the first tier the overflowed rows become empty (0 steps), so its replay and reverse
+    # passes skip them instead of integrating a truncated record whose result is replaced
+    n_acc.index_fill_(0, rows, 0)
     parts = [(None, r0)]
     for srows, rr in (sub.parts if isinstance(sub, RecordSet) else [(None, sub)]):
         parts.append((rows if srows is None else rows.index_select(0, srows), rr))

@@ -139,6 +139,9 @@ def test_overflowed_rows_are_resolved_in_larger_tiers(fake):
     assert np.all(r.status.numpy() == 0)
     np.testing.assert_array_equal(r.y_final.numpy(), np.repeat(steps[:, None], 3, axis=1))
     caps = {int(rr.cap): (None if rows is None else rows.tolist()) for rows, rr in r.parts}
+    # a tier's own counts leave out the rows a later tier re-solved
+    tier0 = r.parts[0][1]
+    assert tier0.n_acc.tolist() == [5, 3, 0, 7, 0, 2, 0, 0]
     assert caps == {8: None, 32: [2, 4, 6, 7], 128: [2, 4, 7], 512: [4, 7], 2048: [7]}
     # the trajectory's final tier serves its replay and its gradient
     final_cap = np.array([8, 8, 128, 8, 512, 8, 32, 2048])

@@ -36,6 +36,17 @@ N_DEFAULT = 1 << 20
 L2_BYTES = 126 * 1024 * 1024
 
 
+# DRAM bytes per trajectory of each kernel on this workload, from ncu captures at n = 2^18
+# (dram__bytes_read.sum + dram__bytes_write.sum per launch / 2^18), by checkpoint interval;
+# profiles/tsit5_f64_lorenz_bench_n2e20_launches_n2e18_K3_K4.md and
+# profiles/tsit5_f64_lorenz_n2e18_K8.md.  Traffic grows with the trajectory count.
+DRAM_BYTES_PER_TRAJ = {
+    "tsit5_adjoint_kernel": {3: 5.035797e9 / 2**18, 4: 3.714259e9 / 2**18,
+                             8: 2.455204e9 / 2**18},
+    "tsit5_record_kernel": {3: 3.260184e9 / 2**18, 4: 2.790004e9 / 2**18},
+}
+
+
 def make_inputs(n: int, seed: int):
     rng = np.random.default_rng(seed)
     y0 = np.array([1.0, 0.0, 0.0]) + rng.normal(0.0, 0.1, (n, 3))
@@ -457,7 +468,14 @@ def run_b200(args) -> None:
     achieved = kernels[dom]["tflops"]
     roofline = {
         "bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-        "frac": achieved / fp64_peak, "traffic": None, "kernel": dom,
+        "frac": achieved / fp64_peak,
+        "traffic": (DRAM_BYTES_PER_TRAJ[dom][K] * n if K in DRAM_BYTES_PER_TRAJ.get(dom, {})
+                    else None),
+        "traffic_source": (f"ncu capture of {dom} at n=2^18, K={K}, scaled to n={n} "
+                           "(bytes grow with the trajectory count)"
+                           if K in DRAM_BYTES_PER_TRAJ.get(dom, {}) else
+                           f"no ncu capture at K={K}"),
+        "kernel": dom,
         "peak_source": "measured in this run: libgsprobe FP64 FMA loop (8 chains/thread)",
         "per_kernel": kernels,
         "hbm": {"algorithmic_bytes_per_step": rec_bytes + ck_bytes + io_bytes,

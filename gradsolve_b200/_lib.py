@@ -51,6 +51,11 @@ _SIGS = {
     "gs_replay_saveat": (c_int, [c_int, c_int, c_int, c_ll, c_void_p, c_void_p, c_double,
                                  c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p, c_ll,
                                  c_int, c_void_p, c_void_p, c_void_p]),
+    "gs_fwd_record_saveat": (c_int, [c_int, c_int, c_int, c_ll, c_void_p, c_void_p, c_double,
+                                     c_void_p, c_double, c_double, c_double, c_double, c_int,
+                                     c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, c_void_p, c_ll, c_int, c_void_p,
+                                     c_void_p]),
     "gs_adjoint_saveat": (c_int, [c_int, c_int, c_int, c_ll, c_void_p, c_void_p, c_void_p,
                                   c_int, c_void_p, c_int, c_void_p, c_ll, c_int, c_void_p,
                                   c_void_p, c_void_p, c_void_p, c_void_p]),

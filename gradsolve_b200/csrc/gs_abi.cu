@@ -669,31 +669,75 @@ int launch_saveat(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint) {
   return cuda_check("replay_saveat_kernel");
 }
 
-template <class F>
-int launch_saveat_tsit5(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint, bool mixed) {
-  return mixed ? launch_saveat<F, gs::Tsit5MixedStep>(a, s, adjoint)
-               : launch_saveat<F, gs::Tsit5F64Step>(a, s, adjoint);
+// Persistent saveat reverse pass; the work counter sits in the control block after the
+// checkpoint slots, like the other reverse passes'.
+template <class F, class M>
+int launch_adjoint_saveat_persistent(const gs::SaveatArgs& a, cudaStream_t s, bool use_counter) {
+  const SegCfg c = seg_cfg(a.ck_every, F::D + 1);
+  unsigned long long* counter =
+      use_counter ? ctrl_counter(a.ckpt, a.n, a.ck_slots, F::D, gs::kCtrlAdj) : nullptr;
+  unsigned grid = 0;
+  int rc;
+  if ((rc = allow_smem(gs::adjoint_saveat_persistent_kernel<F, M>, c.smem))) return rc;
+  if ((rc = persistent_grid(gs::adjoint_saveat_persistent_kernel<F, M>, c.block, c.smem, a.n,
+                            &grid)))
+    return rc;
+  if ((rc = zero_counter(counter, s))) return rc;
+  gs::adjoint_saveat_persistent_kernel<F, M><<<grid, c.block, c.smem, s>>>(a, counter);
+  return cuda_check("adjoint_saveat_persistent_kernel");
+}
+
+template <class F, class M>
+int launch_saveat_sched(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint, int sched) {
+  if (adjoint && sched != GS_SCHED_STATIC)
+    return launch_adjoint_saveat_persistent<F, M>(a, s, sched == GS_SCHED_REFILL);
+  return launch_saveat<F, M>(a, s, adjoint);
 }
 
 template <class F>
-int launch_saveat_ros23(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint) {
-  return launch_saveat<F, gs::Ros23Step>(a, s, adjoint);
+int launch_saveat_tsit5(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint, bool mixed,
+                        int sched) {
+  return mixed ? launch_saveat_sched<F, gs::Tsit5MixedStep>(a, s, adjoint, sched)
+               : launch_saveat_sched<F, gs::Tsit5F64Step>(a, s, adjoint, sched);
 }
 
+template <class F>
+int launch_saveat_ros23(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint, int sched) {
+  return launch_saveat_sched<F, gs::Ros23Step>(a, s, adjoint, sched);
+}
+
+// precision carries GS_PREC_* and, for the reverse pass, GS_SCHED_* (AUTO = one thread per
+// trajectory; REFILL / STRIDED = persistent lanes).  The forward replay runs one thread per
+// trajectory.
 int saveat_dispatch(int method, int field, int precision, const gs::SaveatArgs& a, void* stream,
                     bool adjoint) {
   const cudaStream_t s = (cudaStream_t)stream;
+  const int prec = precision & GS_PREC_MASK;
+  const int sched = adjoint ? adjoint_schedule(precision) : GS_SCHED_STATIC;
   if (method == GS_METHOD_TSIT5) {
-    if (precision != GS_PREC_F64 && precision != GS_PREC_MIXED)
-      return fail(GS_ERR_PRECISION, "saveat: unknown precision mode " + std::to_string(precision));
-    GS_TSIT5_DISPATCH(field, launch_saveat_tsit5, a, s, adjoint, precision == GS_PREC_MIXED)
+    if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED)
+      return fail(GS_ERR_PRECISION, "saveat: unknown precision mode " + std::to_string(prec));
+    GS_TSIT5_DISPATCH(field, launch_saveat_tsit5, a, s, adjoint, prec == GS_PREC_MIXED, sched)
   }
   if (method == GS_METHOD_ROS23) {
-    if (precision != GS_PREC_F64)
+    if (prec != GS_PREC_F64)
       return fail(GS_ERR_PRECISION, "saveat: Rosenbrock23 runs in float64 only");
-    GS_ROS23_DISPATCH(field, launch_saveat_ros23, a, s, adjoint)
+    GS_ROS23_DISPATCH(field, launch_saveat_ros23, a, s, adjoint, sched)
   }
   return fail(GS_ERR_ARG, "saveat: unknown method " + std::to_string(method));
+}
+
+// Forward with record and dense output: the persistent kernel (lanes refilled from the work
+// counter for uneven batches, strided otherwise).
+template <class F>
+int launch_fwd_saveat_tsit5(const gs::RecordArgs& a, cudaStream_t s, bool mixed, bool refill) {
+  return mixed ? launch_record_persistent<F, gs::LaneTsit5Mixed<F>>(a, s, refill)
+               : launch_record_persistent<F, gs::LaneTsit5F64<F>>(a, s, refill);
+}
+
+template <class F>
+int launch_fwd_saveat_ros23(const gs::RecordArgs& a, cudaStream_t s, bool refill) {
+  return launch_record_persistent<F, gs::LaneRos23<F>>(a, s, refill);
 }
 
 int check_saveat(const char* who, long long n, const double* p, const double* rec,
@@ -728,6 +772,45 @@ extern "C" int gs_replay_saveat(int method, int field, int precision, long long 
   gs::SaveatArgs a{n, y0, p, t0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every), ckpt,
                    ts, ts_ld, K, ys, y_final, nullptr, nullptr, nullptr, nullptr, cap};
   return saveat_dispatch(method, field, precision, a, stream, false);
+}
+
+extern "C" int gs_fwd_record_saveat(int method, int field, int precision, long long n,
+                                    const double* y0, const double* p, double t0,
+                                    const double* t1v, double t1, double rtol, double atol,
+                                    double dt0, int max_steps, int cap, int ckpt_every,
+                                    double* rec, double* ckpt, double* y_final, int* n_acc,
+                                    int* n_rej, int* status, const double* ts, long long ts_ld,
+                                    int K, double* ys, void* stream) {
+  const char* who = "gs_fwd_record_saveat";
+  int rc = check_record_args(who, n, y0, p, rtol, atol, max_steps, cap, ckpt_every, rec, ckpt,
+                             y_final, n_acc, n_rej, status);
+  if (rc) return rc;
+  if (K < 0 || ts_ld < 0 || (ts_ld != 0 && ts_ld < K))
+    return fail(GS_ERR_ARG, std::string(who) + ": bad saveat sizes");
+  int D, P;
+  if ((rc = field_dims(field, &D, &P))) return rc;
+  if (n == 0) return GS_OK;
+  if (K > 0 && (!ts || !ys)) return fail(GS_ERR_ARG, std::string(who) + ": ts and ys are required");
+  const int prec = precision & GS_PREC_MASK;
+  const int sched = precision & GS_SCHED_MASK;
+  // refill needs the work counter in the checkpoint buffer's control block
+  const bool refill = ckpt != nullptr &&
+                      (sched == GS_SCHED_REFILL || (sched == GS_SCHED_AUTO && t1v != nullptr));
+  gs::RecordArgs a{n, y0, p, t0, t1, rtol, atol, dt0, t1v, max_steps, cap, ckpt_every,
+                   gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status,
+                   ts, ts_ld, K, K > 0 ? ys : nullptr};
+  const cudaStream_t s = (cudaStream_t)stream;
+  if (method == GS_METHOD_TSIT5) {
+    if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED)
+      return fail(GS_ERR_PRECISION, std::string(who) + ": unknown precision mode " + std::to_string(prec));
+    GS_TSIT5_DISPATCH(field, launch_fwd_saveat_tsit5, a, s, prec == GS_PREC_MIXED, refill)
+  }
+  if (method == GS_METHOD_ROS23) {
+    if (prec != GS_PREC_F64)
+      return fail(GS_ERR_PRECISION, std::string(who) + ": Rosenbrock23 runs in float64 only");
+    GS_ROS23_DISPATCH(field, launch_fwd_saveat_ros23, a, s, refill)
+  }
+  return fail(GS_ERR_ARG, std::string(who) + ": unknown method " + std::to_string(method));
 }
 
 extern "C" int gs_adjoint_saveat(int method, int field, int precision, long long n,

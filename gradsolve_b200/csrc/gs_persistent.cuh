@@ -48,6 +48,7 @@ struct Fetch {
 template <class F>
 struct LaneTsit5F64 {
   static constexpr int D = F::D, QK = 10;
+  using Step = Tsit5F64Step;  // the replay step (saveat re-steps)
   double k1[D], k7[D];
   __device__ __forceinline__ void start(const double* y, const double* p, const float*) {
     F::rhs(y, p, k1);
@@ -77,6 +78,7 @@ struct LaneTsit5F64 {
 template <class F>
 struct LaneTsit5Mixed {
   static constexpr int D = F::D, QK = 10;
+  using Step = Tsit5MixedStep;
   double k1[D], k7[D], c[D], c5[D];
   __device__ __forceinline__ void start(const double* y, const double* p, const float*) {
     F::rhs(y, p, k1);
@@ -116,6 +118,7 @@ struct LaneTsit5Mixed {
 template <class F>
 struct LaneRos23 {
   static constexpr int D = F::D, QK = 6;
+  using Step = Ros23Step;
   __device__ __forceinline__ void start(const double*, const double*, const float*) {}
   __device__ __forceinline__ double trial(const double* y, const double* p, const float*, double h,
                                           double rtol, double atol, double* ynew) {
@@ -149,6 +152,13 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
   float pf[P];
   int acc = 0, rej = 0, it = 0, ck_cnt = 0, ck_slot = 0;
   double b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
+  // dense output: the saveat rules of replay_saveat_kernel (gs_saveat.cuh) applied while the
+  // trajectory is integrated -- a time bracketed by an accepted step [t, t+h] gets one
+  // replay step of size ts - t from that step's start state
+  const bool sv_on = a.ys != nullptr;
+  const double* tsr = nullptr;
+  double* ysr = nullptr;
+  int kk = 0;
   L lane;
   auto begin = [&](long long jj) {
 #pragma unroll
@@ -162,6 +172,15 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
     b0 = b1 = b2 = b3 = 0.0;
     if (ck_on) store_ckpt<D>(a.ckpt, a.n, jj, 0, y, t);
     lane.start(y, p, pf);
+    if (sv_on) {
+      tsr = a.ts + jj * a.ts_ld;
+      ysr = a.ys + jj * (long long)a.K * D;
+      kk = 0;
+      while (kk < a.K && tsr[kk] <= t) {  // never bracketed: y0
+        store_row<D>(ysr + (long long)kk * D, y);
+        ++kk;
+      }
+    }
   };
   if (j < a.n) begin(j);
   while (j < a.n) {
@@ -183,6 +202,17 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
           if ((rec_on || ck_on) && acc >= a.cap) {
             st = 3;
           } else {
+            if (sv_on) {
+              const double tn = t + h;
+              while (kk < a.K && tsr[kk] <= tn) {  // bracketed by this step: re-step to ts
+                double yk[D], ck[D];
+#pragma unroll
+                for (int i = 0; i < D; ++i) { yk[i] = y[i]; ck[i] = 0.0; }
+                L::Step::template step<F>(yk, ck, p, pf, tsr[kk] - t);
+                store_row<D>(ysr + (long long)kk * D, yk);
+                ++kk;
+              }
+            }
             t = t + h;
 #pragma unroll
             for (int i = 0; i < D; ++i) y[i] = ynew[i];
@@ -214,6 +244,10 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
       }
 #pragma unroll
       for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
+      if (sv_on) {  // times at or past the final accumulated time take y_final itself
+        for (int k = a.K - 1; k >= 0 && tsr[k] >= t; --k) store_row<D>(ysr + (long long)k * D, y);
+        for (int k = kk; k < a.K; ++k) store_row<D>(ysr + (long long)k * D, y);
+      }
       a.n_acc[j] = acc;
       a.n_rej[j] = rej;
       a.status[j] = st;
@@ -290,6 +324,120 @@ __global__ void __launch_bounds__(128) adjoint_persistent_kernel(const AdjointAr
 #pragma unroll
         for (int i = 0; i < P; ++i) a.gp[j * P + i] = gp[i];
       }
+      take();
+    }
+  }
+}
+
+// ---- persistent saveat reverse pass (one segment per iteration) -------------------------------
+// Per trajectory the arithmetic of adjoint_saveat_kernel (gs_saveat.cuh); the lane carries the
+// trajectory's cursor (segment, saveat times not yet assigned, whether the final cotangents
+// have joined) between iterations and refills itself when the trajectory is done.
+template <class F, class M>
+__global__ void __launch_bounds__(128) adjoint_saveat_persistent_kernel(
+    const SaveatArgs a, unsigned long long* counter) {
+  constexpr int D = F::D, P = F::P;
+  Fetch fetch(counter);
+  const int K = a.ck_every;
+  SegBuf<D + 1> seg;  // states and step start times (index D)
+  double p[P], lam[D], gp[P];
+  float pf[P];
+  const double* ts = nullptr;
+  const double* ysb = nullptr;
+  int na = 0, sg = -1, kk = 0;
+  bool fin_done = false;
+  long long j;
+  auto finish = [&]() {  // times never bracketed (ts <= t0) take y0: their cotangent joins lam
+    for (int k = 0; k < kk; ++k) {
+#pragma unroll
+      for (int i = 0; i < D; ++i) lam[i] += ysb[(long long)k * D + i];
+    }
+    if (a.gy0) {
+#pragma unroll
+      for (int i = 0; i < D; ++i) a.gy0[j * D + i] = lam[i];
+    }
+    if (a.gp) {
+#pragma unroll
+      for (int i = 0; i < P; ++i) a.gp[j * P + i] = gp[i];
+    }
+  };
+  auto take = [&]() {
+    for (;;) {
+      j = fetch.get();
+      if (j >= a.n) return;
+#pragma unroll
+      for (int i = 0; i < P; ++i) { p[i] = a.p[j * P + i]; pf[i] = (float)p[i]; gp[i] = 0.0; }
+#pragma unroll
+      for (int i = 0; i < D; ++i) lam[i] = a.ybar ? a.ybar[j * D + i] : 0.0;
+      ts = a.ts + j * a.ts_ld;
+      ysb = a.ysbar + j * (long long)a.K * D;
+      na = steps_in_record(a.n_acc, j, a.cap);
+      sg = (na + K - 1) / K - 1;
+      kk = a.K;
+      fin_done = false;
+      if (sg >= 0) return;
+      const double tfin = a.t0;  // no steps: every time >= t0 is y_final = y0
+      while (kk > 0 && ts[kk - 1] >= tfin) {
+        --kk;
+#pragma unroll
+        for (int i = 0; i < D; ++i) lam[i] += ysb[(long long)kk * D + i];
+      }
+      finish();
+    }
+  };
+  take();
+  while (j < a.n) {
+    const int start = sg * K;
+    double y[D], c[D];
+    double t = load_ckpt<D>(a.ckpt, a.n, j, sg, y);
+#pragma unroll
+    for (int i = 0; i < D; ++i) { seg.at(0, i) = y[i]; c[i] = 0.0; }
+    seg.at(0, D) = t;
+    for (int q = 1; q <= K; ++q) {  // states y_{start+q} and times (q = K: segment end)
+      const int s = start + q - 1;
+      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      if (dt > 0.0) {
+        if (q < K) M::template step<F>(y, c, p, pf, dt);
+        t = t + dt;
+      }
+      if (q < K) {
+#pragma unroll
+        for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
+        seg.at(q, D) = t;
+      }
+    }
+    if (!fin_done) {  // the trajectory's last segment comes first: t is t_fin
+      fin_done = true;
+      while (kk > 0 && ts[kk - 1] >= t) {
+        --kk;
+#pragma unroll
+        for (int i = 0; i < D; ++i) lam[i] += ysb[(long long)kk * D + i];
+      }
+    }
+    for (int q = K - 1; q >= 0; --q) {
+      const int s = start + q;
+      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      if (dt > 0.0) {
+        double ys[D], add[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) { ys[i] = seg.at(q, i); add[i] = 0.0; }
+        const double ts0 = seg.at(q, D);
+        while (kk > 0 && ts[kk - 1] > ts0) {  // re-steps bracketed by this step
+          --kk;
+          double w[D];
+#pragma unroll
+          for (int i = 0; i < D; ++i) w[i] = ysb[(long long)kk * D + i];
+          M::template vjp<F>(ys, p, pf, ts[kk] - ts0, w, gp);
+#pragma unroll
+          for (int i = 0; i < D; ++i) add[i] += w[i];
+        }
+        M::template vjp<F>(ys, p, pf, dt, lam, gp);
+#pragma unroll
+        for (int i = 0; i < D; ++i) lam[i] += add[i];
+      }
+    }
+    if (--sg < 0) {
+      finish();
       take();
     }
   }

@@ -373,6 +373,12 @@ struct RecordArgs {
   int* n_acc;
   int* n_rej;
   int* status;
+  // dense output produced by the forward itself (persistent kernel only): requested times,
+  // row j at ts + j * ts_ld (ts_ld = 0: one shared row), K per trajectory, states (n, K, D)
+  const double* ts = nullptr;
+  long long ts_ld = 0;
+  int K = 0;
+  double* ys = nullptr;
 };
 
 struct AdjointArgs {

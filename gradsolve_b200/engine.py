@@ -138,6 +138,7 @@ class Record:
     n_rej: torch.Tensor      # (n,) int32
     status: torch.Tensor     # (n,) int32
     uneven: bool = False     # per-trajectory end times: the reverse pass refills lanes
+    ys: Optional[torch.Tensor] = None  # (n, K, D) dense output of the forward, if asked for
 
     def padded_dts(self, S: Optional[int] = None) -> torch.Tensor:
         """The record in the reference's (n, S) zero-padded layout."""
@@ -191,6 +192,7 @@ class RecordSet:
     n_rej: torch.Tensor
     status: torch.Tensor
     uneven: bool = False
+    ys: Optional[torch.Tensor] = None
 
     @property
     def cap(self) -> int:
@@ -262,12 +264,15 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
                    cap0: int = DEFAULT_CAP0, checkpoint="auto",
                    budget_bytes: Optional[int] = None, precision: str = "float64",
                    record: bool = True, workspace: Optional[Record] = None,
-                   schedule: str = "auto") -> Record:
+                   schedule: str = "auto", saveat_ts: Optional[torch.Tensor] = None) -> Record:
     """Adaptive solve on the device; with ``record`` the dts and checkpoints are kept.
 
     ``y0`` (n, D) and ``p`` (n, P) float64 contiguous device tensors.  ``workspace``: a Record
     from an earlier call of the same shape whose buffers are reused (overwritten) instead of
-    allocating new ones -- the steady-state pattern of a training loop."""
+    allocating new ones -- the steady-state pattern of a training loop.  ``saveat_ts`` ((K,)
+    shared or (n, K) per trajectory, sorted): the forward also produces the dense output
+    ``r.ys`` (n, K, D) -- what ``replay_saveat`` gives on the recorded mesh -- so the
+    recording point needs no replay pass."""
     n = y0.shape[0]
     device = y0.device
     L = _lib.lib()
@@ -300,12 +305,23 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
         rec, ckpt = ws.rec, ws.ckpt
     else:
         rec, ckpt = _alloc_record(n, cap, spec.dim, K, device)
-    _lib.check(fn(spec.code, mode, n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
-                  float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), cap, K,
-                  _ptr(rec), _ptr(ckpt), _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status),
-                  _stream()), fn.__name__)
+    ys = None
+    if saveat_ts is None:
+        _lib.check(fn(spec.code, mode, n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
+                      float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), cap, K,
+                      _ptr(rec), _ptr(ckpt), _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status),
+                      _stream()), fn.__name__)
+    else:
+        ts, ld, Kt = _ts_arg(saveat_ts, n)
+        ys = (ws.ys if ws is not None and ws.ys is not None and ws.ys.shape == (n, Kt, spec.dim)
+              else torch.empty((n, Kt, spec.dim), dtype=torch.float64, device=device))
+        _lib.check(L.gs_fwd_record_saveat(
+            _METHOD_CODE[method], spec.code, mode, n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
+            float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), cap, K, _ptr(rec),
+            _ptr(ckpt), _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status), _ptr(ts), ld, Kt,
+            _ptr(ys), _stream()), "gs_fwd_record_saveat")
     r0 = Record(method, spec, n, float(t0), cap, K, rec, ckpt, yf, n_acc, n_rej, status,
-                uneven=t1v is not None)
+                uneven=t1v is not None, ys=ys)
     if n == 0 or cap >= max_steps:
         return r0
     rows = torch.nonzero(status == 3).squeeze(1)
@@ -320,7 +336,9 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
                          checkpoint=checkpoint, budget_bytes=budget_bytes,
                          precision=precision,
                          workspace=ws_sub if (ws_sub is not None and ws_sub.n == rows.numel())
-                         else None, schedule=schedule)
+                         else None, schedule=schedule,
+                         saveat_ts=None if saveat_ts is None else
+                         (saveat_ts if saveat_ts.ndim == 1 else _take(saveat_ts, rows)))
     # the batch's results: the first tier's, with the overflowed rows replaced.  The first
     # tier's own Record keeps its counts (at most its capacity) for its own kernels.
     yf_all, acc_all, rej_all, st_all = yf.clone(), n_acc.clone(), n_rej.clone(), status.clone()
@@ -328,6 +346,10 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
     acc_all.index_copy_(0, rows, sub.n_acc)
     rej_all.index_copy_(0, rows, sub.n_rej)
     st_all.index_copy_(0, rows, sub.status)
+    ys_all = None
+    if ys is not None:
+        ys_all = ys.clone()
+        ys_all.index_copy_(0, rows, sub.ys)
     # in the first tier the overflowed rows become empty (0 steps), so its replay and reverse
     # passes skip them instead of integrating a truncated record whose result is replaced
     n_acc.index_fill_(0, rows, 0)
@@ -335,7 +357,7 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
     for srows, rr in (sub.parts if isinstance(sub, RecordSet) else [(None, sub)]):
         parts.append((rows if srows is None else rows.index_select(0, srows), rr))
     return RecordSet(method, spec, n, float(t0), parts, sub, yf_all, acc_all, rej_all, st_all,
-                     uneven=t1v is not None)
+                     uneven=t1v is not None, ys=ys_all)
 
 
 def raise_on_failed(r: Record, max_steps: int, t1) -> None:
@@ -495,14 +517,18 @@ def _replay_saveat_one(r: Record, y0: torch.Tensor, p: torch.Tensor, ts: torch.T
 
 def adjoint_saveat(r, p: torch.Tensor, ts: torch.Tensor, ysbar: torch.Tensor,
                    ybar: Optional[torch.Tensor] = None, *, want_y0: bool = True,
-                   want_p: bool = True, precision: str = "float64"):
-    """(dL/dy0, dL/dp) for cotangents ysbar = dL/dys (n, K, D) and ybar = dL/dy_final."""
+                   want_p: bool = True, precision: str = "float64", schedule: str = "auto"):
+    """(dL/dy0, dL/dp) for cotangents ysbar = dL/dys (n, K, D) and ybar = dL/dy_final.
+    ``schedule="auto"`` refills lanes from a work counter for an uneven batch (per-trajectory
+    end times), else runs one thread per trajectory."""
     gy0 = gp = None
     per_row = ts.ndim == 2
+    if schedule == "auto" and r.uneven:
+        schedule = "refill"
     for rows, rr in _parts(r):
         a, b = _adjoint_saveat_one(rr, _take(p, rows), _take(ts, rows) if per_row else ts,
                                    _take(ysbar, rows), _take(ybar, rows), want_y0=want_y0,
-                                   want_p=want_p, precision=precision)
+                                   want_p=want_p, precision=precision, schedule=schedule)
         if rows is None:
             gy0, gp = a, b
         else:
@@ -515,14 +541,14 @@ def adjoint_saveat(r, p: torch.Tensor, ts: torch.Tensor, ysbar: torch.Tensor,
 
 def _adjoint_saveat_one(r: Record, p: torch.Tensor, ts: torch.Tensor, ysbar: torch.Tensor,
                         ybar: Optional[torch.Tensor], *, want_y0: bool, want_p: bool,
-                        precision: str):
+                        precision: str, schedule: str):
     ts, ld, K = _ts_arg(ts, r.n)
     gy0 = torch.empty((r.n, r.spec.dim), dtype=torch.float64, device=p.device) if want_y0 else None
     gp = torch.empty((r.n, p.shape[1]), dtype=torch.float64, device=p.device) if want_p else None
     ysbar = ysbar.to(torch.float64).contiguous()
     ybar = None if ybar is None else ybar.to(torch.float64).contiguous()
     _lib.check(_lib.lib().gs_adjoint_saveat(
-        _METHOD_CODE[r.method], r.spec.code, _PREC[precision], r.n, _ptr(p), _ptr(r.rec),
-        _ptr(r.n_acc), max(r.cap, 1), _ptr(r.ckpt), r.ckpt_every, _ptr(ts), ld, K, _ptr(ysbar),
+        _METHOD_CODE[r.method], r.spec.code, _PREC[precision] | _SCHED[schedule], r.n, _ptr(p),
+        _ptr(r.rec), _ptr(r.n_acc), max(r.cap, 1), _ptr(r.ckpt), r.ckpt_every, _ptr(ts), ld, K, _ptr(ysbar),
         _ptr(ybar), _ptr(gy0), _ptr(gp), _stream()), "gs_adjoint_saveat")
     return gy0, gp

@@ -201,10 +201,30 @@ int gs_replay_saveat(int method, int field, int precision, long long n, const do
                      double* ys, double* y_final, void* stream);
 
 /*
+ * The adaptive forward with record (gs_tsit5_fwd_record / gs_ros23_fwd_record) that also
+ * produces the dense output of gs_replay_saveat at the same time: each requested time is
+ * re-stepped from the start of the accepted step that brackets it, as the trajectory is
+ * integrated, so the recording point needs no separate replay pass.  ys equals what
+ * gs_replay_saveat gives on the recorded mesh (bitwise for Tsit5).  Runs the persistent
+ * kernel: lanes refilled from a work counter when trajectories have their own end times (or
+ * GS_SCHED_REFILL is set; needs ckpt), strided otherwise.  No counterpart in the reference,
+ * whose saveat always replays the recorded mesh (gradsolve/warp/warp_replay.py:58-84).
+ * method: GS_METHOD_TSIT5 (float64 or mixed) or GS_METHOD_ROS23 (float64).
+ */
+int gs_fwd_record_saveat(int method, int field, int precision, long long n, const double* y0,
+                         const double* p, double t0, const double* t1v, double t1, double rtol,
+                         double atol, double dt0, int max_steps, int cap, int ckpt_every,
+                         double* rec, double* ckpt, double* y_final, int* n_acc, int* n_rej,
+                         int* status, const double* ts, long long ts_ld, int K, double* ys,
+                         void* stream);
+
+/*
  * Adjoint of gs_replay_saveat for a loss of the saved states (and optionally y_final):
  * ysbar (n, K, D) = dL/dys, ybar (n, D) = dL/dy_final or NULL -> gy0, gp (either may be
  * NULL).  The gradient jax.grad takes through replay_solve_saveat_jax
- * (gradsolve/warp/warp_replay.py:58-84, gradsolve/api.py:748-752).
+ * (gradsolve/warp/warp_replay.py:58-84, gradsolve/api.py:748-752).  precision may carry
+ * GS_SCHED_REFILL / GS_SCHED_STRIDED (persistent lanes, for uneven batches); AUTO runs one
+ * thread per trajectory.
  */
 int gs_adjoint_saveat(int method, int field, int precision, long long n, const double* p,
                       const double* rec, const int* n_acc, int cap, const double* ckpt,

@@ -50,12 +50,19 @@ def test_saveat_values_and_gradients_vs_oracle(gslib, oracle, cuda, method, case
     rng = np.random.default_rng(7)
     ysbar = rng.normal(size=tuple(ys.shape))
     ybar = rng.normal(size=tuple(yf.shape))
-    gy0, gp = engine.adjoint_saveat(r, p, ts_t, torch.tensor(ysbar, device=cuda),
-                                    torch.tensor(ybar, device=cuda))
     oy, op = oracle.replay_saveat_vjp(method, field, g["y0"], g["params"], g["dts"],
                                       np.array(ts), ysbar, ybar)
-    assert rowrel(gy0.cpu().numpy(), oy) <= 1e-9
-    assert rowrel(gp.cpu().numpy(), op[:, : spec.nparam]) <= 1e-9
+    outs = {}
+    for sched in ("static", "refill", "strided"):  # one thread per trajectory / persistent lanes
+        gy0, gp = engine.adjoint_saveat(r, p, ts_t, torch.tensor(ysbar, device=cuda),
+                                        torch.tensor(ybar, device=cuda), schedule=sched)
+        assert rowrel(gy0.cpu().numpy(), oy) <= 1e-9, sched
+        assert rowrel(gp.cpu().numpy(), op[:, : spec.nparam]) <= 1e-9, sched
+        outs[sched] = (gy0.cpu(), gp.cpu())
+    if method == "tsit5":  # same expressions, same lane code: bitwise
+        for sched in ("refill", "strided"):
+            assert torch.equal(outs[sched][0], outs["static"][0])
+            assert torch.equal(outs[sched][1], outs["static"][1])
 
 
 def test_per_trajectory_end_times_and_rows(gslib, oracle, cuda):
@@ -161,3 +168,44 @@ def test_mixed_saveat_close_to_f64(gslib, cuda):
     _, ysm = engine.replay_saveat(r, y0, p, ts_t, precision="mixed")
     gm = engine.adjoint_saveat(r, p, ts_t, ysbar, precision="mixed")[1]
     assert rowrel(gm.cpu().numpy(), g64.cpu().numpy()) <= 1e-3
+
+
+@pytest.mark.parametrize("method,field,prec", [("tsit5", "vdp", "float64"),
+                                               ("tsit5", "vdp", "mixed"),
+                                               ("tsit5", "lorenz", "float64"),
+                                               ("rosenbrock23", "vdp", "float64")])
+def test_forward_dense_output_equals_replay(gslib, cuda, method, field, prec):
+    """The forward that re-steps each bracketed time as it integrates gives the dense output
+    of replay_saveat on the recorded mesh (Tsit5 bitwise; Rosenbrock23 to rounding, the
+    persistent kernel contracting multiply-adds differently), with per-trajectory end times
+    and time rows, and with records split in tiers (a small first capacity)."""
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    spec = field_spec(field)
+    rng = np.random.default_rng(11)
+    n = 700
+    y0 = torch.tensor(rng.uniform(-2, 2, (n, spec.dim)), device=cuda)
+    if field == "vdp":
+        p = torch.tensor(10 ** rng.uniform(-1, 1.5, (n, 1)), device=cuda)
+    else:
+        p = torch.tensor(rng.uniform(20, 30, (n, 1)), device=cuda)
+        y0 = y0 + torch.tensor([1.0, 0.0, 0.0], device=cuda)
+    t1v = torch.tensor(10 ** rng.uniform(-1, 1, n), device=cuda)
+    ts = t1v[:, None] * torch.linspace(0.0, 1.0, 16, dtype=torch.float64, device=cuda)[None, :]
+    ts[:, 5] = ts[:, 4]  # a repeated time
+    for cap0 in (1024, 16):  # one record, and tiers
+        r = engine.forward_record(method, spec, y0, p, t0=0.0, t1=float(t1v.max()), t1v=t1v,
+                                  rtol=1e-6, atol=1e-9, max_steps=200000, cap0=cap0,
+                                  checkpoint=4, precision=prec, saveat_ts=ts)
+        torch.cuda.synchronize()
+        assert int((r.status != 0).sum()) == 0
+        yf, ys = engine.replay_saveat(r, y0, p, ts, write_ckpt=False, precision=prec)
+        torch.cuda.synchronize()
+        assert r.ys.shape == ys.shape
+        if method == "tsit5":
+            assert torch.equal(r.ys, ys), cap0
+            assert torch.equal(r.y_final, yf)
+        else:
+            assert rowrel(r.ys.cpu().numpy(), ys.cpu().numpy()) <= 1e-10
+        assert torch.equal(r.ys[:, -1], r.y_final)  # ts[-1] = t1: y_final itself
+        assert torch.equal(r.ys[:, 0], y0)          # ts[0] = t0: y0 itself

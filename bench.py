@@ -597,9 +597,9 @@ def run_workload(args) -> None:
             pt = torch.tensor(g.pilot_p, device=dev)
             r = engine.forward_record(g.method, g.spec, g.y0_d, pt, t0=0.0, t1=g.t1,
                                       t1v=g.t1v_d, rtol=g.rtol, atol=g.atol, dt0=g.dt0,
-                                      cap0=g.cap, checkpoint="auto")
+                                      cap0=g.cap, checkpoint=8, saveat_ts=g.ts_d)
             engine.raise_on_failed(r, 100000, g.t1)
-            g.target = engine.replay_saveat(r, g.y0_d, pt, g.ts_d, write_ckpt=False)[1]
+            g.target = r.ys
             del r
             torch.cuda.empty_cache()
         g.ws = None
@@ -617,10 +617,12 @@ def run_workload(args) -> None:
         """forward (record) + loss cotangent + reverse pass; with ``r`` given, the record is
         replayed instead (same mesh) in precision ``prec``."""
         if r is None:
+            # the forward also produces the saved states (no replay at the recording point)
             r = engine.forward_record(g.method, g.spec, g.y0_d, g.p_d, t0=0.0, t1=g.t1,
                                       t1v=g.t1v_d, rtol=g.rtol, atol=g.atol, dt0=g.dt0,
                                       max_steps=100000, cap0=g.cap, checkpoint=args.checkpoint,
-                                      precision=prec, workspace=g.ws, schedule=args.schedule)
+                                      precision=prec, workspace=g.ws, schedule=args.schedule,
+                                      saveat_ts=g.ts_d)
             g.ws = r
             replay_ck = False
         else:
@@ -632,10 +634,14 @@ def run_workload(args) -> None:
                                      precision=prec, schedule=args.schedule,
                                      variant=args.adjoint_variant)
         else:
-            _yf, ys = engine.replay_saveat(r, g.y0_d, g.p_d, g.ts_d, write_ckpt=replay_ck,
-                                           precision=prec)
+            if replay_ck:
+                _yf, ys = engine.replay_saveat(r, g.y0_d, g.p_d, g.ts_d, write_ckpt=True,
+                                               precision=prec)
+            else:
+                ys = r.ys
             gy0, gp = engine.adjoint_saveat(r, g.p_d, g.ts_d, cotangent(g, r, prec, ys),
-                                            want_y0=False, precision=prec)
+                                            want_y0=False, precision=prec,
+                                            schedule=args.schedule)
         return r, gp
 
     def prec_of(g, variant):

@@ -7,9 +7,13 @@
 //   k3 = W\(f(ynew) - e32 (k2 - F1) - 2 (k1 - F0));  err_vec = h/6 (k1 - 2 k2 + k3);
 //   WRMS norm, accept iff err <= 1, dt = h*clip(0.9*max(err,1e-10)^(-1/3), 0.2, 5) after both
 //   outcomes.  W is factored once per attempt (partial pivoting, division by the pivot) and
-//   the three solves reuse the factors: the same operations, in the same order, as the
+//   the three solves reuse the factors: the same elimination, in the same order, as the
 //   reference kernel's three fresh eliminations (_gauss_solve, :346-381), because a row swap
-//   moves the stored multipliers with the row.  The 3x3 LU stays in registers.
+//   moves the stored multipliers with the row.  The 3x3 LU stays in registers.  The
+//   multipliers are divisions by the pivot, as in the reference; the back substitutions
+//   multiply by the pivot's reciprocal, computed once per factorisation, instead of dividing
+//   by it in every solve (within an ulp of the division per solve; it takes the dependent
+//   divisions off each attempt's critical path).
 // Replay: gradsolve/solvers/rosenbrock23_step.py:47-66 (no k3) with the analytic Jacobian.
 // Adjoint: reverse of that step, including the second-order term through W = I - d dt J(y,p):
 //   Wbar = -(W^-T k2bar) k2'^T - (W^-T k1bar) k1^T,  then  d<-d dt Wbar, J(y,p)>/d(y,p).
@@ -24,6 +28,7 @@ namespace gs {
 template <int D>
 struct LU {
   double a[D * D];  // L (unit, below diagonal) and U (on/above), row-swapped
+  double inv[D];    // 1 / U's diagonal
   int piv[D];
 };
 
@@ -64,6 +69,8 @@ __device__ __forceinline__ void lu_factor(LU<D>& f) {
       for (int c = col + 1; c < D; ++c) f.a[r * D + c] = f.a[r * D + c] - factor * f.a[col * D + c];
     }
   }
+#pragma unroll
+  for (int i = 0; i < D; ++i) f.inv[i] = 1.0 / f.a[i * D + i];
 }
 
 // x = W^-1 b
@@ -90,7 +97,7 @@ __device__ __forceinline__ void lu_solve(const LU<D>& f, const double* b, double
     double s = x[i];
 #pragma unroll
     for (int c = i + 1; c < D; ++c) s = s - f.a[i * D + c] * x[c];
-    x[i] = s / f.a[i * D + i];
+    x[i] = s * f.inv[i];
   }
 }
 
@@ -102,7 +109,7 @@ __device__ __forceinline__ void lu_solve_t(const LU<D>& f, const double* b, doub
     double s = b[i];
 #pragma unroll
     for (int jj = 0; jj < i; ++jj) s = s - f.a[jj * D + i] * x[jj];
-    x[i] = s / f.a[i * D + i];
+    x[i] = s * f.inv[i];
   }
 #pragma unroll
   for (int ii = 0; ii < D; ++ii) {

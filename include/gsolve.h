@@ -205,7 +205,8 @@ int gs_replay_saveat(int method, int field, int precision, long long n, const do
  * produces the dense output of gs_replay_saveat at the same time: each requested time is
  * re-stepped from the start of the accepted step that brackets it, as the trajectory is
  * integrated, so the recording point needs no separate replay pass.  ys equals what
- * gs_replay_saveat gives on the recorded mesh (bitwise for Tsit5).  Runs the persistent
+ * gs_replay_saveat gives on the recorded mesh to rounding (the same step function, compiled
+ * into another kernel).  Runs the persistent
  * kernel: lanes refilled from a work counter when trajectories have their own end times (or
  * GS_SCHED_REFILL is set; needs ckpt), strided otherwise.  No counterpart in the reference,
  * whose saveat always replays the recorded mesh (gradsolve/warp/warp_replay.py:58-84).

@@ -176,9 +176,11 @@ def test_mixed_saveat_close_to_f64(gslib, cuda):
                                                ("rosenbrock23", "vdp", "float64")])
 def test_forward_dense_output_equals_replay(gslib, cuda, method, field, prec):
     """The forward that re-steps each bracketed time as it integrates gives the dense output
-    of replay_saveat on the recorded mesh (Tsit5 bitwise; Rosenbrock23 to rounding, the
-    persistent kernel contracting multiply-adds differently), with per-trajectory end times
-    and time rows, and with records split in tiers (a small first capacity)."""
+    of replay_saveat on the recorded mesh, with per-trajectory end times and time rows, and
+    with records split in tiers (a small first capacity).  The re-step is the replay's own
+    step function, but inlined into a different kernel the compiler may contract its
+    multiply-adds differently, so saved states agree to rounding (each is one step from a
+    bitwise-equal state); y0 and y_final rows are copies and equal bitwise."""
     from gradsolve_b200 import engine
     from gradsolve_b200.fields import field_spec
     spec = field_spec(field)
@@ -202,10 +204,8 @@ def test_forward_dense_output_equals_replay(gslib, cuda, method, field, prec):
         yf, ys = engine.replay_saveat(r, y0, p, ts, write_ckpt=False, precision=prec)
         torch.cuda.synchronize()
         assert r.ys.shape == ys.shape
+        assert rowrel(r.ys.cpu().numpy(), ys.cpu().numpy()) <= 1e-12, cap0
         if method == "tsit5":
-            assert torch.equal(r.ys, ys), cap0
             assert torch.equal(r.y_final, yf)
-        else:
-            assert rowrel(r.ys.cpu().numpy(), ys.cpu().numpy()) <= 1e-10
         assert torch.equal(r.ys[:, -1], r.y_final)  # ts[-1] = t1: y_final itself
         assert torch.equal(r.ys[:, 0], y0)          # ts[0] = t0: y0 itself

@@ -177,10 +177,17 @@ class RecordSet:
     re-solves the whole batch instead (gradsolve/solvers/record_jax.py:192-199).  Memory then
     follows the step-count distribution (the sum over tiers of rows x capacity) rather than
     n x the longest trajectory, and each tier's launch holds trajectories of similar length.
-    ``parts`` lists (rows, Record): rows None for the first tier (all trajectories), else the
+
+    ``parts`` lists (rows, Record): rows None for a tier covering every trajectory, else the
     sorted batch indices the tier covers; a later tier's results replace the earlier ones for
-    its rows.  Per-trajectory results are bitwise those of a single record (trajectories are
-    independent and every tier runs the same kernel)."""
+    its rows.  Per-trajectory results are those of a single record (trajectories are
+    independent and every tier runs the same kernel).
+
+    A RecordSet passed back as the ``workspace`` of the next solve of the same batch is a
+    plan: each trajectory goes straight to the tier that held it last time, every tier is
+    launched at once on its own stream (the long-trajectory tier overlaps the bulk instead of
+    following it), and only trajectories that outgrow their tier are re-solved.  The replay
+    and reverse passes also run the tiers concurrently, on the same streams."""
     method: str
     spec: FieldSpec
     n: int
@@ -193,6 +200,7 @@ class RecordSet:
     status: torch.Tensor
     uneven: bool = False
     ys: Optional[torch.Tensor] = None
+    streams: Optional[list] = None  # per part: None (the caller's stream) or a side stream
 
     @property
     def cap(self) -> int:
@@ -205,6 +213,16 @@ class RecordSet:
     @property
     def nbytes(self) -> int:
         return sum(r.rec.numel() * 8 + r.ckpt.numel() * 8 for _, r in self.parts)
+
+    def plan_rows(self) -> list:
+        """For each part, the rows whose final tier it is (sorted)."""
+        owner = torch.zeros(self.n, dtype=torch.int64, device=self.y_final.device)
+        for k, (rows, _r) in enumerate(self.parts):
+            if rows is None:
+                owner.fill_(k)
+            else:
+                owner.index_fill_(0, rows, k)
+        return [torch.nonzero(owner == k).squeeze(1) for k in range(len(self.parts))]
 
     def padded_dts(self, S: Optional[int] = None) -> torch.Tensor:
         if S is None:
@@ -229,6 +247,8 @@ class RecordSet:
             if prow is None:
                 out.copy_(r.dts_rows(rows, S))
                 continue
+            if prow.numel() == 0:
+                continue
             pos = torch.searchsorted(prow, rows).clamp_max(prow.numel() - 1)
             hit = prow[pos] == rows
             if bool(hit.any()):
@@ -242,9 +262,51 @@ def _parts(r):
 
 
 def _take(t: Optional[torch.Tensor], rows: Optional[torch.Tensor]):
+    """Rows of t on the current stream (t stays alive until this stream has read it)."""
     if t is None or rows is None:
         return t
+    if t.is_cuda:
+        t.record_stream(torch.cuda.current_stream())
     return t.index_select(0, rows).contiguous()
+
+
+def _take_ts(ts: Optional[torch.Tensor], rows: Optional[torch.Tensor]):
+    return ts if (ts is None or ts.ndim == 1) else _take(ts, rows)
+
+
+def _side_stream(device):
+    """A stream for a tier that should overlap the others (None off the GPU: tiers then run
+    one after another on the current stream)."""
+    return torch.cuda.Stream(device=device) if device.type == "cuda" else None
+
+
+def _over_parts(r, fn) -> list:
+    """fn(record, rows) -> tuple of tensors (or None), for every part of r.  The first part
+    runs on the caller's stream; the others on their own streams, launched first so that
+    they overlap it.  Returns [(rows, outputs)], all ready for use on the caller's stream."""
+    parts = _parts(r)
+    streams = getattr(r, "streams", None) or [None] * len(parts)
+    if all(st is None for st in streams):
+        return [(rows, fn(rr, rows)) for rows, rr in parts]
+    main = torch.cuda.current_stream()
+    out = [None] * len(parts)
+    order = [k for k in range(len(parts)) if streams[k] is not None] + \
+            [k for k in range(len(parts)) if streams[k] is None]
+    for k in order:
+        st = streams[k]
+        if st is None:
+            out[k] = fn(parts[k][1], parts[k][0])
+            continue
+        st.wait_stream(main)
+        with torch.cuda.stream(st):
+            out[k] = fn(parts[k][1], parts[k][0])
+    for k in range(len(parts)):
+        if streams[k] is not None:
+            main.wait_stream(streams[k])
+            for t in out[k]:
+                if t is not None:
+                    t.record_stream(main)
+    return [(parts[k][0], out[k]) for k in range(len(parts))]
 
 
 def _alloc_record(n: int, cap: int, dim: int, K: int, device) -> tuple:
@@ -263,101 +325,198 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
                    t1v: Optional[torch.Tensor] = None, max_steps: int = 100000,
                    cap0: int = DEFAULT_CAP0, checkpoint="auto",
                    budget_bytes: Optional[int] = None, precision: str = "float64",
-                   record: bool = True, workspace: Optional[Record] = None,
-                   schedule: str = "auto", saveat_ts: Optional[torch.Tensor] = None) -> Record:
+                   record: bool = True, workspace=None,
+                   schedule: str = "auto", saveat_ts: Optional[torch.Tensor] = None):
     """Adaptive solve on the device; with ``record`` the dts and checkpoints are kept.
 
-    ``y0`` (n, D) and ``p`` (n, P) float64 contiguous device tensors.  ``workspace``: a Record
-    from an earlier call of the same shape whose buffers are reused (overwritten) instead of
-    allocating new ones -- the steady-state pattern of a training loop.  ``saveat_ts`` ((K,)
-    shared or (n, K) per trajectory, sorted): the forward also produces the dense output
-    ``r.ys`` (n, K, D) -- what ``replay_saveat`` gives on the recorded mesh -- so the
-    recording point needs no replay pass."""
+    ``y0`` (n, D) and ``p`` (n, P) float64 contiguous device tensors.  ``workspace``: the
+    Record (or RecordSet) of an earlier call on the same batch, whose buffers are reused
+    (overwritten) instead of allocating new ones -- the steady-state pattern of a training
+    loop; a RecordSet also plans the tiers.  ``saveat_ts`` ((K,) shared or (n, K) per
+    trajectory, sorted): the forward also produces the dense output ``r.ys`` (n, K, D) --
+    what ``replay_saveat`` gives on the recorded mesh -- so the recording point needs no
+    replay pass.  Returns a Record, or a RecordSet when trajectories needed more than ``cap0``
+    steps."""
     n = y0.shape[0]
     device = y0.device
-    L = _lib.lib()
-    fn = L.gs_tsit5_fwd_record if method == METHOD_TSIT5 else L.gs_ros23_fwd_record
     ws = workspace if (workspace is not None and workspace.n == n and
-                       workspace.spec.dim == spec.dim) else None
-    yf = ws.y_final if ws is not None else torch.empty_like(y0)
-    n_acc = ws.n_acc if ws is not None else torch.empty(n, dtype=torch.int32, device=device)
-    n_rej = ws.n_rej if ws is not None else torch.empty(n, dtype=torch.int32, device=device)
-    status = ws.status if ws is not None else torch.empty(n, dtype=torch.int32, device=device)
-    dt0_arg = -1.0 if dt0 is None else float(dt0)
-    mode = _PREC[precision] | _SCHED[schedule]
+                       workspace.spec.dim == spec.dim and workspace.method == method) else None
+    kw = dict(t0=t0, t1=t1, rtol=rtol, atol=atol, dt0=dt0, max_steps=max_steps,
+              checkpoint=checkpoint, budget_bytes=budget_bytes, precision=precision,
+              schedule=schedule)
     if not record:
-        _lib.check(fn(spec.code, mode, n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
-                      float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), 0, 1, None,
-                      None, _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status), _stream()),
+        L = _lib.lib()
+        fn = L.gs_tsit5_fwd_record if method == METHOD_TSIT5 else L.gs_ros23_fwd_record
+        wsr = ws if isinstance(ws, Record) else None
+        yf = wsr.y_final if wsr is not None else torch.empty_like(y0)
+        n_acc, n_rej, status = (
+            (wsr.n_acc, wsr.n_rej, wsr.status) if wsr is not None else
+            tuple(torch.empty(n, dtype=torch.int32, device=device) for _ in range(3)))
+        _lib.check(fn(spec.code, _PREC[precision] | _SCHED[schedule], n, _ptr(y0), _ptr(p),
+                      float(t0), _ptr(t1v), float(t1), float(rtol), float(atol),
+                      -1.0 if dt0 is None else float(dt0), int(max_steps), 0, 1, None, None,
+                      _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status), _stream()),
                    fn.__name__)
         empty = torch.empty(0, dtype=torch.float64, device=device)
         return Record(method, spec, n, float(t0), 0, 1, empty, empty, yf, n_acc, n_rej, status,
                       uneven=t1v is not None)
-    ws_sub = ws.sub if isinstance(ws, RecordSet) else None
-    ws = ws.parts[0][1] if isinstance(ws, RecordSet) else ws
-    cap = max(1, min(int(cap0), int(max_steps)))
     if checkpoint == "auto" and tuned_ckpt_every(method, spec, precision) is None and n >= 4096:
         autotune_ckpt_every(method, spec, y0, p, t0=t0, t1=t1, t1v=t1v, rtol=rtol, atol=atol,
                             max_steps=max_steps, precision=precision)
-    K = choose_ckpt_every(checkpoint, spec.dim, n, cap, budget_bytes,
+    if isinstance(ws, RecordSet):
+        return _forward_planned(method, spec, y0, p, t1v, saveat_ts, ws, kw)
+    cap = max(1, min(int(cap0), int(max_steps)))
+    r0 = _forward_one(method, spec, y0, p, t1v, saveat_ts, cap, ws, kw)
+    return _grow(method, spec, y0, p, t1v, saveat_ts, r0, None, kw)
+
+
+def _forward_one(method, spec, y0, p, t1v, saveat_ts, cap, ws, kw) -> Record:
+    """One record of capacity ``cap`` for all rows of y0 (buffers reused from ws if they
+    match), on the current stream."""
+    n = y0.shape[0]
+    device = y0.device
+    L = _lib.lib()
+    precision = kw["precision"]
+    K = choose_ckpt_every(kw["checkpoint"], spec.dim, n, cap, kw["budget_bytes"],
                           tuned_ckpt_every(method, spec, precision))
-    if ws is not None and ws.cap == cap and ws.ckpt_every == K and ws.rec.numel() > 2:
+    ok = ws is not None and ws.n == n
+    yf = ws.y_final if ok else torch.empty_like(y0)
+    n_acc, n_rej, status = ((ws.n_acc, ws.n_rej, ws.status) if ok else
+                            tuple(torch.empty(n, dtype=torch.int32, device=device)
+                                  for _ in range(3)))
+    if ok and ws.cap == cap and ws.ckpt_every == K and ws.rec.numel() > 2:
         rec, ckpt = ws.rec, ws.ckpt
     else:
         rec, ckpt = _alloc_record(n, cap, spec.dim, K, device)
+    mode = _PREC[precision] | _SCHED[kw["schedule"]]
+    dt0_arg = -1.0 if kw["dt0"] is None else float(kw["dt0"])
+    args = (float(kw["t0"]), _ptr(t1v), float(kw["t1"]), float(kw["rtol"]), float(kw["atol"]),
+            dt0_arg, int(kw["max_steps"]), cap, K, _ptr(rec), _ptr(ckpt), _ptr(yf),
+            _ptr(n_acc), _ptr(n_rej), _ptr(status))
     ys = None
-    if saveat_ts is None:
-        _lib.check(fn(spec.code, mode, n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
-                      float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), cap, K,
-                      _ptr(rec), _ptr(ckpt), _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status),
-                      _stream()), fn.__name__)
+    if n == 0:
+        pass
+    elif saveat_ts is None:
+        fn = L.gs_tsit5_fwd_record if method == METHOD_TSIT5 else L.gs_ros23_fwd_record
+        _lib.check(fn(spec.code, mode, n, _ptr(y0), _ptr(p), *args, _stream()), fn.__name__)
     else:
         ts, ld, Kt = _ts_arg(saveat_ts, n)
-        ys = (ws.ys if ws is not None and ws.ys is not None and ws.ys.shape == (n, Kt, spec.dim)
+        ys = (ws.ys if ok and ws.ys is not None and ws.ys.shape == (n, Kt, spec.dim)
               else torch.empty((n, Kt, spec.dim), dtype=torch.float64, device=device))
-        _lib.check(L.gs_fwd_record_saveat(
-            _METHOD_CODE[method], spec.code, mode, n, _ptr(y0), _ptr(p), float(t0), _ptr(t1v),
-            float(t1), float(rtol), float(atol), dt0_arg, int(max_steps), cap, K, _ptr(rec),
-            _ptr(ckpt), _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status), _ptr(ts), ld, Kt,
-            _ptr(ys), _stream()), "gs_fwd_record_saveat")
-    r0 = Record(method, spec, n, float(t0), cap, K, rec, ckpt, yf, n_acc, n_rej, status,
-                uneven=t1v is not None, ys=ys)
-    if n == 0 or cap >= max_steps:
+        _lib.check(L.gs_fwd_record_saveat(_METHOD_CODE[method], spec.code, mode, n, _ptr(y0),
+                                          _ptr(p), *args, _ptr(ts), ld, Kt, _ptr(ys),
+                                          _stream()), "gs_fwd_record_saveat")
+    if n == 0 and saveat_ts is not None:
+        ys = torch.empty((0, _ts_arg(saveat_ts, 0)[2] if saveat_ts.ndim == 1 else
+                          saveat_ts.shape[1], spec.dim), dtype=torch.float64, device=device)
+    return Record(method, spec, n, float(kw["t0"]), cap, K, rec, ckpt, yf, n_acc, n_rej,
+                  status, uneven=t1v is not None, ys=ys)
+
+
+def _assemble(method, spec, n, device, parts, t1v, saveat_ts, streams, sub=None):
+    """Batch-order results of the parts (later parts win for shared rows)."""
+    D = spec.dim
+    yf = torch.empty((n, D), dtype=torch.float64, device=device)
+    n_acc, n_rej, status = (torch.empty(n, dtype=torch.int32, device=device) for _ in range(3))
+    ys = None
+    for rows, rr in parts:
+        if rows is None:
+            yf.copy_(rr.y_final), n_acc.copy_(rr.n_acc), n_rej.copy_(rr.n_rej)
+            status.copy_(rr.status)
+        else:
+            yf.index_copy_(0, rows, rr.y_final)
+            n_acc.index_copy_(0, rows, rr.n_acc)
+            n_rej.index_copy_(0, rows, rr.n_rej)
+            status.index_copy_(0, rows, rr.status)
+        if rr.ys is not None:
+            if ys is None:
+                ys = torch.empty((n,) + tuple(rr.ys.shape[1:]), dtype=torch.float64,
+                                 device=device)
+            if rows is None:
+                ys.copy_(rr.ys)
+            else:
+                ys.index_copy_(0, rows, rr.ys)
+    return RecordSet(method, spec, n, float(parts[0][1].t0), parts, sub, yf, n_acc, n_rej,
+                     status, uneven=t1v is not None, ys=ys, streams=streams)
+
+
+def _grow(method, spec, y0, p, t1v, saveat_ts, r0, streams, kw):
+    """Re-solve the rows of r0 (a Record over all of y0's rows) that overflowed it, in further
+    tiers; r0 alone when nothing overflowed."""
+    n = y0.shape[0]
+    max_steps = int(kw["max_steps"])
+    if n == 0 or r0.cap >= max_steps:
         return r0
-    rows = torch.nonzero(status == 3).squeeze(1)
+    rows = torch.nonzero(r0.status == 3).squeeze(1)
     if rows.numel() == 0:
         return r0
-    # the next tier: only the trajectories whose record overflowed, with TIER_GROWTH x capacity
-    sub = forward_record(method, spec, y0.index_select(0, rows).contiguous(),
-                         p.index_select(0, rows).contiguous(), t0=t0, t1=t1, rtol=rtol,
-                         atol=atol, dt0=dt0,
-                         t1v=None if t1v is None else t1v.index_select(0, rows).contiguous(),
-                         max_steps=max_steps, cap0=min(TIER_GROWTH * cap, int(max_steps)),
-                         checkpoint=checkpoint, budget_bytes=budget_bytes,
-                         precision=precision,
-                         workspace=ws_sub if (ws_sub is not None and ws_sub.n == rows.numel())
-                         else None, schedule=schedule,
-                         saveat_ts=None if saveat_ts is None else
-                         (saveat_ts if saveat_ts.ndim == 1 else _take(saveat_ts, rows)))
-    # the batch's results: the first tier's, with the overflowed rows replaced.  The first
-    # tier's own Record keeps its counts (at most its capacity) for its own kernels.
-    yf_all, acc_all, rej_all, st_all = yf.clone(), n_acc.clone(), n_rej.clone(), status.clone()
-    yf_all.index_copy_(0, rows, sub.y_final)
-    acc_all.index_copy_(0, rows, sub.n_acc)
-    rej_all.index_copy_(0, rows, sub.n_rej)
-    st_all.index_copy_(0, rows, sub.status)
-    ys_all = None
-    if ys is not None:
-        ys_all = ys.clone()
-        ys_all.index_copy_(0, rows, sub.ys)
+    sub = forward_record(method, spec, _take(y0, rows), _take(p, rows), t1v=_take(t1v, rows),
+                         cap0=min(TIER_GROWTH * r0.cap, max_steps),
+                         saveat_ts=_take_ts(saveat_ts, rows), **kw)
+    parts = [(None, r0)]
+    for srows, rr in _parts(sub):
+        parts.append((rows if srows is None else rows.index_select(0, srows), rr))
+    out = _assemble(method, spec, n, y0.device, parts, t1v, saveat_ts,
+                    [None] + [_side_stream(y0.device) for _ in parts[1:]], sub)
     # in the first tier the overflowed rows become empty (0 steps), so its replay and reverse
     # passes skip them instead of integrating a truncated record whose result is replaced
-    n_acc.index_fill_(0, rows, 0)
-    parts = [(None, r0)]
-    for srows, rr in (sub.parts if isinstance(sub, RecordSet) else [(None, sub)]):
-        parts.append((rows if srows is None else rows.index_select(0, srows), rr))
-    return RecordSet(method, spec, n, float(t0), parts, sub, yf_all, acc_all, rej_all, st_all,
-                     uneven=t1v is not None, ys=ys_all)
+    r0.n_acc.index_fill_(0, rows, 0)
+    return out
+
+
+def _forward_planned(method, spec, y0, p, t1v, saveat_ts, ws: RecordSet, kw):
+    """The tiers of ws, re-solved directly: every trajectory in the tier that held it last
+    time, all tiers at once (side streams), overflowing rows re-solved afterwards."""
+    n = y0.shape[0]
+    rows_by_part = ws.plan_rows()
+    keep = [k for k in range(len(ws.parts)) if rows_by_part[k].numel() > 0]
+    old = [ws.streams[k] if ws.streams is not None else None for k in keep]
+    streams = [None] + [old[i] if old[i] is not None else _side_stream(y0.device)
+                        for i in range(1, len(keep))]
+    plan = [(rows_by_part[k], ws.parts[k][1]) for k in keep]
+    launch = lambda rows, wsr: _forward_one(  # noqa: E731
+        method, spec, _take(y0, rows), _take(p, rows), _take(t1v, rows),
+        _take_ts(saveat_ts, rows), wsr.cap, wsr, kw)
+    out = [None] * len(plan)
+    if all(st is None for st in streams):
+        out = [(rows, launch(rows, wsr)) for rows, wsr in plan]
+    else:
+        main = torch.cuda.current_stream()
+        for i in list(range(1, len(plan))) + [0]:  # the side tiers first, to overlap tier 0
+            rows, wsr = plan[i]
+            st = streams[i]
+            if st is not None:
+                st.wait_stream(main)
+            with torch.cuda.stream(st if st is not None else main):
+                out[i] = (rows, launch(rows, wsr))
+        for i in range(1, len(plan)):
+            main.wait_stream(streams[i])
+            rr = out[i][1]
+            for t in (rr.y_final, rr.n_acc, rr.n_rej, rr.status, rr.ys):
+                if t is not None:
+                    t.record_stream(main)
+    res = _assemble(method, spec, n, y0.device, out, t1v, saveat_ts, streams)
+    # trajectories that outgrew their planned tier: solved again with more capacity
+    over = torch.nonzero(res.status == 3).squeeze(1)
+    if over.numel() == 0:
+        return res
+    cap_of_row = torch.zeros(n, dtype=torch.int64, device=y0.device)
+    for rows, rr in out:
+        cap_of_row.index_fill_(0, rows, rr.cap)
+    grown = min(TIER_GROWTH * int(cap_of_row[over].max().item()), int(kw["max_steps"]))
+    sub = forward_record(method, spec, _take(y0, over), _take(p, over), t1v=_take(t1v, over),
+                         cap0=grown, saveat_ts=_take_ts(saveat_ts, over), **kw)
+    parts = list(out)
+    for rows, rr in out:  # empty the overflowed rows in the tiers that held them
+        pos = torch.searchsorted(rows, over).clamp_max(max(rows.numel() - 1, 0))
+        hit = rows[pos] == over if rows.numel() else torch.zeros_like(over, dtype=torch.bool)
+        if bool(hit.any()):
+            rr.n_acc.index_fill_(0, pos[hit], 0)
+    for srows, rr in _parts(sub):
+        parts.append((over if srows is None else over.index_select(0, srows), rr))
+    return _assemble(method, spec, n, y0.device, parts, t1v, saveat_ts,
+                     streams + [_side_stream(y0.device) for _ in parts[len(out):]],
+                     sub)
 
 
 def raise_on_failed(r: Record, max_steps: int, t1) -> None:
@@ -386,14 +545,24 @@ def raise_on_failed(r: Record, max_steps: int, t1) -> None:
 def replay(r, y0: torch.Tensor, p: torch.Tensor, *, write_ckpt: bool = True,
            precision: str = "float64") -> torch.Tensor:
     """Frozen-mesh replay at (y0, p); refreshes the checkpoints for a following adjoint."""
-    out = None
-    for rows, rr in _parts(r):
-        yf = _replay_one(rr, _take(y0, rows), _take(p, rows), write_ckpt=write_ckpt,
-                         precision=precision)
+    res = _over_parts(r, lambda rr, rows: (_replay_one(
+        rr, _take(y0, rows), _take(p, rows), write_ckpt=write_ckpt, precision=precision),))
+    return _scatter(r, res, 0)
+
+
+def _scatter(r, res, i):
+    """Output i of every part, in batch order (later parts win for shared rows)."""
+    first = res[0][1][i]
+    if len(res) == 1 and res[0][0] is None:
+        return first
+    if first is None:
+        return None
+    out = torch.empty((r.n,) + tuple(first.shape[1:]), dtype=first.dtype, device=first.device)
+    for rows, outs in res:
         if rows is None:
-            out = yf
+            out.copy_(outs[i])
         else:
-            out.index_copy_(0, rows, yf)
+            out.index_copy_(0, rows, outs[i])
     return out
 
 
@@ -421,19 +590,12 @@ def adjoint(r, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
     inputs from the segment's forward pass, "recompute" re-evaluates them in the reverse
     sweep; "auto" is "recompute" (the larger stage buffer costs more occupancy than the
     saved stage evaluations gain for the built-in fields)."""
-    gy0 = gp = None
-    for rows, rr in _parts(r):
-        a, b = _adjoint_one(rr, _take(p, rows), _take(ybar, rows), want_y0=want_y0,
-                            want_p=want_p, precision=precision, schedule=schedule,
-                            variant=variant)
-        if rows is None:
-            gy0, gp = a, b
-        else:
-            if a is not None:
-                gy0.index_copy_(0, rows, a)
-            if b is not None:
-                gp.index_copy_(0, rows, b)
-    return gy0, gp
+    if schedule == "auto" and r.uneven:
+        schedule = "refill"
+    res = _over_parts(r, lambda rr, rows: _adjoint_one(
+        rr, _take(p, rows), _take(ybar, rows), want_y0=want_y0, want_p=want_p,
+        precision=precision, schedule=schedule, variant=variant))
+    return _scatter(r, res, 0), _scatter(r, res, 1)
 
 
 def _adjoint_one(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool,
@@ -488,18 +650,10 @@ def replay_saveat(r, y0: torch.Tensor, p: torch.Tensor, ts: torch.Tensor, *,
                   write_ckpt: bool = True, precision: str = "float64"):
     """Frozen-mesh replay with dense output at ``ts`` ((K,) shared or (n, K) per trajectory).
     Returns (y_final (n, D), ys (n, K, D)); refreshes the checkpoints for the adjoint."""
-    yf = ys = None
-    per_row = ts.ndim == 2
-    for rows, rr in _parts(r):
-        a, b = _replay_saveat_one(rr, _take(y0, rows), _take(p, rows),
-                                  _take(ts, rows) if per_row else ts, write_ckpt=write_ckpt,
-                                  precision=precision)
-        if rows is None:
-            yf, ys = a, b
-        else:
-            yf.index_copy_(0, rows, a)
-            ys.index_copy_(0, rows, b)
-    return yf, ys
+    res = _over_parts(r, lambda rr, rows: _replay_saveat_one(
+        rr, _take(y0, rows), _take(p, rows), _take_ts(ts, rows), write_ckpt=write_ckpt,
+        precision=precision))
+    return _scatter(r, res, 0), _scatter(r, res, 1)
 
 
 def _replay_saveat_one(r: Record, y0: torch.Tensor, p: torch.Tensor, ts: torch.Tensor, *,
@@ -521,22 +675,12 @@ def adjoint_saveat(r, p: torch.Tensor, ts: torch.Tensor, ysbar: torch.Tensor,
     """(dL/dy0, dL/dp) for cotangents ysbar = dL/dys (n, K, D) and ybar = dL/dy_final.
     ``schedule="auto"`` refills lanes from a work counter for an uneven batch (per-trajectory
     end times), else runs one thread per trajectory."""
-    gy0 = gp = None
-    per_row = ts.ndim == 2
     if schedule == "auto" and r.uneven:
         schedule = "refill"
-    for rows, rr in _parts(r):
-        a, b = _adjoint_saveat_one(rr, _take(p, rows), _take(ts, rows) if per_row else ts,
-                                   _take(ysbar, rows), _take(ybar, rows), want_y0=want_y0,
-                                   want_p=want_p, precision=precision, schedule=schedule)
-        if rows is None:
-            gy0, gp = a, b
-        else:
-            if a is not None:
-                gy0.index_copy_(0, rows, a)
-            if b is not None:
-                gp.index_copy_(0, rows, b)
-    return gy0, gp
+    res = _over_parts(r, lambda rr, rows: _adjoint_saveat_one(
+        rr, _take(p, rows), _take_ts(ts, rows), _take(ysbar, rows), _take(ybar, rows),
+        want_y0=want_y0, want_p=want_p, precision=precision, schedule=schedule))
+    return _scatter(r, res, 0), _scatter(r, res, 1)
 
 
 def _adjoint_saveat_one(r: Record, p: torch.Tensor, ts: torch.Tensor, ysbar: torch.Tensor,

@@ -204,8 +204,23 @@ def test_forward_dense_output_equals_replay(gslib, cuda, method, field, prec):
         yf, ys = engine.replay_saveat(r, y0, p, ts, write_ckpt=False, precision=prec)
         torch.cuda.synchronize()
         assert r.ys.shape == ys.shape
-        assert rowrel(r.ys.cpu().numpy(), ys.cpu().numpy()) <= 1e-12, cap0
-        if method == "tsit5":
-            assert torch.equal(r.y_final, yf)
+        # float32 stage increments round at ~1e-7 of the step: the two kernels' contractions
+        # differ at that level in the float32-stage mode
+        tol = 1e-12 if prec == "float64" else 1e-6
+        assert rowrel(r.ys.cpu().numpy(), ys.cpu().numpy()) <= tol, cap0
+        assert rowrel(r.y_final.cpu().numpy(), yf.cpu().numpy()) <= tol, cap0
         assert torch.equal(r.ys[:, -1], r.y_final)  # ts[-1] = t1: y_final itself
         assert torch.equal(r.ys[:, 0], y0)          # ts[0] = t0: y0 itself
+    # the tiered record as the workspace of the next solve: planned tiers on their own
+    # streams, the same per-trajectory results, and the same gradient
+    assert isinstance(r, engine.RecordSet) and len(r.parts) > 1
+    ysbar = torch.tensor(rng.normal(size=tuple(r.ys.shape)), device=cuda)
+    g1 = engine.adjoint_saveat(r, p, ts, ysbar, precision=prec)
+    r2 = engine.forward_record(method, spec, y0, p, t0=0.0, t1=float(t1v.max()), t1v=t1v,
+                               rtol=1e-6, atol=1e-9, max_steps=200000, cap0=16, checkpoint=4,
+                               precision=prec, saveat_ts=ts, workspace=r)
+    g2 = engine.adjoint_saveat(r2, p, ts, ysbar, precision=prec)
+    torch.cuda.synchronize()
+    for a, b in ((r.ys, r2.ys), (r.y_final, r2.y_final), (r.n_acc, r2.n_acc),
+                 (g1[0], g2[0]), (g1[1], g2[1])):
+        assert torch.equal(a, b)

@@ -198,3 +198,54 @@ def test_saveat_on_tiers_uses_each_rows_times(fake):
     ysbar = torch.ones((n, 2, 3), dtype=torch.float64) * torch.arange(n)[:, None, None]
     _gy0, gp = engine.adjoint_saveat(r, p, ts, ysbar)
     np.testing.assert_array_equal(gp[:, 0].numpy(), 6.0 * np.arange(n) + 1e6 * final_cap)
+
+
+def test_planned_tiers_from_the_workspace(fake):
+    """With the previous RecordSet as workspace, every trajectory goes straight to the tier
+    that held it (the side tiers are launched first), nothing is re-solved, and the results
+    are those of the first solve."""
+    spec = field_spec("lorenz")
+    steps = np.array([5, 3, 40, 7, 300, 2, 17, 1000], dtype=np.float64)
+    n = steps.size
+    y0 = torch.zeros((n, 3), dtype=torch.float64)
+    p = torch.tensor(steps[:, None])
+    kw = dict(t0=0.0, t1=1.0, rtol=1e-6, atol=1e-6, max_steps=5000, cap0=8, checkpoint=4,
+              budget_bytes=1 << 40)
+    r1 = engine.forward_record("tsit5", spec, y0, p, **kw)
+    fake.launches.clear()
+    r2 = engine.forward_record("tsit5", spec, y0, p, workspace=r1, **kw)
+    # (off the GPU the tiers run one after another; on it, side tiers first, concurrently)
+    assert sorted(fake.launches) == [(1, 32), (1, 128), (1, 512), (1, 2048), (4, 8)]
+    assert isinstance(r2, engine.RecordSet)
+    np.testing.assert_array_equal(r2.n_acc.numpy(), steps.astype(np.int32))
+    np.testing.assert_array_equal(r2.y_final.numpy(), r1.y_final.numpy())
+    np.testing.assert_array_equal(r2.padded_dts().numpy(), r1.padded_dts().numpy())
+    ybar = torch.arange(n * 3, dtype=torch.float64).reshape(n, 3)
+    a1, b1 = engine.adjoint(r1, p, ybar)
+    a2, b2 = engine.adjoint(r2, p, ybar)
+    np.testing.assert_array_equal(a1.numpy(), a2.numpy())
+    np.testing.assert_array_equal(b1.numpy(), b2.numpy())
+    # a third solve reuses the planned tiers' own buffers
+    fake.launches.clear()
+    r3 = engine.forward_record("tsit5", spec, y0, p, workspace=r2, **kw)
+    assert sorted(fake.launches) == [(1, 32), (1, 128), (1, 512), (1, 2048), (4, 8)]
+    assert r3.parts[0][1].rec.data_ptr() == r2.parts[0][1].rec.data_ptr()
+
+
+def test_planned_tier_outgrown(fake):
+    spec = field_spec("lorenz")
+    steps = np.array([5, 3, 40], dtype=np.float64)
+    y0 = torch.zeros((3, 3), dtype=torch.float64)
+    kw = dict(t0=0.0, t1=1.0, rtol=1e-6, atol=1e-6, max_steps=5000, cap0=8, checkpoint=4,
+              budget_bytes=1 << 40)
+    r1 = engine.forward_record("tsit5", spec, y0, torch.tensor(steps[:, None]), **kw)
+    steps2 = np.array([5, 20, 40], dtype=np.float64)  # row 1 now needs more than its tier
+    fake.launches.clear()
+    r2 = engine.forward_record("tsit5", spec, y0, torch.tensor(steps2[:, None]), workspace=r1,
+                               **kw)
+    # planned tiers (cap 8: rows 0, 1; cap 128: row 2), then row 1 again with 4 x 8
+    assert sorted(fake.launches[:2]) == [(1, 128), (2, 8)] and fake.launches[2:] == [(1, 32)]
+    np.testing.assert_array_equal(r2.n_acc.numpy(), steps2.astype(np.int32))
+    assert np.all(r2.status.numpy() == 0)
+    yf = engine.replay(r2, y0, torch.tensor(steps2[:, None]))
+    np.testing.assert_array_equal(yf[:, 0].numpy(), steps2 + 1000.0 * np.array([8, 32, 128]))

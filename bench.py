@@ -786,6 +786,87 @@ def cpu_workload_rate(groups, target_s: float) -> dict:
 
 
 
+# ------------------------------------------------------------------------------------
+# the reference's own published configuration (H200 NVL numbers, benchmarks/*.ipynb outputs)
+# ------------------------------------------------------------------------------------
+H200_GRAD_MS = {1e-3: 1.056, 1e-4: 1.479, 1e-5: 2.306, 1e-6: 3.417, 1e-7: 5.331, 1e-8: 8.342}
+H200_FWD_MS = {1e-3: 0.276, 1e-6: 0.657, 1e-8: 1.424}
+
+
+def run_published(args) -> None:
+    """Lorenz, rho = linspace(0, 21, n), y0 = (1, 0, 0), t in [0, 1], atol = rtol * 1e-3
+    (benchmarks/reverse_mode_vs_diffrax.py:59-65, benchmarks/forward_vs_diffeqgpu.py:116):
+    the gradient of sum(y_final^2) on a recorded mesh (replay + reverse pass, what
+    jax.grad of the closure runs per call) at n = 32768, and the forward-only solve lane at
+    n = 524288, beside the reference's published H200 NVL times."""
+    import torch
+
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+
+    spec = field_spec("lorenz")
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def inputs(n):
+        y0 = torch.tensor(np.tile([1.0, 0.0, 0.0], (n, 1)), device=dev)
+        rho = torch.tensor(np.linspace(0.0, 21.0, n)[:, None], device=dev)
+        return y0, rho
+
+    def timed(fn, reps):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        ms = []
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms)), float(np.min(ms))
+
+    grad = {}
+    y0, rho = inputs(32768)
+    for rtol in sorted(H200_GRAD_MS, reverse=True):
+        r = engine.forward_record("tsit5", spec, y0, rho, t0=0.0, t1=1.0, rtol=rtol,
+                                  atol=rtol * 1e-3, checkpoint="auto")
+        ybar = 2.0 * r.y_final
+
+        def g():
+            engine.replay(r, y0, rho, write_ckpt=True)
+            engine.adjoint(r, rho, ybar, want_y0=False)
+
+        def rec():
+            engine.forward_record("tsit5", spec, y0, rho, t0=0.0, t1=1.0, rtol=rtol,
+                                  atol=rtol * 1e-3, checkpoint="auto", workspace=r)
+        med, best = timed(g, args.steps)
+        rmed, _ = timed(rec, args.steps)
+        grad[f"{rtol:g}"] = {"ms": med, "ms_best": best, "h200_warp_replay_ms": H200_GRAD_MS[rtol],
+                             "ratio_h200_over_b200": H200_GRAD_MS[rtol] / best,
+                             "record_ms": rmed, "accepted_max": int(r.n_acc.max())}
+    fwd = {}
+    y0, rho = inputs(524288)
+    for rtol in sorted(H200_FWD_MS, reverse=True):
+        def f():
+            engine.forward_record("tsit5", spec, y0, rho, t0=0.0, t1=1.0, rtol=rtol,
+                                  atol=rtol * 1e-3, record=False)
+        med, best = timed(f, args.steps)
+        fwd[f"{rtol:g}"] = {"ms": med, "ms_best": best, "h200_cuda_tsit5_ms": H200_FWD_MS[rtol],
+                            "ratio_h200_over_b200": H200_FWD_MS[rtol] / best,
+                            "solves_per_s": 524288 / (best * 1e-3)}
+    print(json.dumps({
+        "workload": "published_h200", "n_gpus": 1, "dtype": "f64",
+        "data": "Lorenz, rho = linspace(0, 21, n), y0 = (1, 0, 0), t in [0, 1], atol = rtol*1e-3",
+        "gradient_n32768": grad, "forward_only_n524288": fwd,
+        "timing": "B200: CUDA events around the kernels (L2 flushed), median and best of "
+                  f"{args.steps}; H200: the reference's notebooks, host wall clock of the "
+                  "jitted call, best of 5",
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -803,12 +884,14 @@ def main():
     ap.add_argument("--schedule", default="auto", choices=["auto", "static", "refill", "strided"])
     ap.add_argument("--adjoint-variant", default="auto", choices=["auto", "stages", "recompute"])
     ap.add_argument("--workload", default="lorenz_2e20",
-                    choices=["lorenz_2e20"] + sorted(WORKLOAD_N))
+                    choices=["lorenz_2e20", "published_h200"] + sorted(WORKLOAD_N))
     args = ap.parse_args()
     if args.checkpoint not in ("sqrt", "all", "auto"):
         args.checkpoint = int(args.checkpoint)
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "published_h200":
+        run_published(args)
     elif args.workload != "lorenz_2e20":
         run_workload(args)
     else:

@@ -217,11 +217,12 @@ def _solve_saveat(name, problem, y0, params, saveat, *, rtol, atol, device, max_
     ts = validate_saveat(saveat, float(problem.t0), t1s,
                          None if t1v is None else t1v.cpu().numpy(), y0_t.shape[0])
     ms = int(max_steps or DEFAULT_MAX_STEPS[name])
+    # the forward re-steps each saved time as it integrates: no replay pass
     r = engine.forward_record(method, spec, y0_t, pk, t0=float(problem.t0), t1=t1s, t1v=t1v,
-                              rtol=rtol, atol=atol, max_steps=ms, checkpoint="sqrt")
+                              rtol=rtol, atol=atol, max_steps=ms, checkpoint="sqrt",
+                              saveat_ts=torch.as_tensor(ts, device=dev))
     engine.raise_on_failed(r, ms, t1s)
-    yf, ys = engine.replay_saveat(r, y0_t, pk, torch.as_tensor(ts, device=dev),
-                                  write_ckpt=False)
+    yf, ys = r.y_final, r.ys
     return SolveResult(y_final=yf.cpu().numpy(), y_saved=ys.cpu().numpy(), ts_saved=ts,
                        accepted_steps=r.n_acc.cpu().numpy().astype(np.int64),
                        rejected_steps=r.n_rej.cpu().numpy().astype(np.int64), solver=name)
@@ -242,17 +243,19 @@ def _normalize_wrt(wrt) -> tuple:
 
 def build_replay_state(problem, y0, params, *, method: str, rtol: float, atol: float,
                        device="cuda", max_steps: Optional[int] = None, checkpoint="auto",
-                       t1=None, precision: str = "float64"):
-    """Record the mesh once and return (ReplayState, y0 tensor, params tensor)."""
+                       t1=None, precision: str = "float64", saveat=None):
+    """Record the mesh once and return (ReplayState, y0 tensor, params tensor).  With saveat
+    (validated times on the device) the recording pass also keeps the saved states, which the
+    closure returns at the recording point instead of replaying."""
     dev = _device(device)
     spec, y0_t, p_t, pk = _prepare(problem, y0, params, dev)
     t1s, t1v = _t1_arg(problem, t1, dev)
     ms = int(max_steps or 100000)
     r = engine.forward_record(method, spec, y0_t, pk, t0=float(problem.t0), t1=t1s, t1v=t1v,
                               rtol=rtol, atol=atol, max_steps=ms, checkpoint=checkpoint,
-                              precision=precision)
+                              precision=precision, saveat_ts=saveat)
     engine.raise_on_failed(r, ms, t1s)
-    state = ReplayState(r, y0_t, pk, spec.nparam, precision=precision)
+    state = ReplayState(r, y0_t, pk, spec.nparam, precision=precision, ts_rec=saveat)
     return state, y0_t, p_t
 
 
@@ -264,17 +267,21 @@ def _make_reverse(name):
         if checkpoint is None:
             checkpoint = "auto" if remat is None else ("sqrt" if remat else "all")
         ms = max_steps or DEFAULT_MAX_STEPS[name]
+        ts = None
+        if saveat is not None:
+            dev0 = _device(device)
+            t1s, t1v = _t1_arg(problem, t1, dev0)
+            n = np.asarray(y0).shape[0] if not isinstance(y0, torch.Tensor) else y0.shape[0]
+            ts = torch.as_tensor(
+                validate_saveat(saveat, float(problem.t0), t1s,
+                                None if t1v is None else t1v.cpu().numpy(), n),
+                device=dev0)
         state, y0_t, p_t = build_replay_state(problem, y0, params, method=method, rtol=rtol,
                                               atol=atol, device=device, max_steps=ms,
                                               checkpoint=checkpoint, t1=t1,
-                                              precision=precision)
+                                              precision=precision, saveat=ts)
         dev = y0_t.device
         if saveat is not None:
-            t1s, t1v = _t1_arg(problem, t1, dev)
-            ts = torch.as_tensor(
-                validate_saveat(saveat, float(problem.t0), t1s,
-                                None if t1v is None else t1v.cpu().numpy(), y0_t.shape[0]),
-                device=dev)
 
             def kernel(z, p):  # the dense time series (n, k, dim), gradsolve/api.py:748-752
                 return saveat_apply(state, _as_tensor(z, dev), _as_tensor(p, dev), ts)

@@ -70,7 +70,9 @@ def choose_ckpt_every(policy, dim: int, n: int, cap: int, budget_bytes: Optional
         raise ValueError(f"checkpoint policy must be 'auto', 'all', 'sqrt' or an int; got {policy!r}")
     if budget_bytes is None:
         free, _total = torch.cuda.mem_get_info()
-        budget_bytes = free // 4
+        # memory the caching allocator holds but does not use is free for this purpose too
+        cached = torch.cuda.memory_reserved() - torch.cuda.memory_allocated()
+        budget_bytes = (free + max(cached, 0)) // 4
     K = tuned or 8
     while K < kmax and (cap // K + 2) * n * ckpt_width(dim) * 8 > budget_bytes:
         K *= 2
@@ -377,9 +379,12 @@ def _forward_one(method, spec, y0, p, t1v, saveat_ts, cap, ws, kw) -> Record:
     device = y0.device
     L = _lib.lib()
     precision = kw["precision"]
-    K = choose_ckpt_every(kw["checkpoint"], spec.dim, n, cap, kw["budget_bytes"],
-                          tuned_ckpt_every(method, spec, precision))
     ok = ws is not None and ws.n == n
+    if kw["checkpoint"] == "auto" and ok and ws.cap == cap and ws.rec.numel() > 2:
+        K = ws.ckpt_every  # sticky: the workspace's interval, so its buffers are reused
+    else:
+        K = choose_ckpt_every(kw["checkpoint"], spec.dim, n, cap, kw["budget_bytes"],
+                              tuned_ckpt_every(method, spec, precision))
     yf = ws.y_final if ok else torch.empty_like(y0)
     n_acc, n_rej, status = ((ws.n_acc, ws.n_rej, ws.status) if ok else
                             tuple(torch.empty(n, dtype=torch.int32, device=device)

@@ -6,7 +6,8 @@ A drop-in for the Tsit5 and Rosenbrock23 record-and-replay engines of gradsolve
 ABI of ``libgsolve.so`` (include/gsolve.h); PyTorch provides device memory, streams and
 autograd plumbing.
 """
-from .api import ALIASES, ENGINE_REGISTRY, grad_closure, solve  # noqa: F401
+from .api import (ALIASES, ENGINE_REGISTRY, grad_closure, register_field,  # noqa: F401
+                  register_jax_field, solve)
 from .base import Problem, Route, SolveResult  # noqa: F401
 from .fields import field_for, field_spec  # noqa: F401
 

@@ -70,6 +70,18 @@ class GsolveError(RuntimeError):
     """A libgsolve call returned a non-zero status."""
 
 
+_FIELD_LIBS: dict = {}
+
+
+def _load(path) -> ctypes.CDLL:
+    L = ctypes.CDLL(str(path))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    return L
+
+
 def lib():
     """Load libgsolve.so (once).  Raises if it has not been built."""
     global _LIB
@@ -78,18 +90,25 @@ def lib():
             raise RuntimeError(
                 f"{LIB_PATH} is missing: build it with `python -m gradsolve_b200.csrc.build` "
                 "(gradsolve_b200 has no CPU fallback).")
-        L = ctypes.CDLL(str(LIB_PATH))
-        for name, (res, args) in _SIGS.items():
-            fn = getattr(L, name)
-            fn.restype = res
-            fn.argtypes = args
-        _LIB = L
+        _LIB = _load(LIB_PATH)
     return _LIB
 
 
-def check(rc: int, what: str) -> None:
+def lib_for(spec):
+    """The library that serves a field: libgsolve.so, or a generated field's own library
+    (same C ABI, built by gradsolve_b200.fieldgen)."""
+    path = getattr(spec, "lib", "")
+    if not path:
+        return lib()
+    L = _FIELD_LIBS.get(path)
+    if L is None:
+        L = _FIELD_LIBS[path] = _load(path)
+    return L
+
+
+def check(rc: int, what: str, L=None) -> None:
     if rc != GS_OK:
-        msg = lib().gs_last_error().decode(errors="replace")
+        msg = (L or lib()).gs_last_error().decode(errors="replace")
         raise GsolveError(f"{what} failed ({rc}): {msg}")
 
 

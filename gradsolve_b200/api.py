@@ -342,3 +342,30 @@ for _name in list(ENGINE_REGISTRY):
                                         _make_reverse(_name))
 
 __all__ = ["solve", "grad_closure", "ENGINE_REGISTRY", "ALIASES", "FieldSpec"]
+
+
+def register_field(name: str, f, dim: int, n_params: int, *, stiff: bool = False) -> FieldSpec:
+    """Register a Python right-hand side ``f(t, y, p) -> dy`` (autonomous: t unused) so that
+    a Problem of that ``name`` routes to the B200 kernels like a built-in field.
+
+    Same contract as the reference's ``register_jax_field(name, f_jax, dim, n_params, *,
+    stiff=False)`` (gradsolve/__init__.py:31-42, gradsolve/warp/jax_field.py:517-560):
+    idempotent per name; ``stiff=True`` also derives the Jacobian so the Rosenbrock23 engine
+    can serve it.  ``f`` is traced once with symbolic scalars (``gradsolve_b200.fieldgen``);
+    the RHS, its VJP and (stiff) Jacobian and second-order term are generated as CUDA and
+    compiled into the field's own library (cached on disk by content)."""
+    from . import fieldgen
+    from . import fields as F
+    if name in F._USER:
+        return F._USER[name]
+    d = fieldgen.Derived(f, dim, n_params, stiff)
+    code = fieldgen.USER_CODE_BASE + (sum(name.encode()) * 7919) % 90000
+    path = fieldgen.build_field_library(fieldgen.emit_struct(d, name, code))
+    spec = FieldSpec(f"user_{name}", code, d.D, d.P, bool(stiff), str(path))
+    F._USER[name] = spec
+    return spec
+
+
+# the reference's name for the same registration (its f is a JAX function; here any
+# function of symbolic scalars: Python arithmetic, numpy ufuncs, gradsolve_b200.fieldgen)
+register_jax_field = register_field

@@ -19,6 +19,12 @@
 #include "gs_tableau.cuh"
 #include "gs_tsit5.cuh"
 
+#ifdef GS_USER_FIELD_HEADER
+// A library built for one generated field (gradsolve_b200/fieldgen.py): the header defines
+// gs::UserField, GS_USER_FIELD_CODE and GS_USER_STIFF, and only that field is dispatched.
+#include GS_USER_FIELD_HEADER
+#endif
+
 namespace {
 
 thread_local std::string g_err;
@@ -41,6 +47,37 @@ constexpr int kBlock = 128;
 
 unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
+#ifdef GS_USER_FIELD_HEADER
+int field_dims(int field, int* D, int* P) {
+  if (field == GS_USER_FIELD_CODE) {
+    *D = gs::UserField::D;
+    *P = gs::UserField::P;
+    return GS_OK;
+  }
+  return fail(GS_ERR_FIELD, "this library serves the generated field " +
+                                std::to_string(GS_USER_FIELD_CODE) + " only; got " +
+                                std::to_string(field));
+}
+
+#define GS_TSIT5_DISPATCH(field, FN, ...)                                                   \
+  switch (field) {                                                                          \
+    case GS_USER_FIELD_CODE: return FN<gs::UserField>(__VA_ARGS__);                        \
+    default: return fail(GS_ERR_FIELD, "unknown field code " + std::to_string(field));      \
+  }
+
+#if GS_USER_STIFF
+#define GS_ROS23_DISPATCH(field, FN, ...)                                                   \
+  switch (field) {                                                                          \
+    case GS_USER_FIELD_CODE: return FN<gs::UserField>(__VA_ARGS__);                        \
+    default: return fail(GS_ERR_FIELD, "unknown field code " + std::to_string(field));      \
+  }
+#else
+#define GS_ROS23_DISPATCH(field, FN, ...)                                                   \
+  return fail(GS_ERR_FIELD, "field " + std::to_string(field) +                              \
+                                " was registered without stiff=True (no Jacobian)");
+#endif
+
+#else
 int field_dims(int field, int* D, int* P) {
   switch (field) {
     case gs::FIELD_LORENZ: *D = 3; *P = 1; return GS_OK;
@@ -87,6 +124,8 @@ int field_dims(int field, int* D, int* P) {
       return fail(GS_ERR_FIELD,                                                             \
                   "field " + std::to_string(field) + " has no analytic Jacobian for Rosenbrock23"); \
   }
+
+#endif  // GS_USER_FIELD_HEADER
 
 // Launch shape of the adjoint kernels: each thread keeps its segment of K states (W doubles
 // each) in shared memory, so the block shrinks (by powers of two, at least one warp) until the

@@ -147,9 +147,9 @@ class Record:
         if S is None:
             S = int(self.n_acc.max().item()) if self.n else 0
         out = torch.zeros((self.n, S), dtype=torch.float64, device=self.rec.device)
-        _lib.check(_lib.lib().gs_record_to_padded(self.n, self.cap, _ptr(self.rec),
-                                                  _ptr(self.n_acc), S, _ptr(out), _stream()),
-                   "gs_record_to_padded")
+        L = _lib.lib_for(self.spec)
+        _lib.check(L.gs_record_to_padded(self.n, self.cap, _ptr(self.rec), _ptr(self.n_acc), S,
+                                         _ptr(out), _stream()), "gs_record_to_padded", L)
         return out
 
     def dts_rows(self, rows: torch.Tensor, S: Optional[int] = None) -> torch.Tensor:
@@ -347,7 +347,7 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
               checkpoint=checkpoint, budget_bytes=budget_bytes, precision=precision,
               schedule=schedule)
     if not record:
-        L = _lib.lib()
+        L = _lib.lib_for(spec)
         fn = L.gs_tsit5_fwd_record if method == METHOD_TSIT5 else L.gs_ros23_fwd_record
         wsr = ws if isinstance(ws, Record) else None
         yf = wsr.y_final if wsr is not None else torch.empty_like(y0)
@@ -358,7 +358,7 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
                       float(t0), _ptr(t1v), float(t1), float(rtol), float(atol),
                       -1.0 if dt0 is None else float(dt0), int(max_steps), 0, 1, None, None,
                       _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status), _stream()),
-                   fn.__name__)
+                   fn.__name__, L)
         empty = torch.empty(0, dtype=torch.float64, device=device)
         return Record(method, spec, n, float(t0), 0, 1, empty, empty, yf, n_acc, n_rej, status,
                       uneven=t1v is not None)
@@ -377,7 +377,7 @@ def _forward_one(method, spec, y0, p, t1v, saveat_ts, cap, ws, kw) -> Record:
     match), on the current stream."""
     n = y0.shape[0]
     device = y0.device
-    L = _lib.lib()
+    L = _lib.lib_for(spec)
     precision = kw["precision"]
     ok = ws is not None and ws.n == n
     if kw["checkpoint"] == "auto" and ok and ws.cap == cap and ws.rec.numel() > 2:
@@ -403,14 +403,14 @@ def _forward_one(method, spec, y0, p, t1v, saveat_ts, cap, ws, kw) -> Record:
         pass
     elif saveat_ts is None:
         fn = L.gs_tsit5_fwd_record if method == METHOD_TSIT5 else L.gs_ros23_fwd_record
-        _lib.check(fn(spec.code, mode, n, _ptr(y0), _ptr(p), *args, _stream()), fn.__name__)
+        _lib.check(fn(spec.code, mode, n, _ptr(y0), _ptr(p), *args, _stream()), fn.__name__, L)
     else:
         ts, ld, Kt = _ts_arg(saveat_ts, n)
         ys = (ws.ys if ok and ws.ys is not None and ws.ys.shape == (n, Kt, spec.dim)
               else torch.empty((n, Kt, spec.dim), dtype=torch.float64, device=device))
         _lib.check(L.gs_fwd_record_saveat(_METHOD_CODE[method], spec.code, mode, n, _ptr(y0),
                                           _ptr(p), *args, _ptr(ts), ld, Kt, _ptr(ys),
-                                          _stream()), "gs_fwd_record_saveat")
+                                          _stream()), "gs_fwd_record_saveat", L)
     if n == 0 and saveat_ts is not None:
         ys = torch.empty((0, _ts_arg(saveat_ts, 0)[2] if saveat_ts.ndim == 1 else
                           saveat_ts.shape[1], spec.dim), dtype=torch.float64, device=device)
@@ -573,12 +573,12 @@ def _scatter(r, res, i):
 
 def _replay_one(r: Record, y0: torch.Tensor, p: torch.Tensor, *, write_ckpt: bool,
                 precision: str) -> torch.Tensor:
-    L = _lib.lib()
+    L = _lib.lib_for(r.spec)
     fn = L.gs_tsit5_replay if r.method == METHOD_TSIT5 else L.gs_ros23_replay
     yf = torch.empty_like(y0)
-    _lib.check(fn(r.spec.code, _PREC[precision], r.n, _ptr(y0), _ptr(p), float(r.t0), _ptr(r.rec),
-                  _ptr(r.n_acc), max(r.cap, 1), r.ckpt_every,
-                  _ptr(r.ckpt) if write_ckpt else None, _ptr(yf), _stream()), fn.__name__)
+    _lib.check(fn(r.spec.code, _PREC[precision], r.n, _ptr(y0), _ptr(p), float(r.t0),
+                  _ptr(r.rec), _ptr(r.n_acc), max(r.cap, 1), r.ckpt_every,
+                  _ptr(r.ckpt) if write_ckpt else None, _ptr(yf), _stream()), fn.__name__, L)
     return yf
 
 
@@ -605,18 +605,18 @@ def adjoint(r, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
 
 def _adjoint_one(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool,
                  want_p: bool, precision: str, schedule: str, variant: str):
-    L = _lib.lib()
+    L = _lib.lib_for(r.spec)
     fn = L.gs_tsit5_adjoint if r.method == METHOD_TSIT5 else L.gs_ros23_adjoint
     gy0 = torch.empty((r.n, r.spec.dim), dtype=torch.float64, device=p.device) if want_y0 else None
     gp = torch.empty((r.n, p.shape[1]), dtype=torch.float64, device=p.device) if want_p else None
     ybar = ybar.contiguous()
     if schedule == "auto" and r.uneven:
         schedule = "refill"
-    flags = _PREC[precision] | _SCHED[schedule] | (_ADJ[variant] if fn is L.gs_tsit5_adjoint else 0)
-    _lib.check(fn(r.spec.code, flags, r.n, _ptr(p), _ptr(r.rec),
-                  _ptr(r.n_acc),
+    flags = (_PREC[precision] | _SCHED[schedule] |
+             (_ADJ[variant] if r.method == METHOD_TSIT5 else 0))
+    _lib.check(fn(r.spec.code, flags, r.n, _ptr(p), _ptr(r.rec), _ptr(r.n_acc),
                   max(r.cap, 1), _ptr(r.ckpt), r.ckpt_every, _ptr(ybar), _ptr(gy0), _ptr(gp),
-                  _stream()), fn.__name__)
+                  _stream()), fn.__name__, L)
     return gy0, gp
 
 
@@ -630,9 +630,9 @@ def record_from_padded(method: str, spec: FieldSpec, dts: torch.Tensor, t0: floa
     K = choose_ckpt_every(checkpoint, spec.dim, n, cap, budget_bytes)
     rec, ckpt = _alloc_record(n, cap, spec.dim, K, dts.device)
     n_steps = torch.empty(n, dtype=torch.int32, device=dts.device)
-    _lib.check(_lib.lib().gs_record_from_padded(n, S, _ptr(dts), S, _ptr(rec), cap,
-                                                _ptr(n_steps), _stream()),
-               "gs_record_from_padded")
+    L = _lib.lib_for(spec)
+    _lib.check(L.gs_record_from_padded(n, S, _ptr(dts), S, _ptr(rec), cap, _ptr(n_steps),
+                                       _stream()), "gs_record_from_padded", L)
     zeros = torch.zeros(n, dtype=torch.int32, device=dts.device)
     yf = torch.empty((n, spec.dim), dtype=torch.float64, device=dts.device)
     return Record(method, spec, n, float(t0), cap, K, rec, ckpt, yf, n_steps, zeros,
@@ -666,11 +666,12 @@ def _replay_saveat_one(r: Record, y0: torch.Tensor, p: torch.Tensor, ts: torch.T
     ts, ld, K = _ts_arg(ts, r.n)
     yf = torch.empty_like(y0)
     ys = torch.empty((r.n, K, r.spec.dim), dtype=torch.float64, device=y0.device)
-    _lib.check(_lib.lib().gs_replay_saveat(
+    L = _lib.lib_for(r.spec)
+    _lib.check(L.gs_replay_saveat(
         _METHOD_CODE[r.method], r.spec.code, _PREC[precision], r.n, _ptr(y0), _ptr(p),
         float(r.t0), _ptr(r.rec), _ptr(r.n_acc), max(r.cap, 1), r.ckpt_every,
         _ptr(r.ckpt) if write_ckpt else None, _ptr(ts), ld, K, _ptr(ys), _ptr(yf), _stream()),
-        "gs_replay_saveat")
+        "gs_replay_saveat", L)
     return yf, ys
 
 
@@ -696,8 +697,9 @@ def _adjoint_saveat_one(r: Record, p: torch.Tensor, ts: torch.Tensor, ysbar: tor
     gp = torch.empty((r.n, p.shape[1]), dtype=torch.float64, device=p.device) if want_p else None
     ysbar = ysbar.to(torch.float64).contiguous()
     ybar = None if ybar is None else ybar.to(torch.float64).contiguous()
-    _lib.check(_lib.lib().gs_adjoint_saveat(
+    L = _lib.lib_for(r.spec)
+    _lib.check(L.gs_adjoint_saveat(
         _METHOD_CODE[r.method], r.spec.code, _PREC[precision] | _SCHED[schedule], r.n, _ptr(p),
         _ptr(r.rec), _ptr(r.n_acc), max(r.cap, 1), _ptr(r.ckpt), r.ckpt_every, _ptr(ts), ld, K, _ptr(ysbar),
-        _ptr(ybar), _ptr(gy0), _ptr(gp), _stream()), "gs_adjoint_saveat")
+        _ptr(ybar), _ptr(gy0), _ptr(gp), _stream()), "gs_adjoint_saveat", L)
     return gy0, gp

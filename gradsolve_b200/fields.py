@@ -40,6 +40,11 @@ class FieldSpec:
     dim: int      # state dimension D
     nparam: int   # parameters the kernel reads (P)
     stiff_ok: bool  # has an analytic Jacobian (Rosenbrock23 capable)
+    lib: str = ""   # the generated field's own library (empty: libgsolve.so)
+
+
+# problem name -> FieldSpec of a generated field (register_field)
+_USER: dict = {}
 
 
 _STATIC = {
@@ -54,6 +59,9 @@ _STATIC = {
 def field_spec(key: str) -> FieldSpec:
     if key in _STATIC:
         return _STATIC[key]
+    for spec in _USER.values():
+        if spec.key == key:
+            return spec
     if key.startswith("linear_"):
         try:
             d = int(key.split("_", 1)[1])
@@ -68,6 +76,8 @@ def field_spec(key: str) -> FieldSpec:
 def field_for(problem) -> FieldSpec | None:
     """The kernel field for ``problem`` (by name), or None when no field is registered."""
     nm = getattr(problem, "name", "")
+    if nm in _USER:
+        return _USER[nm]
     if nm == "diffeqgpu_lorenz":
         return _STATIC["lorenz"]
     if nm == "lorenz":
@@ -101,6 +111,8 @@ def kernel_params(spec: FieldSpec, params: np.ndarray) -> np.ndarray:
     if params.ndim != 2:
         raise ValueError(f"params must be (n, P); got shape {params.shape}")
     n = params.shape[0]
+    if spec.lib and params.shape[1] == 0:  # a generated field without parameters
+        return np.zeros((n, spec.nparam))
     if spec.key.startswith("linear_"):
         return np.zeros((n, 1)) if params.shape[1] == 0 else params[:, :1]
     if params.shape[1] < spec.nparam:

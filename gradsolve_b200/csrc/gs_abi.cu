@@ -145,6 +145,9 @@ SegCfg seg_cfg(int K, int W) {
   return {block, per_thread * block};
 }
 
+// The same shrinking rule for a per-thread size given in doubles.
+SegCfg seg_cfg_doubles(int doubles_per_thread) { return seg_cfg(1, doubles_per_thread); }
+
 template <class Kern>
 int allow_smem(Kern kernel, size_t smem) {
   if (smem <= 48u * 1024u) return GS_OK;
@@ -273,15 +276,16 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
       gs::tsit5_adjoint_stages_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
       return cuda_check("tsit5_adjoint_stages_kernel");
     }
-    const SegCfg c = seg_cfg(a.ck_every, F::D);
-    if (mixed) {
-      if ((rc = allow_smem(gs::tsit5_mixed_adjoint_kernel<F>, c.smem))) return rc;
-      gs::tsit5_mixed_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
-      return cuda_check("tsit5_mixed_adjoint_kernel");
+    if (!mixed) {
+      const SegCfg c = seg_cfg_doubles(gs::adjoint_smem_doubles<F::D>(a.ck_every));
+      if ((rc = allow_smem(gs::tsit5_adjoint_kernel<F>, c.smem))) return rc;
+      gs::tsit5_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+      return cuda_check("tsit5_adjoint_kernel");
     }
-    if ((rc = allow_smem(gs::tsit5_adjoint_kernel<F>, c.smem))) return rc;
-    gs::tsit5_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
-    return cuda_check("tsit5_adjoint_kernel");
+    const SegCfg c = seg_cfg(a.ck_every, F::D);
+    if ((rc = allow_smem(gs::tsit5_mixed_adjoint_kernel<F>, c.smem))) return rc;
+    gs::tsit5_mixed_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+    return cuda_check("tsit5_mixed_adjoint_kernel");
   }
   const bool counter = sched == GS_SCHED_REFILL;
   return mixed ? launch_adjoint_persistent<F, gs::Tsit5MixedStep>(a, cap, s, counter)
@@ -646,7 +650,7 @@ int launch_tsit5_vjp_static(long long n, long long S, long long ld, const double
   gs::tsit5_replay_kernel<F><<<grid_for(n), kBlock, 0, s>>>(ra);
   if ((rc = cuda_check("tsit5_replay_kernel"))) return rc;
   gs::AdjointArgs aa{n, p, rec, n_steps, ckpt, K, ybar, gy0, gp, cap};
-  const SegCfg c = seg_cfg(K, F::D);
+  const SegCfg c = seg_cfg_doubles(gs::adjoint_smem_doubles<F::D>(K));
   if ((rc = allow_smem(gs::tsit5_adjoint_kernel<F>, c.smem))) return rc;
   gs::tsit5_adjoint_kernel<F><<<grid_for_block(n, c.block), c.block, c.smem, s>>>(aa);
   return cuda_check("tsit5_adjoint_kernel");

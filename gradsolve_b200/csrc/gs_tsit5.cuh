@@ -571,6 +571,58 @@ __global__ void __launch_bounds__(128) tsit5_replay_kernel(const ReplayArgs a) {
 }
 
 // --- reverse-replay adjoint ---------------------------------------------------------------
+// Each thread's shared memory holds its segment's K states and, double-buffered, the K dts
+// and the checkpoint of a segment: while a segment is recomputed and differentiated, the
+// next one's checkpoint and dts are already on their way (cp.async, global -> shared, no
+// register staging), so segment starts do not wait on DRAM, and each dt is read from DRAM
+// once instead of once per sweep.
+template <int D>
+GS_HD int adjoint_smem_doubles(int K) { return K * D + 2 * K + 2 * ((D + 2) & ~1); }
+
+template <int D>
+struct AdjBuf {
+  static constexpr int CW = (D + 2) & ~1;
+  double* base;
+  int stride, K;
+  __device__ __forceinline__ AdjBuf(int k) : base(gs_seg_smem + threadIdx.x), stride(blockDim.x), K(k) {}
+  __device__ __forceinline__ double& st(int q, int i) { return base[(q * D + i) * stride]; }
+  __device__ __forceinline__ double& dt(int b, int q) { return base[(K * D + b * K + q) * stride]; }
+  __device__ __forceinline__ double& ck(int b, int i) {
+    return base[(K * D + 2 * K + b * CW + i) * stride];
+  }
+};
+
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_src) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Start the copies of segment sg's checkpoint and dts (steps at or past na read as 0).
+template <int D>
+__device__ __forceinline__ void prefetch_segment(AdjBuf<D>& buf, int b, const double* ckpt,
+                                                 const double* rec, long long n, long long j,
+                                                 int sg, int K, int na) {
+  constexpr int CW = (D + 2) & ~1;
+  const double* src = ckpt + ((size_t)sg * (size_t)n + (size_t)j) * CW;
+#pragma unroll
+  for (int i = 0; i < CW; ++i) cp_async8(&buf.ck(b, i), src + i);
+  const int start = sg * K;
+  for (int q = 0; q < K; ++q) {
+    const int s = start + q;
+    if (s < na)
+      cp_async8(&buf.dt(b, q), rec + rec_index(j, s, n));
+    else
+      buf.dt(b, q) = 0.0;
+  }
+  cp_async_commit();
+}
+
 template <class F>
 __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a) {
   constexpr int D = F::D, P = F::P;
@@ -587,30 +639,33 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a)
   const int na = steps_in_record(a.n_acc, j, a.cap);
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
-  SegBuf<D> seg;
+  AdjBuf<D> buf(K);
+  int b = 0;
+  if (nseg > 0) prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
   for (int sg = nseg - 1; sg >= 0; --sg) {
-    const int start = sg * K;
+    cp_async_wait_all();  // this segment's checkpoint and dts have landed
     double y[D];
-    load_ckpt<D>(a.ckpt, a.n, j, sg, y);
 #pragma unroll
-    for (int i = 0; i < D; ++i) seg.at(0, i) = y[i];
+    for (int i = 0; i < D; ++i) y[i] = buf.ck(b, i);
+    if (sg > 0) prefetch_segment<D>(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
+#pragma unroll
+    for (int i = 0; i < D; ++i) buf.st(0, i) = y[i];
     for (int q = 1; q < K; ++q) {
-      const int s = start + q - 1;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      const double dt = buf.dt(b, q - 1);
       if (dt != 0.0) tsit5_replay_step<F>(y, p, dt);
 #pragma unroll
-      for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
+      for (int i = 0; i < D; ++i) buf.st(q, i) = y[i];
     }
     for (int q = K - 1; q >= 0; --q) {
-      const int s = start + q;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      const double dt = buf.dt(b, q);
       if (dt != 0.0) {
         double ys[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) ys[i] = seg.at(q, i);
+        for (int i = 0; i < D; ++i) ys[i] = buf.st(q, i);
         tsit5_step_vjp<F>(ys, p, dt, lam, gp);
       }
     }
+    b ^= 1;
   }
   if (a.gy0) {
 #pragma unroll

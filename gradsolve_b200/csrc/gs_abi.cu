@@ -160,6 +160,36 @@ int allow_smem(Kern kernel, size_t smem) {
 
 unsigned grid_for_block(long long n, unsigned block) { return (unsigned)((n + block - 1) / block); }
 
+// Block size (128, 64 or 32) that keeps the most threads resident per SM for a kernel whose
+// threads each use doubles_per_thread of dynamic shared memory (registers and shared memory
+// both limit residency; smaller blocks pack the shared memory more finely).  Ties keep the
+// larger block.  Sets the kernel's dynamic shared memory limit for the chosen size.
+template <class Kern>
+int occupancy_cfg(Kern kernel, int doubles_per_thread, SegCfg* out) {
+  SegCfg best{0, 0};
+  long long best_res = -1;
+  for (unsigned block : {128u, 64u, 32u}) {
+    const size_t smem = (size_t)doubles_per_thread * sizeof(double) * block;
+    if (smem > kSegBudget) continue;
+    int rc = allow_smem(kernel, smem);
+    if (rc) return rc;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem);
+    if (e != cudaSuccess)
+      return fail(GS_ERR_CUDA, std::string("CUDA: occupancy query: ") + cudaGetErrorString(e));
+    const long long res = (long long)per_sm * block;
+    if (res > best_res) {
+      best_res = res;
+      best = {block, smem};
+    }
+  }
+  if (best_res <= 0)
+    return fail(GS_ERR_ARG, "segment buffer does not fit shared memory (checkpoint interval "
+                            "too large for this state dimension)");
+  *out = best;
+  return allow_smem(kernel, best.smem);
+}
+
 // ---- scheduling ------------------------------------------------------------------------------
 // GS_SCHED_* flags ride in the high bits of the precision argument.  AUTO: one thread per
 // trajectory (hardware block scheduling) for a shared end time, lane refill with a work
@@ -269,16 +299,19 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
     int rc;
     // the stage-keeping variant needs 6*D doubles per step of the segment; where that does not
     // fit one warp's worth of shared memory (large K and D) the stages are recomputed instead
-    const SegCfg cs = seg_cfg(a.ck_every, 6 * F::D);
-    if (!mixed && variant == GS_ADJ_STAGES && cs.smem <= kSegBudget) {
-      const SegCfg c = cs;
-      if ((rc = allow_smem(gs::tsit5_adjoint_stages_kernel<F>, c.smem))) return rc;
+    const int stage_doubles = gs::adjoint_smem_doubles<F::D, 6 * F::D>(a.ck_every);
+    if (!mixed && variant == GS_ADJ_STAGES &&
+        (size_t)stage_doubles * sizeof(double) * 32u <= kSegBudget) {
+      SegCfg c;
+      if ((rc = occupancy_cfg(gs::tsit5_adjoint_stages_kernel<F>, stage_doubles, &c))) return rc;
       gs::tsit5_adjoint_stages_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
       return cuda_check("tsit5_adjoint_stages_kernel");
     }
     if (!mixed) {
-      const SegCfg c = seg_cfg_doubles(gs::adjoint_smem_doubles<F::D>(a.ck_every));
-      if ((rc = allow_smem(gs::tsit5_adjoint_kernel<F>, c.smem))) return rc;
+      SegCfg c;
+      if ((rc = occupancy_cfg(gs::tsit5_adjoint_kernel<F>,
+                              gs::adjoint_smem_doubles<F::D>(a.ck_every), &c)))
+        return rc;
       gs::tsit5_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
       return cuda_check("tsit5_adjoint_kernel");
     }

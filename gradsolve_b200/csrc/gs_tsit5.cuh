@@ -576,19 +576,20 @@ __global__ void __launch_bounds__(128) tsit5_replay_kernel(const ReplayArgs a) {
 // next one's checkpoint and dts are already on their way (cp.async, global -> shared, no
 // register staging), so segment starts do not wait on DRAM, and each dt is read from DRAM
 // once instead of once per sweep.
-template <int D>
-GS_HD int adjoint_smem_doubles(int K) { return K * D + 2 * K + 2 * ((D + 2) & ~1); }
+// W doubles of segment state per step (D: the states; 6 D: states and stage inputs).
+template <int D, int W = D>
+GS_HD int adjoint_smem_doubles(int K) { return K * W + 2 * K + 2 * ((D + 2) & ~1); }
 
-template <int D>
+template <int D, int W = D>
 struct AdjBuf {
   static constexpr int CW = (D + 2) & ~1;
   double* base;
   int stride, K;
   __device__ __forceinline__ AdjBuf(int k) : base(gs_seg_smem + threadIdx.x), stride(blockDim.x), K(k) {}
-  __device__ __forceinline__ double& st(int q, int i) { return base[(q * D + i) * stride]; }
-  __device__ __forceinline__ double& dt(int b, int q) { return base[(K * D + b * K + q) * stride]; }
+  __device__ __forceinline__ double& st(int q, int i) { return base[(q * W + i) * stride]; }
+  __device__ __forceinline__ double& dt(int b, int q) { return base[(K * W + b * K + q) * stride]; }
   __device__ __forceinline__ double& ck(int b, int i) {
-    return base[(K * D + 2 * K + b * CW + i) * stride];
+    return base[(K * W + 2 * K + b * CW + i) * stride];
   }
 };
 
@@ -604,8 +605,8 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 // Start the copies of segment sg's checkpoint and dts (steps at or past na read as 0).
-template <int D>
-__device__ __forceinline__ void prefetch_segment(AdjBuf<D>& buf, int b, const double* ckpt,
+template <int D, int W>
+__device__ __forceinline__ void prefetch_segment(AdjBuf<D, W>& buf, int b, const double* ckpt,
                                                  const double* rec, long long n, long long j,
                                                  int sg, int K, int na) {
   constexpr int CW = (D + 2) & ~1;
@@ -641,13 +642,13 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a)
   const int nseg = (na + K - 1) / K;
   AdjBuf<D> buf(K);
   int b = 0;
-  if (nseg > 0) prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
+  if (nseg > 0) prefetch_segment(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
   for (int sg = nseg - 1; sg >= 0; --sg) {
     cp_async_wait_all();  // this segment's checkpoint and dts have landed
     double y[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) y[i] = buf.ck(b, i);
-    if (sg > 0) prefetch_segment<D>(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
+    if (sg > 0) prefetch_segment(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
 #pragma unroll
     for (int i = 0; i < D; ++i) buf.st(0, i) = y[i];
     for (int q = 1; q < K; ++q) {
@@ -681,6 +682,7 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a)
 // The segment's forward pass stores, per step, y and the stage inputs s2..s6 (6*D doubles) in
 // the shared-memory segment buffer, so the reverse sweep runs the step VJPs without
 // recomputing the stages: one stage evaluation per step instead of two, for 6x the buffer.
+// The next segment's checkpoint and dts are prefetched as in tsit5_adjoint_kernel.
 // Same states (tsit5_stage_states<F, true> evaluates tsit5_replay_step's expressions) and the
 // same VJP code (tsit5_vjp_core) as tsit5_adjoint_kernel.
 template <class F>
@@ -711,16 +713,19 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_stages_kernel(const Adjoint
   const int na = steps_in_record(a.n_acc, j, a.cap);
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
-  SegBuf<6 * D> seg;
+  AdjBuf<D, 6 * D> buf(K);  // per step: y and the stage inputs s2..s6; dts, checkpoints
+  int b = 0;
+  if (nseg > 0) prefetch_segment(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
   for (int sg = nseg - 1; sg >= 0; --sg) {
-    const int start = sg * K;
+    cp_async_wait_all();  // this segment's checkpoint and dts have landed
     double y[D];
-    load_ckpt<D>(a.ckpt, a.n, j, sg, y);
-    for (int q = 0; q < K; ++q) {
-      const int s = start + q;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
 #pragma unroll
-      for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
+    for (int i = 0; i < D; ++i) y[i] = buf.ck(b, i);
+    if (sg > 0) prefetch_segment(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
+    for (int q = 0; q < K; ++q) {
+      const double dt = buf.dt(b, q);
+#pragma unroll
+      for (int i = 0; i < D; ++i) buf.st(q, i) = y[i];
       if (dt != 0.0) {
         StageStates<F> S;
         if (q + 1 < K) {
@@ -733,25 +738,25 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_stages_kernel(const Adjoint
         }
 #pragma unroll
         for (int i = 0; i < D; ++i) {
-          seg.at(q, D + i) = S.s2[i];
-          seg.at(q, 2 * D + i) = S.s3[i];
-          seg.at(q, 3 * D + i) = S.s4[i];
-          seg.at(q, 4 * D + i) = S.s5[i];
-          seg.at(q, 5 * D + i) = S.s6[i];
+          buf.st(q, D + i) = S.s2[i];
+          buf.st(q, 2 * D + i) = S.s3[i];
+          buf.st(q, 3 * D + i) = S.s4[i];
+          buf.st(q, 4 * D + i) = S.s5[i];
+          buf.st(q, 5 * D + i) = S.s6[i];
         }
       }
     }
     for (int q = K - 1; q >= 0; --q) {
-      const int s = start + q;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      const double dt = buf.dt(b, q);
       if (dt != 0.0) {
         double ys[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) ys[i] = seg.at(q, i);
-        const SegStages<F> src{seg.base, seg.stride, q};
+        for (int i = 0; i < D; ++i) ys[i] = buf.st(q, i);
+        const SegStages<F> src{buf.base, buf.stride, q};
         tsit5_vjp_core<F>(ys, src, p, dt, lam, gp);
       }
     }
+    b ^= 1;
   }
   if (a.gy0) {
 #pragma unroll

@@ -239,7 +239,9 @@ int zero_counter(unsigned long long* c, cudaStream_t s) {
 }
 
 template <class F, class L>
-int launch_record_persistent(const gs::RecordArgs& a, cudaStream_t s, bool use_counter) {
+int launch_record_persistent(const gs::RecordArgs& a_in, cudaStream_t s, bool use_counter) {
+  gs::RecordArgs a = a_in;
+  a.ctrl = gs::make_ctrl_consts(F::D, L::QK);
   unsigned long long* counter =
       use_counter ? ctrl_counter(a.ckpt, a.n, a.ck_slots, F::D, gs::kCtrlFwd) : nullptr;
   unsigned grid = 0;
@@ -270,7 +272,9 @@ int launch_adjoint_persistent(const gs::AdjointArgs& a, int cap, cudaStream_t s,
 
 // mixed = float32 stages (GS_PREC_MIXED, gs_mixed.cuh), else float64 throughout.
 template <class F>
-int launch_tsit5_record(const gs::RecordArgs& a, cudaStream_t s, bool mixed, int sched) {
+int launch_tsit5_record(const gs::RecordArgs& a_in, cudaStream_t s, bool mixed, int sched) {
+  gs::RecordArgs a = a_in;
+  a.ctrl = gs::make_ctrl_consts(F::D, 10);  // Tsit5: err^(-1/5) = m^(-1/10)
   if (sched == GS_SCHED_STATIC) {
     if (mixed) {
       gs::tsit5_mixed_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
@@ -325,7 +329,9 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
                : launch_adjoint_persistent<F, gs::Tsit5F64Step>(a, cap, s, counter);
 }
 template <class F>
-int launch_ros23_record(const gs::RecordArgs& a, cudaStream_t s, int sched) {
+int launch_ros23_record(const gs::RecordArgs& a_in, cudaStream_t s, int sched) {
+  gs::RecordArgs a = a_in;
+  a.ctrl = gs::make_ctrl_consts(F::D, 6);  // Rosenbrock23: err^(-1/3) = m^(-1/6)
   if (sched == GS_SCHED_STATIC) {
     gs::ros23_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
     return cuda_check("ros23_record_kernel");
@@ -874,7 +880,7 @@ extern "C" int gs_fwd_record_saveat(int method, int field, int precision, long l
                       (sched == GS_SCHED_REFILL || (sched == GS_SCHED_AUTO && t1v != nullptr));
   gs::RecordArgs a{n, y0, p, t0, t1, rtol, atol, dt0, t1v, max_steps, cap, ckpt_every,
                    gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status,
-                   ts, ts_ld, K, K > 0 ? ys : nullptr};
+                   gs::CtrlConsts{}, ts, ts_ld, K, K > 0 ? ys : nullptr};
   const cudaStream_t s = (cudaStream_t)stream;
   if (method == GS_METHOD_TSIT5) {
     if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED)

@@ -270,12 +270,12 @@ __global__ void __launch_bounds__(128) tsit5_mixed_record_kernel(const RecordArg
       ed[i] = (double)(hf * (T::E2 * S.dk2[i] + T::E3 * S.dk3[i] + T::E4 * S.dk4[i] +
                              T::E5 * S.dk5[i] + T::E6 * S.dk6[i] + T::E7 * dk7));
     }
-    const double m = wrms_mean<D>(ed, y, y5, a.rtol, a.atol);
+    const double m = wrms_sumsq<D>(ed, y, y5, a.rtol, a.atol);
     if (!(m == m)) {
       st = 1;
       break;
     }
-    if (m <= kAcceptMax) {
+    if (m <= a.ctrl.accept_sum) {
       if ((rec_on || ck_on) && acc >= a.cap) {
         st = 3;
         break;
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(128) tsit5_mixed_record_kernel(const RecordArg
     } else {
       ++rej;
     }
-    dt = step_from_mean<10>(m, h);
+    dt = step_from_sum<10>(m, h, a.ctrl);
   }
   if (st == 0 && !(t >= t1)) st = 1;
   if (rec_on) {

@@ -53,7 +53,7 @@ struct LaneTsit5F64 {
   __device__ __forceinline__ void start(const double* y, const double* p, const float*) {
     F::rhs(y, p, k1);
   }
-  // candidate y5 for step h; returns the mean of squares of the scaled error
+  // candidate y5 for step h; returns the sum of squares of the scaled error
   __device__ __forceinline__ double trial(const double* y, const double* p, const float*, double h,
                                           double rtol, double atol, double* y5) {
     using T = Tsit5;
@@ -66,7 +66,7 @@ struct LaneTsit5F64 {
     for (int i = 0; i < D; ++i)
       e[i] = h * (T::E1 * k1[i] + T::E2 * S.k2[i] + T::E3 * S.k3[i] + T::E4 * S.k4[i] +
                   T::E5 * S.k5[i] + T::E6 * S.k6[i] + T::E7 * k7[i]);
-    return wrms_mean<D>(e, y, y5, rtol, atol);
+    return wrms_sumsq<D>(e, y, y5, rtol, atol);
   }
   __device__ __forceinline__ void commit() {
 #pragma unroll
@@ -106,7 +106,7 @@ struct LaneTsit5Mixed {
       ed[i] = (double)(hf * (T::E2 * S.dk2[i] + T::E3 * S.dk3[i] + T::E4 * S.dk4[i] +
                              T::E5 * S.dk5[i] + T::E6 * S.dk6[i] + T::E7 * dk7));
     }
-    return wrms_mean<D>(ed, y, y5, rtol, atol);
+    return wrms_sumsq<D>(ed, y, y5, rtol, atol);
   }
   __device__ __forceinline__ void commit() {
 #pragma unroll
@@ -132,7 +132,7 @@ struct LaneRos23 {
     lu_solve<D>(c.W, r3, k3);
 #pragma unroll
     for (int i = 0; i < D; ++i) ev[i] = (h / 6.0) * (c.k1[i] - 2.0 * c.k2[i] + k3[i]);
-    return wrms_mean<D>(ev, y, ynew, rtol, atol);
+    return wrms_sumsq<D>(ev, y, ynew, rtol, atol);
   }
   __device__ __forceinline__ void commit() {}
   // the step no longer advances time: status 2 (gradsolve/solvers/record_jax.py:109)
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
         ++it;
         if (!(m == m)) {
           st = 1;
-        } else if (m <= kAcceptMax) {
+        } else if (m <= a.ctrl.accept_sum) {
           if ((rec_on || ck_on) && acc >= a.cap) {
             st = 3;
           } else {
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
         } else {
           ++rej;
         }
-        if (st < 0) dt = step_from_mean<L::QK>(m, h);
+        if (st < 0) dt = step_from_sum<L::QK>(m, h, a.ctrl);
       }
     }
     if (st >= 0) {  // finished: write this trajectory's outputs, take the next one

@@ -33,27 +33,32 @@ int gs_probe_fp32(float* out, int blocks, int iters, void* stream) {
 // ---- controller check: the solver's pow-free step factor vs CUDA's pow --------------------
 #include "gs_tsit5.cuh"
 
-__global__ void step_factor_probe(const double* m, long long n, int order, double* fast,
-                                  double* ref, int* accept_fast, int* accept_ref) {
+__global__ void step_factor_probe(const double* S, long long n, int order, int D,
+                                  gs::CtrlConsts c, double* fast, double* ref, int* accept_fast,
+                                  int* accept_ref) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double x = m[i];
-  fast[i] = order == 5 ? gs::step_from_mean<10>(x, 1.0) : gs::step_from_mean<6>(x, 1.0);
-  const double err = sqrt(x);
+  const double x = S[i];  // the solver's sum of squares; the reference's mean is fl(x / D)
+  fast[i] = order == 5 ? gs::step_from_sum<10>(x, 1.0, c) : gs::step_from_sum<6>(x, 1.0, c);
+  const double err = sqrt(x / (double)D);
   const double e = err > 1e-10 ? err : 1e-10;
   double fac = 0.9 * pow(e, order == 5 ? -0.2 : -1.0 / 3.0);
   fac = fac > 0.2 ? fac : 0.2;
   fac = 5.0 < fac ? 5.0 : fac;
   ref[i] = fac;
-  accept_fast[i] = x <= gs::kAcceptMax;
+  accept_fast[i] = x <= c.accept_sum;
   accept_ref[i] = err <= 1.0;
 }
 
-extern "C" int gs_probe_step_factor(const double* m, long long n, int order, double* fast,
+// The solver's controller (accept test and step factor from the sum of squares, for state
+// dimension D) against sqrt and pow of the mean, for n sums of squares S.
+extern "C" int gs_probe_step_factor(const double* S, long long n, int order, int D, double* fast,
                                     double* ref, int* accept_fast, int* accept_ref,
                                     void* stream) {
   if (n <= 0) return 0;
+  if (D < 1 || (order != 5 && order != 3)) return -1;
+  const gs::CtrlConsts c = gs::make_ctrl_consts(D, order == 5 ? 10 : 6);
   step_factor_probe<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
-      m, n, order, fast, ref, accept_fast, accept_ref);
+      S, n, order, D, c, fast, ref, accept_fast, accept_ref);
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }

@@ -270,12 +270,12 @@ __global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
     lu_solve<D>(c.W, r3, k3);
 #pragma unroll
     for (int i = 0; i < D; ++i) ev[i] = (h / 6.0) * (c.k1[i] - 2.0 * c.k2[i] + k3[i]);
-    const double m = wrms_mean<D>(ev, y, ynew, a.rtol, a.atol);
+    const double m = wrms_sumsq<D>(ev, y, ynew, a.rtol, a.atol);
     if (!(m == m)) {
       st = 1;
       break;
     }
-    if (m <= kAcceptMax) {
+    if (m <= a.ctrl.accept_sum) {
       if ((rec_on || ck_on) && acc >= a.cap) {
         st = 3;
         break;
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
     } else {
       ++rej;
     }
-    dt = step_from_mean<6>(m, h);
+    dt = step_from_sum<6>(m, h, a.ctrl);
   }
   if (st == 0 && !(t >= t1)) st = 1;
   if (rec_on) {

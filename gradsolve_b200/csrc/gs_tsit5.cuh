@@ -29,6 +29,8 @@
 // a warp stay in the same phase (recompute vs VJP) instead of diverging.  With K = 1 every
 // state is a checkpoint and nothing is recomputed.
 #pragma once
+#include <cmath>
+
 #include "gs_fields.cuh"
 #include "gs_tableau.cuh"
 
@@ -117,28 +119,52 @@ __device__ __forceinline__ double inv_root(double m) {
   return y;
 }
 
-// K = 10 for Tsit5 (q = 5), K = 6 for Rosenbrock23 (q = 3).  Returns the new dt.
+// The kernels work with the SUM of squares S (m = fl(S / D)), which spares the division by D
+// in every attempt.  The constants below are computed on the host (make_ctrl_consts) for the
+// field's D and the method's root order K:
+//  * accept_sum is the largest double S with fl(S / D) <= 1 + 2^-52; division by D is
+//    correctly rounded and monotone, so S <= accept_sum <=> m <= 1 + 2^-52: the accept test
+//    is still the reference's bit for bit;
+//  * 0.9 m^(-1/K) = scale S^(-1/K) with scale = 0.9 D^(1/K); the clips are at D 0.18^K and
+//    D 4.5^K.
+struct CtrlConsts {
+  double accept_sum, lo, hi, scale;
+};
+
+__host__ inline CtrlConsts make_ctrl_consts(int D, int K) {
+  const double A = kAcceptMax, dd = (double)D;
+  double x = A * dd;  // then walk to the last double whose quotient still rounds to <= A
+  while (x / dd > A) x = std::nextafter(x, 0.0);
+  while (std::nextafter(x, 1e300) / dd <= A) x = std::nextafter(x, 1e300);
+  CtrlConsts c;
+  c.accept_sum = x;
+  c.lo = dd * std::pow(0.18, K);
+  c.hi = dd * std::pow(4.5, K);
+  c.scale = Ctrl::SAFETY * std::pow(dd, 1.0 / K);
+  return c;
+}
+
+// K = 10 for Tsit5 (q = 5), K = 6 for Rosenbrock23 (q = 3).  Returns the new dt from the sum
+// of squares S.
 template <int K>
-__device__ __forceinline__ double step_from_mean(double m, double h) {
-  constexpr double lo = K == 10 ? 3.570467226623999e-08 : 3.401222399999999e-05;  // 0.18^K
-  constexpr double hi = K == 10 ? 3405062.8916015625 : 8303.765625;                   // 4.5^K
+__device__ __forceinline__ double step_from_sum(double S, double h, const CtrlConsts& c) {
   double fac;
-  if (m <= lo) {
+  if (S <= c.lo) {
     fac = Ctrl::FAC_MAX;
-  } else if (m >= hi) {
+  } else if (S >= c.hi) {
     fac = Ctrl::FAC_MIN;
   } else {
-    fac = Ctrl::SAFETY * inv_root<K>(m);
+    fac = c.scale * inv_root<K>(S);
     fac = fac > Ctrl::FAC_MIN ? fac : Ctrl::FAC_MIN;
     fac = Ctrl::FAC_MAX < fac ? Ctrl::FAC_MAX : fac;
   }
   return h * fac;
 }
 
-// mean of squares (e_i / sc_i)^2 in numpy's summation order (the reference's np.mean)
+// sum of squares (e_i / sc_i)^2 in numpy's summation order (the reference's np.mean times D)
 template <int D>
-__device__ __forceinline__ double wrms_mean(const double* e, const double* y, const double* yn,
-                                            double rtol, double atol) {
+__device__ __forceinline__ double wrms_sumsq(const double* e, const double* y, const double* yn,
+                                             double rtol, double atol) {
   double q[D];
 #pragma unroll
   for (int i = 0; i < D; ++i) {
@@ -146,7 +172,7 @@ __device__ __forceinline__ double wrms_mean(const double* e, const double* y, co
     const double c = e[i] / sc;
     q[i] = c * c;
   }
-  return wrms_sum<D>(q) / (double)D;
+  return wrms_sum<D>(q);
 }
 
 // --- the shared stage arithmetic ------------------------------------------------------
@@ -373,6 +399,7 @@ struct RecordArgs {
   int* n_acc;
   int* n_rej;
   int* status;
+  CtrlConsts ctrl{};  // set by the launcher for the field's D and the method's order
   // dense output produced by the forward itself (persistent kernel only): requested times,
   // row j at ts + j * ts_ld (ts_ld = 0: one shared row), K per trajectory, states (n, K, D)
   const double* ts = nullptr;
@@ -492,12 +519,12 @@ __global__ void __launch_bounds__(128) tsit5_record_kernel(const RecordArgs a) {
     for (int i = 0; i < D; ++i)
       e[i] = h * (T::E1 * k1[i] + T::E2 * S.k2[i] + T::E3 * S.k3[i] + T::E4 * S.k4[i] +
                   T::E5 * S.k5[i] + T::E6 * S.k6[i] + T::E7 * k7[i]);
-    const double m = wrms_mean<D>(e, y, y5, a.rtol, a.atol);
+    const double m = wrms_sumsq<D>(e, y, y5, a.rtol, a.atol);
     if (!(m == m)) {  // NaN error: dt would turn NaN and the loop could never finish
       st = 1;
       break;
     }
-    if (m <= kAcceptMax) {  // err = sqrt(m) <= 1
+    if (m <= a.ctrl.accept_sum) {  // err = sqrt(m / D) <= 1
       if ((rec_on || ck_on) && acc >= a.cap) {
         st = 3;
         break;
@@ -523,7 +550,7 @@ __global__ void __launch_bounds__(128) tsit5_record_kernel(const RecordArgs a) {
     } else {
       ++rej;
     }
-    dt = step_from_mean<10>(m, h);
+    dt = step_from_sum<10>(m, h, a.ctrl);
   }
   if (st == 0 && !(t >= t1)) st = 1;
   if (rec_on) {

@@ -123,8 +123,7 @@ __device__ __forceinline__ double inv_root(double m) {
 // in every attempt.  The constants below are computed on the host (make_ctrl_consts) for the
 // field's D and the method's root order K:
 //  * accept_sum is the largest double S with fl(S / D) <= 1 + 2^-52; division by D is
-//    correctly rounded and monotone, so S <= accept_sum <=> m <= 1 + 2^-52: the accept test
-//    is still the reference's bit for bit;
+//    correctly rounded and monotone, so S <= accept_sum <=> m <= 1 + 2^-52;
 //  * 0.9 m^(-1/K) = scale S^(-1/K) with scale = 0.9 D^(1/K); the clips are at D 0.18^K and
 //    D 4.5^K.
 struct CtrlConsts {
@@ -161,16 +160,43 @@ __device__ __forceinline__ double step_from_sum(double S, double h, const CtrlCo
   return h * fac;
 }
 
-// sum of squares (e_i / sc_i)^2 in numpy's summation order (the reference's np.mean times D)
+// sum of squares (e_i / sc_i)^2 in numpy's summation order (the reference's np.mean times D).
+// For D <= 4 the D quotients share one division: with P = prod sc_j, e_i / sc_i is taken as
+// e_i * ((prod_{j != i} sc_j) / P), within a few ulp of the quotient (the controller and the
+// accept test read it at that level only where the reference's own Warp and numpy paths
+// already differ), unless P leaves the normal range, where each quotient is divided out.
 template <int D>
 __device__ __forceinline__ double wrms_sumsq(const double* e, const double* y, const double* yn,
                                              double rtol, double atol) {
-  double q[D];
+  double sc[D], q[D];
 #pragma unroll
-  for (int i = 0; i < D; ++i) {
-    const double sc = atol + rtol * fmax(fabs(y[i]), fabs(yn[i]));
-    const double c = e[i] / sc;
-    q[i] = c * c;
+  for (int i = 0; i < D; ++i) sc[i] = atol + rtol * fmax(fabs(y[i]), fabs(yn[i]));
+  bool shared = false;
+  if constexpr (D >= 2 && D <= 4) {
+    double pre[D], suf[D];  // products of the scales before / after component i
+    pre[0] = 1.0;
+#pragma unroll
+    for (int i = 1; i < D; ++i) pre[i] = pre[i - 1] * sc[i - 1];
+    suf[D - 1] = 1.0;
+#pragma unroll
+    for (int i = D - 2; i >= 0; --i) suf[i] = suf[i + 1] * sc[i + 1];
+    const double P = pre[D - 1] * sc[D - 1];
+    if (P > 1e-290 && P < 1e290) {
+      shared = true;
+      const double r = 1.0 / P;
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        const double c = e[i] * ((pre[i] * suf[i]) * r);
+        q[i] = c * c;
+      }
+    }
+  }
+  if (!shared) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      const double c = e[i] / sc[i];
+      q[i] = c * c;
+    }
   }
   return wrms_sum<D>(q);
 }
@@ -488,8 +514,11 @@ __device__ __forceinline__ double load_rec(const double* rec, long long n, long 
 }
 
 // --- forward adaptive solve with record --------------------------------------------------
+// Bounded to 6 resident blocks of 128 per SM (80 registers): with the shared-reciprocal error
+// norm the unbounded kernel takes 84 and drops to 5 blocks; the few bytes it spills at 80 cost
+// less than the lost warps (11.63 vs 11.73 ms on the Lorenz 2^20 bench forward).
 template <class F>
-__global__ void __launch_bounds__(128) tsit5_record_kernel(const RecordArgs a) {
+__global__ void __launch_bounds__(128, 6) tsit5_record_kernel(const RecordArgs a) {
   constexpr int D = F::D, P = F::P;
   using T = Tsit5;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;

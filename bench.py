@@ -260,15 +260,33 @@ def run_reference(args) -> None:
 # ------------------------------------------------------------------------------------
 # the B200 arm
 # ------------------------------------------------------------------------------------
+class _NoGC:
+    """Python's garbage collector paused around a timed loop, as timeit does: a collection
+    that lands between a synchronising host call and the next launch would leave the GPU idle
+    inside the events and be billed to the kernels."""
+
+    def __enter__(self):
+        import gc
+        gc.collect()
+        self.was = gc.isenabled()
+        gc.disable()
+
+    def __exit__(self, *exc):
+        import gc
+        if self.was:
+            gc.enable()
+
+
 def _time_steps(torch, step, steps, flush, stream):
     """Run `steps` timed steps (L2 flushed before each, outside the events); returns the
     per-step (forward, adjoint, whole) milliseconds and the last step's outputs."""
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(steps)]
     out = None
-    for k in range(steps):
-        flush.zero_()
-        out = step(ev[k])
-    torch.cuda.synchronize()
+    with _NoGC():
+        for k in range(steps):
+            flush.zero_()
+            out = step(ev[k])
+        torch.cuda.synchronize()
     fwd = [e[0].elapsed_time(e[1]) for e in ev]
     adj = [e[2].elapsed_time(e[3]) for e in ev]
     whole = [e[0].elapsed_time(e[3]) for e in ev]
@@ -395,12 +413,13 @@ def run_b200(args) -> None:
                 fwd_only()
             evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                    for _ in range(args.steps)]
-            for e0, e1 in evs:
-                flush.zero_()
-                e0.record(stream)
-                rs = fwd_only()
-                e1.record(stream)
-            torch.cuda.synchronize()
+            with _NoGC():
+                for e0, e1 in evs:
+                    flush.zero_()
+                    e0.record(stream)
+                    rs = fwd_only()
+                    e1.record(stream)
+                torch.cuda.synchronize()
             s_ms = float(np.mean([e0.elapsed_time(e1) for e0, e1 in evs]))
             s_ms = max_over_ranks(s_ms, dev)
             s_att = int((rs.n_acc.to(torch.int64) + rs.n_rej.to(torch.int64)).sum().item())
@@ -655,6 +674,8 @@ def run_workload(args) -> None:
         evs = [[torch.cuda.Event(enable_timing=True) for _ in range(len(groups) + 1)]
                for _ in range(args.steps)]
         outs = None
+        nogc = _NoGC()
+        nogc.__enter__()
         for e in evs:
             flush.zero_()
             e[0].record(stream)
@@ -663,6 +684,7 @@ def run_workload(args) -> None:
                 outs.append(group_step(g, prec_of(g, variant)))
                 e[k + 1].record(stream)
         torch.cuda.synchronize()
+        nogc.__exit__(None, None, None)
         per_group = [float(np.mean([e[k].elapsed_time(e[k + 1]) for e in evs]))
                      for k in range(len(groups))]
         steps_ms = [e[0].elapsed_time(e[-1]) for e in evs]
@@ -818,14 +840,16 @@ def run_published(args) -> None:
         for _ in range(max(3, args.warmup)):
             fn()
         ms = []
-        for _ in range(reps):
-            flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            fn()
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms.append(e0.elapsed_time(e1))
+        with _NoGC():
+            for _ in range(reps):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms.append(e0.elapsed_time(e1))
         return float(np.median(ms)), float(np.min(ms))
 
     grad = {}

@@ -181,8 +181,8 @@ class RecordSet:
     n x the longest trajectory, and each tier's launch holds trajectories of similar length.
 
     ``parts`` lists (rows, Record): rows None for a tier covering every trajectory, else the
-    sorted batch indices the tier covers; a later tier's results replace the earlier ones for
-    its rows.  Per-trajectory results are those of a single record (trajectories are
+    batch indices the tier covers, in the tier's order; a later tier's results replace the
+    earlier ones for its rows.  Per-trajectory results are those of a single record (trajectories are
     independent and every tier runs the same kernel).
 
     A RecordSet passed back as the ``workspace`` of the next solve of the same batch is a
@@ -217,14 +217,23 @@ class RecordSet:
         return sum(r.rec.numel() * 8 + r.ckpt.numel() * 8 for _, r in self.parts)
 
     def plan_rows(self) -> list:
-        """For each part, the rows whose final tier it is (sorted)."""
+        """For each part, the rows whose final tier it is, longest first (by this record's
+        step counts): lanes refilled from a work counter then take the long trajectories
+        first, and the short ones fill in around them instead of the long ones ending last."""
         owner = torch.zeros(self.n, dtype=torch.int64, device=self.y_final.device)
         for k, (rows, _r) in enumerate(self.parts):
             if rows is None:
                 owner.fill_(k)
             else:
                 owner.index_fill_(0, rows, k)
-        return [torch.nonzero(owner == k).squeeze(1) for k in range(len(self.parts))]
+        out = []
+        for k in range(len(self.parts)):
+            rows = torch.nonzero(owner == k).squeeze(1)
+            if rows.numel() > 1:
+                cost = (self.n_acc + self.n_rej).index_select(0, rows).to(torch.int64)
+                rows = rows.index_select(0, torch.argsort(cost, descending=True, stable=True))
+            out.append(rows)
+        return out
 
     def padded_dts(self, S: Optional[int] = None) -> torch.Tensor:
         if S is None:
@@ -251,12 +260,19 @@ class RecordSet:
                 continue
             if prow.numel() == 0:
                 continue
-            pos = torch.searchsorted(prow, rows).clamp_max(prow.numel() - 1)
-            hit = prow[pos] == rows
+            pos = _positions(prow, rows, self.n)
+            hit = pos >= 0
             if bool(hit.any()):
                 sel = torch.nonzero(hit).squeeze(1)
                 out.index_copy_(0, sel, r.dts_rows(pos[sel], S))
         return out
+
+
+def _positions(part_rows: torch.Tensor, rows: torch.Tensor, n: int) -> torch.Tensor:
+    """For each of ``rows``, its position in ``part_rows`` (any order), or -1."""
+    inv = torch.full((n,), -1, dtype=torch.int64, device=part_rows.device)
+    inv.index_copy_(0, part_rows, torch.arange(part_rows.numel(), device=part_rows.device))
+    return inv[rows]
 
 
 def _parts(r):
@@ -513,8 +529,8 @@ def _forward_planned(method, spec, y0, p, t1v, saveat_ts, ws: RecordSet, kw):
                          cap0=grown, saveat_ts=_take_ts(saveat_ts, over), **kw)
     parts = list(out)
     for rows, rr in out:  # empty the overflowed rows in the tiers that held them
-        pos = torch.searchsorted(rows, over).clamp_max(max(rows.numel() - 1, 0))
-        hit = rows[pos] == over if rows.numel() else torch.zeros_like(over, dtype=torch.bool)
+        pos = _positions(rows, over, n)
+        hit = pos >= 0
         if bool(hit.any()):
             rr.n_acc.index_fill_(0, pos[hit], 0)
     for srows, rr in _parts(sub):

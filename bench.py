@@ -429,6 +429,12 @@ def run_b200(args) -> None:
     clk = clocks.stop()
 
     # ---- e2e through the public API, host buffers, H2D + D2H inside the timed region ----
+    # the step workspaces above are done with: give their memory back before the API path
+    # allocates its own records (it holds one closure's record at a time)
+    step = mstep = r = rm = gpm = yf_sm = gp_sm = None
+    import gc
+    gc.collect()
+    torch.cuda.empty_cache()
     e2e = None
     if not args.no_e2e:
         import gradsolve_b200 as gsb

@@ -38,12 +38,11 @@ L2_BYTES = 126 * 1024 * 1024
 
 # DRAM bytes per trajectory of each kernel on this workload, from ncu captures at n = 2^18
 # (dram__bytes_read.sum + dram__bytes_write.sum per launch / 2^18), by checkpoint interval;
-# profiles/tsit5_f64_lorenz_bench_n2e20_launches_n2e18_K3_K4.md and
-# profiles/tsit5_f64_lorenz_n2e18_K8.md.  Traffic grows with the trajectory count.
+# profiles/tsit5_f64_lorenz_bench_n2e20_launches_n2e18_K2.md.  Traffic grows with the
+# trajectory count.
 DRAM_BYTES_PER_TRAJ = {
-    "tsit5_adjoint_kernel": {3: 5.035797e9 / 2**18, 4: 3.714259e9 / 2**18,
-                             8: 2.455204e9 / 2**18},
-    "tsit5_record_kernel": {3: 3.260184e9 / 2**18, 4: 2.790004e9 / 2**18},
+    "tsit5_adjoint_kernel": {2: 6.120321e9 / 2**18},
+    "tsit5_record_kernel": {2: 4.208535e9 / 2**18},
 }
 
 

@@ -6,14 +6,14 @@
 //   W = I - d*h*J(y);  k1 = W\f(y);  k2 = W\(f(y + h/2 k1) - k1) + k1;  ynew = y + h k2;
 //   k3 = W\(f(ynew) - e32 (k2 - F1) - 2 (k1 - F0));  err_vec = h/6 (k1 - 2 k2 + k3);
 //   WRMS norm, accept iff err <= 1, dt = h*clip(0.9*max(err,1e-10)^(-1/3), 0.2, 5) after both
-//   outcomes.  W is factored once per attempt (partial pivoting, division by the pivot) and
-//   the three solves reuse the factors: the same elimination, in the same order, as the
+//   outcomes.  W is factored once per attempt (partial pivoting) and the three solves reuse
+//   the factors: the same elimination, in the same order, as the
 //   reference kernel's three fresh eliminations (_gauss_solve, :346-381), because a row swap
 //   moves the stored multipliers with the row.  The 3x3 LU stays in registers.  The
-//   multipliers are divisions by the pivot, as in the reference; the back substitutions
-//   multiply by the pivot's reciprocal, computed once per factorisation, instead of dividing
-//   by it in every solve (within an ulp of the division per solve; it takes the dependent
-//   divisions off each attempt's critical path).
+//   multipliers and the back substitutions multiply by the pivot's reciprocal, computed once
+//   per column, where the reference divides by the pivot in each (within an ulp of the
+//   division each time; it takes the dependent divisions off each attempt's critical path:
+//   D divisions per factorisation instead of D (D + 1) / 2 + D per solve).
 // Replay: gradsolve/solvers/rosenbrock23_step.py:47-66 (no k3) with the analytic Jacobian.
 // Adjoint: reverse of that step, including the second-order term through W = I - d dt J(y,p):
 //   Wbar = -(W^-T k2bar) k2'^T - (W^-T k1bar) k1^T,  then  d<-d dt Wbar, J(y,p)>/d(y,p).
@@ -61,16 +61,16 @@ __device__ __forceinline__ void lu_factor(LU<D>& f) {
         }
       }
     }
+    // one reciprocal of the pivot serves the column's multipliers and the back substitutions
+    f.inv[col] = 1.0 / f.a[col * D + col];
 #pragma unroll
     for (int r = col + 1; r < D; ++r) {
-      const double factor = f.a[r * D + col] / f.a[col * D + col];
+      const double factor = f.a[r * D + col] * f.inv[col];
       f.a[r * D + col] = factor;
 #pragma unroll
       for (int c = col + 1; c < D; ++c) f.a[r * D + c] = f.a[r * D + c] - factor * f.a[col * D + c];
     }
   }
-#pragma unroll
-  for (int i = 0; i < D; ++i) f.inv[i] = 1.0 / f.a[i * D + i];
 }
 
 // x = W^-1 b

@@ -252,7 +252,6 @@ __global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
   const bool ck_on = a.ckpt != nullptr;
   if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
   int acc = 0, rej = 0, st = 0, ck_cnt = 0, ck_slot = 0;
-  double b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
   for (int it = 0; it < a.max_steps; ++it) {
     if (t >= t1) break;
     const double h = (t1 - t < dt) ? (t1 - t) : dt;
@@ -283,13 +282,7 @@ __global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
       t = t + h;
 #pragma unroll
       for (int i = 0; i < D; ++i) y[i] = ynew[i];
-      if (rec_on) {
-        b0 = b1;
-        b1 = b2;
-        b2 = b3;
-        b3 = h;
-        if ((acc & 3) == 3) store_rec_chunk(a.rec, a.n, j, acc >> 2, b0, b1, b2, b3);
-      }
+      if (rec_on) a.rec[rec_index(j, acc, a.n)] = h;
       ++acc;
       if (ck_on && ++ck_cnt == a.ck_every) {
         ck_cnt = 0;
@@ -301,13 +294,8 @@ __global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
     dt = step_from_sum<6>(m, h, a.ctrl);
   }
   if (st == 0 && !(t >= t1)) st = 1;
-  if (rec_on) {
-    switch (acc & 3) {
-      case 1: store_rec_chunk(a.rec, a.n, j, acc >> 2, b3, 0.0, 0.0, 0.0); break;
-      case 2: store_rec_chunk(a.rec, a.n, j, acc >> 2, b2, b3, 0.0, 0.0); break;
-      case 3: store_rec_chunk(a.rec, a.n, j, acc >> 2, b1, b2, b3, 0.0); break;
-      default: break;
-    }
+  if (rec_on) {  // zero-pad the last sector (identity steps)
+    for (int s = acc; (s & 3) != 0; ++s) a.rec[rec_index(j, s, a.n)] = 0.0;
   }
 #pragma unroll
   for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];

@@ -12,11 +12,14 @@
 //   p, gp                   : (n, P) row-major float64
 //   dt record               : chunk-interleaved, 4 steps per 32-byte sector:
 //                             step s of trajectory j lives at ((s/4)*n + j)*4 + s%4.
-//                             A thread buffers 4 accepted dt's in registers and writes the
-//                             whole sector at once (two 16-byte stores), so the record is
-//                             written and read in full sectors even though trajectories
-//                             accept steps at different times.  Entries past n_acc[j] in
-//                             trajectory j's last sector are 0 (identity steps).
+//                             The one-thread-per-trajectory forward kernels store each
+//                             accepted dt as it comes (8 bytes into its sector; the lanes of a
+//                             warp hold consecutive j, and L2 merges a sector's four writes
+//                             before it goes to DRAM -- faster than holding four dt's in
+//                             registers and writing the whole sector at once); the persistent
+//                             kernels, whose lanes hold scattered j, buffer the sector in
+//                             registers.  Entries past n_acc[j] in trajectory j's last sector
+//                             are 0 (identity steps).
 //   checkpoints             : slot c of trajectory j = (y after c*K accepted steps, t), at
 //                             ((c*n + j) * CW) with CW = D+1 rounded up to even (16-byte
 //                             aligned); slot 0 is (y0, t0).  K = ckpt_every.
@@ -536,7 +539,6 @@ __global__ void __launch_bounds__(128, 6) tsit5_record_kernel(const RecordArgs a
   if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
   F::rhs(y, p, k1);
   int acc = 0, rej = 0, st = 0, ck_cnt = 0, ck_slot = 0;
-  double b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
   for (int it = 0; it < a.max_steps; ++it) {
     if (t >= t1) break;
     const double h = (t1 - t < dt) ? (t1 - t) : dt;
@@ -564,13 +566,7 @@ __global__ void __launch_bounds__(128, 6) tsit5_record_kernel(const RecordArgs a
         y[i] = y5[i];
         k1[i] = k7[i];
       }
-      if (rec_on) {
-        b0 = b1;
-        b1 = b2;
-        b2 = b3;
-        b3 = h;
-        if ((acc & 3) == 3) store_rec_chunk(a.rec, a.n, j, acc >> 2, b0, b1, b2, b3);
-      }
+      if (rec_on) a.rec[rec_index(j, acc, a.n)] = h;
       ++acc;
       if (ck_on && ++ck_cnt == a.ck_every) {
         ck_cnt = 0;
@@ -582,13 +578,8 @@ __global__ void __launch_bounds__(128, 6) tsit5_record_kernel(const RecordArgs a
     dt = step_from_sum<10>(m, h, a.ctrl);
   }
   if (st == 0 && !(t >= t1)) st = 1;
-  if (rec_on) {
-    switch (acc & 3) {  // zero-padded last sector
-      case 1: store_rec_chunk(a.rec, a.n, j, acc >> 2, b3, 0.0, 0.0, 0.0); break;
-      case 2: store_rec_chunk(a.rec, a.n, j, acc >> 2, b2, b3, 0.0, 0.0); break;
-      case 3: store_rec_chunk(a.rec, a.n, j, acc >> 2, b1, b2, b3, 0.0); break;
-      default: break;
-    }
+  if (rec_on) {  // zero-pad the last sector (identity steps)
+    for (int s = acc; (s & 3) != 0; ++s) a.rec[rec_index(j, s, a.n)] = 0.0;
   }
 #pragma unroll
   for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];

@@ -301,10 +301,11 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
                          int sched, int variant) {
   if (sched == GS_SCHED_STATIC) {
     int rc;
-    // the stage-keeping variant needs 6*D doubles per step of the segment; where that does not
-    // fit one warp's worth of shared memory (large K and D) the stages are recomputed instead
-    const int stage_doubles = gs::adjoint_smem_doubles<F::D, 6 * F::D>(a.ck_every);
-    if (!mixed && variant == GS_ADJ_STAGES &&
+    // the stage-keeping variant needs 5*D more doubles per replayed step of the segment; where
+    // that does not fit one warp's worth of shared memory (large K and D) the stages are
+    // recomputed instead
+    const int stage_doubles = gs::adjoint_stages_smem_doubles<F::D>(a.ck_every);
+    if (!mixed && variant != GS_ADJ_RECOMPUTE &&
         (size_t)stage_doubles * sizeof(double) * 32u <= kSegBudget) {
       SegCfg c;
       if ((rc = occupancy_cfg(gs::tsit5_adjoint_stages_kernel<F>, stage_doubles, &c))) return rc;

@@ -652,8 +652,8 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 // Start the copies of segment sg's checkpoint and dts (steps at or past na read as 0).
-template <int D, int W>
-__device__ __forceinline__ void prefetch_segment(AdjBuf<D, W>& buf, int b, const double* ckpt,
+template <int D, class Buf>
+__device__ __forceinline__ void prefetch_segment(Buf& buf, int b, const double* ckpt,
                                                  const double* rec, long long n, long long j,
                                                  int sg, int K, int na) {
   constexpr int CW = (D + 2) & ~1;
@@ -689,13 +689,13 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a)
   const int nseg = (na + K - 1) / K;
   AdjBuf<D> buf(K);
   int b = 0;
-  if (nseg > 0) prefetch_segment(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
+  if (nseg > 0) prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
   for (int sg = nseg - 1; sg >= 0; --sg) {
     cp_async_wait_all();  // this segment's checkpoint and dts have landed
     double y[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) y[i] = buf.ck(b, i);
-    if (sg > 0) prefetch_segment(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
+    if (sg > 0) prefetch_segment<D>(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
 #pragma unroll
     for (int i = 0; i < D; ++i) buf.st(0, i) = y[i];
     for (int q = 1; q < K; ++q) {
@@ -726,21 +726,47 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a)
 }
 
 // --- reverse-replay adjoint that keeps the stage inputs -----------------------------------
-// The segment's forward pass stores, per step, y and the stage inputs s2..s6 (6*D doubles) in
-// the shared-memory segment buffer, so the reverse sweep runs the step VJPs without
-// recomputing the stages: one stage evaluation per step instead of two, for 6x the buffer.
-// The next segment's checkpoint and dts are prefetched as in tsit5_adjoint_kernel.
-// Same states (tsit5_stage_states<F, true> evaluates tsit5_replay_step's expressions) and the
-// same VJP code (tsit5_vjp_core) as tsit5_adjoint_kernel.
+// The segment's replay evaluates the stages of its first K-1 steps anyway: this variant keeps
+// their inputs s2..s6 (5*D doubles per step) in the shared-memory buffer, so those steps'
+// VJPs run without recomputing them; only the segment's last step, which the replay does not
+// take, recomputes its stages.  Per segment: K stage evaluations instead of 2K-1, for
+// (K-1)*5*D more doubles of buffer per thread.  Same states (tsit5_stage_states<F, true>
+// evaluates tsit5_replay_step's expressions), the same VJP code (tsit5_vjp_core), and the
+// same checkpoint/dt prefetch as tsit5_adjoint_kernel.
+template <int D>
+GS_HD int adjoint_stages_smem_doubles(int K) {
+  return K * D + (K - 1) * 5 * D + 2 * K + 2 * ((D + 2) & ~1);
+}
+
+template <int D>
+struct AdjStageBuf {
+  static constexpr int CW = (D + 2) & ~1;
+  double* base;
+  int stride, K;
+  __device__ __forceinline__ AdjStageBuf(int k)
+      : base(gs_seg_smem + threadIdx.x), stride(blockDim.x), K(k) {}
+  __device__ __forceinline__ double& st(int q, int i) { return base[(q * D + i) * stride]; }
+  // stage input s_M (M = 2..6) of step q < K-1
+  __device__ __forceinline__ double& stg(int q, int m, int i) {
+    return base[(K * D + (q * 5 + (m - 2)) * D + i) * stride];
+  }
+  __device__ __forceinline__ double& dt(int b, int q) {
+    return base[(K * D + (K - 1) * 5 * D + b * K + q) * stride];
+  }
+  __device__ __forceinline__ double& ck(int b, int i) {
+    return base[(K * D + (K - 1) * 5 * D + 2 * K + b * CW + i) * stride];
+  }
+};
+
 template <class F>
-struct SegStages {
+struct KeptStages {  // tsit5_vjp_core's stage source: the kept inputs of step q
   static constexpr int D = F::D;
-  const double* base;
-  int stride, q;
+  AdjStageBuf<D>* buf;
+  int q;
   template <int M>
   __device__ __forceinline__ void get(double* out) const {
 #pragma unroll
-    for (int i = 0; i < D; ++i) out[i] = base[(q * 6 * D + (M - 1) * D + i) * stride];
+    for (int i = 0; i < D; ++i) out[i] = buf->stg(q, M, i);
   }
 };
 
@@ -760,46 +786,52 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_stages_kernel(const Adjoint
   const int na = steps_in_record(a.n_acc, j, a.cap);
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
-  AdjBuf<D, 6 * D> buf(K);  // per step: y and the stage inputs s2..s6; dts, checkpoints
+  AdjStageBuf<D> buf(K);
   int b = 0;
-  if (nseg > 0) prefetch_segment(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
+  if (nseg > 0) prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
   for (int sg = nseg - 1; sg >= 0; --sg) {
     cp_async_wait_all();  // this segment's checkpoint and dts have landed
     double y[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) y[i] = buf.ck(b, i);
-    if (sg > 0) prefetch_segment(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
-    for (int q = 0; q < K; ++q) {
-      const double dt = buf.dt(b, q);
+    if (sg > 0) prefetch_segment<D>(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
 #pragma unroll
-      for (int i = 0; i < D; ++i) buf.st(q, i) = y[i];
+    for (int i = 0; i < D; ++i) buf.st(0, i) = y[i];
+    for (int q = 1; q < K; ++q) {  // replay steps 0..K-2, keeping their stage inputs
+      const double dt = buf.dt(b, q - 1);
       if (dt != 0.0) {
         StageStates<F> S;
-        if (q + 1 < K) {
-          double yn[D];
-          tsit5_stage_states<F, true>(y, p, dt, S, yn);
-#pragma unroll
-          for (int i = 0; i < D; ++i) y[i] = yn[i];
-        } else {
-          tsit5_stage_states<F, false>(y, p, dt, S, nullptr);
-        }
+        double yn[D];
+        tsit5_stage_states<F, true>(y, p, dt, S, yn);
 #pragma unroll
         for (int i = 0; i < D; ++i) {
-          buf.st(q, D + i) = S.s2[i];
-          buf.st(q, 2 * D + i) = S.s3[i];
-          buf.st(q, 3 * D + i) = S.s4[i];
-          buf.st(q, 4 * D + i) = S.s5[i];
-          buf.st(q, 5 * D + i) = S.s6[i];
+          y[i] = yn[i];
+          buf.stg(q - 1, 2, i) = S.s2[i];
+          buf.stg(q - 1, 3, i) = S.s3[i];
+          buf.stg(q - 1, 4, i) = S.s4[i];
+          buf.stg(q - 1, 5, i) = S.s5[i];
+          buf.stg(q - 1, 6, i) = S.s6[i];
         }
       }
+#pragma unroll
+      for (int i = 0; i < D; ++i) buf.st(q, i) = y[i];
     }
-    for (int q = K - 1; q >= 0; --q) {
+    {  // the segment's last step: its stages were not evaluated by the replay
+      const double dt = buf.dt(b, K - 1);
+      if (dt != 0.0) {
+        double ys[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) ys[i] = buf.st(K - 1, i);
+        tsit5_step_vjp<F>(ys, p, dt, lam, gp);
+      }
+    }
+    for (int q = K - 2; q >= 0; --q) {
       const double dt = buf.dt(b, q);
       if (dt != 0.0) {
         double ys[D];
 #pragma unroll
         for (int i = 0; i < D; ++i) ys[i] = buf.st(q, i);
-        const SegStages<F> src{buf.base, buf.stride, q};
+        const KeptStages<F> src{&buf, q};
         tsit5_vjp_core<F>(ys, src, p, dt, lam, gp);
       }
     }

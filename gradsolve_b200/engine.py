@@ -607,10 +607,9 @@ def adjoint(r, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
     """(dL/dy0, dL/dp) for cotangent ybar = dL/dy_final, using the record's checkpoints.
     ``schedule="auto"`` refills lanes from a work counter when the record came from an
     uneven batch (per-trajectory end times), else runs one thread per trajectory.
-    ``variant`` (Tsit5, float64, one thread per trajectory): "stages" keeps each step's stage
-    inputs from the segment's forward pass, "recompute" re-evaluates them in the reverse
-    sweep; "auto" is "recompute" (the larger stage buffer costs more occupancy than the
-    saved stage evaluations gain for the built-in fields)."""
+    ``variant`` (Tsit5, float64, one thread per trajectory): "stages" keeps the stage inputs
+    the segment's replay evaluates, "recompute" re-evaluates every step's stages in the
+    reverse sweep; "auto" is "stages" (recompute where its buffer would not fit)."""
     if schedule == "auto" and r.uneven:
         schedule = "refill"
     res = _over_parts(r, lambda rr, rows: _adjoint_one(

@@ -347,10 +347,19 @@ int launch_ros23_replay(const gs::ReplayArgs& a, cudaStream_t s) {
 template <class F>
 int launch_ros23_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, int sched) {
   if (sched == GS_SCHED_STATIC) {
-    const SegCfg c = seg_cfg(a.ck_every, F::D);
+    SegCfg c;
     int rc;
-    if ((rc = allow_smem(gs::ros23_adjoint_kernel<F>, c.smem))) return rc;
-    gs::ros23_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+    const int keep = gs::ros23_adjoint_smem_doubles<F::D, true>(a.ck_every);
+    if ((size_t)keep * sizeof(double) * 32u <= kSegBudget) {
+      if ((rc = occupancy_cfg(gs::ros23_adjoint_kernel<F, true>, keep, &c))) return rc;
+      gs::ros23_adjoint_kernel<F, true><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+      return cuda_check("ros23_adjoint_kernel");
+    }
+    // large K and D: the kept quantities would not fit shared memory; recompute them
+    if ((rc = occupancy_cfg(gs::ros23_adjoint_kernel<F, false>,
+                            gs::ros23_adjoint_smem_doubles<F::D, false>(a.ck_every), &c)))
+      return rc;
+    gs::ros23_adjoint_kernel<F, false><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
     return cuda_check("ros23_adjoint_kernel");
   }
   return launch_adjoint_persistent<F, gs::Ros23Step>(a, cap, s, sched == GS_SCHED_REFILL);

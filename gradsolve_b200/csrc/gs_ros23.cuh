@@ -153,7 +153,7 @@ template <class F>
 struct RosCore {
   static constexpr int D = F::D;
   LU<D> W;
-  double F0[D], k1[D], F1[D], k2[D];
+  double F0[D], k1[D], F1[D], k2p[D], k2[D];  // k2 = k2p + k1
 };
 
 template <class F>
@@ -169,9 +169,9 @@ __device__ __forceinline__ void ros23_core(const double* y, const double* p, dou
   F::rhs(s, p, c.F1);
 #pragma unroll
   for (int i = 0; i < D; ++i) s[i] = c.F1[i] - c.k1[i];
-  lu_solve<D>(c.W, s, c.k2);
+  lu_solve<D>(c.W, s, c.k2p);
 #pragma unroll
-  for (int i = 0; i < D; ++i) c.k2[i] = c.k2[i] + c.k1[i];
+  for (int i = 0; i < D; ++i) c.k2[i] = c.k2p[i] + c.k1[i];
 #pragma unroll
   for (int i = 0; i < D; ++i) ynew[i] = y[i] + h * c.k2[i];
 }
@@ -186,22 +186,14 @@ __device__ __forceinline__ void ros23_replay_step(double* y, const double* p, do
   for (int i = 0; i < D; ++i) y[i] = yn[i];
 }
 
+// Reverse of one replay step from the step's forward quantities: the factors of W, k1, the
+// stage state s1 = y + dt/2 k1 and k2' = W \ (f(s1) - k1).
 template <class F>
-__device__ __forceinline__ void ros23_step_vjp(const double* y, const double* p, double dt,
-                                               double* lam, double* gp) {
+__device__ __forceinline__ void ros23_vjp_core(const double* y, const double* p, double dt,
+                                               const LU<F::D>& W, const double* k1,
+                                               const double* s1, const double* k2p, double* lam,
+                                               double* gp) {
   constexpr int D = F::D;
-  LU<D> W;
-  double F0[D], k1[D], s1[D], F1[D], r2[D], k2p[D];
-  ros23_build_w<F>(y, p, dt, W);
-  F::rhs(y, p, F0);
-  lu_solve<D>(W, F0, k1);
-#pragma unroll
-  for (int i = 0; i < D; ++i) s1[i] = y[i] + 0.5 * dt * k1[i];
-  F::rhs(s1, p, F1);
-#pragma unroll
-  for (int i = 0; i < D; ++i) r2[i] = F1[i] - k1[i];
-  lu_solve<D>(W, r2, k2p);
-
   double yb[D], k2b[D], k1b[D], r2b[D], s1b[D], r1b[D], G[D * D];
 #pragma unroll
   for (int i = 0; i < D; ++i) {
@@ -233,6 +225,20 @@ __device__ __forceinline__ void ros23_step_vjp(const double* y, const double* p,
   F::jac_contract_grad(y, p, G, yb, gp);
 #pragma unroll
   for (int i = 0; i < D; ++i) lam[i] = yb[i];
+}
+
+// Reverse of one replay step at (y, dt), recomputing its forward quantities (the expressions
+// of ros23_core).
+template <class F>
+__device__ __forceinline__ void ros23_step_vjp(const double* y, const double* p, double dt,
+                                               double* lam, double* gp) {
+  constexpr int D = F::D;
+  RosCore<F> c;
+  double yn[D], s1[D];
+  ros23_core<F>(y, p, dt, c, yn);
+#pragma unroll
+  for (int i = 0; i < D; ++i) s1[i] = y[i] + 0.5 * dt * c.k1[i];
+  ros23_vjp_core<F>(y, p, dt, c.W, c.k1, s1, c.k2p, lam, gp);
 }
 
 template <class F>
@@ -332,7 +338,64 @@ __global__ void __launch_bounds__(128) ros23_replay_kernel(const ReplayArgs a) {
   for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
 }
 
-template <class F>
+// Reverse pass.  As tsit5_adjoint_stages_kernel: the next segment's checkpoint and dts are
+// prefetched (cp.async) into the shared-memory segment buffer, and the segment's replay keeps
+// what the step VJPs need -- the factors of W (D^2 + 2D values), k1, s1 and k2' -- for the
+// K-1 steps it takes, so only the segment's last step recomputes its forward quantities.
+// kKeep = false (where the kept quantities would not fit shared memory): every step's VJP
+// recomputes them, and the buffer holds only the states, dts and checkpoints.
+template <int D, bool kKeep>
+GS_HD int ros23_adjoint_smem_doubles(int K) {
+  return K * D + (kKeep ? (K - 1) * (D * D + 5 * D) : 0) + 2 * K + 2 * ((D + 2) & ~1);
+}
+
+template <int D, bool kKeep>
+struct AdjRosBuf {
+  static constexpr int CW = (D + 2) & ~1;
+  static constexpr int R = kKeep ? D * D + 5 * D : 0;  // kept values per step
+  double* base;
+  int stride, K;
+  __device__ __forceinline__ AdjRosBuf(int k)
+      : base(gs_seg_smem + threadIdx.x), stride(blockDim.x), K(k) {}
+  __device__ __forceinline__ double& st(int q, int i) { return base[(q * D + i) * stride]; }
+  __device__ __forceinline__ double& kept(int q, int v) {
+    return base[(K * D + q * R + v) * stride];
+  }
+  __device__ __forceinline__ double& dt(int b, int q) {
+    return base[(K * D + (K - 1) * R + b * K + q) * stride];
+  }
+  __device__ __forceinline__ double& ck(int b, int i) {
+    return base[(K * D + (K - 1) * R + 2 * K + b * CW + i) * stride];
+  }
+  // layout of a kept step: W.a, W.inv, W.piv (as doubles), k1, s1, k2' (kKeep only)
+  __device__ __forceinline__ void keep(int q, const LU<D>& W, const double* k1, const double* s1,
+                                       const double* k2p) {
+#pragma unroll
+    for (int v = 0; v < D * D; ++v) kept(q, v) = W.a[v];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      kept(q, D * D + i) = W.inv[i];
+      kept(q, D * D + D + i) = (double)W.piv[i];
+      kept(q, D * D + 2 * D + i) = k1[i];
+      kept(q, D * D + 3 * D + i) = s1[i];
+      kept(q, D * D + 4 * D + i) = k2p[i];
+    }
+  }
+  __device__ __forceinline__ void restore(int q, LU<D>& W, double* k1, double* s1, double* k2p) {
+#pragma unroll
+    for (int v = 0; v < D * D; ++v) W.a[v] = kept(q, v);
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      W.inv[i] = kept(q, D * D + i);
+      W.piv[i] = (int)kept(q, D * D + D + i);
+      k1[i] = kept(q, D * D + 2 * D + i);
+      s1[i] = kept(q, D * D + 3 * D + i);
+      k2p[i] = kept(q, D * D + 4 * D + i);
+    }
+  }
+};
+
+template <class F, bool kKeep>
 __global__ void __launch_bounds__(128) ros23_adjoint_kernel(const AdjointArgs a) {
   constexpr int D = F::D, P = F::P;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -348,30 +411,51 @@ __global__ void __launch_bounds__(128) ros23_adjoint_kernel(const AdjointArgs a)
   const int na = steps_in_record(a.n_acc, j, a.cap);
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
-  SegBuf<D> seg;
+  AdjRosBuf<D, kKeep> buf(K);
+  int b = 0;
+  if (nseg > 0) prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
   for (int sg = nseg - 1; sg >= 0; --sg) {
-    const int start = sg * K;
+    cp_async_wait_all();  // this segment's checkpoint and dts have landed
     double y[D];
-    load_ckpt<D>(a.ckpt, a.n, j, sg, y);
 #pragma unroll
-    for (int i = 0; i < D; ++i) seg.at(0, i) = y[i];
-    for (int q = 1; q < K; ++q) {
-      const int s = start + q - 1;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
-      if (dt != 0.0) ros23_replay_step<F>(y, p, dt);
+    for (int i = 0; i < D; ++i) y[i] = buf.ck(b, i);
+    if (sg > 0) prefetch_segment<D>(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
 #pragma unroll
-      for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
+    for (int i = 0; i < D; ++i) buf.st(0, i) = y[i];
+    for (int q = 1; q < K; ++q) {  // replay steps 0..K-2, keeping their forward quantities
+      const double dt = buf.dt(b, q - 1);
+      if (dt != 0.0) {
+        RosCore<F> c;
+        double yn[D], s1[D];
+        ros23_core<F>(y, p, dt, c, yn);
+        if constexpr (kKeep) {
+#pragma unroll
+          for (int i = 0; i < D; ++i) s1[i] = y[i] + 0.5 * dt * c.k1[i];
+          buf.keep(q - 1, c.W, c.k1, s1, c.k2p);
+        }
+#pragma unroll
+        for (int i = 0; i < D; ++i) y[i] = yn[i];
+      }
+#pragma unroll
+      for (int i = 0; i < D; ++i) buf.st(q, i) = y[i];
     }
     for (int q = K - 1; q >= 0; --q) {
-      const int s = start + q;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      const double dt = buf.dt(b, q);
       if (dt != 0.0) {
         double ys[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) ys[i] = seg.at(q, i);
-        ros23_step_vjp<F>(ys, p, dt, lam, gp);
+        for (int i = 0; i < D; ++i) ys[i] = buf.st(q, i);
+        if (kKeep && q < K - 1) {  // kept by the replay
+          double k1[D], s1[D], k2p[D];
+          LU<D> W;
+          buf.restore(q, W, k1, s1, k2p);
+          ros23_vjp_core<F>(ys, p, dt, W, k1, s1, k2p, lam, gp);
+        } else {  // the segment's last step (or nothing kept): recompute
+          ros23_step_vjp<F>(ys, p, dt, lam, gp);
+        }
       }
     }
+    b ^= 1;
   }
   if (a.gy0) {
 #pragma unroll

@@ -17,6 +17,8 @@
 // Per-trajectory arithmetic is exactly that of gs_tsit5.cuh / gs_mixed.cuh / gs_ros23.cuh:
 // results do not depend on which lane integrates which trajectory.
 #pragma once
+#include <math_constants.h>
+
 #include "gs_mixed.cuh"
 #include "gs_ros23.cuh"
 #include "gs_saveat.cuh"
@@ -151,7 +153,6 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
   double y[D], ynew[D], p[P], t = 0.0, t1 = 0.0, dt = 0.0;
   float pf[P];
   int acc = 0, rej = 0, it = 0, ck_cnt = 0, ck_slot = 0;
-  double b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
   // dense output: the saveat rules of replay_saveat_kernel (gs_saveat.cuh) applied while the
   // trajectory is integrated -- a time bracketed by an accepted step [t, t+h] gets one
   // replay step of size ts - t from that step's start state
@@ -159,6 +160,9 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
   const double* tsr = nullptr;
   double* ysr = nullptr;
   int kk = 0;
+  // the next requested time, held in a register: the bracket test of every accepted step
+  // then waits on no load (infinity once every time is assigned)
+  double tnext = CUDART_INF;
   L lane;
   auto begin = [&](long long jj) {
 #pragma unroll
@@ -169,7 +173,6 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
     t1 = a.t1v ? a.t1v[jj] : a.t1;
     dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
     acc = rej = it = ck_cnt = ck_slot = 0;
-    b0 = b1 = b2 = b3 = 0.0;
     if (ck_on) store_ckpt<D>(a.ckpt, a.n, jj, 0, y, t);
     lane.start(y, p, pf);
     if (sv_on) {
@@ -180,6 +183,7 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
         store_row<D>(ysr + (long long)kk * D, y);
         ++kk;
       }
+      tnext = kk < a.K ? tsr[kk] : CUDART_INF;
     }
   };
   if (j < a.n) begin(j);
@@ -204,23 +208,21 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
           } else {
             if (sv_on) {
               const double tn = t + h;
-              while (kk < a.K && tsr[kk] <= tn) {  // bracketed by this step: re-step to ts
+              while (tnext <= tn) {  // bracketed by this step: re-step to ts
                 double yk[D], ck[D];
 #pragma unroll
                 for (int i = 0; i < D; ++i) { yk[i] = y[i]; ck[i] = 0.0; }
-                L::Step::template step<F>(yk, ck, p, pf, tsr[kk] - t);
+                L::Step::template step<F>(yk, ck, p, pf, tnext - t);
                 store_row<D>(ysr + (long long)kk * D, yk);
                 ++kk;
+                tnext = kk < a.K ? tsr[kk] : CUDART_INF;
               }
             }
             t = t + h;
 #pragma unroll
             for (int i = 0; i < D; ++i) y[i] = ynew[i];
             lane.commit();
-            if (rec_on) {
-              b0 = b1; b1 = b2; b2 = b3; b3 = h;
-              if ((acc & 3) == 3) store_rec_chunk(a.rec, a.n, j, acc >> 2, b0, b1, b2, b3);
-            }
+            if (rec_on) a.rec[rec_index(j, acc, a.n)] = h;
             ++acc;
             if (ck_on && ++ck_cnt == a.ck_every) {
               ck_cnt = 0;
@@ -234,13 +236,8 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
       }
     }
     if (st >= 0) {  // finished: write this trajectory's outputs, take the next one
-      if (rec_on) {
-        switch (acc & 3) {
-          case 1: store_rec_chunk(a.rec, a.n, j, acc >> 2, b3, 0.0, 0.0, 0.0); break;
-          case 2: store_rec_chunk(a.rec, a.n, j, acc >> 2, b2, b3, 0.0, 0.0); break;
-          case 3: store_rec_chunk(a.rec, a.n, j, acc >> 2, b1, b2, b3, 0.0); break;
-          default: break;
-        }
+      if (rec_on) {  // zero-pad the last sector (identity steps)
+        for (int s = acc; (s & 3) != 0; ++s) a.rec[rec_index(j, s, a.n)] = 0.0;
       }
 #pragma unroll
       for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];

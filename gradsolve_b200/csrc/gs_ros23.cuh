@@ -445,14 +445,19 @@ __global__ void __launch_bounds__(128) ros23_adjoint_kernel(const AdjointArgs a)
         double ys[D];
 #pragma unroll
         for (int i = 0; i < D; ++i) ys[i] = buf.st(q, i);
-        if (kKeep && q < K - 1) {  // kept by the replay
-          double k1[D], s1[D], k2p[D];
-          LU<D> W;
-          buf.restore(q, W, k1, s1, k2p);
-          ros23_vjp_core<F>(ys, p, dt, W, k1, s1, k2p, lam, gp);
-        } else {  // the segment's last step (or nothing kept): recompute
-          ros23_step_vjp<F>(ys, p, dt, lam, gp);
+        // one VJP call site: the forward quantities come from the replay's kept copy, or
+        // (the segment's last step, or nothing kept) are recomputed here
+        RosCore<F> c;
+        double s1[D];
+        if (kKeep && q < K - 1) {
+          buf.restore(q, c.W, c.k1, s1, c.k2p);
+        } else {
+          double yn[D];
+          ros23_core<F>(ys, p, dt, c, yn);
+#pragma unroll
+          for (int i = 0; i < D; ++i) s1[i] = ys[i] + 0.5 * dt * c.k1[i];
         }
+        ros23_vjp_core<F>(ys, p, dt, c.W, c.k1, s1, c.k2p, lam, gp);
       }
     }
     b ^= 1;

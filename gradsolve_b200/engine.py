@@ -96,10 +96,13 @@ def tuned_ckpt_every(method: str, spec: FieldSpec, precision: str) -> Optional[i
 def autotune_ckpt_every(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tensor, *,
                         t0: float, t1: float, rtol: float, atol: float,
                         t1v: Optional[torch.Tensor] = None, max_steps: int = 100000,
-                        precision: str = "float64", sample: int = 1 << 17,
-                        candidates=TUNE_CANDIDATES) -> int:
-    """Time forward + reverse pass for each candidate K on up to ``sample`` trajectories
-    (about two waves of the GPU) and cache the fastest."""
+                        precision: str = "float64", sample: int = 1 << 19,
+                        candidates=TUNE_CANDIDATES, reps: int = 2) -> int:
+    """Time forward + reverse pass for each candidate K on up to ``sample`` trajectories and
+    cache the fastest (best of ``reps`` timings).  The sample spans several waves of the GPU:
+    the candidates' reverse passes hold different numbers of blocks per SM (their shared
+    memory grows with K), and on one or two waves the partial last wave, not the kernel,
+    would decide."""
     m = min(y0.shape[0], sample)
     ys, ps = y0[:m].contiguous(), p[:m].contiguous()
     tv = None if t1v is None else t1v[:m].contiguous()
@@ -111,13 +114,15 @@ def autotune_ckpt_every(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch
         ybar = torch.ones_like(r.y_final)
         adjoint(r, ps, ybar, precision=precision)  # warm
         # forward (checkpoint writes grow as K shrinks) + reverse pass, buffers reused
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        r = forward_record(method, spec, ys, ps, workspace=r, **kw)
-        adjoint(r, ps, ybar, precision=precision)
-        e1.record()
-        e1.synchronize()
-        ms = e0.elapsed_time(e1)
+        ms = float("inf")
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r = forward_record(method, spec, ys, ps, workspace=r, **kw)
+            adjoint(r, ps, ybar, precision=precision)
+            e1.record()
+            e1.synchronize()
+            ms = min(ms, e0.elapsed_time(e1))
         if ms < best_ms:
             best, best_ms = K, ms
     _TUNED[(method, spec.key, precision)] = best
@@ -294,8 +299,12 @@ def _take_ts(ts: Optional[torch.Tensor], rows: Optional[torch.Tensor]):
 
 def _side_stream(device):
     """A stream for a tier that should overlap the others (None off the GPU: tiers then run
-    one after another on the current stream)."""
-    return torch.cuda.Stream(device=device) if device.type == "cuda" else None
+    one after another on the current stream).  Side streams carry the longer tiers, whose
+    few, long trajectories set the end of the launch: they get the higher priority, so their
+    blocks are placed first whenever the bulk tier and they compete for SMs."""
+    if device.type != "cuda":
+        return None
+    return torch.cuda.Stream(device=device, priority=-1)
 
 
 def _over_parts(r, fn) -> list:

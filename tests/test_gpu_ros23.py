@@ -54,7 +54,9 @@ def test_forward_record_matches_reference(gslib, oracle, cuda, case):
     check_dts(r.padded_dts().cpu().numpy(), o["dts"])
 
 
-@pytest.mark.parametrize("checkpoint", [1, 16, "sqrt"])
+# K = 64: the kept factors of a segment's replay no longer fit shared memory (D = 3), so the
+# reverse pass recomputes every step's factors -- the other of its two code paths
+@pytest.mark.parametrize("checkpoint", [1, 2, 16, 64, "sqrt"])
 @pytest.mark.parametrize("case", CASES)
 def test_adjoint_of_reference_dts(gslib, oracle, cuda, case, checkpoint):
     from gradsolve_b200 import engine

@@ -283,6 +283,10 @@ def _time_steps(torch, step, steps, flush, stream):
     out = None
     with _NoGC():
         for k in range(steps):
+            # the previous step's outputs are released first, as a training loop consumes a
+            # gradient before the next step: holding them would make every other step allocate
+            # fresh device memory (cudaMalloc) inside its events
+            out = None
             flush.zero_()
             out = step(ev[k])
         torch.cuda.synchronize()
@@ -365,6 +369,7 @@ def run_b200(args) -> None:
     acc = int(r.n_acc.to(torch.int64).sum().item())
     S = int(r.n_acc.max().item())
     K = r.ckpt_every
+    r = gp = None  # the warm-up's outputs (the record stays alive as the step's workspace)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -382,6 +387,7 @@ def run_b200(args) -> None:
         mstep = make_step("mixed")
         for _ in range(args.warmup):
             rm, gpm = mstep()
+        rm = gpm = None
         m_fwd, m_adj, m_step, (rm, gpm) = _time_steps(torch, mstep, args.steps, flush, stream)
         m_ms = float(np.mean(m_step))
         m_ms = max_over_ranks(m_ms, dev)
@@ -412,8 +418,10 @@ def run_b200(args) -> None:
                 fwd_only()
             evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                    for _ in range(args.steps)]
+            rs = None
             with _NoGC():
                 for e0, e1 in evs:
+                    rs = None  # release the previous solve's outputs before the next allocates
                     flush.zero_()
                     e0.record(stream)
                     rs = fwd_only()
@@ -456,16 +464,20 @@ def run_b200(args) -> None:
             e2e_step()
         torch.cuda.synchronize()
         ke = max(1, min(args.steps, 5))
-        t0 = time.perf_counter()
-        for _ in range(ke):
-            e2e_step()
-        torch.cuda.synchronize()
-        el = (time.perf_counter() - t0) / ke
+        with _NoGC():
+            t0 = time.perf_counter()
+            marks = [t0]
+            for _ in range(ke):
+                e2e_step()  # ends on the loss read-back: the step's work is done
+                marks.append(time.perf_counter())
+            torch.cuda.synchronize()
+            el = (time.perf_counter() - t0) / ke
         el = max_over_ranks(el, dev)
         e2e = {"value": n * world / el, "unit": UNIT,
                "h2d_bytes_per_step": int(y0_h.numel() * 8 + rho_h.numel() * 8),
                "d2h_bytes_per_step": int(grad_h.numel() * 8 + 8),
-               "ms_per_step": el * 1e3, "api": "gradsolve_b200.grad_closure + torch autograd"}
+               "ms_per_step": el * 1e3, "api": "gradsolve_b200.grad_closure + torch autograd",
+               "ms_steps": [round((b - a) * 1e3, 3) for a, b in zip(marks, marks[1:])]}
 
     if rank != 0:
         if world > 1:

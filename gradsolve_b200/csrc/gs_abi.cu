@@ -255,7 +255,7 @@ int launch_record_persistent(const gs::RecordArgs& a_in, cudaStream_t s, bool us
 template <class F, class M>
 int launch_adjoint_persistent(const gs::AdjointArgs& a, int cap, cudaStream_t s,
                               bool use_counter) {
-  const SegCfg c = seg_cfg(a.ck_every, F::D);
+  const SegCfg c = seg_cfg_doubles(gs::adjoint_smem_doubles<F::D>(a.ck_every));
   unsigned long long* counter =
       use_counter ? ctrl_counter(const_cast<double*>(a.ckpt), a.n,
                                  gs_ckpt_slots(cap, a.ck_every), F::D, gs::kCtrlAdj)
@@ -320,8 +320,10 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
       gs::tsit5_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
       return cuda_check("tsit5_adjoint_kernel");
     }
-    const SegCfg c = seg_cfg(a.ck_every, F::D);
-    if ((rc = allow_smem(gs::tsit5_mixed_adjoint_kernel<F>, c.smem))) return rc;
+    SegCfg c;
+    if ((rc = occupancy_cfg(gs::tsit5_mixed_adjoint_kernel<F>,
+                            gs::adjoint_smem_doubles<F::D>(a.ck_every), &c)))
+      return rc;
     gs::tsit5_mixed_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
     return cuda_check("tsit5_mixed_adjoint_kernel");
   }
@@ -751,9 +753,11 @@ namespace {
 template <class F, class M>
 int launch_saveat(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint) {
   if (adjoint) {
-    const SegCfg c = seg_cfg(a.ck_every, F::D + 1);
+    SegCfg c;
     int rc;
-    if ((rc = allow_smem(gs::adjoint_saveat_kernel<F, M>, c.smem))) return rc;
+    if ((rc = occupancy_cfg(gs::adjoint_saveat_kernel<F, M>,
+                            gs::adjoint_smem_doubles<F::D, F::D + 1>(a.ck_every), &c)))
+      return rc;
     gs::adjoint_saveat_kernel<F, M><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
     return cuda_check("adjoint_saveat_kernel");
   }
@@ -765,7 +769,7 @@ int launch_saveat(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint) {
 // checkpoint slots, like the other reverse passes'.
 template <class F, class M>
 int launch_adjoint_saveat_persistent(const gs::SaveatArgs& a, cudaStream_t s, bool use_counter) {
-  const SegCfg c = seg_cfg(a.ck_every, F::D + 1);
+  const SegCfg c = seg_cfg_doubles(gs::adjoint_smem_doubles<F::D, F::D + 1>(a.ck_every));
   unsigned long long* counter =
       use_counter ? ctrl_counter(a.ckpt, a.n, a.ck_slots, F::D, gs::kCtrlAdj) : nullptr;
   unsigned grid = 0;

@@ -351,30 +351,34 @@ __global__ void __launch_bounds__(128) tsit5_mixed_adjoint_kernel(const AdjointA
   const int na = steps_in_record(a.n_acc, j, a.cap);
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
-  SegBuf<D> seg;
+  // segment buffer and cp.async prefetch of the next segment: as tsit5_adjoint_kernel
+  AdjBuf<D> buf(K);
+  int b = 0;
+  if (nseg > 0) prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
   for (int sg = nseg - 1; sg >= 0; --sg) {
-    const int start = sg * K;
+    cp_async_wait_all();
     double y[D], c[D];
-    load_ckpt<D>(a.ckpt, a.n, j, sg, y);
 #pragma unroll
-    for (int i = 0; i < D; ++i) { seg.at(0, i) = y[i]; c[i] = 0.0; }
+    for (int i = 0; i < D; ++i) { y[i] = buf.ck(b, i); c[i] = 0.0; }
+    if (sg > 0) prefetch_segment<D>(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
+#pragma unroll
+    for (int i = 0; i < D; ++i) buf.st(0, i) = y[i];
     for (int q = 1; q < K; ++q) {
-      const int s = start + q - 1;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      const double dt = buf.dt(b, q - 1);
       if (dt != 0.0) mixed_replay_step<F>(y, c, p, pf, dt);
 #pragma unroll
-      for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
+      for (int i = 0; i < D; ++i) buf.st(q, i) = y[i];
     }
     for (int q = K - 1; q >= 0; --q) {
-      const int s = start + q;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      const double dt = buf.dt(b, q);
       if (dt != 0.0) {
         double ys[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) ys[i] = seg.at(q, i);
+        for (int i = 0; i < D; ++i) ys[i] = buf.st(q, i);
         mixed_step_vjp<F>(ys, p, pf, dt, lam, gp);
       }
     }
+    b ^= 1;
   }
   if (a.gy0) {
 #pragma unroll

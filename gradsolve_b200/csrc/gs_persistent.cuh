@@ -255,18 +255,23 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
 }
 
 // ---- persistent reverse pass (one segment of K steps per iteration) --------------------------
+// The shared-memory segment buffer is that of the one-thread-per-trajectory reverse passes
+// (AdjBuf: the K states, and double-buffered the dts and checkpoint of a segment): while a
+// segment is replayed and differentiated, the copies of the trajectory's previous segment are
+// in flight (cp.async), so a lane waits on DRAM once per trajectory instead of once per step.
 template <class F, class M>
 __global__ void __launch_bounds__(128) adjoint_persistent_kernel(const AdjointArgs a,
                                                                  unsigned long long* counter) {
   constexpr int D = F::D, P = F::P;
   Fetch fetch(counter);
   const int K = a.ck_every;
-  SegBuf<D> seg;
+  AdjBuf<D> buf(K);
   double p[P], lam[D], gp[P];
   float pf[P];
-  int na = 0, sg = -1;
+  int na = 0, sg = -1, b = 0;
   long long j;
-  // take trajectories until one has work (n_acc = 0 ones finish at once: gy0 = ybar)
+  // take trajectories until one has work (n_acc = 0 ones finish at once: gy0 = ybar), and
+  // start the copies of its last segment into buffer b
   auto take = [&]() {
     for (;;) {
       j = fetch.get();
@@ -277,7 +282,10 @@ __global__ void __launch_bounds__(128) adjoint_persistent_kernel(const AdjointAr
       for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
       na = steps_in_record(a.n_acc, j, a.cap);
       sg = (na + K - 1) / K - 1;
-      if (sg >= 0) return;
+      if (sg >= 0) {
+        prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, sg, K, na);
+        return;
+      }
       if (a.gy0) {
 #pragma unroll
         for (int i = 0; i < D; ++i) a.gy0[j * D + i] = lam[i];
@@ -290,28 +298,29 @@ __global__ void __launch_bounds__(128) adjoint_persistent_kernel(const AdjointAr
   };
   take();
   while (j < a.n) {
-    const int start = sg * K;
+    cp_async_wait_all();  // this segment's checkpoint and dts have landed
     double y[D], c[D];
-    load_ckpt<D>(a.ckpt, a.n, j, sg, y);
 #pragma unroll
-    for (int i = 0; i < D; ++i) { seg.at(0, i) = y[i]; c[i] = 0.0; }
+    for (int i = 0; i < D; ++i) { y[i] = buf.ck(b, i); c[i] = 0.0; }
+    if (sg > 0) prefetch_segment<D>(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
+#pragma unroll
+    for (int i = 0; i < D; ++i) buf.st(0, i) = y[i];
     for (int q = 1; q < K; ++q) {
-      const int s = start + q - 1;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      const double dt = buf.dt(b, q - 1);
       if (dt != 0.0) M::template step<F>(y, c, p, pf, dt);
 #pragma unroll
-      for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
+      for (int i = 0; i < D; ++i) buf.st(q, i) = y[i];
     }
     for (int q = K - 1; q >= 0; --q) {
-      const int s = start + q;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      const double dt = buf.dt(b, q);
       if (dt != 0.0) {
         double ys[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) ys[i] = seg.at(q, i);
+        for (int i = 0; i < D; ++i) ys[i] = buf.st(q, i);
         M::template vjp<F>(ys, p, pf, dt, lam, gp);
       }
     }
+    b ^= 1;
     if (--sg < 0) {
       if (a.gy0) {
 #pragma unroll
@@ -329,21 +338,28 @@ __global__ void __launch_bounds__(128) adjoint_persistent_kernel(const AdjointAr
 // ---- persistent saveat reverse pass (one segment per iteration) -------------------------------
 // Per trajectory the arithmetic of adjoint_saveat_kernel (gs_saveat.cuh); the lane carries the
 // trajectory's cursor (segment, saveat times not yet assigned, whether the final cotangents
-// have joined) between iterations and refills itself when the trajectory is done.
+// have joined) between iterations and refills itself when the trajectory is done.  Segments
+// are prefetched as in adjoint_persistent_kernel (the buffer's states carry their step start
+// time at index D), and the latest time not yet assigned is held in a register.
 template <class F, class M>
 __global__ void __launch_bounds__(128) adjoint_saveat_persistent_kernel(
     const SaveatArgs a, unsigned long long* counter) {
   constexpr int D = F::D, P = F::P;
   Fetch fetch(counter);
   const int K = a.ck_every;
-  SegBuf<D + 1> seg;  // states and step start times (index D)
+  AdjBuf<D, D + 1> buf(K);
   double p[P], lam[D], gp[P];
   float pf[P];
   const double* ts = nullptr;
   const double* ysb = nullptr;
-  int na = 0, sg = -1, kk = 0;
+  int na = 0, sg = -1, kk = 0, b = 0;
+  double tlast = -CUDART_INF;  // ts[kk - 1], or -inf once every time is assigned
   bool fin_done = false;
   long long j;
+  auto pop = [&]() {  // time kk - 1 is assigned (the caller has taken its cotangent)
+    --kk;
+    tlast = kk > 0 ? ts[kk - 1] : -CUDART_INF;
+  };
   auto finish = [&]() {  // times never bracketed (ts <= t0) take y0: their cotangent joins lam
     for (int k = 0; k < kk; ++k) {
 #pragma unroll
@@ -371,60 +387,66 @@ __global__ void __launch_bounds__(128) adjoint_saveat_persistent_kernel(
       na = steps_in_record(a.n_acc, j, a.cap);
       sg = (na + K - 1) / K - 1;
       kk = a.K;
+      tlast = kk > 0 ? ts[kk - 1] : -CUDART_INF;
       fin_done = false;
-      if (sg >= 0) return;
+      if (sg >= 0) {
+        prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, sg, K, na);
+        return;
+      }
       const double tfin = a.t0;  // no steps: every time >= t0 is y_final = y0
-      while (kk > 0 && ts[kk - 1] >= tfin) {
-        --kk;
+      while (tlast >= tfin) {
 #pragma unroll
-        for (int i = 0; i < D; ++i) lam[i] += ysb[(long long)kk * D + i];
+        for (int i = 0; i < D; ++i) lam[i] += ysb[(long long)(kk - 1) * D + i];
+        pop();
       }
       finish();
     }
   };
   take();
   while (j < a.n) {
-    const int start = sg * K;
+    cp_async_wait_all();  // this segment's checkpoint (state and time) and dts have landed
     double y[D], c[D];
-    double t = load_ckpt<D>(a.ckpt, a.n, j, sg, y);
 #pragma unroll
-    for (int i = 0; i < D; ++i) { seg.at(0, i) = y[i]; c[i] = 0.0; }
-    seg.at(0, D) = t;
+    for (int i = 0; i < D; ++i) { y[i] = buf.ck(b, i); c[i] = 0.0; }
+    double t = buf.ck(b, D);
+    if (sg > 0) prefetch_segment<D>(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
+#pragma unroll
+    for (int i = 0; i < D; ++i) buf.st(0, i) = y[i];
+    buf.st(0, D) = t;
     for (int q = 1; q <= K; ++q) {  // states y_{start+q} and times (q = K: segment end)
-      const int s = start + q - 1;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      const double dt = buf.dt(b, q - 1);
       if (dt > 0.0) {
         if (q < K) M::template step<F>(y, c, p, pf, dt);
         t = t + dt;
       }
       if (q < K) {
 #pragma unroll
-        for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
-        seg.at(q, D) = t;
+        for (int i = 0; i < D; ++i) buf.st(q, i) = y[i];
+        buf.st(q, D) = t;
       }
     }
     if (!fin_done) {  // the trajectory's last segment comes first: t is t_fin
       fin_done = true;
-      while (kk > 0 && ts[kk - 1] >= t) {
-        --kk;
+      while (tlast >= t) {
 #pragma unroll
-        for (int i = 0; i < D; ++i) lam[i] += ysb[(long long)kk * D + i];
+        for (int i = 0; i < D; ++i) lam[i] += ysb[(long long)(kk - 1) * D + i];
+        pop();
       }
     }
     for (int q = K - 1; q >= 0; --q) {
-      const int s = start + q;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      const double dt = buf.dt(b, q);
       if (dt > 0.0) {
         double ys[D], add[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) { ys[i] = seg.at(q, i); add[i] = 0.0; }
-        const double ts0 = seg.at(q, D);
-        while (kk > 0 && ts[kk - 1] > ts0) {  // re-steps bracketed by this step
-          --kk;
+        for (int i = 0; i < D; ++i) { ys[i] = buf.st(q, i); add[i] = 0.0; }
+        const double ts0 = buf.st(q, D);
+        while (tlast > ts0) {  // re-steps bracketed by this step
+          const double tk = tlast;
           double w[D];
 #pragma unroll
-          for (int i = 0; i < D; ++i) w[i] = ysb[(long long)kk * D + i];
-          M::template vjp<F>(ys, p, pf, ts[kk] - ts0, w, gp);
+          for (int i = 0; i < D; ++i) w[i] = ysb[(long long)(kk - 1) * D + i];
+          pop();
+          M::template vjp<F>(ys, p, pf, tk - ts0, w, gp);
 #pragma unroll
           for (int i = 0; i < D; ++i) add[i] += w[i];
         }
@@ -433,6 +455,7 @@ __global__ void __launch_bounds__(128) adjoint_saveat_persistent_kernel(
         for (int i = 0; i < D; ++i) lam[i] += add[i];
       }
     }
+    b ^= 1;
     if (--sg < 0) {
       finish();
       take();

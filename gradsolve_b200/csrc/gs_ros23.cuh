@@ -53,11 +53,10 @@ __device__ __forceinline__ void lu_factor(LU<D>& f) {
         // select-based swap keeps the matrix in registers (no dynamic indexing)
 #pragma unroll
         for (int r = col + 1; r < D; ++r) {
-          if (r == pv) {
-            const double tmp = f.a[col * D + c];
-            f.a[col * D + c] = f.a[r * D + c];
-            f.a[r * D + c] = tmp;
-          }
+          const bool sw = r == pv;
+          const double u = f.a[col * D + c], v = f.a[r * D + c];
+          f.a[col * D + c] = sw ? v : u;
+          f.a[r * D + c] = sw ? u : v;
         }
       }
     }
@@ -82,11 +81,13 @@ __device__ __forceinline__ void lu_solve(const LU<D>& f, const double* b, double
   for (int k = 0; k < D; ++k) {
 #pragma unroll
     for (int r = k + 1; r < D; ++r) {
-      if (r == f.piv[k]) {
-        const double tmp = x[k];
-        x[k] = x[r];
-        x[r] = tmp;
-      }
+      // selects, not a branch: written as an if, the compiler turns the swap into an
+      // indexed access x[piv[k]] and moves x to local memory (a stack frame, L1/L2 traffic
+      // every solve); as selects x stays in registers
+      const bool sw = r == f.piv[k];
+      const double xk = x[k], xr = x[r];
+      x[k] = sw ? xr : xk;
+      x[r] = sw ? xk : xr;
     }
 #pragma unroll
     for (int r = k + 1; r < D; ++r) x[r] = x[r] - f.a[r * D + k] * x[k];
@@ -124,11 +125,13 @@ __device__ __forceinline__ void lu_solve_t(const LU<D>& f, const double* b, doub
     const int k = D - 1 - kk;
 #pragma unroll
     for (int r = k + 1; r < D; ++r) {
-      if (r == f.piv[k]) {
-        const double tmp = x[k];
-        x[k] = x[r];
-        x[r] = tmp;
-      }
+      // selects, not a branch: written as an if, the compiler turns the swap into an
+      // indexed access x[piv[k]] and moves x to local memory (a stack frame, L1/L2 traffic
+      // every solve); as selects x stays in registers
+      const bool sw = r == f.piv[k];
+      const double xk = x[k], xr = x[r];
+      x[k] = sw ? xr : xk;
+      x[r] = sw ? xk : xr;
     }
   }
 }
@@ -346,27 +349,23 @@ __global__ void __launch_bounds__(128) ros23_replay_kernel(const ReplayArgs a) {
 // recomputes them, and the buffer holds only the states, dts and checkpoints.
 template <int D, bool kKeep>
 GS_HD int ros23_adjoint_smem_doubles(int K) {
-  return K * D + (kKeep ? (K - 1) * (D * D + 5 * D) : 0) + 2 * K + 2 * ((D + 2) & ~1);
+  return K * D + (kKeep ? (K - 1) * (D * D + 5 * D) : 0) + seg_io_doubles<D>(K);
 }
 
 template <int D, bool kKeep>
 struct AdjRosBuf {
-  static constexpr int CW = (D + 2) & ~1;
   static constexpr int R = kKeep ? D * D + 5 * D : 0;  // kept values per step
   double* base;
   int stride, K;
+  SegIO<D> io;
   __device__ __forceinline__ AdjRosBuf(int k)
-      : base(gs_seg_smem + threadIdx.x), stride(blockDim.x), K(k) {}
+      : base(gs_seg_smem + threadIdx.x), stride(blockDim.x), K(k), io(k * D + (k - 1) * R, k) {}
   __device__ __forceinline__ double& st(int q, int i) { return base[(q * D + i) * stride]; }
   __device__ __forceinline__ double& kept(int q, int v) {
     return base[(K * D + q * R + v) * stride];
   }
-  __device__ __forceinline__ double& dt(int b, int q) {
-    return base[(K * D + (K - 1) * R + b * K + q) * stride];
-  }
-  __device__ __forceinline__ double& ck(int b, int i) {
-    return base[(K * D + (K - 1) * R + 2 * K + b * CW + i) * stride];
-  }
+  __device__ __forceinline__ double& dt(int b, int q) { return io.dt(b, q); }
+  __device__ __forceinline__ double& ck(int b, int i) { return io.ck(b, i); }
   // layout of a kept step: W.a, W.inv, W.piv (as doubles), k1, s1, k2' (kKeep only)
   __device__ __forceinline__ void keep(int q, const LU<D>& W, const double* k1, const double* s1,
                                        const double* k2p) {

@@ -17,6 +17,8 @@
 // rebuilt from the checkpoints (which store t) with the replay's own additions, so the bracket
 // decisions are bitwise those of the forward.
 #pragma once
+#include <math_constants.h>
+
 #include "gs_mixed.cuh"
 #include "gs_ros23.cuh"
 #include "gs_tsit5.cuh"
@@ -161,59 +163,72 @@ __global__ void __launch_bounds__(128) adjoint_saveat_kernel(const SaveatArgs a)
   const int na = steps_in_record(a.n_acc, j, a.cap);
   const int K = a.ck_every;
   const int nseg = (na + K - 1) / K;
-  SegBuf<D + 1> seg;  // states and step start times (index D)
-  int kk = a.K;           // times [0, kk) not yet assigned to a step
-  bool fin_done = false;  // cotangents of times >= t_fin joined lam
+  // segment buffer (states with their step start time at index D) and cp.async prefetch of
+  // the next segment's checkpoint and dts, as in tsit5_adjoint_kernel
+  AdjBuf<D, D + 1> buf(K);
+  int b = 0;
+  int kk = a.K;  // times [0, kk) not yet assigned to a step
+  // ts[kk - 1] held in a register (-inf once every time is assigned)
+  double tlast = kk > 0 ? ts[kk - 1] : -CUDART_INF;
+  auto pop = [&]() {
+    --kk;
+    tlast = kk > 0 ? ts[kk - 1] : -CUDART_INF;
+  };
   if (nseg == 0) {
     const double tfin = a.t0;
-    while (kk > 0 && ts[kk - 1] >= tfin) {
-      --kk;
+    while (tlast >= tfin) {
 #pragma unroll
-      for (int i = 0; i < D; ++i) lam[i] += ysb[(long long)kk * D + i];
+      for (int i = 0; i < D; ++i) lam[i] += ysb[(long long)(kk - 1) * D + i];
+      pop();
     }
+  } else {
+    prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
   }
+  bool fin_done = false;  // cotangents of times >= t_fin joined lam
   for (int sg = nseg - 1; sg >= 0; --sg) {
-    const int start = sg * K;
+    cp_async_wait_all();
     double y[D], c[D];
-    double t = load_ckpt<D>(a.ckpt, a.n, j, sg, y);
 #pragma unroll
-    for (int i = 0; i < D; ++i) { seg.at(0, i) = y[i]; c[i] = 0.0; }
-    seg.at(0, D) = t;
+    for (int i = 0; i < D; ++i) { y[i] = buf.ck(b, i); c[i] = 0.0; }
+    double t = buf.ck(b, D);
+    if (sg > 0) prefetch_segment<D>(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
+#pragma unroll
+    for (int i = 0; i < D; ++i) buf.st(0, i) = y[i];
+    buf.st(0, D) = t;
     for (int q = 1; q <= K; ++q) {  // states y_{start+q} and times (q = K: segment end)
-      const int s = start + q - 1;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      const double dt = buf.dt(b, q - 1);
       if (dt > 0.0) {
         if (q < K) M::template step<F>(y, c, p, pf, dt);
         t = t + dt;
       }
       if (q < K) {
 #pragma unroll
-        for (int i = 0; i < D; ++i) seg.at(q, i) = y[i];
-        seg.at(q, D) = t;
+        for (int i = 0; i < D; ++i) buf.st(q, i) = y[i];
+        buf.st(q, D) = t;
       }
     }
     if (!fin_done) {  // first processed segment: t is t_fin
       fin_done = true;
-      while (kk > 0 && ts[kk - 1] >= t) {
-        --kk;
+      while (tlast >= t) {
 #pragma unroll
-        for (int i = 0; i < D; ++i) lam[i] += ysb[(long long)kk * D + i];
+        for (int i = 0; i < D; ++i) lam[i] += ysb[(long long)(kk - 1) * D + i];
+        pop();
       }
     }
     for (int q = K - 1; q >= 0; --q) {
-      const int s = start + q;
-      const double dt = s < na ? load_rec(a.rec, a.n, j, s) : 0.0;
+      const double dt = buf.dt(b, q);
       if (dt > 0.0) {
         double ys[D], add[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) { ys[i] = seg.at(q, i); add[i] = 0.0; }
-        const double ts0 = seg.at(q, D);
-        while (kk > 0 && ts[kk - 1] > ts0) {  // re-steps bracketed by this step
-          --kk;
+        for (int i = 0; i < D; ++i) { ys[i] = buf.st(q, i); add[i] = 0.0; }
+        const double ts0 = buf.st(q, D);
+        while (tlast > ts0) {  // re-steps bracketed by this step
+          const double tk = tlast;
           double w[D];
 #pragma unroll
-          for (int i = 0; i < D; ++i) w[i] = ysb[(long long)kk * D + i];
-          M::template vjp<F>(ys, p, pf, ts[kk] - ts0, w, gp);
+          for (int i = 0; i < D; ++i) w[i] = ysb[(long long)(kk - 1) * D + i];
+          pop();
+          M::template vjp<F>(ys, p, pf, tk - ts0, w, gp);
 #pragma unroll
           for (int i = 0; i < D; ++i) add[i] += w[i];
         }
@@ -222,6 +237,7 @@ __global__ void __launch_bounds__(128) adjoint_saveat_kernel(const SaveatArgs a)
         for (int i = 0; i < D; ++i) lam[i] += add[i];
       }
     }
+    b ^= 1;
   }
   // remaining times were never bracketed (ts <= t0): their value is y0
   for (int k = 0; k < kk; ++k) {

@@ -41,19 +41,11 @@ namespace gs {
 
 constexpr int KMAX = 64;  // largest checkpoint interval the adjoint supports
 
-// Per-thread segment buffer of the adjoint kernels, in dynamic shared memory (launched with
-// K * W * 8 * blockDim bytes): element (q, i) of thread t lives at
-// smem[(q * W + i) * blockDim + t], so a warp's accesses to one element are consecutive
-// 8-byte words (no bank conflicts).  W = D (states) or D + 1 (states and step start time).
+// Per-thread segment buffers of the adjoint kernels live in dynamic shared memory: element e
+// of thread t sits at smem[e * blockDim + t], so a warp's accesses to one element are
+// consecutive 8-byte words (no bank conflicts).  The layouts (AdjBuf, AdjStageBuf, AdjRosBuf)
+// are defined with the kernels that use them.
 extern __shared__ double gs_seg_smem[];
-
-template <int W>
-struct SegBuf {
-  double* base;
-  int stride;
-  __device__ __forceinline__ SegBuf() : base(gs_seg_smem + threadIdx.x), stride(blockDim.x) {}
-  __device__ __forceinline__ double& at(int q, int i) { return base[(q * W + i) * stride]; }
-};
 
 GS_HD int ckpt_width(int D) { return (D + 2) & ~1; }
 
@@ -517,11 +509,12 @@ __device__ __forceinline__ double load_rec(const double* rec, long long n, long 
 }
 
 // --- forward adaptive solve with record --------------------------------------------------
-// Bounded to 6 resident blocks of 128 per SM (80 registers): with the shared-reciprocal error
-// norm the unbounded kernel takes 84 and drops to 5 blocks; the few bytes it spills at 80 cost
-// less than the lost warps (11.63 vs 11.73 ms on the Lorenz 2^20 bench forward).
+// Bounded to 6 resident blocks of 128 per SM (80 registers) for D <= 4: with the
+// shared-reciprocal error norm the unbounded kernel takes 84 and drops to 5 blocks; the few
+// bytes it spills at 80 cost less than the lost warps (11.63 vs 11.73 ms on the Lorenz 2^20
+// bench forward; 7 blocks at 72 registers: 11.35 ms).  Larger states keep their registers.
 template <class F>
-__global__ void __launch_bounds__(128, 6) tsit5_record_kernel(const RecordArgs a) {
+__global__ void __launch_bounds__(128, (F::D <= 4 ? 6 : 1)) tsit5_record_kernel(const RecordArgs a) {
   constexpr int D = F::D, P = F::P;
   using T = Tsit5;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -623,26 +616,22 @@ __global__ void __launch_bounds__(128) tsit5_replay_kernel(const ReplayArgs a) {
 // next one's checkpoint and dts are already on their way (cp.async, global -> shared, no
 // register staging), so segment starts do not wait on DRAM, and each dt is read from DRAM
 // once instead of once per sweep.
-// W doubles of segment state per step (D: the states; 6 D: states and stage inputs).
-template <int D, int W = D>
-GS_HD int adjoint_smem_doubles(int K) { return K * W + 2 * K + 2 * ((D + 2) & ~1); }
-
-template <int D, int W = D>
-struct AdjBuf {
-  static constexpr int CW = (D + 2) & ~1;
-  double* base;
-  int stride, K;
-  __device__ __forceinline__ AdjBuf(int k) : base(gs_seg_smem + threadIdx.x), stride(blockDim.x), K(k) {}
-  __device__ __forceinline__ double& st(int q, int i) { return base[(q * W + i) * stride]; }
-  __device__ __forceinline__ double& dt(int b, int q) { return base[(K * W + b * K + q) * stride]; }
-  __device__ __forceinline__ double& ck(int b, int i) {
-    return base[(K * W + 2 * K + b * CW + i) * stride];
-  }
-};
-
+//
+// The dts and the checkpoint sit in 16-byte units (unit u of thread t at unit u * blockDim +
+// t), so that each is fetched with 16-byte copies: a checkpoint is CW / 2 copies and, for an
+// even segment start and length, a pair of dts (two 8-byte slots of one 32-byte record
+// sector) is one.  One copy per 16 bytes matters when a warp's lanes are at different
+// segments (ragged step counts, refilled lanes): their requests cannot coalesce, and 8-byte
+// copies sent a sector to L2 once per 8 bytes (Robertson reverse pass: 3.8 GB of L2 requests
+// for 0.93 GB of record and checkpoints).
 __device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_src) {
   const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+// both addresses 16-byte aligned
+__device__ __forceinline__ void cp_async16(double2* smem_dst, const double* gmem_src) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem_src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -651,22 +640,83 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Start the copies of segment sg's checkpoint and dts (steps at or past na read as 0).
+// Doubles per thread of the double-buffered dts + checkpoint area.
+template <int D>
+GS_HD int seg_io_doubles(int K) { return 2 * 2 * (((K + 1) >> 1) + ((D + 2) & ~1) / 2); }
+
+template <int D>
+struct SegIO {
+  static constexpr int CW = (D + 2) & ~1, CU = CW / 2;  // checkpoint doubles, units
+  double2* base;
+  int stride, KU;  // KU: 16-byte units of dts per buffer
+  // `off`: doubles per thread before the area (the block's shared memory is thread-strided
+  // in 8-byte elements up to it; blockDim is a multiple of 32, so the area is 16-byte aligned)
+  __device__ __forceinline__ SegIO(int off, int K)
+      : base(reinterpret_cast<double2*>(gs_seg_smem + (size_t)off * blockDim.x) + threadIdx.x),
+        stride(blockDim.x), KU((K + 1) >> 1) {}
+  __device__ __forceinline__ double2* unit(int b, int u) { return base + (b * (KU + CU) + u) * stride; }
+  __device__ __forceinline__ double& dt(int b, int q) {
+    return reinterpret_cast<double*>(unit(b, q >> 1))[q & 1];
+  }
+  __device__ __forceinline__ double& ck(int b, int i) {
+    return reinterpret_cast<double*>(unit(b, KU + (i >> 1)))[i & 1];
+  }
+};
+
+// W doubles of segment state per step (D: the states; D + 1: states and step start time).
+template <int D, int W = D>
+GS_HD int adjoint_smem_doubles(int K) { return K * W + seg_io_doubles<D>(K); }
+
+template <int D, int W = D>
+struct AdjBuf {
+  double* base;
+  int stride;
+  SegIO<D> io;
+  __device__ __forceinline__ AdjBuf(int K)
+      : base(gs_seg_smem + threadIdx.x), stride(blockDim.x), io(K * W, K) {}
+  __device__ __forceinline__ double& st(int q, int i) { return base[(q * W + i) * stride]; }
+  __device__ __forceinline__ double& dt(int b, int q) { return io.dt(b, q); }
+  __device__ __forceinline__ double& ck(int b, int i) { return io.ck(b, i); }
+};
+
+// Start the copies of segment sg's checkpoint and dts into buffer b of buf.io (steps at or
+// past na read as 0).  Record addresses: step s of trajectory j at rec_index(j, s, n), so an
+// even s and s + 1 share a 16-byte aligned half sector.
 template <int D, class Buf>
 __device__ __forceinline__ void prefetch_segment(Buf& buf, int b, const double* ckpt,
                                                  const double* rec, long long n, long long j,
                                                  int sg, int K, int na) {
-  constexpr int CW = (D + 2) & ~1;
+  SegIO<D>& io = buf.io;
+  constexpr int CW = SegIO<D>::CW;
   const double* src = ckpt + ((size_t)sg * (size_t)n + (size_t)j) * CW;
 #pragma unroll
-  for (int i = 0; i < CW; ++i) cp_async8(&buf.ck(b, i), src + i);
+  for (int u = 0; u < CW / 2; ++u) cp_async16(io.unit(b, io.KU + u), src + 2 * u);
   const int start = sg * K;
-  for (int q = 0; q < K; ++q) {
-    const int s = start + q;
-    if (s < na)
-      cp_async8(&buf.dt(b, q), rec + rec_index(j, s, n));
-    else
-      buf.dt(b, q) = 0.0;
+  // (the loops stay rolled: unrolled, the copies of the pair loop raised the stage-keeping
+  // kernel from 90 to 118 registers)
+  if (((start | K) & 1) == 0) {  // even start and length: pairs of dts, 16 bytes each
+#pragma unroll 1
+    for (int q = 0; q < K; q += 2) {
+      const int s = start + q;
+      if (s + 1 < na) {
+        cp_async16(io.unit(b, q >> 1), rec + rec_index(j, s, n));
+      } else {
+        if (s < na)
+          cp_async8(&io.dt(b, q), rec + rec_index(j, s, n));
+        else
+          io.dt(b, q) = 0.0;
+        io.dt(b, q + 1) = 0.0;
+      }
+    }
+  } else {
+#pragma unroll 1
+    for (int q = 0; q < K; ++q) {
+      const int s = start + q;
+      if (s < na)
+        cp_async8(&io.dt(b, q), rec + rec_index(j, s, n));
+      else
+        io.dt(b, q) = 0.0;
+    }
   }
   cp_async_commit();
 }
@@ -735,27 +785,24 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a)
 // same checkpoint/dt prefetch as tsit5_adjoint_kernel.
 template <int D>
 GS_HD int adjoint_stages_smem_doubles(int K) {
-  return K * D + (K - 1) * 5 * D + 2 * K + 2 * ((D + 2) & ~1);
+  return K * D + (K - 1) * 5 * D + seg_io_doubles<D>(K);
 }
 
 template <int D>
 struct AdjStageBuf {
-  static constexpr int CW = (D + 2) & ~1;
   double* base;
   int stride, K;
+  SegIO<D> io;
   __device__ __forceinline__ AdjStageBuf(int k)
-      : base(gs_seg_smem + threadIdx.x), stride(blockDim.x), K(k) {}
+      : base(gs_seg_smem + threadIdx.x), stride(blockDim.x), K(k),
+        io(k * D + (k - 1) * 5 * D, k) {}
   __device__ __forceinline__ double& st(int q, int i) { return base[(q * D + i) * stride]; }
   // stage input s_M (M = 2..6) of step q < K-1
   __device__ __forceinline__ double& stg(int q, int m, int i) {
     return base[(K * D + (q * 5 + (m - 2)) * D + i) * stride];
   }
-  __device__ __forceinline__ double& dt(int b, int q) {
-    return base[(K * D + (K - 1) * 5 * D + b * K + q) * stride];
-  }
-  __device__ __forceinline__ double& ck(int b, int i) {
-    return base[(K * D + (K - 1) * 5 * D + 2 * K + b * CW + i) * stride];
-  }
+  __device__ __forceinline__ double& dt(int b, int q) { return io.dt(b, q); }
+  __device__ __forceinline__ double& ck(int b, int i) { return io.ck(b, i); }
 };
 
 template <class F>

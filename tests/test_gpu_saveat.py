@@ -96,6 +96,50 @@ def test_per_trajectory_end_times_and_rows(gslib, oracle, cuda):
     assert rowrel(gp.cpu().numpy(), op) <= 1e-9
 
 
+@pytest.mark.parametrize("method", ["tsit5", "rosenbrock23"])
+def test_saveat_schedules_with_empty_trajectories(gslib, oracle, cuda, method):
+    """Persistent saveat reverse passes (lanes refilled from a counter, strided lanes) against
+    one thread per trajectory and the oracle, on a batch where every fifth trajectory has no
+    steps (t1 = t0) and the others end at their own times, with a segment length that leaves
+    partial last segments."""
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    rng = np.random.default_rng(11)
+    n = 160
+    mu = 10 ** rng.uniform(-1, 0.9, (n, 1)) if method == "tsit5" else \
+        10 ** rng.uniform(1.0, 1.5, (n, 1))
+    t1v = 10 ** rng.uniform(-1, np.log10(3.0), n)
+    t1v[::5] = 0.0
+    y0 = rng.uniform(-2, 2, (n, 2))
+    ts = np.stack([np.linspace(0.0, t, 16) for t in t1v])
+    spec = field_spec("vdp")
+    r = engine.forward_record(method, spec, torch.tensor(y0, device=cuda),
+                              torch.tensor(mu, device=cuda), t0=0.0, t1=float(t1v.max()),
+                              t1v=torch.tensor(t1v, device=cuda), rtol=1e-6, atol=1e-9,
+                              max_steps=50000, checkpoint=5)
+    assert (r.status.cpu().numpy() == 0).all()
+    assert (r.n_acc.cpu().numpy()[::5] == 0).all()
+    dts = r.padded_dts().cpu().numpy()
+    mu_t, ts_t = torch.tensor(mu, device=cuda), torch.tensor(ts, device=cuda)
+    ysbar = rng.normal(size=(n, 16, 2))
+    ybar = rng.normal(size=(n, 2))
+    oy, op = oracle.replay_saveat_vjp(method, "vdp", y0, mu, dts, ts, ysbar, ybar)
+    outs = {}
+    for sched in ("static", "refill", "strided"):
+        gy0, gp = engine.adjoint_saveat(r, mu_t, ts_t, torch.tensor(ysbar, device=cuda),
+                                        torch.tensor(ybar, device=cuda), schedule=sched)
+        assert rowrel(gy0.cpu().numpy(), oy) <= 1e-9, sched
+        assert rowrel(gp.cpu().numpy(), op) <= 1e-9, sched
+        outs[sched] = (gy0.cpu(), gp.cpu())
+    # no steps: the gradient is the cotangent of y_final plus those of every saved time (= y0)
+    e = outs["refill"][0].numpy()[::5]
+    np.testing.assert_allclose(e, ybar[::5] + ysbar[::5].sum(axis=1), rtol=0, atol=1e-12)
+    if method == "tsit5":  # same expressions, same lane code: bitwise
+        for sched in ("refill", "strided"):
+            assert torch.equal(outs[sched][0], outs["static"][0])
+            assert torch.equal(outs[sched][1], outs["static"][1])
+
+
 def test_stiff_vdp_saveat(gslib, oracle, cuda):
     """VdP at mu >= 10 through Rosenbrock23 (the stiff half of the uneven workload)."""
     from gradsolve_b200 import engine

@@ -267,7 +267,9 @@ def test_schedules_give_identical_results(gslib, cuda, precision):
     n = 3000  # more trajectories than one wave of a small grid, uneven horizons
     y0 = torch.tensor(np.array([1.0, 0.0, 0.0]) + rng.normal(0, 0.1, (n, 3)), device=cuda)
     p = torch.tensor(rng.uniform(20, 30, (n, 1)), device=cuda)
-    t1v = torch.tensor(rng.uniform(0.5, 3.0, n), device=cuda)
+    t1v_np = rng.uniform(0.5, 3.0, n)
+    t1v_np[::7] = 0.0  # trajectories with no steps, interleaved with the others
+    t1v = torch.tensor(t1v_np, device=cuda)
     outs = {}
     for sched in ("static", "refill", "strided"):
         r = engine.forward_record("tsit5", spec, y0, p, t0=0.0, t1=3.0, t1v=t1v, rtol=1e-8,

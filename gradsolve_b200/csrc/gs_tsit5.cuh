@@ -620,10 +620,8 @@ __global__ void __launch_bounds__(128) tsit5_replay_kernel(const ReplayArgs a) {
 // The dts and the checkpoint sit in 16-byte units (unit u of thread t at unit u * blockDim +
 // t), so that each is fetched with 16-byte copies: a checkpoint is CW / 2 copies and, for an
 // even segment start and length, a pair of dts (two 8-byte slots of one 32-byte record
-// sector) is one.  One copy per 16 bytes matters when a warp's lanes are at different
-// segments (ragged step counts, refilled lanes): their requests cannot coalesce, and 8-byte
-// copies sent a sector to L2 once per 8 bytes (Robertson reverse pass: 3.8 GB of L2 requests
-// for 0.93 GB of record and checkpoints).
+// sector) is one -- half the copy instructions of 8-byte copies (Lorenz reverse pass at
+// K = 2: 3.89 -> 3.78 ms per 2^18 launch).
 __device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_src) {
   const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(gmem_src) : "memory");

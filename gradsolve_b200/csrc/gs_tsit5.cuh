@@ -105,9 +105,23 @@ __device__ __forceinline__ double pow_k(double y) {
   }
 }
 
+// The first guess uses the hardware's approximate base-2 logarithm and exponential (PTX
+// lg2.approx / ex2.approx, ~2^-22 relative): m lies in the controller's unclipped range
+// (about 1e-8 .. 1e8 times D), where neither leaves the normal float range.
+__device__ __forceinline__ float lg2_approx(float x) {
+  float r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 template <int K>
 __device__ __forceinline__ double inv_root(double m) {
-  double y = (double)exp2f(__log2f((float)m) * (-1.0f / (float)K));
+  double y = (double)ex2_approx(lg2_approx((float)m) * (-1.0f / (float)K));
   constexpr double kp1 = K + 1.0, rk = 1.0 / K;
 #pragma unroll
   for (int it = 0; it < 2; ++it) y = (y * fma(-m, pow_k<K>(y), kp1)) * rk;
@@ -529,6 +543,9 @@ __global__ void __launch_bounds__(128, (F::D <= 4 ? 6 : 1)) tsit5_record_kernel(
   double dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
   const bool rec_on = a.rec != nullptr;
   const bool ck_on = a.ckpt != nullptr;
+  // this trajectory's slots of the current record sector (rec_index, advanced per sector)
+  double* rp = rec_on ? a.rec + j * 4 : nullptr;
+  const long long rstride = 4 * a.n;
   if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
   F::rhs(y, p, k1);
   int acc = 0, rej = 0, st = 0, ck_cnt = 0, ck_slot = 0;
@@ -559,7 +576,10 @@ __global__ void __launch_bounds__(128, (F::D <= 4 ? 6 : 1)) tsit5_record_kernel(
         y[i] = y5[i];
         k1[i] = k7[i];
       }
-      if (rec_on) a.rec[rec_index(j, acc, a.n)] = h;
+      if (rec_on) {
+        rp[acc & 3] = h;
+        if ((acc & 3) == 3) rp += rstride;
+      }
       ++acc;
       if (ck_on && ++ck_cnt == a.ck_every) {
         ck_cnt = 0;
@@ -572,7 +592,7 @@ __global__ void __launch_bounds__(128, (F::D <= 4 ? 6 : 1)) tsit5_record_kernel(
   }
   if (st == 0 && !(t >= t1)) st = 1;
   if (rec_on) {  // zero-pad the last sector (identity steps)
-    for (int s = acc; (s & 3) != 0; ++s) a.rec[rec_index(j, s, a.n)] = 0.0;
+    for (int s = acc; (s & 3) != 0; ++s) rp[s & 3] = 0.0;
   }
 #pragma unroll
   for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];

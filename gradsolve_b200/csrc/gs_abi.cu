@@ -133,6 +133,7 @@ int field_dims(int field, int* D, int* P) {
 struct SegCfg {
   unsigned block;
   size_t smem;
+  long long resident;  // threads per SM at this shape (occupancy_cfg)
 };
 
 constexpr size_t kSegBudget = 200u * 1024u;
@@ -142,7 +143,7 @@ SegCfg seg_cfg(int K, int W) {
   const size_t budget = kSegBudget;
   unsigned block = kBlock;
   while (block > 32 && per_thread * block > budget) block /= 2;
-  return {block, per_thread * block};
+  return {block, per_thread * block, 0};
 }
 
 // The same shrinking rule for a per-thread size given in doubles.
@@ -164,10 +165,10 @@ unsigned grid_for_block(long long n, unsigned block) { return (unsigned)((n + bl
 // threads each use doubles_per_thread of dynamic shared memory (registers and shared memory
 // both limit residency; smaller blocks pack the shared memory more finely).  Ties keep the
 // larger block.  Sets the kernel's dynamic shared memory limit for the chosen size.
+// occupancy_probe leaves out->resident = 0 (and reports no error) when no block size fits.
 template <class Kern>
-int occupancy_cfg(Kern kernel, int doubles_per_thread, SegCfg* out) {
-  SegCfg best{0, 0};
-  long long best_res = -1;
+int occupancy_probe(Kern kernel, int doubles_per_thread, SegCfg* out) {
+  SegCfg best{0, 0, 0};
   for (unsigned block : {128u, 64u, 32u}) {
     const size_t smem = (size_t)doubles_per_thread * sizeof(double) * block;
     if (smem > kSegBudget) continue;
@@ -178,16 +179,30 @@ int occupancy_cfg(Kern kernel, int doubles_per_thread, SegCfg* out) {
     if (e != cudaSuccess)
       return fail(GS_ERR_CUDA, std::string("CUDA: occupancy query: ") + cudaGetErrorString(e));
     const long long res = (long long)per_sm * block;
-    if (res > best_res) {
-      best_res = res;
-      best = {block, smem};
-    }
+    if (res > best.resident) best = {block, smem, res};
   }
-  if (best_res <= 0)
+  *out = best;
+  return best.resident > 0 ? allow_smem(kernel, best.smem) : GS_OK;
+}
+
+template <class Kern>
+int occupancy_cfg(Kern kernel, int doubles_per_thread, SegCfg* out) {
+  int rc = occupancy_probe(kernel, doubles_per_thread, out);
+  if (rc) return rc;
+  if (out->resident <= 0)
     return fail(GS_ERR_ARG, "segment buffer does not fit shared memory (checkpoint interval "
                             "too large for this state dimension)");
-  *out = best;
-  return allow_smem(kernel, best.smem);
+  return GS_OK;
+}
+
+// The reverse passes that keep a segment's forward quantities (Tsit5 stage inputs,
+// Rosenbrock23 factors) save the recomputation of K-1 of every K step forwards, but their
+// buffer grows with K and costs resident threads.  They are taken while they keep at least
+// 3/5 of the recomputing kernel's residency: measured on Lorenz (Tsit5) the keeping kernel
+// still wins at K = 4 (residency 384 vs 640 threads/SM: 15.9 vs 16.9 ms), and on VdP
+// (Rosenbrock23, K = 8: 192 vs 640) it lost by 1.6x.
+bool keeping_pays(const SegCfg& keep, const SegCfg& recompute) {
+  return keep.resident > 0 && keep.resident * 5 >= recompute.resident * 3;
 }
 
 // ---- scheduling ------------------------------------------------------------------------------
@@ -301,23 +316,28 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
                          int sched, int variant) {
   if (sched == GS_SCHED_STATIC) {
     int rc;
-    // the stage-keeping variant needs 5*D more doubles per replayed step of the segment; where
-    // that does not fit one warp's worth of shared memory (large K and D) the stages are
-    // recomputed instead
-    const int stage_doubles = gs::adjoint_stages_smem_doubles<F::D>(a.ck_every);
-    if (!mixed && variant != GS_ADJ_RECOMPUTE &&
-        (size_t)stage_doubles * sizeof(double) * 32u <= kSegBudget) {
-      SegCfg c;
-      if ((rc = occupancy_cfg(gs::tsit5_adjoint_stages_kernel<F>, stage_doubles, &c))) return rc;
-      gs::tsit5_adjoint_stages_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
-      return cuda_check("tsit5_adjoint_stages_kernel");
-    }
     if (!mixed) {
-      SegCfg c;
-      if ((rc = occupancy_cfg(gs::tsit5_adjoint_kernel<F>,
-                              gs::adjoint_smem_doubles<F::D>(a.ck_every), &c)))
+      // the stage-keeping variant needs 5*D more doubles per replayed step of the segment:
+      // taken when asked for (while it fits) or, by default, while it keeps enough residency
+      SegCfg ck{0, 0, 0}, cr{0, 0, 0};
+      if (variant != GS_ADJ_RECOMPUTE &&
+          (rc = occupancy_probe(gs::tsit5_adjoint_stages_kernel<F>,
+                                gs::adjoint_stages_smem_doubles<F::D>(a.ck_every), &ck)))
         return rc;
-      gs::tsit5_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+      if ((rc = occupancy_probe(gs::tsit5_adjoint_kernel<F>,
+                                gs::adjoint_smem_doubles<F::D>(a.ck_every), &cr)))
+        return rc;
+      if (ck.resident > 0 && (variant == GS_ADJ_STAGES || keeping_pays(ck, cr))) {
+        if ((rc = allow_smem(gs::tsit5_adjoint_stages_kernel<F>, ck.smem))) return rc;
+        gs::tsit5_adjoint_stages_kernel<F>
+            <<<grid_for_block(a.n, ck.block), ck.block, ck.smem, s>>>(a);
+        return cuda_check("tsit5_adjoint_stages_kernel");
+      }
+      if (cr.resident <= 0)
+        return fail(GS_ERR_ARG, "segment buffer does not fit shared memory (checkpoint "
+                                "interval too large for this state dimension)");
+      if ((rc = allow_smem(gs::tsit5_adjoint_kernel<F>, cr.smem))) return rc;
+      gs::tsit5_adjoint_kernel<F><<<grid_for_block(a.n, cr.block), cr.block, cr.smem, s>>>(a);
       return cuda_check("tsit5_adjoint_kernel");
     }
     SegCfg c;
@@ -349,19 +369,25 @@ int launch_ros23_replay(const gs::ReplayArgs& a, cudaStream_t s) {
 template <class F>
 int launch_ros23_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, int sched) {
   if (sched == GS_SCHED_STATIC) {
-    SegCfg c;
+    SegCfg ck{0, 0, 0}, cr{0, 0, 0};
     int rc;
-    const int keep = gs::ros23_adjoint_smem_doubles<F::D, true>(a.ck_every);
-    if ((size_t)keep * sizeof(double) * 32u <= kSegBudget) {
-      if ((rc = occupancy_cfg(gs::ros23_adjoint_kernel<F, true>, keep, &c))) return rc;
-      gs::ros23_adjoint_kernel<F, true><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+    if ((rc = occupancy_probe(gs::ros23_adjoint_kernel<F, true>,
+                              gs::ros23_adjoint_smem_doubles<F::D, true>(a.ck_every), &ck)))
+      return rc;
+    if ((rc = occupancy_probe(gs::ros23_adjoint_kernel<F, false>,
+                              gs::ros23_adjoint_smem_doubles<F::D, false>(a.ck_every), &cr)))
+      return rc;
+    if (keeping_pays(ck, cr)) {
+      if ((rc = allow_smem(gs::ros23_adjoint_kernel<F, true>, ck.smem))) return rc;
+      gs::ros23_adjoint_kernel<F, true><<<grid_for_block(a.n, ck.block), ck.block, ck.smem, s>>>(a);
       return cuda_check("ros23_adjoint_kernel");
     }
-    // large K and D: the kept quantities would not fit shared memory; recompute them
-    if ((rc = occupancy_cfg(gs::ros23_adjoint_kernel<F, false>,
-                            gs::ros23_adjoint_smem_doubles<F::D, false>(a.ck_every), &c)))
-      return rc;
-    gs::ros23_adjoint_kernel<F, false><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+    // large K: the kept factors would cost too many resident threads (or not fit); recompute
+    if (cr.resident <= 0)
+      return fail(GS_ERR_ARG, "segment buffer does not fit shared memory (checkpoint interval "
+                              "too large for this state dimension)");
+    if ((rc = allow_smem(gs::ros23_adjoint_kernel<F, false>, cr.smem))) return rc;
+    gs::ros23_adjoint_kernel<F, false><<<grid_for_block(a.n, cr.block), cr.block, cr.smem, s>>>(a);
     return cuda_check("ros23_adjoint_kernel");
   }
   return launch_adjoint_persistent<F, gs::Ros23Step>(a, cap, s, sched == GS_SCHED_REFILL);
@@ -823,17 +849,28 @@ int saveat_dispatch(int method, int field, int precision, const gs::SaveatArgs& 
   return fail(GS_ERR_ARG, "saveat: unknown method " + std::to_string(method));
 }
 
-// Forward with record and dense output: the persistent kernel (lanes refilled from the work
-// counter for uneven batches, strided otherwise).
-template <class F>
-int launch_fwd_saveat_tsit5(const gs::RecordArgs& a, cudaStream_t s, bool mixed, bool refill) {
-  return mixed ? launch_record_persistent<F, gs::LaneTsit5Mixed<F>>(a, s, refill)
-               : launch_record_persistent<F, gs::LaneTsit5F64<F>>(a, s, refill);
+// Forward with record and dense output: one thread per trajectory (kStatic), or persistent
+// lanes refilled from the work counter (kRefill) or strided (kStrided).
+enum FwdLanes { kStatic, kRefill, kStrided };
+
+template <class F, class L>
+int launch_fwd_lanes(const gs::RecordArgs& a_in, cudaStream_t s, FwdLanes lanes) {
+  if (lanes != kStatic) return launch_record_persistent<F, L>(a_in, s, lanes == kRefill);
+  gs::RecordArgs a = a_in;
+  a.ctrl = gs::make_ctrl_consts(F::D, L::QK);
+  gs::record_static_kernel<F, L><<<grid_for(a.n), kBlock, 0, s>>>(a);
+  return cuda_check("record_static_kernel");
 }
 
 template <class F>
-int launch_fwd_saveat_ros23(const gs::RecordArgs& a, cudaStream_t s, bool refill) {
-  return launch_record_persistent<F, gs::LaneRos23<F>>(a, s, refill);
+int launch_fwd_saveat_tsit5(const gs::RecordArgs& a, cudaStream_t s, bool mixed, FwdLanes lanes) {
+  return mixed ? launch_fwd_lanes<F, gs::LaneTsit5Mixed<F>>(a, s, lanes)
+               : launch_fwd_lanes<F, gs::LaneTsit5F64<F>>(a, s, lanes);
+}
+
+template <class F>
+int launch_fwd_saveat_ros23(const gs::RecordArgs& a, cudaStream_t s, FwdLanes lanes) {
+  return launch_fwd_lanes<F, gs::LaneRos23<F>>(a, s, lanes);
 }
 
 int check_saveat(const char* who, long long n, const double* p, const double* rec,
@@ -889,9 +926,13 @@ extern "C" int gs_fwd_record_saveat(int method, int field, int precision, long l
   if (K > 0 && (!ts || !ys)) return fail(GS_ERR_ARG, std::string(who) + ": ts and ys are required");
   const int prec = precision & GS_PREC_MASK;
   const int sched = precision & GS_SCHED_MASK;
-  // refill needs the work counter in the checkpoint buffer's control block
-  const bool refill = ckpt != nullptr &&
-                      (sched == GS_SCHED_REFILL || (sched == GS_SCHED_AUTO && t1v != nullptr));
+  // AUTO: lanes refilled from a work counter for per-trajectory end times, else one thread per
+  // trajectory; refill needs the counter in the checkpoint buffer's control block
+  const bool want_refill =
+      sched == GS_SCHED_REFILL || (sched == GS_SCHED_AUTO && t1v != nullptr);
+  const FwdLanes lanes = (want_refill && ckpt != nullptr) ? kRefill
+                         : (sched == GS_SCHED_STATIC || sched == GS_SCHED_AUTO) ? kStatic
+                                                                                 : kStrided;
   gs::RecordArgs a{n, y0, p, t0, t1, rtol, atol, dt0, t1v, max_steps, cap, ckpt_every,
                    gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status,
                    gs::CtrlConsts{}, ts, ts_ld, K, K > 0 ? ys : nullptr};
@@ -899,12 +940,12 @@ extern "C" int gs_fwd_record_saveat(int method, int field, int precision, long l
   if (method == GS_METHOD_TSIT5) {
     if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED)
       return fail(GS_ERR_PRECISION, std::string(who) + ": unknown precision mode " + std::to_string(prec));
-    GS_TSIT5_DISPATCH(field, launch_fwd_saveat_tsit5, a, s, prec == GS_PREC_MIXED, refill)
+    GS_TSIT5_DISPATCH(field, launch_fwd_saveat_tsit5, a, s, prec == GS_PREC_MIXED, lanes)
   }
   if (method == GS_METHOD_ROS23) {
     if (prec != GS_PREC_F64)
       return fail(GS_ERR_PRECISION, std::string(who) + ": Rosenbrock23 runs in float64 only");
-    GS_ROS23_DISPATCH(field, launch_fwd_saveat_ros23, a, s, refill)
+    GS_ROS23_DISPATCH(field, launch_fwd_saveat_ros23, a, s, lanes)
   }
   return fail(GS_ERR_ARG, std::string(who) + ": unknown method " + std::to_string(method));
 }

@@ -141,6 +141,135 @@ struct LaneRos23 {
   __device__ __forceinline__ bool degenerate(double t, double h) const { return t + h == t; }
 };
 
+// ---- one thread per trajectory: forward with record and saved states ------------------------
+// The per-attempt code of record_persistent_kernel (the same lane policies, accept logic and
+// saveat re-steps) without the refill machinery: every thread integrates one trajectory.  On
+// Rosenbrock23 the refill state costs registers (VdP: 82 vs 61) and with them resident warps,
+// which this latency-bound method needs -- at full occupancy the one-thread-per-trajectory
+// forward ran 30% faster.  Uneven batches balance here when their rows come sorted by length
+// (the planned tiers of a RecordSet do), since neighbouring threads then take similar numbers
+// of attempts.
+// A saveat re-step, out of line: re-steps are rare (a few per trajectory against thousands of
+// attempts), and inlined, the step's temporaries would raise the register count of the whole
+// attempt loop.  Arguments and result travel by value (no address of a register array).
+template <int N>
+struct DVec {
+  double v[N];
+};
+template <int N>
+struct FVec {
+  float v[N];
+};
+template <class F, class L>
+__device__ __noinline__ DVec<F::D> restep_out_of_line(DVec<F::D> y, DVec<F::P> p,
+                                                      FVec<F::P> pf, double dt) {
+  double c[F::D];
+#pragma unroll
+  for (int i = 0; i < F::D; ++i) c[i] = 0.0;
+  L::Step::template step<F>(y.v, c, p.v, pf.v, dt);
+  return y;
+}
+
+template <class F, class L>
+__global__ void __launch_bounds__(128) record_static_kernel(const RecordArgs a) {
+  constexpr int D = F::D, P = F::P;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  const bool rec_on = a.rec != nullptr;
+  const bool ck_on = a.ckpt != nullptr;
+  const bool sv_on = a.ys != nullptr;
+  double y[D], ynew[D], p[P];
+  float pf[P];
+#pragma unroll
+  for (int i = 0; i < D; ++i) y[i] = a.y0[j * D + i];
+#pragma unroll
+  for (int i = 0; i < P; ++i) { p[i] = a.p[j * P + i]; pf[i] = (float)p[i]; }
+  double t = a.t0;
+  const double t1 = a.t1v ? a.t1v[j] : a.t1;
+  double dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
+  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
+  L lane;
+  lane.start(y, p, pf);
+  const double* tsr = sv_on ? a.ts + j * a.ts_ld : nullptr;
+  double* ysr = sv_on ? a.ys + j * (long long)a.K * D : nullptr;
+  int kk = 0;
+  double tnext = CUDART_INF;  // the next requested time (infinity once all are assigned)
+  if (sv_on) {
+    while (kk < a.K && tsr[kk] <= t) {  // never bracketed: y0
+      store_row<D>(ysr + (long long)kk * D, y);
+      ++kk;
+    }
+    tnext = kk < a.K ? tsr[kk] : CUDART_INF;
+  }
+  double* rp = rec_on ? a.rec + j * 4 : nullptr;  // this trajectory's slots of the sector
+  const long long rstride = 4 * a.n;
+  int acc = 0, rej = 0, st = 0, ck_cnt = 0, ck_slot = 0;
+  for (int it = 0; it < a.max_steps; ++it) {
+    if (t >= t1) break;
+    const double h = (t1 - t < dt) ? (t1 - t) : dt;
+    if (lane.degenerate(t, h)) {
+      st = 2;
+      break;
+    }
+    const double m = lane.trial(y, p, pf, h, a.rtol, a.atol, ynew);
+    if (!(m == m)) {
+      st = 1;
+      break;
+    }
+    if (m <= a.ctrl.accept_sum) {
+      if ((rec_on || ck_on) && acc >= a.cap) {
+        st = 3;
+        break;
+      }
+      if (sv_on) {
+        const double tn = t + h;
+        while (tnext <= tn) {  // bracketed by this step: re-step to ts
+          DVec<D> yv;
+          DVec<P> pv;
+          FVec<P> pfv;
+#pragma unroll
+          for (int i = 0; i < D; ++i) yv.v[i] = y[i];
+#pragma unroll
+          for (int i = 0; i < P; ++i) { pv.v[i] = p[i]; pfv.v[i] = pf[i]; }
+          const DVec<D> yk = restep_out_of_line<F, L>(yv, pv, pfv, tnext - t);
+          store_row<D>(ysr + (long long)kk * D, yk.v);
+          ++kk;
+          tnext = kk < a.K ? tsr[kk] : CUDART_INF;
+        }
+      }
+      t = t + h;
+#pragma unroll
+      for (int i = 0; i < D; ++i) y[i] = ynew[i];
+      lane.commit();
+      if (rec_on) {
+        rp[acc & 3] = h;
+        if ((acc & 3) == 3) rp += rstride;
+      }
+      ++acc;
+      if (ck_on && ++ck_cnt == a.ck_every) {
+        ck_cnt = 0;
+        if (++ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, ck_slot, y, t);
+      }
+    } else {
+      ++rej;
+    }
+    dt = step_from_sum<L::QK>(m, h, a.ctrl);
+  }
+  if (st == 0 && !(t >= t1)) st = 1;
+  if (rec_on) {  // zero-pad the last sector (identity steps)
+    for (int s = acc; (s & 3) != 0; ++s) rp[s & 3] = 0.0;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
+  if (sv_on) {  // times at or past the final accumulated time take y_final itself
+    for (int k = a.K - 1; k >= 0 && tsr[k] >= t; --k) store_row<D>(ysr + (long long)k * D, y);
+    for (int k = kk; k < a.K; ++k) store_row<D>(ysr + (long long)k * D, y);
+  }
+  a.n_acc[j] = acc;
+  a.n_rej[j] = rej;
+  a.status[j] = st;
+}
+
 // ---- persistent forward with record ---------------------------------------------------------
 template <class F, class L>
 __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs a,
@@ -209,11 +338,15 @@ __global__ void __launch_bounds__(128) record_persistent_kernel(const RecordArgs
             if (sv_on) {
               const double tn = t + h;
               while (tnext <= tn) {  // bracketed by this step: re-step to ts
-                double yk[D], ck[D];
+                DVec<D> yv;
+                DVec<P> pv;
+                FVec<P> pfv;
 #pragma unroll
-                for (int i = 0; i < D; ++i) { yk[i] = y[i]; ck[i] = 0.0; }
-                L::Step::template step<F>(yk, ck, p, pf, tnext - t);
-                store_row<D>(ysr + (long long)kk * D, yk);
+                for (int i = 0; i < D; ++i) yv.v[i] = y[i];
+#pragma unroll
+                for (int i = 0; i < P; ++i) { pv.v[i] = p[i]; pfv.v[i] = pf[i]; }
+                const DVec<D> yk = restep_out_of_line<F, L>(yv, pv, pfv, tnext - t);
+                store_row<D>(ysr + (long long)kk * D, yk.v);
                 ++kk;
                 tnext = kk < a.K ? tsr[kk] : CUDART_INF;
               }

@@ -504,9 +504,17 @@ def _forward_planned(method, spec, y0, p, t1v, saveat_ts, ws: RecordSet, kw):
     streams = [None] + [old[i] if old[i] is not None else _side_stream(y0.device)
                         for i in range(1, len(keep))]
     plan = [(rows_by_part[k], ws.parts[k][1]) for k in keep]
+    # A planned tier's rows come sorted by their previous cost, so neighbouring threads take
+    # similar numbers of attempts and one thread per trajectory stays balanced.  Rosenbrock23
+    # then runs that way: it is latency-bound, and the one-thread kernel holds more warps
+    # than the refilled lanes (uneven VdP: its group 36.6 -> 34.2 ms); Tsit5 keeps the
+    # refilled lanes, which its many very short trajectories favour (11.5 vs 15.7 ms).
+    kwp = kw
+    if method == METHOD_ROS23 and kw["schedule"] == "auto":
+        kwp = dict(kw, schedule="static")
     launch = lambda rows, wsr: _forward_one(  # noqa: E731
         method, spec, _take(y0, rows), _take(p, rows), _take(t1v, rows),
-        _take_ts(saveat_ts, rows), wsr.cap, wsr, kw)
+        _take_ts(saveat_ts, rows), wsr.cap, wsr, kwp)
     out = [None] * len(plan)
     if all(st is None for st in streams):
         out = [(rows, launch(rows, wsr)) for rows, wsr in plan]
@@ -618,7 +626,8 @@ def adjoint(r, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
     uneven batch (per-trajectory end times), else runs one thread per trajectory.
     ``variant`` (Tsit5, float64, one thread per trajectory): "stages" keeps the stage inputs
     the segment's replay evaluates, "recompute" re-evaluates every step's stages in the
-    reverse sweep; "auto" is "stages" (recompute where its buffer would not fit)."""
+    reverse sweep; "auto" is "stages" while its buffer leaves it at least 3/5 of the
+    recomputing kernel's resident threads, else "recompute"."""
     if schedule == "auto" and r.uneven:
         schedule = "refill"
     res = _over_parts(r, lambda rr, rows: _adjoint_one(

@@ -69,7 +69,9 @@ extern "C" {
  * from the segment's states.  STAGES: the segment's replay keeps the stage inputs of the steps
  * it evaluates (5*D doubles per step of shared memory), so only each segment's last step
  * evaluates its stages twice; falls back to RECOMPUTE where that buffer would not fit.  AUTO
- * (0): STAGES (measured 4-6% faster on B200 for the built-in fields at K = 2..4). */
+ * (0): STAGES while its shared memory leaves it at least 3/5 of RECOMPUTE's resident threads
+ * per SM (the autotuned K = 2 of the built-in fields: equal residency, 4-6% faster), else
+ * RECOMPUTE.  gs_ros23_adjoint applies the same rule to keeping the factors of W. */
 #define GS_ADJ_AUTO 0x000
 #define GS_ADJ_RECOMPUTE 0x400
 #define GS_ADJ_STAGES 0x800
@@ -206,9 +208,10 @@ int gs_replay_saveat(int method, int field, int precision, long long n, const do
  * re-stepped from the start of the accepted step that brackets it, as the trajectory is
  * integrated, so the recording point needs no separate replay pass.  ys equals what
  * gs_replay_saveat gives on the recorded mesh to rounding (the same step function, compiled
- * into another kernel).  Runs the persistent
- * kernel: lanes refilled from a work counter when trajectories have their own end times (or
- * GS_SCHED_REFILL is set; needs ckpt), strided otherwise.  No counterpart in the reference,
+ * into another kernel).  Schedules: lanes refilled from a work counter (GS_SCHED_REFILL, or
+ * AUTO when trajectories have their own end times; needs ckpt), persistent strided lanes
+ * (GS_SCHED_STRIDED), one thread per trajectory otherwise (GS_SCHED_STATIC, or AUTO with a
+ * shared end time).  No counterpart in the reference,
  * whose saveat always replays the recorded mesh (gradsolve/warp/warp_replay.py:58-84).
  * method: GS_METHOD_TSIT5 (float64 or mixed) or GS_METHOD_ROS23 (float64).
  */

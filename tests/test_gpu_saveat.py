@@ -256,7 +256,9 @@ def test_forward_dense_output_equals_replay(gslib, cuda, method, field, prec):
         assert torch.equal(r.ys[:, -1], r.y_final)  # ts[-1] = t1: y_final itself
         assert torch.equal(r.ys[:, 0], y0)          # ts[0] = t0: y0 itself
     # the tiered record as the workspace of the next solve: planned tiers on their own
-    # streams, the same per-trajectory results, and the same gradient
+    # streams, the same per-trajectory results, and the same gradient (Rosenbrock23's planned
+    # tiers run one thread per trajectory instead of refilled lanes: the same expressions in
+    # another kernel, equal to rounding, with the same step counts)
     assert isinstance(r, engine.RecordSet) and len(r.parts) > 1
     ysbar = torch.tensor(rng.normal(size=tuple(r.ys.shape)), device=cuda)
     g1 = engine.adjoint_saveat(r, p, ts, ysbar, precision=prec)
@@ -265,6 +267,10 @@ def test_forward_dense_output_equals_replay(gslib, cuda, method, field, prec):
                                precision=prec, saveat_ts=ts, workspace=r)
     g2 = engine.adjoint_saveat(r2, p, ts, ysbar, precision=prec)
     torch.cuda.synchronize()
-    for a, b in ((r.ys, r2.ys), (r.y_final, r2.y_final), (r.n_acc, r2.n_acc),
-                 (g1[0], g2[0]), (g1[1], g2[1])):
-        assert torch.equal(a, b)
+    assert torch.equal(r.n_acc, r2.n_acc)
+    for a, b in ((r.ys, r2.ys), (r.y_final, r2.y_final), (g1[0], g2[0]), (g1[1], g2[1])):
+        if method == "tsit5":
+            assert torch.equal(a, b)
+        else:
+            a, b = a.reshape(a.shape[0], -1).cpu().numpy(), b.reshape(b.shape[0], -1).cpu().numpy()
+            assert rowrel(a, b) <= 1e-10

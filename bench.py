@@ -722,11 +722,18 @@ def run_workload(args) -> None:
         att = int((r.n_acc.to(torch.int64) + r.n_rej.to(torch.int64)).sum().item())
         acc = int(r.n_acc.to(torch.int64).sum().item())
         fl = flops.gradient_flops(g.method, g.field, att, acc)
+        resteps = 0  # requested times strictly inside (t0, t1): one re-step each
+        if g.ts is not None:
+            t1row = (np.full(g.ts.shape[0], g.t1) if g.t1v is None else g.t1v)[:, None]
+            resteps = int(((g.ts > 0.0) & (g.ts < t1row)).sum())
+        fl_sv = fl + flops.saveat_flops(g.method, g.field, resteps)
         infos.append({"group": g.name, "method": g.method, "field": g.field, "n": r.n,
                       "attempts": att, "accepted": acc, "record_len_max": int(r.n_acc.max()),
                       "checkpoint_every": r.ckpt_every, "ms": t_ms,
                       "tflops": fl / (t_ms * 1e-3) / 1e12,
-                      "saveat_points": None if g.ts is None else int(g.ts.shape[1])})
+                      "saveat_points": None if g.ts is None else int(g.ts.shape[1]),
+                      "saveat_resteps": resteps,
+                      "tflops_incl_saveat": fl_sv / (t_ms * 1e-3) / 1e12})
         g.gp64 = gp.clone()
         g.r64 = r
 
@@ -783,6 +790,7 @@ def run_workload(args) -> None:
     fp64_peak = probe_fp64_tflops(torch, stream)
     for info in infos:
         info["frac_of_fp64_peak"] = info["tflops"] / fp64_peak
+        info["frac_of_fp64_peak_incl_saveat"] = info["tflops_incl_saveat"] / fp64_peak
     cpu = None
     if world == 1 and not args.no_cpu:
         cpu = cpu_workload_rate(groups, args.cpu_seconds)

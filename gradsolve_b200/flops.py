@@ -31,3 +31,13 @@ def adjoint_flops(method: str, field: str, accepted: int) -> int:
 
 def gradient_flops(method: str, field: str, attempts: int, accepted: int) -> int:
     return solve_flops(method, field, attempts) + adjoint_flops(method, field, accepted)
+
+
+def saveat_flops(method: str, field: str, resteps: int) -> int:
+    """Dense output on the frozen mesh: each requested time inside (t0, t_fin) is one step of
+    the method from the bracketing step's start (F_step) and, in the reverse pass, that
+    step's VJP (F_vjp) -- the reference's bracket-and-re-step (gradsolve/solvers/dense.py:
+    106-163); times at t0 or t_fin are copies."""
+    c = COUNTS[(method, field)]
+    return (c["F_step"] + c["F_vjp"]) * int(resteps)
+

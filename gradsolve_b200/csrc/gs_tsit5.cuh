@@ -12,21 +12,19 @@
 //   p, gp                   : (n, P) row-major float64
 //   dt record               : chunk-interleaved, 4 steps per 32-byte sector:
 //                             step s of trajectory j lives at ((s/4)*n + j)*4 + s%4.
-//                             The one-thread-per-trajectory forward kernels store each
-//                             accepted dt as it comes (8 bytes into its sector; the lanes of a
-//                             warp hold consecutive j, and L2 merges a sector's four writes
-//                             before it goes to DRAM -- faster than holding four dt's in
-//                             registers and writing the whole sector at once); the persistent
-//                             kernels, whose lanes hold scattered j, buffer the sector in
-//                             registers.  Entries past n_acc[j] in trajectory j's last sector
-//                             are 0 (identity steps).
+//                             The forward kernels store each accepted dt as it comes (8
+//                             bytes into its sector; L2 merges a sector's four writes before
+//                             it goes to DRAM -- faster than holding four dt's in registers
+//                             and writing the whole sector at once).  Entries past n_acc[j]
+//                             in trajectory j's last sector are 0 (identity steps).
 //   checkpoints             : slot c of trajectory j = (y after c*K accepted steps, t), at
 //                             ((c*n + j) * CW) with CW = D+1 rounded up to even (16-byte
 //                             aligned); slot 0 is (y0, t0).  K = ckpt_every.
 //
 // The adjoint walks each trajectory's record backwards in segments of K steps.  For a
-// segment it reloads the checkpoint, recomputes the K-1 interior states into a per-thread
-// array, then applies the step VJPs in reverse.  Every trajectory runs whole segments
+// segment it takes the checkpoint (prefetched into shared memory), recomputes the K-1
+// interior states into a per-thread shared-memory buffer, then applies the step VJPs in
+// reverse.  Every trajectory runs whole segments
 // (n_acc padded up to a multiple of K with dt = 0 identity steps, which are exact
 // identities in value and gradient, gradsolve/solvers/tsit5_step.py:84-86), so the lanes of
 // a warp stay in the same phase (recompute vs VJP) instead of diverging.  With K = 1 every

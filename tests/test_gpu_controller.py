@@ -1,5 +1,6 @@
 """The forward kernels' controller (gs_tsit5.cuh step_from_sum: the accept test and the
-Newton reciprocal root on the sum of squares S, with host-computed constants for the state
+reciprocal root on the sum of squares S -- a float32 first guess refined by one second-order
+series step -- with host-computed constants for the state
 dimension D) against the reference's formula on the mean m = S / D evaluated with CUDA's sqrt
 and pow: accept iff sqrt(m) <= 1, factor 0.9 * max(sqrt(m), 1e-10)^(-1/q) clipped to
 [0.2, 5] (gradsolve/solvers/tsit5_replay.py:122, gradsolve/warp/_warp_rosenbrock.py:448-450)."""
@@ -45,6 +46,6 @@ def test_step_factor_matches_pow(gslib, cuda, order, D):
     f = fast.cpu().numpy()
     r = ref.cpu().numpy()
     ulp = np.abs(f - r) / np.spacing(r)
-    # D = 1: the Newton root agrees with pow to a few ulp; other D add the rounding of
+    # D = 1: the refined root agrees with pow to a few ulp; other D add the rounding of
     # 0.9 D^(1/K) and of the mean the reference forms
     assert ulp.max() <= (4 if D == 1 else 8), f"max {ulp.max()} ulp"

@@ -42,7 +42,7 @@ L2_BYTES = 126 * 1024 * 1024
 # trajectory count.
 DRAM_BYTES_PER_TRAJ = {
     "tsit5_adjoint_stages_kernel": {2: 6.053869e9 / 2**18},
-    "tsit5_record_kernel": {2: 4.543860e9 / 2**18},
+    "tsit5_record_kernel": {2: 4.504846e9 / 2**18},
 }
 
 

@@ -274,3 +274,45 @@ def test_forward_dense_output_equals_replay(gslib, cuda, method, field, prec):
         else:
             a, b = a.reshape(a.shape[0], -1).cpu().numpy(), b.reshape(b.shape[0], -1).cpu().numpy()
             assert rowrel(a, b) <= 1e-10
+
+
+@pytest.mark.parametrize("method,prec", [("tsit5", "float64"), ("tsit5", "mixed"),
+                                         ("rosenbrock23", "float64")])
+def test_forward_dense_output_schedules(gslib, cuda, method, prec):
+    """The forward with saved states on its three schedules -- one thread per trajectory,
+    lanes refilled from a work counter, strided lanes -- and with a shared end time (the
+    automatic choice is then one thread per trajectory): the same counts and dts, the same
+    saved states (Tsit5 bitwise: one lane policy; Rosenbrock23 to rounding, the compiler
+    contracting multiply-adds differently in the two kernels)."""
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    spec = field_spec("vdp")
+    rng = np.random.default_rng(13)
+    n = 500
+    y0 = torch.tensor(rng.uniform(-2, 2, (n, 2)), device=cuda)
+    lo, hi = (-1.0, 0.9) if method == "tsit5" else (1.0, 1.6)
+    p = torch.tensor(10 ** rng.uniform(lo, hi, (n, 1)), device=cuda)
+    for shared in (False, True):
+        t1v = None if shared else torch.tensor(10 ** rng.uniform(-1, 0.7, n), device=cuda)
+        t1 = 3.0 if shared else float(t1v.max())
+        row = torch.linspace(0.0, 1.0, 12, dtype=torch.float64, device=cuda)
+        ts = t1 * row if shared else t1v[:, None] * row[None, :]
+        outs = {}
+        for sched in ("static", "refill", "strided", "auto"):
+            r = engine.forward_record(method, spec, y0, p, t0=0.0, t1=t1, t1v=t1v, rtol=1e-6,
+                                      atol=1e-9, max_steps=50000, cap0=4096, checkpoint=4,
+                                      precision=prec, saveat_ts=ts, schedule=sched)
+            torch.cuda.synchronize()
+            assert int((r.status != 0).sum()) == 0, sched
+            outs[sched] = (r.n_acc.cpu(), r.padded_dts().cpu().numpy(), r.ys.cpu().numpy(),
+                           r.y_final.cpu().numpy())
+        ref = outs["static"]
+        for sched in ("refill", "strided", "auto"):
+            got = outs[sched]
+            assert torch.equal(got[0], ref[0]), (shared, sched)
+            if method == "tsit5":
+                for a, b in zip(got[1:], ref[1:]):
+                    np.testing.assert_array_equal(a, b)
+            else:
+                assert rowrel(got[2].reshape(n, -1), ref[2].reshape(n, -1)) <= 1e-10
+                assert rowrel(got[3], ref[3]) <= 1e-10

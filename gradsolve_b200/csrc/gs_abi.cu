@@ -319,18 +319,28 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
     if (!mixed) {
       // the stage-keeping variant needs 5*D more doubles per replayed step of the segment:
       // taken when asked for (while it fits) or, by default, while it keeps enough residency
+      // K = 2 (the autotuned interval of the built-in fields) has an unrolled instance, taken
+      // where it keeps as many threads resident as the general one
+      auto stages = gs::tsit5_adjoint_stages_kernel<F>;
       SegCfg ck{0, 0, 0}, cr{0, 0, 0};
-      if (variant != GS_ADJ_RECOMPUTE &&
-          (rc = occupancy_probe(gs::tsit5_adjoint_stages_kernel<F>,
-                                gs::adjoint_stages_smem_doubles<F::D>(a.ck_every), &ck)))
-        return rc;
+      const int sd = gs::adjoint_stages_smem_doubles<F::D>(a.ck_every);
+      if (variant != GS_ADJ_RECOMPUTE) {
+        if ((rc = occupancy_probe(stages, sd, &ck))) return rc;
+        if (a.ck_every == 2) {
+          SegCfg c2{0, 0, 0};
+          if ((rc = occupancy_probe(gs::tsit5_adjoint_stages_k2_kernel<F>, sd, &c2))) return rc;
+          if (c2.resident > 0 && c2.resident >= ck.resident) {
+            stages = gs::tsit5_adjoint_stages_k2_kernel<F>;
+            ck = c2;
+          }
+        }
+      }
       if ((rc = occupancy_probe(gs::tsit5_adjoint_kernel<F>,
                                 gs::adjoint_smem_doubles<F::D>(a.ck_every), &cr)))
         return rc;
       if (ck.resident > 0 && (variant == GS_ADJ_STAGES || keeping_pays(ck, cr))) {
-        if ((rc = allow_smem(gs::tsit5_adjoint_stages_kernel<F>, ck.smem))) return rc;
-        gs::tsit5_adjoint_stages_kernel<F>
-            <<<grid_for_block(a.n, ck.block), ck.block, ck.smem, s>>>(a);
+        if ((rc = allow_smem(stages, ck.smem))) return rc;
+        stages<<<grid_for_block(a.n, ck.block), ck.block, ck.smem, s>>>(a);
         return cuda_check("tsit5_adjoint_stages_kernel");
       }
       if (cr.resident <= 0)

@@ -835,8 +835,11 @@ struct KeptStages {  // tsit5_vjp_core's stage source: the kept inputs of step q
   }
 };
 
-template <class F>
-__global__ void __launch_bounds__(128) tsit5_adjoint_stages_kernel(const AdjointArgs a) {
+// KC > 0: the segment length fixed at compile time (the autotuned K = 2 of the built-in
+// fields), so the segment loops unroll and the buffer offsets are constants; KC = 0 reads K
+// from the arguments.
+template <class F, int KC>
+__device__ __forceinline__ void tsit5_adjoint_stages_body(const AdjointArgs& a) {
   constexpr int D = F::D, P = F::P;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.n) return;
@@ -849,7 +852,7 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_stages_kernel(const Adjoint
 #pragma unroll
   for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
   const int na = steps_in_record(a.n_acc, j, a.cap);
-  const int K = a.ck_every;
+  const int K = KC > 0 ? KC : a.ck_every;
   const int nseg = (na + K - 1) / K;
   AdjStageBuf<D> buf(K);
   int b = 0;
@@ -910,6 +913,18 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_stages_kernel(const Adjoint
 #pragma unroll
     for (int i = 0; i < P; ++i) a.gp[j * P + i] = gp[i];
   }
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) tsit5_adjoint_stages_kernel(const AdjointArgs a) {
+  tsit5_adjoint_stages_body<F, 0>(a);
+}
+
+// K = 2, bounded to 5 blocks of 128 per SM: unrolled without the bound, the segment's two
+// steps interleave into 128 registers (4 blocks)
+template <class F>
+__global__ void __launch_bounds__(128, 5) tsit5_adjoint_stages_k2_kernel(const AdjointArgs a) {
+  tsit5_adjoint_stages_body<F, 2>(a);
 }
 
 }  // namespace gs

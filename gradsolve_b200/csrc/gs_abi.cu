@@ -388,8 +388,19 @@ int launch_ros23_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, int 
                               gs::ros23_adjoint_smem_doubles<F::D, false>(a.ck_every), &cr)))
       return rc;
     if (keeping_pays(ck, cr)) {
-      if ((rc = allow_smem(gs::ros23_adjoint_kernel<F, true>, ck.smem))) return rc;
-      gs::ros23_adjoint_kernel<F, true><<<grid_for_block(a.n, ck.block), ck.block, ck.smem, s>>>(a);
+      auto keep = gs::ros23_adjoint_kernel<F, true>;
+      if (a.ck_every == 2) {  // the unrolled instance, where it keeps the residency
+        SegCfg c2{0, 0, 0};
+        if ((rc = occupancy_probe(gs::ros23_adjoint_k2_kernel<F>,
+                                  gs::ros23_adjoint_smem_doubles<F::D, true>(2), &c2)))
+          return rc;
+        if (c2.resident > 0 && c2.resident >= ck.resident) {
+          keep = gs::ros23_adjoint_k2_kernel<F>;
+          ck = c2;
+        }
+      }
+      if ((rc = allow_smem(keep, ck.smem))) return rc;
+      keep<<<grid_for_block(a.n, ck.block), ck.block, ck.smem, s>>>(a);
       return cuda_check("ros23_adjoint_kernel");
     }
     // large K: the kept factors would cost too many resident threads (or not fit); recompute

@@ -394,8 +394,9 @@ struct AdjRosBuf {
   }
 };
 
-template <class F, bool kKeep>
-__global__ void __launch_bounds__(128) ros23_adjoint_kernel(const AdjointArgs a) {
+// KC > 0: the segment length fixed at compile time (as tsit5_adjoint_stages_body).
+template <class F, bool kKeep, int KC>
+__device__ __forceinline__ void ros23_adjoint_body(const AdjointArgs& a) {
   constexpr int D = F::D, P = F::P;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.n) return;
@@ -408,7 +409,7 @@ __global__ void __launch_bounds__(128) ros23_adjoint_kernel(const AdjointArgs a)
 #pragma unroll
   for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
   const int na = steps_in_record(a.n_acc, j, a.cap);
-  const int K = a.ck_every;
+  const int K = KC > 0 ? KC : a.ck_every;
   const int nseg = (na + K - 1) / K;
   AdjRosBuf<D, kKeep> buf(K);
   int b = 0;
@@ -469,6 +470,17 @@ __global__ void __launch_bounds__(128) ros23_adjoint_kernel(const AdjointArgs a)
 #pragma unroll
     for (int i = 0; i < P; ++i) a.gp[j * P + i] = gp[i];
   }
+}
+
+template <class F, bool kKeep>
+__global__ void __launch_bounds__(128) ros23_adjoint_kernel(const AdjointArgs a) {
+  ros23_adjoint_body<F, kKeep, 0>(a);
+}
+
+// K = 2 with the kept factors, unrolled; bounded to 4 blocks of 128 per SM
+template <class F>
+__global__ void __launch_bounds__(128, 4) ros23_adjoint_k2_kernel(const AdjointArgs a) {
+  ros23_adjoint_body<F, true, 2>(a);
 }
 
 }  // namespace gs

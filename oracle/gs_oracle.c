@@ -1,8 +1,8 @@
 /*
  * gs_oracle.c -- CPU oracle for the ensemble adaptive solve and its replay adjoint.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA path is compared
- * against; it is never linked into, loaded by, or called from the product library
+ * TEST INFRASTRUCTURE ONLY.  This file is the reference result that the CUDA path is
+ * compared against; it is never linked into, loaded by, or called from the product library
  * (gradsolve_b200/, libgsolve.so).  Only tests/, __graft_entry__.smoke() and the
  * cpu_baseline / reference legs of bench.py load it.
  *

@@ -2,7 +2,7 @@
 
 Nothing in the product package ``gradsolve_b200`` imports this module.  It is loaded by
 the tests, by ``__graft_entry__.smoke()`` and by the CPU legs of ``bench.py``, always as
-the checker or the timed CPU baseline, never as the path being measured.
+the result compared against or the timed CPU baseline, never as the path being measured.
 
 Three layers:
 

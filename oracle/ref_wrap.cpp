@@ -1,5 +1,6 @@
 // ref_wrap.cpp -- batch entry point around the reference's own hand-CUDA forward, compiled
-// for the host.  TEST INFRASTRUCTURE ONLY (the checker / CPU baseline, never the product).
+// for the host.  TEST INFRASTRUCTURE ONLY (a result to compare against and a CPU baseline,
+// never the product).
 //
 // REF_SOURCE names a template from gradsolve/cuda/kernels/*.cu.in filled by
 // oracle/build_ref.py exactly as gradsolve/cuda/_codegen.py:42-55 fills it; that file is

@@ -1,7 +1,7 @@
 """Generate the golden vectors under tests/golden/ from the reference's own code.
 
 Runs only where the reference source tree is present (it is read from
-``$GRADSOLVE_REFERENCE``, default ``/root/reference``); the GPU box never runs this.
+``$GRADSOLVE_REFERENCE``, default ``/root/reference``); the GPU test runs never run this.
 What it executes, verbatim, from the reference:
 
 * ``gradsolve/solvers/tsit5_step.py`` -- imported by file path (it has no imports), for

@@ -364,13 +364,9 @@ def run_b200(args) -> None:
     step = make_step("float64")
     for _ in range(args.warmup):  # warm-up (also sizes the record so timed steps never regrow)
         r, gp = step()
-    torch.cuda.synchronize()
-    assert int((r.status != 0).sum().item()) == 0, "warm-up solve failed"
-    att = int((r.n_acc.to(torch.int64) + r.n_rej.to(torch.int64)).sum().item())
-    acc = int(r.n_acc.to(torch.int64).sum().item())
-    S = int(r.n_acc.max().item())
-    K = r.ckpt_every
     r = gp = None  # the warm-up's outputs (the record stays alive as the step's workspace)
+    # the timed steps follow the warm-up directly (the GPU does not idle between them); the
+    # step statistics are read from the last timed step, which integrates the same batch
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -380,7 +376,12 @@ def run_b200(args) -> None:
     ms_per_step = float(np.mean(step_ms))
     ms_per_step = max_over_ranks(ms_per_step, dev)
     value = n * world / (ms_per_step * 1e-3)
+    assert int((r.status != 0).sum().item()) == 0, "solve failed"
     assert torch.isfinite(gp).all()
+    att = int((r.n_acc.to(torch.int64) + r.n_rej.to(torch.int64)).sum().item())
+    acc = int(r.n_acc.to(torch.int64).sum().item())
+    S = int(r.n_acc.max().item())
+    K = r.ckpt_every
 
     # ---- the float32-stage variant on the same workload, and its accuracy ---------------
     mixed = None

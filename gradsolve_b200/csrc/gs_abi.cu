@@ -295,7 +295,10 @@ int launch_tsit5_record(const gs::RecordArgs& a_in, cudaStream_t s, bool mixed, 
       gs::tsit5_mixed_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
       return cuda_check("tsit5_mixed_record_kernel");
     }
-    gs::tsit5_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    if (!a.rec && !a.ckpt)
+      gs::tsit5_record_kernel<F, false><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    else
+      gs::tsit5_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
     return cuda_check("tsit5_record_kernel");
   }
   const bool counter = sched == GS_SCHED_REFILL;

@@ -527,7 +527,9 @@ __device__ __forceinline__ double load_rec(const double* rec, long long n, long 
 // shared-reciprocal error norm the unbounded kernel takes 84 and drops to 5 blocks; the few
 // bytes it spills at 80 cost less than the lost warps (11.63 vs 11.73 ms on the Lorenz 2^20
 // bench forward; 7 blocks at 72 registers: 11.35 ms).  Larger states keep their registers.
-template <class F>
+// kStore = false: the forward-only solve (no record, no checkpoints), with the store paths
+// compiled out.
+template <class F, bool kStore = true>
 __global__ void __launch_bounds__(128, (F::D <= 4 ? 6 : 1)) tsit5_record_kernel(const RecordArgs a) {
   constexpr int D = F::D, P = F::P;
   using T = Tsit5;
@@ -541,8 +543,8 @@ __global__ void __launch_bounds__(128, (F::D <= 4 ? 6 : 1)) tsit5_record_kernel(
   double t = a.t0;
   const double t1 = a.t1v ? a.t1v[j] : a.t1;
   double dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
-  const bool rec_on = a.rec != nullptr;
-  const bool ck_on = a.ckpt != nullptr;
+  const bool rec_on = kStore && a.rec != nullptr;
+  const bool ck_on = kStore && a.ckpt != nullptr;
   // this trajectory's slots of the current record sector (rec_index, advanced per sector)
   double* rp = rec_on ? a.rec + j * 4 : nullptr;
   const long long rstride = 4 * a.n;

@@ -369,7 +369,10 @@ int launch_ros23_record(const gs::RecordArgs& a_in, cudaStream_t s, int sched) {
   gs::RecordArgs a = a_in;
   a.ctrl = gs::make_ctrl_consts(F::D, 6);  // Rosenbrock23: err^(-1/3) = m^(-1/6)
   if (sched == GS_SCHED_STATIC) {
-    gs::ros23_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    if (!a.rec && !a.ckpt)
+      gs::ros23_record_kernel<F, false><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    else
+      gs::ros23_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
     return cuda_check("ros23_record_kernel");
   }
   return launch_record_persistent<F, gs::LaneRos23<F>>(a, s, sched == GS_SCHED_REFILL);

@@ -244,7 +244,8 @@ __device__ __forceinline__ void ros23_step_vjp(const double* y, const double* p,
   ros23_vjp_core<F>(y, p, dt, c.W, c.k1, s1, c.k2p, lam, gp);
 }
 
-template <class F>
+// kStore = false: the forward-only solve (no record, no checkpoints), stores compiled out.
+template <class F, bool kStore = true>
 __global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
   constexpr int D = F::D, P = F::P;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -257,8 +258,8 @@ __global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
   double t = a.t0;
   const double t1 = a.t1v ? a.t1v[j] : a.t1;
   double dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
-  const bool rec_on = a.rec != nullptr;
-  const bool ck_on = a.ckpt != nullptr;
+  const bool rec_on = kStore && a.rec != nullptr;
+  const bool ck_on = kStore && a.ckpt != nullptr;
   if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
   int acc = 0, rej = 0, st = 0, ck_cnt = 0, ck_slot = 0;
   for (int it = 0; it < a.max_steps; ++it) {

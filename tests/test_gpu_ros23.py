@@ -128,3 +128,27 @@ def test_stiff_grad_closure_canonical_robertson(oracle, cuda):
     fd = oracle.fd_grad(loss, y0)
     g = z.grad.cpu().numpy()
     assert float(np.linalg.norm(g - fd) / np.linalg.norm(fd)) <= 1e-6
+
+
+@pytest.mark.parametrize("method,case,field", [("rosenbrock23", "robertson_stiff", "robertson"),
+                                               ("tsit5", "lorenz_scale", "lorenz")])
+def test_forward_only_solve_matches_recording_forward(gslib, cuda, method, case, field):
+    """The forward-only solve (no record, no checkpoints: the store paths compiled out of
+    the kernel) takes the recording forward's steps: the same counts and statuses, and
+    y_final to rounding (another instance of the same expressions)."""
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    g = load_golden(case)
+    spec = field_spec(field)
+    y0 = torch.tensor(g["y0"], device=cuda)
+    p = torch.tensor(g["params"][:, : spec.nparam], device=cuda).contiguous()
+    kw = dict(t0=float(g["t0"]), t1=float(g["t1"]), rtol=float(g["rtol"]),
+              atol=float(g["atol"]), max_steps=50000, schedule="static")
+    if "dt0" in g:
+        kw["dt0"] = float(g["dt0"])
+    a = engine.forward_record(method, spec, y0, p, record=True, **kw)
+    b = engine.forward_record(method, spec, y0, p, record=False, **kw)
+    torch.cuda.synchronize()
+    for x, y in ((a.n_acc, b.n_acc), (a.n_rej, b.n_rej), (a.status, b.status)):
+        assert torch.equal(x, y)
+    assert rel(b.y_final.cpu().numpy(), a.y_final.cpu().numpy(), 1e-12) <= 1e-12

@@ -127,6 +127,9 @@ int gs_max_ckpt_every(void);
  *   A trajectory that would accept more than cap steps stops with status 3 when rec or ckpt
  *   is given.  y_final is the last reached state (rows with status != 0 are not NaN'd here;
  *   the reference's driver does that, gradsolve/warp/warp_ode.py:319).
+ *   With rec and ckpt both NULL this is the forward-only solve (the reference's cuda_tsit5
+ *   lane, gradsolve/cuda/kernels/tsit5_template.cu.in), run by a kernel instance with the
+ *   store paths compiled out.
  */
 int gs_tsit5_fwd_record(int field, int precision, long long n, const double* y0,
                         const double* p, double t0, const double* t1v, double t1, double rtol,

@@ -507,8 +507,8 @@ def _forward_planned(method, spec, y0, p, t1v, saveat_ts, ws: RecordSet, kw):
     # A planned tier's rows come sorted by their previous cost, so neighbouring threads take
     # similar numbers of attempts and one thread per trajectory stays balanced.  Rosenbrock23
     # then runs that way: it is latency-bound, and the one-thread kernel holds more warps
-    # than the refilled lanes (uneven VdP: its group 36.6 -> 34.2 ms); Tsit5 keeps the
-    # refilled lanes, which its many very short trajectories favour (11.5 vs 15.7 ms).
+    # than the refilled lanes (uneven VdP: its group 36.6 -> 35.5 ms); Tsit5 keeps the
+    # refilled lanes (its group measured 11.44 ms refilled, 11.54 one thread per trajectory).
     kwp = kw
     if method == METHOD_ROS23 and kw["schedule"] == "auto":
         kwp = dict(kw, schedule="static")

@@ -523,6 +523,69 @@ __device__ __forceinline__ double load_rec(const double* rec, long long n, long 
 }
 
 // --- forward adaptive solve with record --------------------------------------------------
+// Per-trajectory bookkeeping of the forward, carried from attempt to attempt.
+struct FwdCounters {
+  double t, dt;
+  int it, acc, rej, st, ck_cnt, ck_slot;
+  double* rp;  // this trajectory's slots of the current record sector (rec_index, advanced)
+};
+
+// One attempt from the state (y, k1) (k1 = f(y), FSAL).  The candidate is computed into
+// (yo, ko); returns true when the integration goes on from (yo, ko) -- which after a rejection
+// receive a copy of (y, k1) -- and false when it stops with its state in (y, k1).  The kernel
+// alternates the two register sets, so an accepted step (the common case) moves no state.
+template <class F>
+__device__ __forceinline__ bool tsit5_attempt(const RecordArgs& a, long long j,
+                                              const double* p, double t1, bool rec_on,
+                                              bool ck_on, long long rstride, FwdCounters& c,
+                                              const double* y, const double* k1, double* yo,
+                                              double* ko) {
+  constexpr int D = F::D;
+  using T = Tsit5;
+  if (c.it >= a.max_steps || c.t >= t1) return false;
+  ++c.it;
+  const double h = (t1 - c.t < c.dt) ? (t1 - c.t) : c.dt;
+  Stages<F> S;
+  tsit5_k2_to_k6<F>(y, p, k1, h, S);
+  tsit5_y5<F>(y, k1, S, h, yo);
+  F::rhs(yo, p, ko);
+  double e[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+    e[i] = h * (T::E1 * k1[i] + T::E2 * S.k2[i] + T::E3 * S.k3[i] + T::E4 * S.k4[i] +
+                T::E5 * S.k5[i] + T::E6 * S.k6[i] + T::E7 * ko[i]);
+  const double m = wrms_sumsq<D>(e, y, yo, a.rtol, a.atol);
+  if (!(m == m)) {  // NaN error: dt would turn NaN and the loop could never finish
+    c.st = 1;
+    return false;
+  }
+  if (m <= a.ctrl.accept_sum) {  // err = sqrt(m / D) <= 1
+    if ((rec_on || ck_on) && c.acc >= a.cap) {
+      c.st = 3;
+      return false;
+    }
+    c.t = c.t + h;
+    if (rec_on) {
+      c.rp[c.acc & 3] = h;
+      if ((c.acc & 3) == 3) c.rp += rstride;
+    }
+    ++c.acc;
+    if (ck_on && ++c.ck_cnt == a.ck_every) {
+      c.ck_cnt = 0;
+      if (++c.ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, c.ck_slot, yo, c.t);
+    }
+  } else {
+    ++c.rej;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      yo[i] = y[i];
+      ko[i] = k1[i];
+    }
+  }
+  c.dt = step_from_sum<10>(m, h, a.ctrl);
+  return true;
+}
+
 // Bounded to 6 resident blocks of 128 per SM (80 registers) for D <= 4: with the
 // shared-reciprocal error norm the unbounded kernel takes 84 and drops to 5 blocks; the few
 // bytes it spills at 80 cost less than the lost warps (11.63 vs 11.73 ms on the Lorenz 2^20
@@ -532,75 +595,41 @@ __device__ __forceinline__ double load_rec(const double* rec, long long n, long 
 template <class F, bool kStore = true>
 __global__ void __launch_bounds__(128, (F::D <= 4 ? 6 : 1)) tsit5_record_kernel(const RecordArgs a) {
   constexpr int D = F::D, P = F::P;
-  using T = Tsit5;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.n) return;
-  double y[D], p[P], k1[D], y5[D], k7[D], e[D];
+  double ya[D], ka[D], yb[D], kb[D], p[P];
 #pragma unroll
-  for (int i = 0; i < D; ++i) y[i] = a.y0[j * D + i];
+  for (int i = 0; i < D; ++i) ya[i] = a.y0[j * D + i];
 #pragma unroll
   for (int i = 0; i < P; ++i) p[i] = a.p[j * P + i];
-  double t = a.t0;
   const double t1 = a.t1v ? a.t1v[j] : a.t1;
-  double dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
   const bool rec_on = kStore && a.rec != nullptr;
   const bool ck_on = kStore && a.ckpt != nullptr;
-  // this trajectory's slots of the current record sector (rec_index, advanced per sector)
-  double* rp = rec_on ? a.rec + j * 4 : nullptr;
   const long long rstride = 4 * a.n;
-  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
-  F::rhs(y, p, k1);
-  int acc = 0, rej = 0, st = 0, ck_cnt = 0, ck_slot = 0;
-  for (int it = 0; it < a.max_steps; ++it) {
-    if (t >= t1) break;
-    const double h = (t1 - t < dt) ? (t1 - t) : dt;
-    Stages<F> S;
-    tsit5_k2_to_k6<F>(y, p, k1, h, S);
-    tsit5_y5<F>(y, k1, S, h, y5);
-    F::rhs(y5, p, k7);
-#pragma unroll
-    for (int i = 0; i < D; ++i)
-      e[i] = h * (T::E1 * k1[i] + T::E2 * S.k2[i] + T::E3 * S.k3[i] + T::E4 * S.k4[i] +
-                  T::E5 * S.k5[i] + T::E6 * S.k6[i] + T::E7 * k7[i]);
-    const double m = wrms_sumsq<D>(e, y, y5, a.rtol, a.atol);
-    if (!(m == m)) {  // NaN error: dt would turn NaN and the loop could never finish
-      st = 1;
+  FwdCounters c;
+  c.t = a.t0;
+  c.dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
+  c.it = c.acc = c.rej = c.st = c.ck_cnt = c.ck_slot = 0;
+  c.rp = rec_on ? a.rec + j * 4 : nullptr;
+  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, ya, c.t);
+  F::rhs(ya, p, ka);
+  bool in_b = false;  // where the state is when the loop stops
+  for (;;) {
+    if (!tsit5_attempt<F>(a, j, p, t1, rec_on, ck_on, rstride, c, ya, ka, yb, kb)) break;
+    if (!tsit5_attempt<F>(a, j, p, t1, rec_on, ck_on, rstride, c, yb, kb, ya, ka)) {
+      in_b = true;
       break;
     }
-    if (m <= a.ctrl.accept_sum) {  // err = sqrt(m / D) <= 1
-      if ((rec_on || ck_on) && acc >= a.cap) {
-        st = 3;
-        break;
-      }
-      t = t + h;
-#pragma unroll
-      for (int i = 0; i < D; ++i) {
-        y[i] = y5[i];
-        k1[i] = k7[i];
-      }
-      if (rec_on) {
-        rp[acc & 3] = h;
-        if ((acc & 3) == 3) rp += rstride;
-      }
-      ++acc;
-      if (ck_on && ++ck_cnt == a.ck_every) {
-        ck_cnt = 0;
-        if (++ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, ck_slot, y, t);
-      }
-    } else {
-      ++rej;
-    }
-    dt = step_from_sum<10>(m, h, a.ctrl);
   }
-  if (st == 0 && !(t >= t1)) st = 1;
+  if (c.st == 0 && !(c.t >= t1)) c.st = 1;
   if (rec_on) {  // zero-pad the last sector (identity steps)
-    for (int s = acc; (s & 3) != 0; ++s) rp[s & 3] = 0.0;
+    for (int s = c.acc; (s & 3) != 0; ++s) c.rp[s & 3] = 0.0;
   }
 #pragma unroll
-  for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
-  a.n_acc[j] = acc;
-  a.n_rej[j] = rej;
-  a.status[j] = st;
+  for (int i = 0; i < D; ++i) a.yf[j * D + i] = in_b ? yb[i] : ya[i];
+  a.n_acc[j] = c.acc;
+  a.n_rej[j] = c.rej;
+  a.status[j] = c.st;
 }
 
 // --- frozen-mesh replay (values), optionally writing checkpoints -------------------------

@@ -244,74 +244,99 @@ __device__ __forceinline__ void ros23_step_vjp(const double* y, const double* p,
   ros23_vjp_core<F>(y, p, dt, c.W, c.k1, s1, c.k2p, lam, gp);
 }
 
+// One attempt from the state y; the candidate is computed into yo.  Returns true when the
+// integration goes on from yo (a copy of y after a rejection) and false when it stops with
+// its state in y -- the register-set alternation of tsit5_attempt.
+template <class F>
+__device__ __forceinline__ bool ros23_attempt(const RecordArgs& a, long long j, const double* p,
+                                              double t1, bool rec_on, bool ck_on,
+                                              long long rstride, FwdCounters& c,
+                                              const double* y, double* yo) {
+  constexpr int D = F::D;
+  if (c.it >= a.max_steps || c.t >= t1) return false;
+  const double h = (t1 - c.t < c.dt) ? (t1 - c.t) : c.dt;
+  if (c.t + h == c.t) {  // the step no longer advances time
+    c.st = 2;
+    return false;
+  }
+  ++c.it;
+  RosCore<F> rc;
+  ros23_core<F>(y, p, h, rc, yo);
+  double F2[D], r3[D], k3[D], ev[D];
+  F::rhs(yo, p, F2);
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+    r3[i] = F2[i] - Ros23::E32 * (rc.k2[i] - rc.F1[i]) - 2.0 * (rc.k1[i] - rc.F0[i]);
+  lu_solve<D>(rc.W, r3, k3);
+#pragma unroll
+  for (int i = 0; i < D; ++i) ev[i] = (h / 6.0) * (rc.k1[i] - 2.0 * rc.k2[i] + k3[i]);
+  const double m = wrms_sumsq<D>(ev, y, yo, a.rtol, a.atol);
+  if (!(m == m)) {
+    c.st = 1;
+    return false;
+  }
+  if (m <= a.ctrl.accept_sum) {
+    if ((rec_on || ck_on) && c.acc >= a.cap) {
+      c.st = 3;
+      return false;
+    }
+    c.t = c.t + h;
+    if (rec_on) {
+      c.rp[c.acc & 3] = h;
+      if ((c.acc & 3) == 3) c.rp += rstride;
+    }
+    ++c.acc;
+    if (ck_on && ++c.ck_cnt == a.ck_every) {
+      c.ck_cnt = 0;
+      if (++c.ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, c.ck_slot, yo, c.t);
+    }
+  } else {
+    ++c.rej;
+#pragma unroll
+    for (int i = 0; i < D; ++i) yo[i] = y[i];
+  }
+  c.dt = step_from_sum<6>(m, h, a.ctrl);
+  return true;
+}
+
 // kStore = false: the forward-only solve (no record, no checkpoints), stores compiled out.
 template <class F, bool kStore = true>
 __global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
   constexpr int D = F::D, P = F::P;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.n) return;
-  double y[D], p[P], ynew[D], ev[D];
+  double ya[D], yb[D], p[P];
 #pragma unroll
-  for (int i = 0; i < D; ++i) y[i] = a.y0[j * D + i];
+  for (int i = 0; i < D; ++i) ya[i] = a.y0[j * D + i];
 #pragma unroll
   for (int i = 0; i < P; ++i) p[i] = a.p[j * P + i];
-  double t = a.t0;
   const double t1 = a.t1v ? a.t1v[j] : a.t1;
-  double dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
   const bool rec_on = kStore && a.rec != nullptr;
   const bool ck_on = kStore && a.ckpt != nullptr;
-  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
-  int acc = 0, rej = 0, st = 0, ck_cnt = 0, ck_slot = 0;
-  for (int it = 0; it < a.max_steps; ++it) {
-    if (t >= t1) break;
-    const double h = (t1 - t < dt) ? (t1 - t) : dt;
-    if (t + h == t) {  // the step no longer advances time
-      st = 2;
+  const long long rstride = 4 * a.n;
+  FwdCounters c;
+  c.t = a.t0;
+  c.dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
+  c.it = c.acc = c.rej = c.st = c.ck_cnt = c.ck_slot = 0;
+  c.rp = rec_on ? a.rec + j * 4 : nullptr;
+  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, ya, c.t);
+  bool in_b = false;  // where the state is when the loop stops
+  for (;;) {
+    if (!ros23_attempt<F>(a, j, p, t1, rec_on, ck_on, rstride, c, ya, yb)) break;
+    if (!ros23_attempt<F>(a, j, p, t1, rec_on, ck_on, rstride, c, yb, ya)) {
+      in_b = true;
       break;
     }
-    RosCore<F> c;
-    ros23_core<F>(y, p, h, c, ynew);
-    double F2[D], r3[D], k3[D];
-    F::rhs(ynew, p, F2);
-#pragma unroll
-    for (int i = 0; i < D; ++i)
-      r3[i] = F2[i] - Ros23::E32 * (c.k2[i] - c.F1[i]) - 2.0 * (c.k1[i] - c.F0[i]);
-    lu_solve<D>(c.W, r3, k3);
-#pragma unroll
-    for (int i = 0; i < D; ++i) ev[i] = (h / 6.0) * (c.k1[i] - 2.0 * c.k2[i] + k3[i]);
-    const double m = wrms_sumsq<D>(ev, y, ynew, a.rtol, a.atol);
-    if (!(m == m)) {
-      st = 1;
-      break;
-    }
-    if (m <= a.ctrl.accept_sum) {
-      if ((rec_on || ck_on) && acc >= a.cap) {
-        st = 3;
-        break;
-      }
-      t = t + h;
-#pragma unroll
-      for (int i = 0; i < D; ++i) y[i] = ynew[i];
-      if (rec_on) a.rec[rec_index(j, acc, a.n)] = h;
-      ++acc;
-      if (ck_on && ++ck_cnt == a.ck_every) {
-        ck_cnt = 0;
-        if (++ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, ck_slot, y, t);
-      }
-    } else {
-      ++rej;
-    }
-    dt = step_from_sum<6>(m, h, a.ctrl);
   }
-  if (st == 0 && !(t >= t1)) st = 1;
+  if (c.st == 0 && !(c.t >= t1)) c.st = 1;
   if (rec_on) {  // zero-pad the last sector (identity steps)
-    for (int s = acc; (s & 3) != 0; ++s) a.rec[rec_index(j, s, a.n)] = 0.0;
+    for (int s = c.acc; (s & 3) != 0; ++s) c.rp[s & 3] = 0.0;
   }
 #pragma unroll
-  for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
-  a.n_acc[j] = acc;
-  a.n_rej[j] = rej;
-  a.status[j] = st;
+  for (int i = 0; i < D; ++i) a.yf[j * D + i] = in_b ? yb[i] : ya[i];
+  a.n_acc[j] = c.acc;
+  a.n_rej[j] = c.rej;
+  a.status[j] = c.st;
 }
 
 template <class F>

@@ -41,9 +41,9 @@ L2_BYTES = 126 * 1024 * 1024
 # profiles/tsit5_f64_lorenz_bench_n2e20_launches_n2e18_K2.md.  Traffic grows with the
 # trajectory count.
 DRAM_BYTES_PER_TRAJ = {
-    "tsit5_adjoint_stages_k2_kernel": {2: 5.753801e9 / 2**18},
+    "tsit5_adjoint_stages_k2_kernel": {2: 5.752840e9 / 2**18},
     "tsit5_adjoint_stages_kernel": {2: 6.053869e9 / 2**18},
-    "tsit5_record_kernel": {2: 4.507144e9 / 2**18},
+    "tsit5_record_kernel": {2: 4.517664e9 / 2**18},
 }
 
 

@@ -229,79 +229,108 @@ __device__ __forceinline__ void mixed_step_vjp(const double* y, const double* p,
 }
 
 // --- forward adaptive solve with record, float32 stages ----------------------------------
+// One float32-stage attempt from the state (y, c, k1) -- c the compensated sum's carry, k1 =
+// f(y) -- into (yo, co, ko), with the register-set alternation of tsit5_attempt: true when
+// the integration goes on from (yo, co, ko), a copy of the state after a rejection.
+template <class F>
+__device__ __forceinline__ bool mixed_attempt(const RecordArgs& a, long long j, const double* p,
+                                              const float* pf, double t1, bool rec_on,
+                                              bool ck_on, long long rstride, FwdCounters& ct,
+                                              const double* y, const double* c,
+                                              const double* k1, double* yo, double* co,
+                                              double* ko) {
+  constexpr int D = F::D;
+  using T = Tsit5f;
+  if (ct.it >= a.max_steps || ct.t >= t1) return false;
+  ++ct.it;
+  const double h = (t1 - ct.t < ct.dt) ? (t1 - ct.t) : ct.dt;
+  const float hf = (float)h;
+  float yf[D], k1f[D];
+  double inc[D], ed[D];
+  to_float<F>(y, yf);
+  to_float<F>(k1, k1f);
+  MixedStages<F> S;
+  mixed_dk2_to_dk6<F>(yf, pf, k1f, hf, S);
+  mixed_increment<F>(k1, S, h, hf, inc);
+#pragma unroll
+  for (int i = 0; i < D; ++i) { yo[i] = y[i]; co[i] = c[i]; }
+  kahan_add<D>(yo, co, inc);
+  F::rhs(yo, p, ko);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    const float dk7 = (float)(ko[i] - k1[i]);
+    ed[i] = (double)(hf * (T::E2 * S.dk2[i] + T::E3 * S.dk3[i] + T::E4 * S.dk4[i] +
+                           T::E5 * S.dk5[i] + T::E6 * S.dk6[i] + T::E7 * dk7));
+  }
+  const double m = wrms_sumsq<D>(ed, y, yo, a.rtol, a.atol);
+  if (!(m == m)) {
+    ct.st = 1;
+    return false;
+  }
+  if (m <= a.ctrl.accept_sum) {
+    if ((rec_on || ck_on) && ct.acc >= a.cap) {
+      ct.st = 3;
+      return false;
+    }
+    ct.t = ct.t + h;
+    if (rec_on) {
+      ct.rp[ct.acc & 3] = h;
+      if ((ct.acc & 3) == 3) ct.rp += rstride;
+    }
+    ++ct.acc;
+    if (ck_on && ++ct.ck_cnt == a.ck_every) {
+      ct.ck_cnt = 0;
+      if (++ct.ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, ct.ck_slot, yo, ct.t);
+    }
+  } else {
+    ++ct.rej;
+#pragma unroll
+    for (int i = 0; i < D; ++i) { yo[i] = y[i]; co[i] = c[i]; ko[i] = k1[i]; }
+  }
+  ct.dt = step_from_sum<10>(m, h, a.ctrl);
+  return true;
+}
+
 template <class F>
 __global__ void __launch_bounds__(128) tsit5_mixed_record_kernel(const RecordArgs a) {
   constexpr int D = F::D, P = F::P;
-  using T = Tsit5f;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.n) return;
-  double y[D], c[D], p[P], k1[D], y5[D], c5[D], k7[D], ed[D], inc[D];
+  double ya[D], ca[D], ka[D], yb[D], cb[D], kb[D], p[P];
   float pf[P];
 #pragma unroll
-  for (int i = 0; i < D; ++i) { y[i] = a.y0[j * D + i]; c[i] = 0.0; }
+  for (int i = 0; i < D; ++i) { ya[i] = a.y0[j * D + i]; ca[i] = 0.0; }
 #pragma unroll
   for (int i = 0; i < P; ++i) { p[i] = a.p[j * P + i]; pf[i] = (float)p[i]; }
-  double t = a.t0;
   const double t1 = a.t1v ? a.t1v[j] : a.t1;
-  double dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
   const bool rec_on = a.rec != nullptr;
   const bool ck_on = a.ckpt != nullptr;
-  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, y, t);
-  F::rhs(y, p, k1);
-  int acc = 0, rej = 0, st = 0, ck_cnt = 0, ck_slot = 0;
-  for (int it = 0; it < a.max_steps; ++it) {
-    if (t >= t1) break;
-    const double h = (t1 - t < dt) ? (t1 - t) : dt;
-    const float hf = (float)h;
-    float yf[D], k1f[D];
-    to_float<F>(y, yf);
-    to_float<F>(k1, k1f);
-    MixedStages<F> S;
-    mixed_dk2_to_dk6<F>(yf, pf, k1f, hf, S);
-    mixed_increment<F>(k1, S, h, hf, inc);
-#pragma unroll
-    for (int i = 0; i < D; ++i) { y5[i] = y[i]; c5[i] = c[i]; }
-    kahan_add<D>(y5, c5, inc);
-    F::rhs(y5, p, k7);
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      const float dk7 = (float)(k7[i] - k1[i]);
-      ed[i] = (double)(hf * (T::E2 * S.dk2[i] + T::E3 * S.dk3[i] + T::E4 * S.dk4[i] +
-                             T::E5 * S.dk5[i] + T::E6 * S.dk6[i] + T::E7 * dk7));
-    }
-    const double m = wrms_sumsq<D>(ed, y, y5, a.rtol, a.atol);
-    if (!(m == m)) {
-      st = 1;
+  const long long rstride = 4 * a.n;
+  FwdCounters ct;
+  ct.t = a.t0;
+  ct.dt = a.dt0 > 0.0 ? a.dt0 : (t1 - a.t0) / 100.0;
+  ct.it = ct.acc = ct.rej = ct.st = ct.ck_cnt = ct.ck_slot = 0;
+  ct.rp = rec_on ? a.rec + j * 4 : nullptr;
+  if (ck_on) store_ckpt<D>(a.ckpt, a.n, j, 0, ya, ct.t);
+  F::rhs(ya, p, ka);
+  bool in_b = false;  // where the state is when the loop stops
+  for (;;) {
+    if (!mixed_attempt<F>(a, j, p, pf, t1, rec_on, ck_on, rstride, ct, ya, ca, ka, yb, cb, kb))
+      break;
+    if (!mixed_attempt<F>(a, j, p, pf, t1, rec_on, ck_on, rstride, ct, yb, cb, kb, ya, ca, ka)) {
+      in_b = true;
       break;
     }
-    if (m <= a.ctrl.accept_sum) {
-      if ((rec_on || ck_on) && acc >= a.cap) {
-        st = 3;
-        break;
-      }
-      t = t + h;
-#pragma unroll
-      for (int i = 0; i < D; ++i) { y[i] = y5[i]; c[i] = c5[i]; k1[i] = k7[i]; }
-      if (rec_on) a.rec[rec_index(j, acc, a.n)] = h;
-      ++acc;
-      if (ck_on && ++ck_cnt == a.ck_every) {
-        ck_cnt = 0;
-        if (++ck_slot < a.ck_slots) store_ckpt<D>(a.ckpt, a.n, j, ck_slot, y, t);
-      }
-    } else {
-      ++rej;
-    }
-    dt = step_from_sum<10>(m, h, a.ctrl);
   }
-  if (st == 0 && !(t >= t1)) st = 1;
+  if (ct.st == 0 && !(ct.t >= t1)) ct.st = 1;
   if (rec_on) {  // zero-pad the last sector (identity steps)
-    for (int s = acc; (s & 3) != 0; ++s) a.rec[rec_index(j, s, a.n)] = 0.0;
+    for (int s = ct.acc; (s & 3) != 0; ++s) ct.rp[s & 3] = 0.0;
   }
 #pragma unroll
-  for (int i = 0; i < D; ++i) a.yf[j * D + i] = y[i];
-  a.n_acc[j] = acc;
-  a.n_rej[j] = rej;
-  a.status[j] = st;
+  for (int i = 0; i < D; ++i) a.yf[j * D + i] = in_b ? yb[i] : ya[i];
+  a.n_acc[j] = ct.acc;
+  a.n_rej[j] = ct.rej;
+  a.status[j] = ct.st;
 }
 
 template <class F>

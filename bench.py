@@ -309,6 +309,52 @@ def _grad_err(g, ref):
             "rel_l2": rel_l2}
 
 
+def headline_checks(torch, engine, spec, r, gp, y0_np, rho_np, inv, dev, m: int = 64) -> dict:
+    """Checks of the timed run's own gradients on m trajectories drawn as the reference's
+    finite-difference test draws them (numpy default_rng(1).choice(n, m)):
+      * oracle: the C oracle's replay and reverse pass over the mesh the GPU recorded --
+        y_final of the replay against the GPU forward's, gradients against the adjoint's;
+      * fd: central differences of sum(y_final_j**2) w.r.t. rho_j, step 1e-6 * max(1, |rho_j|),
+        through the frozen mesh (the GPU replay of the same dts, never re-recorded), against
+        the adjoint's gradient of mean(y_final**2) rescaled to that loss; the error measure
+        max |g - fd| / max(|fd|, 1e-8) of tests/test_adjoint_replay.py:109-123 in the
+        reference."""
+    from oracle import oracle as O
+    O.build()
+    idx = np.random.default_rng(1).choice(r.n, m)
+    rows = torch.tensor(idx, device=dev)
+    dts = r.dts_rows(rows).contiguous()
+    dts_np = dts.cpu().numpy()
+    g = gp[rows].cpu().numpy()                    # d mean(y_final^2) / d rho_j
+    yf = r.y_final[rows].cpu().numpy()
+    y0s, ps = y0_np[idx], rho_np[idx]
+    yf_o = O.replay("tsit5", "lorenz", y0s, ps, dts_np)
+    _gy, g_o = O.replay_vjp("tsit5", "lorenz", y0s, ps, dts_np, (2.0 * inv) * yf)
+    rowrel = lambda a, b: np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-300)
+    q_y, q_g = rowrel(yf, yf_o), rowrel(g, g_o)
+    # frozen-mesh central differences with the GPU replay of the sampled rows
+    sub = engine.record_from_padded("tsit5", spec, dts, T0, checkpoint=1)
+    y0_t = torch.tensor(y0s, device=dev)
+    h = 1e-6 * np.maximum(np.abs(ps), 1.0)
+    y_mid = engine.replay(sub, y0_t, torch.tensor(ps, device=dev), write_ckpt=False)
+    y_p = engine.replay(sub, y0_t, torch.tensor(ps + h, device=dev), write_ckpt=False)
+    y_m = engine.replay(sub, y0_t, torch.tensor(ps - h, device=dev), write_ckpt=False)
+    y_p, y_m = y_p.cpu().numpy(), y_m.cpu().numpy()
+    fd = ((y_p ** 2).sum(axis=1) - (y_m ** 2).sum(axis=1))[:, None] / (2.0 * h)
+    g_sum = g / inv                               # d sum(y_final_j^2) / d rho_j
+    q_fd = np.abs(g_sum - fd).max(axis=1) / np.maximum(np.abs(fd).max(axis=1), 1e-8)
+    return {
+        "rows": m, "sampler": "numpy default_rng(1).choice(n, 64)",
+        "oracle": {"grad_rowrel_max": float(q_g.max()), "grad_rowrel_median": float(np.median(q_g)),
+                   "y_final_rowrel_max": float(q_y.max()),
+                   "within_1e-9": bool(q_g.max() <= 1e-9), "y_final_within_1e-10": bool(q_y.max() <= 1e-10)},
+        "fd": {"eps": "1e-6*max(1,|rho|)", "loss": "sum(y_final_j**2)", "mesh": "frozen (GPU replay)",
+               "rel_err_max": float(q_fd.max()), "rel_err_median": float(np.median(q_fd)),
+               "within_1e-6": bool(q_fd.max() <= 1e-6)},
+        "replay_equals_forward": bool(torch.equal(y_mid, r.y_final[rows])),
+    }
+
+
 def run_b200(args) -> None:
     import torch
     import torch.distributed as dist
@@ -382,6 +428,9 @@ def run_b200(args) -> None:
     acc = int(r.n_acc.to(torch.int64).sum().item())
     S = int(r.n_acc.max().item())
     K = r.ckpt_every
+    # the timed run's own gradients, checked on 64 sampled trajectories (oracle + FD)
+    checks = None if args.no_checks else headline_checks(torch, engine, spec, r, gp, y0_np,
+                                                         rho_np, inv, dev)
 
     # ---- the float32-stage variant on the same workload, and its accuracy ---------------
     mixed = None
@@ -547,6 +596,7 @@ def run_b200(args) -> None:
                    "l2": "flushed between timed steps (record traffic also >> L2)"},
         "gpu_launches": 2 * args.steps,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+        "parity_sample": checks,
         "fwd_ms": fwd_avg, "adj_ms": adj_avg, "mixed": mixed, "solve": solve or None,
         "fwd_ms_steps": [round(x, 3) for x in fwd_ms], "adj_ms_steps": [round(x, 3) for x in adj_ms],
     }
@@ -934,6 +984,8 @@ def main():
     ap.add_argument("--checkpoint", default="auto")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-checks", action="store_true",
+                    help="skip the oracle/FD checks of 64 sampled trajectories (outside timing)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-solve", action="store_true")

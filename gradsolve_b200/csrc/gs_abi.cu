@@ -433,26 +433,41 @@ __global__ void device_tableau_kernel(double* out) {
   for (int i = 0; i < 41; ++i) out[i] = v[i];
 }
 
+// One warp per trajectory: the lanes scan the padded row together (consecutive lanes read
+// consecutive dts, so each pass over a row is one coalesced 256-byte read), agree on the
+// last non-zero step with a warp maximum, then write the row's 4-step sectors, lane c taking
+// sector c (32 contiguous bytes read, one whole 32-byte sector written).  The caller has
+// checked S <= the record's capacity.
+constexpr unsigned kRowsPerBlock = kBlock / 32;
+
 __global__ void record_from_padded_kernel(long long n, long long S, const double* dts,
-                                          long long ld, double* rec, int cap, int* n_steps) {
-  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
+                                          long long ld, double* rec, int* n_steps) {
+  const long long j = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (j >= n) return;  // uniform across the warp: blockDim is a multiple of 32
   const double* row = dts + j * ld;
   long long last = 0;
-  for (long long s = 0; s < S; ++s)
+  for (long long s = lane; s < S; s += 32)
     if (row[s] != 0.0) last = s + 1;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const long long v = __shfl_xor_sync(0xffffffffu, last, o);
+    last = v > last ? v : last;
+  }
   const long long nch = (last + 3) / 4;
-  for (long long c = 0; c < nch; ++c) {
+  for (long long c = lane; c < nch; c += 32) {
     double v[4];
+#pragma unroll
     for (int q = 0; q < 4; ++q) {
       const long long s = c * 4 + q;
       v[q] = s < last ? row[s] : 0.0;
     }
     gs::store_rec_chunk(rec, n, j, (int)c, v[0], v[1], v[2], v[3]);
   }
-  n_steps[j] = (int)last;
-  (void)cap;
+  if (lane == 0) n_steps[j] = (int)last;
 }
+
+unsigned grid_rows(long long n) { return (unsigned)((n + kRowsPerBlock - 1) / kRowsPerBlock); }
 
 __global__ void record_to_padded_kernel(long long n, const double* rec, const int* n_acc,
                                         long long S, double* dts) {
@@ -673,8 +688,8 @@ int gs_record_from_padded(long long n, long long S, const double* dts, long long
     return fail(GS_ERR_ARG, "gs_record_from_padded: null buffer");
   if (!aligned16(rec)) return fail(GS_ERR_ARG, "gs_record_from_padded: rec must be 16-byte aligned");
   if (n == 0) return GS_OK;
-  record_from_padded_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(n, S, dts, ld, rec,
-                                                                               cap, n_steps);
+  record_from_padded_kernel<<<grid_rows(n), kBlock, 0, (cudaStream_t)stream>>>(n, S, dts, ld, rec,
+                                                                                n_steps);
   return cuda_check("record_from_padded_kernel");
 }
 
@@ -709,8 +724,15 @@ int gs_record_to_padded(long long n, int cap, const double* rec, const int* n_ac
 // stream capture.  Every call shares the one array and it keeps the contents of the last
 // call; nothing in it has to start at zero, because every region a call reads is written
 // earlier in the same call.  Calls that overlap on the GPU (on different streams of the
-// same device) race on the array and must be serialised by the caller.
+// same device) race on the array and must be serialised by the caller.  The looked-up
+// address is kept for the life of the process: resetting a device (cudaDeviceReset) after
+// the first call on it is not supported, since the array may move when the module reloads.
+//
+// Only libgsolve.so carries the array.  A generated field's library (compiled from this file
+// with GS_USER_FIELD_HEADER) exports the entry point as a stub that returns GS_ERR_FIELD, so
+// registering N fields does not hold N more arrays on every device.
 // ---------------------------------------------------------------------------------------
+#ifndef GS_USER_FIELD_HEADER
 namespace {
 
 __device__ __align__(256) unsigned char g_vjp_scratch[GS_STATIC_SCRATCH_BYTES];
@@ -747,7 +769,7 @@ int launch_tsit5_vjp_static(long long n, long long S, long long ld, const double
   int* n_steps = reinterpret_cast<int*>(base);
   double* rec = reinterpret_cast<double*>(base + off_rec);
   double* ckpt = reinterpret_cast<double*>(base + off_ckpt);
-  record_from_padded_kernel<<<grid_for(n), kBlock, 0, s>>>(n, S, dts, ld, rec, cap, n_steps);
+  record_from_padded_kernel<<<grid_rows(n), kBlock, 0, s>>>(n, S, dts, ld, rec, n_steps);
   int rc = cuda_check("record_from_padded_kernel");
   if (rc) return rc;
   gs::ReplayArgs ra{n, y0, p, t0, rec, n_steps, K, gs_ckpt_slots(cap, K), ckpt, y_final, cap};
@@ -775,8 +797,15 @@ extern "C" int gs_tsit5_vjp_static(int field, long long n, const double* y0, con
   if (!aligned8(y0) || !aligned8(p) || !aligned8(ybar) || !aligned8(y_final) ||
       (dts && !aligned8(dts)))
     return fail(GS_ERR_ARG, "gs_tsit5_vjp_static: float64 arrays must be 8-byte aligned");
-  if (S > (long long)INT32_MAX / 2)
-    return fail(GS_ERR_ARG, "gs_tsit5_vjp_static: S too large");
+  // refuse before any size product is formed, so none of them can wrap: the step counts
+  // alone take 4 bytes per trajectory and the record 8 bytes per step slot
+  constexpr long long kScratch = (long long)GS_STATIC_SCRATCH_BYTES;
+  if (n > kScratch / 4 || S > kScratch / 8 || n * (S > 0 ? S : 1) > kScratch / 8)
+    return fail(GS_ERR_ARG, "gs_tsit5_vjp_static: n=" + std::to_string(n) + ", S=" +
+                                std::to_string(S) + " does not fit: the static scratch holds " +
+                                std::to_string((size_t)GS_STATIC_SCRATCH_BYTES) +
+                                " bytes (use gs_tsit5_replay + gs_tsit5_adjoint with "
+                                "caller-allocated buffers for larger ensembles)");
   const int cap = S > 0 ? (int)S : 1;
   int K = 1;
   while ((long long)K * K < cap && K < gs::KMAX) ++K;  // ceil(sqrt(S)), at most KMAX
@@ -797,6 +826,15 @@ extern "C" int gs_tsit5_vjp_static(int field, long long n, const double* y0, con
                     gy0, gp, static_cast<unsigned char*>(base), cap, K, b_steps,
                     b_steps + b_rec, (cudaStream_t)stream)
 }
+#else   // a generated field's library: no static array, the entry point refuses
+extern "C" int gs_tsit5_vjp_static(int field, long long, const double*, const double*, double,
+                                   const double*, long long, long long, const double*, double*,
+                                   double*, double*, void*) {
+  return fail(GS_ERR_FIELD, "gs_tsit5_vjp_static: field " + std::to_string(field) +
+                                " is a generated field; the static-scratch entry point is "
+                                "served by libgsolve.so for its built-in fields only");
+}
+#endif  // GS_USER_FIELD_HEADER
 
 // ---------------------------------------------------------------------------------------
 // Dense output (saveat) on the replay, and its adjoint (gs_saveat.cuh).

@@ -251,7 +251,9 @@ int gs_record_to_padded(long long n, int cap, const double* rec, const int* n_ac
                         double* dts, void* stream);
 
 /* Size of the library's own device scratch used by gs_tsit5_vjp_static: 64 MiB, held by
- * every GPU that loads the library until the process exits. */
+ * every GPU that loads libgsolve.so until the process exits.  Only libgsolve.so carries it:
+ * the libraries built for generated fields (gradsolve_b200/fieldgen.py) export
+ * gs_tsit5_vjp_static as a stub that returns GS_ERR_FIELD and hold no such array. */
 #define GS_STATIC_SCRATCH_BYTES (64ull << 20)
 
 /*
@@ -268,9 +270,11 @@ int gs_record_to_padded(long long n, int cap, const double* rec, const int* n_ac
  * n * S <= 7.5e6 steps for the 3-state fields); larger problems return GS_ERR_ARG with the
  * numbers -- use the allocating entry points for them.
  * The first call on each device looks up the array's device address (cudaGetSymbolAddress,
- * with that device current); make that first call before any stream capture.  All calls
- * share the one array, which keeps the last call's contents: calls that overlap on the GPU
- * race and must be serialised by the caller.  Non-stiff (Tsit5) fields only.
+ * with that device current); make that first call before any stream capture.  The address
+ * is kept until the process exits, so resetting the device (cudaDeviceReset) after that
+ * first call is not supported.  All calls share the one array, which keeps the last call's
+ * contents: calls that overlap on the GPU race and must be serialised by the caller.
+ * Non-stiff (Tsit5) built-in fields only (GS_ERR_FIELD from a generated field's library).
  */
 int gs_tsit5_vjp_static(int field, long long n, const double* y0, const double* p, double t0,
                         const double* dts, long long S, long long ld, const double* ybar,

@@ -1,8 +1,8 @@
 """Recipe: build the reference's own hand-CUDA forward for the host, into oracle/_ref/.
 
 TEST INFRASTRUCTURE ONLY.  Reads the templates gradsolve/cuda/kernels/tsit5_template.cu.in
-and rosenbrock23_template.cu.in from the reference tree ($GRADSOLVE_REFERENCE, default
-/root/reference), fills them the way gradsolve/cuda/_codegen.py:32-55 and :65-100 do
+and rosenbrock23_template.cu.in from the reference tree ($GRADSOLVE_REFERENCE, default: a
+``reference`` directory beside the repository's root), fills them the way gradsolve/cuda/_codegen.py:32-55 and :65-100 do
 (str.replace of the scalar type, the tableau #defines taken from the reference's own
 tsit5_step.py / the Rosenbrock coefficients, the field bodies from the reference's own
 gradsolve/cuda/_fields.py and _stiff_fields.py, D and P), and compiles each with
@@ -23,7 +23,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REF = Path(os.environ.get("GRADSOLVE_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("GRADSOLVE_REFERENCE", HERE.parent.parent / "reference"))
 
 _A = ["A21", "A31", "A32", "A41", "A42", "A43", "A51", "A52", "A53", "A54", "A61", "A62", "A63",
       "A64", "A65"]

@@ -1,7 +1,8 @@
 """Generate the golden vectors under tests/golden/ from the reference's own code.
 
 Runs only where the reference source tree is present (it is read from
-``$GRADSOLVE_REFERENCE``, default ``/root/reference``); the GPU test runs never run this.
+``$GRADSOLVE_REFERENCE``, default: a ``reference`` directory beside the repository's root);
+the GPU test runs never run this.
 What it executes, verbatim, from the reference:
 
 * ``gradsolve/solvers/tsit5_step.py`` -- imported by file path (it has no imports), for
@@ -33,8 +34,8 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path(os.environ.get("GRADSOLVE_REFERENCE", "/root/reference"))
 OUT = Path(__file__).resolve().parent
+REF = Path(os.environ.get("GRADSOLVE_REFERENCE", OUT.parent.parent.parent / "reference"))
 
 
 def _load_module(path: Path, name: str):

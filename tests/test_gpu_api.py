@@ -94,6 +94,37 @@ def test_grad_closure_params_matches_oracle(oracle, cuda, remat):
     assert np.max(np.abs(p.grad.cpu().numpy() - ref_gp) / np.abs(ref_gp)) <= 1e-9
 
 
+def test_small_plain_config_through_grad_closure(oracle, cuda):
+    """The small plain configuration exactly: Lorenz (sigma = 10, beta = 8/3, rho the
+    parameter; the reference's 1-column diffeqgpu_lorenz problem), n = 1024, y0 = [1, 0, 0]
+    for all, rho = linspace(20, 30, n) as (n, 1), t in [0, 1], Tsit5 rtol = atol = 1e-8,
+    float64; forward solve plus the gradient of sum(y_final**2) w.r.t. rho through
+    grad_closure, against the oracle: the oracle's own adaptive solve (step counts exact,
+    y_final to 1e-10) and its reverse pass over the recorded mesh (1e-9)."""
+    import gradsolve_b200 as gsb
+    n = 1024
+    y0 = np.tile(np.array([1.0, 0.0, 0.0]), (n, 1))
+    rho = np.linspace(20.0, 30.0, n)[:, None]
+    res = gsb.solve(Lorenz(), y0, rho, rtol=1e-8, atol=1e-8, device="cuda")
+    ref = oracle.record("tsit5", "lorenz", y0, rho, 0.0, 1.0, 1e-8, 1e-8)
+    np.testing.assert_array_equal(res.accepted_steps, ref["n_acc"])
+    np.testing.assert_array_equal(res.rejected_steps, ref["n_rej"])
+    assert np.max(np.abs(res.y_final - ref["y_final"]) / np.abs(ref["y_final"])) <= 1e-10
+    clo = gsb.grad_closure(Lorenz(), y0, rho, rtol=1e-8, atol=1e-8, device="cuda")
+    p = torch.tensor(rho, device="cuda", requires_grad=True)
+    yf = clo(p)
+    (yf ** 2).sum().backward()
+    dts = clo.state.record.padded_dts().cpu().numpy()
+    ry = oracle.replay("tsit5", "lorenz", y0, rho, dts)
+    yfn = yf.detach().cpu().numpy()
+    assert np.max(np.abs(yfn - ry) / np.abs(ry)) <= 1e-10
+    _, rg = oracle.replay_vjp("tsit5", "lorenz", y0, rho, dts, 2.0 * ry)
+    assert np.max(np.abs(p.grad.cpu().numpy() - rg) / np.abs(rg)) <= 1e-9
+    # and against the oracle's gradient on its own recorded mesh (the reference's route)
+    _, rg2 = oracle.replay_vjp("tsit5", "lorenz", y0, rho, ref["dts"], 2.0 * ref["y_final"])
+    assert np.max(np.abs(p.grad.cpu().numpy() - rg2) / np.abs(rg2)) <= 1e-8
+
+
 @pytest.mark.parametrize("wrt", ["y0", ("y0", "params")])
 def test_grad_closure_y0_matches_fd(oracle, cuda, wrt):
     """Frozen-mesh FD of the y0 gradient, rel-L2 <= 1e-6 (tests/test_grad_closure_y0.py:145)."""

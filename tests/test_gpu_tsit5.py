@@ -133,7 +133,7 @@ def test_replay_of_reference_dts(gslib, oracle, cuda, case, field):
     assert rel(yf.cpu().numpy(), ref, 1e-12) <= 1e-10
 
 
-@pytest.mark.parametrize("checkpoint", [1, 3, 8, 64, "sqrt"])
+@pytest.mark.parametrize("checkpoint", [1, 2, 3, 8, 64, "sqrt"])
 @pytest.mark.parametrize("case,field", CASES)
 def test_adjoint_of_reference_dts(gslib, oracle, cuda, case, field, checkpoint):
     from gradsolve_b200 import engine
@@ -141,6 +141,28 @@ def test_adjoint_of_reference_dts(gslib, oracle, cuda, case, field, checkpoint):
     spec, r, y0, p, yf = _replay_reference_dts(cuda, field, g, checkpoint=checkpoint)
     ybar = 2.0 * yf
     gy0, gp = engine.adjoint(r, p, ybar)
+    torch.cuda.synchronize()
+    oy, op = oracle.replay_vjp("tsit5", field, g["y0"], g["params"], g["dts"], ybar.cpu().numpy())
+    assert rel(gy0.cpu().numpy(), oy, 1e-8) <= 1e-9
+    if not field.startswith("linear_"):
+        assert rel(gp.cpu().numpy(), op[:, : spec.nparam], 1e-8) <= 1e-9
+
+
+@pytest.mark.parametrize("variant", ["auto", "stages", "recompute"])
+@pytest.mark.parametrize("case,field", CASES)
+def test_adjoint_at_interval_two_vs_oracle(gslib, oracle, cuda, case, field, variant):
+    """K = 2, the interval the autotuner picks for the built-in fields: "auto" and "stages"
+    run the reverse pass with the segment length fixed at compile time
+    (tsit5_adjoint_stages_k2_kernel) wherever it keeps the general instance's residency,
+    "recompute" the recomputing kernel; each against the oracle's reverse pass on the
+    reference's own dts (rows with an odd step count end on a half-filled segment)."""
+    from gradsolve_b200 import engine
+    g = load_golden(case)
+    spec, r, y0, p, yf = _replay_reference_dts(cuda, field, g, checkpoint=2)
+    assert r.ckpt_every == 2
+    ybar = torch.linspace(-2.0, 3.0, yf.numel(), dtype=torch.float64,
+                          device=cuda).reshape(yf.shape) * yf
+    gy0, gp = engine.adjoint(r, p, ybar, variant=variant)
     torch.cuda.synchronize()
     oy, op = oracle.replay_vjp("tsit5", field, g["y0"], g["params"], g["dts"], ybar.cpu().numpy())
     assert rel(gy0.cpu().numpy(), oy, 1e-8) <= 1e-9

@@ -28,14 +28,15 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-8)))
 
 
-def _static_call(gslib, code, y0, p, dts, ybar):
+def _static_call(gslib, code, y0, p, dts, ybar, *, want_y0=True, want_p=True):
     n, S = dts.shape
     yf = torch.empty_like(y0)
-    gy0 = torch.empty_like(y0)
-    gp = torch.empty_like(p)
+    gy0 = torch.empty_like(y0) if want_y0 else None
+    gp = torch.empty_like(p) if want_p else None
     rc = gslib.lib().gs_tsit5_vjp_static(code, n, y0.data_ptr(), p.data_ptr(), 0.0,
                                          dts.data_ptr(), S, S, ybar.data_ptr(), yf.data_ptr(),
-                                         gy0.data_ptr(), gp.data_ptr(),
+                                         None if gy0 is None else gy0.data_ptr(),
+                                         None if gp is None else gp.data_ptr(),
                                          torch.cuda.current_stream().cuda_stream)
     gslib.check(rc, "gs_tsit5_vjp_static")
     return yf, gy0, gp
@@ -70,6 +71,53 @@ def test_static_vjp_matches_allocating_path_twice(gslib, cuda, cases):
         assert _rel(s_gp, a_gp) <= 1e-9
 
 
+@pytest.mark.parametrize("want", [(False, True), (True, False)])
+def test_static_vjp_with_one_gradient_left_out(gslib, cuda, want):
+    """gy0 or gp may be NULL: the other output is still the allocating path's."""
+    from gradsolve_b200.fields import field_spec
+    g = load_golden("lorenz_scale")
+    spec = field_spec("lorenz")
+    y0 = torch.tensor(g["y0"], device=cuda)
+    p = torch.tensor(g["params"][:, :1], device=cuda).contiguous()
+    dts = torch.tensor(g["dts"], device=cuda)
+    ybar = 2.0 * torch.ones_like(y0)
+    s_yf, s_gy0, s_gp = _static_call(gslib, spec.code, y0, p, dts, ybar, want_y0=want[0],
+                                     want_p=want[1])
+    a_yf, a_gy0, a_gp = _allocating_call("tsit5", "lorenz", y0, p, dts, ybar)
+    torch.cuda.synchronize()
+    assert _rel(s_yf, a_yf) <= 1e-10
+    if want[0]:
+        assert s_gp is None and _rel(s_gy0, a_gy0) <= 1e-9
+    else:
+        assert s_gy0 is None and _rel(s_gp, a_gp) <= 1e-9
+
+
+def test_static_vjp_long_record_takes_the_largest_interval(gslib, cuda):
+    """A record of more than 4096 steps: the entry point checkpoints every 64 steps (its
+    largest interval, ceil(sqrt(S)) capped), the shared-memory sizing of that segment length
+    included; twice in a row, the second call with another cotangent."""
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    spec = field_spec("lorenz")
+    rng = np.random.default_rng(7)
+    n = 48
+    y0 = torch.tensor(np.array([1.0, 0.0, 0.0]) + rng.normal(0.0, 0.1, (n, 3)), device=cuda)
+    p = torch.tensor(rng.uniform(20.0, 30.0, (n, 1)), device=cuda)
+    r = engine.forward_record("tsit5", spec, y0, p, t0=0.0, t1=70.0, rtol=1e-8, atol=1e-8,
+                              max_steps=100000)
+    dts = r.padded_dts().contiguous()
+    assert dts.shape[1] >= 4096
+    for scale in (1.0, -3.0):
+        ybar = scale * torch.linspace(-1.0, 2.0, y0.numel(), dtype=torch.float64,
+                                      device=cuda).reshape(y0.shape)
+        s_yf, s_gy0, s_gp = _static_call(gslib, spec.code, y0, p, dts, ybar)
+        a_yf, a_gy0, a_gp = _allocating_call("tsit5", "lorenz", y0, p, dts, ybar)
+        torch.cuda.synchronize()
+        assert _rel(s_yf, a_yf) <= 1e-10
+        assert _rel(s_gy0, a_gy0) <= 1e-9
+        assert _rel(s_gp, a_gp) <= 1e-9
+
+
 def test_static_vjp_refuses_sizes_beyond_its_scratch(gslib, cuda):
     n, S = 1 << 16, 4096  # a 2 GiB record: far beyond the 64 MiB scratch
     small = torch.zeros(8, dtype=torch.float64, device=cuda)
@@ -79,6 +127,21 @@ def test_static_vjp_refuses_sizes_beyond_its_scratch(gslib, cuda):
     assert rc == -1
     msg = gslib.lib().gs_last_error().decode()
     assert "static scratch holds" in msg and str(64 << 20) in msg
+    # sizes whose byte counts would overflow 64-bit products are refused before any is formed
+    for n, S in ((1 << 62, 1), (1, 1 << 62), (1 << 40, 1 << 30)):
+        rc = gslib.lib().gs_tsit5_vjp_static(1, n, small.data_ptr(), small.data_ptr(), 0.0,
+                                             small.data_ptr(), S, S, small.data_ptr(),
+                                             small.data_ptr(), None, None, None)
+        assert rc == -1 and "does not fit" in gslib.lib().gs_last_error().decode()
+
+
+def test_generated_field_libraries_carry_no_static_scratch():
+    """Only libgsolve.so holds the 64 MiB array; a generated field's library (gs_abi.cu built
+    with GS_USER_FIELD_HEADER) compiles the array out and refuses the entry point."""
+    src = (__import__("conftest").ROOT / "gradsolve_b200" / "csrc" / "gs_abi.cu").read_text()
+    decl = src.index("g_vjp_scratch[GS_STATIC_SCRATCH_BYTES]")
+    guard = src.rfind("#ifndef GS_USER_FIELD_HEADER", 0, decl)
+    assert guard >= 0 and src.find("#endif", guard, decl) < 0
 
 
 def test_static_scratch_size_is_declared(gslib):

@@ -37,7 +37,12 @@
  *            (absent from the reference's registry; reachable there only through
  *            register_jax_field, gradsolve/warp/jax_field.py:393-447)
  *   linear_D gradsolve/warp/_warp_kernel.py:133-155, dy = 1.01*y (p ignored)
+ *   lorenz96_D gradsolve/warp/_warp_kernel.py:175-195, dy_i = (y_{i+1} - y_{i-2}) y_{i-1}
+ *            - y_i + F, cyclic indices, p=[F], D >= 4
  *   robertson gradsolve/warp/_warp_rosenbrock.py:96-139, p=[k1,k2,k3]
+ *   hires    gradsolve/warp/_warp_rosenbrock.py:142-216 (HIRES-8, autonomous, p ignored)
+ *   linstiff gradsolve/warp/_warp_rosenbrock.py:219-252, f = A y with a constant D x D
+ *            matrix A (set by gso_set_linstiff; p ignored)
  */
 #include <math.h>
 #include <stdlib.h>
@@ -116,7 +121,19 @@ static double ROS_D, ROS_E32, ROS_EXP;
 #define MAXD 64
 #define MAXP 8
 
-enum { F_LORENZ = 1, F_VDP = 2, F_LV = 3, F_LINEAR = 4, F_ROBERTSON = 10, F_LORENZ3 = 11 };
+enum { F_LORENZ = 1, F_VDP = 2, F_LV = 3, F_LINEAR = 4, F_LORENZ96 = 5, F_ROBERTSON = 10,
+       F_LORENZ3 = 11, F_HIRES = 12, F_LINSTIFF = 13 };
+
+/* the constant matrix of the linstiff field (row-major, g_ls_D x g_ls_D) */
+static double g_ls_A[MAXD * MAXD];
+static int g_ls_D = 0;
+
+int gso_set_linstiff(int D, const double* A) {
+  if (D < 1 || D > MAXD) return -1;
+  memcpy(g_ls_A, A, sizeof(double) * (size_t)D * (size_t)D);
+  g_ls_D = D;
+  return 0;
+}
 
 typedef struct {
   int id, D, P;
@@ -132,8 +149,11 @@ static int field_make(int code, field_t* f) {
     case F_VDP: f->D = 2; f->P = 1; return 0;
     case F_LV: f->D = 2; f->P = 4; return 0;
     case F_LINEAR: if (D < 1 || D > MAXD) return -1; f->D = D; f->P = 1; return 0;
+    case F_LORENZ96: if (D < 4 || D > MAXD) return -1; f->D = D; f->P = 1; return 0;
     case F_ROBERTSON: f->D = 3; f->P = 3; return 0;
     case F_LORENZ3: f->D = 3; f->P = 3; return 0;
+    case F_HIRES: f->D = 8; f->P = 1; return 0;
+    case F_LINSTIFF: if (D < 1 || D != g_ls_D) return -1; f->D = D; f->P = 1; return 0;
   }
   return -1;
 }
@@ -166,12 +186,37 @@ static void rhs(const field_t* f, const double* y, const double* p, double* dy) 
     case F_LINEAR:
       for (int i = 0; i < f->D; ++i) dy[i] = 1.01 * y[i];
       break;
+    case F_LORENZ96: {
+      const int D = f->D;
+      for (int i = 0; i < D; ++i) {
+        const int ip1 = (i + 1) % D, im1 = (i - 1 + D) % D, im2 = (i - 2 + D) % D;
+        dy[i] = (y[ip1] - y[im2]) * y[im1] - y[i] + p[0];
+      }
+    } break;
     case F_ROBERTSON: {
       const double k1 = p[0], k2 = p[1], k3 = p[2];
       const double a = y[0], b = y[1], c = y[2];
       dy[0] = -k1 * a + k3 * b * c;
       dy[1] = k1 * a - k3 * b * c - k2 * b * b;
       dy[2] = k2 * b * b;
+    } break;
+    case F_HIRES:
+      dy[0] = -1.71 * y[0] + 0.43 * y[1] + 8.32 * y[2] + 0.0007;
+      dy[1] = 1.71 * y[0] - 8.75 * y[1];
+      dy[2] = -10.03 * y[2] + 0.43 * y[3] + 0.035 * y[4];
+      dy[3] = 8.32 * y[1] + 1.71 * y[2] - 1.12 * y[3];
+      dy[4] = -1.745 * y[4] + 0.43 * y[5] + 0.43 * y[6];
+      dy[5] = -280.0 * y[5] * y[7] + 0.69 * y[3] + 1.71 * y[4] - 0.43 * y[5] + 0.69 * y[6];
+      dy[6] = 280.0 * y[5] * y[7] - 1.81 * y[6];
+      dy[7] = -280.0 * y[5] * y[7] + 1.81 * y[6];
+      break;
+    case F_LINSTIFF: {
+      const int D = f->D;
+      for (int i = 0; i < D; ++i) {
+        double acc = 0.0;
+        for (int k = 0; k < D; ++k) acc += g_ls_A[i * D + k] * y[k];
+        dy[i] = acc;
+      }
     } break;
   }
 }
@@ -214,6 +259,36 @@ static void rhs_vjp(const field_t* f, const double* y, const double* p, const do
     case F_LINEAR:
       for (int i = 0; i < f->D; ++i) gy[i] += 1.01 * w[i];
       break;
+    case F_LORENZ96: {
+      const int D = f->D;
+      for (int i = 0; i < D; ++i) {
+        const int ip1 = (i + 1) % D, im1 = (i - 1 + D) % D, im2 = (i - 2 + D) % D;
+        gy[ip1] += y[im1] * w[i];
+        gy[im2] += -y[im1] * w[i];
+        gy[im1] += (y[ip1] - y[im2]) * w[i];
+        gy[i] += -w[i];
+        gp[0] += w[i];
+      }
+    } break;
+    case F_HIRES:
+      gy[0] += -1.71 * w[0] + 1.71 * w[1];
+      gy[1] += 0.43 * w[0] - 8.75 * w[1] + 8.32 * w[3];
+      gy[2] += 8.32 * w[0] - 10.03 * w[2] + 1.71 * w[3];
+      gy[3] += 0.43 * w[2] - 1.12 * w[3] + 0.69 * w[5];
+      gy[4] += 0.035 * w[2] - 1.745 * w[4] + 1.71 * w[5];
+      gy[5] += 0.43 * w[4] + (-280.0 * y[7] - 0.43) * w[5] + 280.0 * y[7] * w[6] -
+               280.0 * y[7] * w[7];
+      gy[6] += 0.43 * w[4] + 0.69 * w[5] - 1.81 * w[6] + 1.81 * w[7];
+      gy[7] += -280.0 * y[5] * w[5] + 280.0 * y[5] * w[6] - 280.0 * y[5] * w[7];
+      break;
+    case F_LINSTIFF: {
+      const int D = f->D;
+      for (int k = 0; k < D; ++k) {
+        double acc = 0.0;
+        for (int i = 0; i < D; ++i) acc += g_ls_A[i * D + k] * w[i];
+        gy[k] += acc;
+      }
+    } break;
     case F_ROBERTSON: {
       const double k1 = p[0], k2 = p[1], k3 = p[2];
       const double a = y[0], b = y[1], c = y[2];
@@ -247,6 +322,20 @@ static void jac(const field_t* f, const double* y, const double* p, double* J) {
     } break;
     case F_LINEAR:
       for (int i = 0; i < D; ++i) J[i * D + i] = 1.01;
+      break;
+    case F_HIRES:
+      J[0 * 8 + 0] = -1.71; J[0 * 8 + 1] = 0.43; J[0 * 8 + 2] = 8.32;
+      J[1 * 8 + 0] = 1.71; J[1 * 8 + 1] = -8.75;
+      J[2 * 8 + 2] = -10.03; J[2 * 8 + 3] = 0.43; J[2 * 8 + 4] = 0.035;
+      J[3 * 8 + 1] = 8.32; J[3 * 8 + 2] = 1.71; J[3 * 8 + 3] = -1.12;
+      J[4 * 8 + 4] = -1.745; J[4 * 8 + 5] = 0.43; J[4 * 8 + 6] = 0.43;
+      J[5 * 8 + 3] = 0.69; J[5 * 8 + 4] = 1.71; J[5 * 8 + 5] = -280.0 * y[7] - 0.43;
+      J[5 * 8 + 6] = 0.69; J[5 * 8 + 7] = -280.0 * y[5];
+      J[6 * 8 + 5] = 280.0 * y[7]; J[6 * 8 + 6] = -1.81; J[6 * 8 + 7] = 280.0 * y[5];
+      J[7 * 8 + 5] = -280.0 * y[7]; J[7 * 8 + 6] = 1.81; J[7 * 8 + 7] = -280.0 * y[5];
+      break;
+    case F_LINSTIFF:
+      memcpy(J, g_ls_A, sizeof(double) * (size_t)D * (size_t)D);
       break;
     default: {
       /* generic: J^T e_j columns through the VJP (used only by the stiff path on a
@@ -282,7 +371,11 @@ static void jac_contract_grad(const field_t* f, const double* y, const double* p
       gy[1] += -2.0 * mu * x * G[2];
       gp[0] += G[2] * (-2.0 * x * v - 1.0) + G[3] * (1.0 - x * x);
     } break;
-    default: break; /* constant Jacobian (linear) */
+    case F_HIRES:
+      gy[5] += -280.0 * G[5 * 8 + 7] + 280.0 * G[6 * 8 + 7] - 280.0 * G[7 * 8 + 7];
+      gy[7] += -280.0 * G[5 * 8 + 5] + 280.0 * G[6 * 8 + 5] - 280.0 * G[7 * 8 + 5];
+      break;
+    default: break; /* constant Jacobian (linear, linstiff) */
   }
 }
 

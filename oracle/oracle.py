@@ -28,15 +28,29 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libgs_oracle.so"
 
-# field codes shared with the C oracle (linear_D is 4000 + D)
-FIELDS = {"lorenz": 1, "vdp": 2, "lv": 3, "robertson": 10, "lorenz3": 11}
+# field codes shared with the C oracle (linear_D is 4000 + D, lorenz96_D 5000 + D, the
+# constant-matrix linstiff field 13000 + D with its matrix set by set_linstiff)
+FIELDS = {"lorenz": 1, "vdp": 2, "lv": 3, "robertson": 10, "lorenz3": 11, "hires": 12}
 METHODS = {"tsit5": 0, "rosenbrock23": 1}
 
 
 def field_code(name: str) -> int:
-    if name.startswith("linear_"):
-        return 4000 + int(name.split("_", 1)[1])
+    for prefix, base in (("linear_", 4000), ("lorenz96_", 5000), ("linstiff_", 13000)):
+        if name.startswith(prefix):
+            return base + int(name.rsplit("_", 1)[1])
     return FIELDS[name]
+
+
+def set_linstiff(A) -> str:
+    """Make the oracle's linstiff field f = A y (constant D x D matrix); returns its field
+    name ``linstiff_<D>`` for the calls that follow."""
+    A = np.ascontiguousarray(np.asarray(A, np.float64))
+    D = A.shape[0]
+    if A.shape != (D, D):
+        raise ValueError(f"linstiff matrix must be square, got {A.shape}")
+    if lib().gso_set_linstiff(D, _dp(A)):
+        raise ValueError(f"linstiff dimension {D} out of range")
+    return f"linstiff_{D}"
 
 
 def build() -> Path:
@@ -66,6 +80,7 @@ def lib():
                                      ctypes.c_double, dp, ctypes.c_long, dp, dp, dp, ctypes.c_int]
         L.gso_field_info.argtypes = [ctypes.c_int, ip, ip]
         L.gso_tsit5_error_weights.argtypes = [dp]
+        L.gso_set_linstiff.argtypes = [ctypes.c_int, dp]
         _LIB = L
     return _LIB
 
@@ -214,6 +229,19 @@ def torch_field(field):
     elif field.startswith("linear_"):
         def f(y, p):
             return 1.01 * y
+    elif field.startswith("lorenz96_"):
+        def f(y, p):
+            return ((torch.roll(y, -1, dims=1) - torch.roll(y, 2, dims=1)) *
+                    torch.roll(y, 1, dims=1) - y + p[:, :1])
+    elif field == "hires":
+        def f(y, p):
+            y0, y1, y2, y3, y4, y5, y6, y7 = (y[:, i] for i in range(8))
+            return torch.stack([
+                -1.71 * y0 + 0.43 * y1 + 8.32 * y2 + 0.0007, 1.71 * y0 - 8.75 * y1,
+                -10.03 * y2 + 0.43 * y3 + 0.035 * y4, 8.32 * y1 + 1.71 * y2 - 1.12 * y3,
+                -1.745 * y4 + 0.43 * y5 + 0.43 * y6,
+                -280.0 * y5 * y7 + 0.69 * y3 + 1.71 * y4 - 0.43 * y5 + 0.69 * y6,
+                280.0 * y5 * y7 - 1.81 * y6, -280.0 * y5 * y7 + 1.81 * y6], dim=1)
     elif field == "robertson":
         def f(y, p):
             k1, k2, k3 = p[:, 0], p[:, 1], p[:, 2]
@@ -285,7 +313,9 @@ def torch_replay_grad(method, field, y0, params, dts, ybar):
     dts_t = torch.tensor(np.asarray(dts, np.float64).reshape(y0_t.shape[0], -1))
     yf = torch_replay(method, field, y0_t, p_t, dts_t)
     loss = (yf * torch.tensor(np.asarray(ybar, np.float64).reshape(yf.shape))).sum()
-    gy0, gp = torch.autograd.grad(loss, [y0_t, p_t])
+    gy0, gp = torch.autograd.grad(loss, [y0_t, p_t], allow_unused=True)
+    if gp is None:  # a field that reads no parameter (linear, hires, linstiff)
+        gp = torch.zeros_like(p_t)
     return gy0.numpy(), gp.numpy()
 
 

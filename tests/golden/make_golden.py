@@ -93,6 +93,35 @@ def f_robertson(t, y, p):
                      k2 * y1 * y1], dtype=np.float64)
 
 
+def f_lorenz96(t, y, p):
+    # the reference's numpy form of its lorenz96 field (gradsolve/warp/_warp_kernel.py:175-182:
+    # roll(-1) / roll(2) / roll(1) are y_{i+1} / y_{i-2} / y_{i-1})
+    return (np.roll(y, -1) - np.roll(y, 2)) * np.roll(y, 1) - y + float(p[0])
+
+
+def f_hires(t, y, p):
+    # HIRES-8 in the operation order of gradsolve/warp/_warp_rosenbrock.py:164-184
+    y0, y1, y2, y3, y4, y5, y6, y7 = (float(v) for v in y)
+    return np.array([
+        -1.71 * y0 + 0.43 * y1 + 8.32 * y2 + 0.0007,
+        1.71 * y0 - 8.75 * y1,
+        -10.03 * y2 + 0.43 * y3 + 0.035 * y4,
+        8.32 * y1 + 1.71 * y2 - 1.12 * y3,
+        -1.745 * y4 + 0.43 * y5 + 0.43 * y6,
+        -280.0 * y5 * y7 + 0.69 * y3 + 1.71 * y4 - 0.43 * y5 + 0.69 * y6,
+        280.0 * y5 * y7 - 1.81 * y6,
+        -280.0 * y5 * y7 + 1.81 * y6], dtype=np.float64)
+
+
+def linstiff_matrix(D: int, seed: int) -> np.ndarray:
+    """A constant stiff operator A = Q diag(-lam) Q^T with eigenvalues spread over four
+    decades and a random orthogonal Q (numpy default_rng(seed))."""
+    rng = np.random.default_rng(seed)
+    Q, _ = np.linalg.qr(rng.normal(size=(D, D)))
+    lam = np.logspace(0.0, 4.0, D)
+    return -(Q * lam) @ Q.T
+
+
 def run_tsit5(tsit5_adaptive, f, y0, params, t0, t1, rtol, atol, max_steps=100000):
     n = y0.shape[0]
     dt0 = (t1 - t0) / 100.0
@@ -104,14 +133,15 @@ def run_tsit5(tsit5_adaptive, f, y0, params, t0, t1, rtol, atol, max_steps=10000
     return _pack(outs, y0, params, t0, t1, rtol, atol)
 
 
-def run_ros23(ros, f, y0, params, t0, t1, rtol, atol, max_steps=50000):
+def run_ros23(ros, f, y0, params, t0, t1, rtol, atol, max_steps=50000, jac=None):
     n = y0.shape[0]
     dt0 = (t1 - t0) / 100.0
+    jac = ros.robertson_jac if jac is None else jac
     outs = []
     for j in range(n):
         p = params[j]
         outs.append(ros.rosenbrock23_adaptive(
-            lambda t, y, p=p: f(t, y, p), lambda y, _p, p=p: ros.robertson_jac(y, p),
+            lambda t, y, p=p: f(t, y, p), lambda y, _p, p=p: jac(y, p),
             y0[j], t0, t1, rtol, atol, dt0, max_steps))
     return _pack(outs, y0, params, t0, t1, rtol, atol)
 
@@ -131,8 +161,49 @@ def _pack(outs, y0, params, t0, t1, rtol, atol):
         y_final=np.stack([np.asarray(o[0], dtype=np.float64) for o in outs]))
 
 
-def main():
+def family_cases(tsit5_adaptive, ros) -> dict:
+    """The reference's other fused-lane fields (gradsolve/warp/warp_ode.py:463-510 and
+    gradsolve/warp/warp_rosenbrock.py:221-254): lorenz96_<D> and linear_ladder_<D> on the
+    Tsit5 lane (D = 5 and 8 one thread per trajectory, 10 and 32 on a group of lanes), hires
+    and a constant-matrix linstiff field on the Rosenbrock23 lane."""
+    cases = {}
+    for D, n, seed in ((5, 4, 11), (8, 6, 12), (32, 6, 13)):
+        rng = np.random.default_rng(seed)
+        F = rng.uniform(7.5, 8.5, (n, 1))
+        y0 = F + rng.normal(0.0, 0.5, (n, D))
+        cases[f"lorenz96_{D}"] = run_tsit5(tsit5_adaptive, f_lorenz96, y0, F, 0.0, 2.0,
+                                           1e-8, 1e-8)
+    for D, n, seed in ((10, 3, 14), (32, 3, 15)):
+        rng = np.random.default_rng(seed)
+        y0 = rng.uniform(-2.0, 2.0, (n, D))
+        cases[f"linear_{D}"] = run_tsit5(tsit5_adaptive, f_linear, y0, np.zeros((n, 1)), 0.0,
+                                         4.0, 1e-10, 1e-10)
+    # HIRES: the standard start (Hairer & Wanner IV.10) with its first and last components
+    # scaled by 1 + U(-0.1, 0.1) per trajectory, t in [0, 321.8122]
+    rng = np.random.default_rng(16)
+    n = 4
+    y0 = np.tile(np.array([1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0057]), (n, 1))
+    y0[:, 0] *= 1.0 + rng.uniform(-0.1, 0.1, n)
+    y0[:, 7] *= 1.0 + rng.uniform(-0.1, 0.1, n)
+    cases["hires"] = run_ros23(ros, f_hires, y0, np.zeros((n, 1)), 0.0, 321.8122, 1e-6, 1e-10,
+                               jac=ros.hires_jac)
+    for D, seed in ((4, 17), (8, 18)):
+        A = linstiff_matrix(D, seed)
+        rng = np.random.default_rng(seed + 100)
+        y0 = rng.uniform(-1.0, 1.0, (3, D))
+        c = run_ros23(ros, lambda t, y, p, A=A: A @ y, y0, np.zeros((3, 1)), 0.0, 1.0, 1e-6,
+                      1e-9, jac=ros.constant_jac(A))
+        c["A"] = A
+        cases[f"linstiff_{D}"] = c
+    return cases
+
+
+def main(only=None):
     ts, tsit5_adaptive, ros = load_reference()
+    if only:  # regenerate just the named cases (the others are deterministic and kept)
+        cases = {k: v for k, v in family_cases(tsit5_adaptive, ros).items() if k in only}
+        _save(cases)
+        return 0
     cases = {}
 
     # tableau, as the reference module evaluates it
@@ -198,6 +269,12 @@ def main():
     cases["robertson_stiff"] = run_ros23(ros, f_robertson, y0, kk[rows], 0.0, 1.0e4, 1e-6, 1e-10)
     cases["robertson_stiff"]["rows"] = rows
 
+    cases.update(family_cases(tsit5_adaptive, ros))
+    _save(cases)
+    return 0
+
+
+def _save(cases):
     for name, d in cases.items():
         np.savez_compressed(OUT / f"{name}.npz", **d)
         print(f"{name}: n={d['y0'].shape[0]} S={d['dts'].shape[1]} "
@@ -206,4 +283,4 @@ def main():
 
 
 if __name__ == "__main__":
-    sys.exit(main())
+    sys.exit(main(sys.argv[1:]))

@@ -7,7 +7,7 @@ ABI of ``libgsolve.so`` (include/gsolve.h); PyTorch provides device memory, stre
 autograd plumbing.
 """
 from .api import (ALIASES, ENGINE_REGISTRY, grad_closure, register_field,  # noqa: F401
-                  register_jax_field, solve)
+                  register_jax_field, register_linstiff, solve)
 from .base import Problem, Route, SolveResult  # noqa: F401
 from .fields import field_for, field_spec  # noqa: F401
 

@@ -96,12 +96,22 @@ def lib():
 
 def lib_for(spec):
     """The library that serves a field: libgsolve.so, or a generated field's own library
-    (same C ABI, built by gradsolve_b200.fieldgen)."""
+    (same C ABI, built by gradsolve_b200.fieldgen; a built-in family member at a dimension
+    the core library does not carry is compiled here on first use).  Fields beyond the fused
+    lanes' dimension limit are refused before any launch."""
+    from .fields import MAX_DIM, dim_limit_message
+    if spec.dim > MAX_DIM:
+        raise RuntimeError(dim_limit_message(spec.dim))
     path = getattr(spec, "lib", "")
     if not path:
         return lib()
     L = _FIELD_LIBS.get(path)
     if L is None:
+        if spec.family and not Path(path).exists():
+            from . import fieldgen
+            built = fieldgen.family_library(*spec.family)
+            if str(built) != path:
+                raise RuntimeError(f"field library {built} is not the expected {path}")
         L = _FIELD_LIBS[path] = _load(path)
     return L
 

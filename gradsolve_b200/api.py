@@ -30,7 +30,7 @@ import torch
 from . import engine
 from . import engine as engine_mod
 from .base import Route, SolveResult
-from .fields import FieldSpec, field_for, kernel_params
+from .fields import MAX_DIM, FieldSpec, dim_limit_message, field_for, kernel_params
 from .torch_adapter import ReplayState, replay_apply, saveat_apply
 
 ENGINE_TSIT5 = "b200_tsit5"
@@ -88,7 +88,10 @@ def _require_field(problem) -> FieldSpec:
         raise ValueError(
             f"gradsolve_b200 has no registered field for problem {getattr(problem, 'name', '?')!r}"
             "; supported names: 'diffeqgpu_lorenz', 'lorenz', 'vdp', 'lotka_volterra', "
-            "'linear_ladder_<D>' (D in 1,2,3,4,8), 'robertson'")
+            "'linear_ladder_<D>', 'lorenz96_<D>' (D >= 4), 'robertson', 'hires', and names "
+            "given to register_field / register_jax_field / register_linstiff")
+    if spec.dim > MAX_DIM:
+        raise RuntimeError(dim_limit_message(spec.dim))
     return spec
 
 
@@ -341,7 +344,8 @@ for _name in list(ENGINE_REGISTRY):
     ENGINE_REGISTRY[_name] = EngineSpec(_s.name, _s.method, _s.supports, _engine_solve(_name),
                                         _make_reverse(_name))
 
-__all__ = ["solve", "grad_closure", "ENGINE_REGISTRY", "ALIASES", "FieldSpec"]
+__all__ = ["solve", "grad_closure", "register_field", "register_jax_field", "register_linstiff",
+           "ENGINE_REGISTRY", "ALIASES", "FieldSpec"]
 
 
 def register_field(name: str, f, dim: int, n_params: int, *, stiff: bool = False) -> FieldSpec:
@@ -358,6 +362,8 @@ def register_field(name: str, f, dim: int, n_params: int, *, stiff: bool = False
     from . import fields as F
     if name in F._USER:
         return F._USER[name]
+    if int(dim) > MAX_DIM:
+        raise RuntimeError(dim_limit_message(int(dim)))
     d = fieldgen.Derived(f, dim, n_params, stiff)
     code = fieldgen.USER_CODE_BASE + (sum(name.encode()) * 7919) % 90000
     path = fieldgen.build_field_library(fieldgen.emit_struct(d, name, code))
@@ -369,3 +375,35 @@ def register_field(name: str, f, dim: int, n_params: int, *, stiff: bool = False
 # the reference's name for the same registration (its f is a JAX function; here any
 # function of symbolic scalars: Python arithmetic, numpy ufuncs, gradsolve_b200.fieldgen)
 register_jax_field = register_field
+
+
+def register_linstiff(key: str, A) -> FieldSpec:
+    """Register the constant-matrix linear stiff field f(y) = A y under ``key`` (a
+    ``linstiff_*`` name by the reference's convention), so a Problem of that name routes to
+    the Rosenbrock23 engine (and the Tsit5 one).  The reference's
+    ``warp_rosenbrock.register_linstiff(key, A)`` (gradsolve/warp/warp_rosenbrock.py:88-95,
+    gradsolve/warp/_warp_rosenbrock.py:219-252): A is (D, D), baked into the field as exact
+    constants, Jacobian = A, parameters ignored; idempotent per key.  The field is generated
+    like any registered one (its own library; zero entries of A are left out of the sums)."""
+    from . import fields as F
+    if key in F._USER:
+        return F._USER[key]
+    A = np.asarray(A, dtype=np.float64)
+    if A.ndim != 2 or A.shape[0] != A.shape[1]:
+        raise ValueError(f"linstiff A must be square (D, D); got {A.shape}")
+    if not np.all(np.isfinite(A)):
+        raise ValueError("linstiff A must be finite")
+    rows = [[float(v) for v in row] for row in A]
+    D = len(rows)
+
+    def f(t, y, p):
+        out = []
+        for i in range(D):
+            acc = 0.0
+            for k in range(D):
+                if rows[i][k] != 0.0:
+                    acc = acc + rows[i][k] * y[k]
+            out.append(acc)
+        return out
+
+    return register_field(key, f, D, 0, stiff=True)

@@ -11,6 +11,7 @@
 #include <string>
 
 #include "../../include/gsolve.h"
+#include "gs_coop.cuh"
 #include "gs_fields.cuh"
 #include "gs_mixed.cuh"
 #include "gs_ros23.cuh"
@@ -90,6 +91,12 @@ int field_dims(int field, int* D, int* P) {
     case 4003: *D = 3; *P = 1; return GS_OK;
     case 4004: *D = 4; *P = 1; return GS_OK;
     case 4008: *D = 8; *P = 1; return GS_OK;
+    case 4010: *D = 10; *P = 1; return GS_OK;
+    case 4032: *D = 32; *P = 1; return GS_OK;
+    case 5004: *D = 4; *P = 1; return GS_OK;
+    case 5008: *D = 8; *P = 1; return GS_OK;
+    case 5032: *D = 32; *P = 1; return GS_OK;
+    case gs::FIELD_HIRES: *D = 8; *P = 1; return GS_OK;
   }
   return fail(GS_ERR_FIELD, "unknown field code " + std::to_string(field));
 }
@@ -107,6 +114,12 @@ int field_dims(int field, int* D, int* P) {
     case 4003: return FN<gs::Linear<3>>(__VA_ARGS__);                                       \
     case 4004: return FN<gs::Linear<4>>(__VA_ARGS__);                                       \
     case 4008: return FN<gs::Linear<8>>(__VA_ARGS__);                                       \
+    case 4010: return FN<gs::Linear<10>>(__VA_ARGS__);                                      \
+    case 4032: return FN<gs::Linear<32>>(__VA_ARGS__);                                      \
+    case 5004: return FN<gs::Lorenz96<4>>(__VA_ARGS__);                                     \
+    case 5008: return FN<gs::Lorenz96<8>>(__VA_ARGS__);                                     \
+    case 5032: return FN<gs::Lorenz96<32>>(__VA_ARGS__);                                    \
+    case gs::FIELD_HIRES: return FN<gs::Hires>(__VA_ARGS__);                                \
     default: return fail(GS_ERR_FIELD, "unknown field code " + std::to_string(field));      \
   }
 
@@ -120,6 +133,7 @@ int field_dims(int field, int* D, int* P) {
     case 4003: return FN<gs::Linear<3>>(__VA_ARGS__);                                       \
     case 4004: return FN<gs::Linear<4>>(__VA_ARGS__);                                       \
     case 4008: return FN<gs::Linear<8>>(__VA_ARGS__);                                       \
+    case gs::FIELD_HIRES: return FN<gs::Hires>(__VA_ARGS__);                                \
     default:                                                                                \
       return fail(GS_ERR_FIELD,                                                             \
                   "field " + std::to_string(field) + " has no analytic Jacobian for Rosenbrock23"); \
@@ -285,9 +299,69 @@ int launch_adjoint_persistent(const gs::AdjointArgs& a, int cap, cudaStream_t s,
   return cuda_check("adjoint_persistent_kernel");
 }
 
+// ---- fields integrated by a group of lanes per trajectory (gs_coop.cuh) ----------------------
+// Their D > 8 states run one group of lanes per trajectory in float64, one trajectory per
+// group (the schedule flags do not apply); the float32-stage mode, the dense output and the
+// static-scratch entry point are not built for them and refuse with GS_ERR_PRECISION /
+// GS_ERR_FIELD.
+template <class F>
+constexpr bool kCoop = gs::group_of<F>::value > 1;
+
+template <class F>
+int coop_refuse(const char* what) {
+  return fail(GS_ERR_FIELD, std::string(what) + " is not built for fields of more than 8 "
+                                "components (D = " + std::to_string(F::D) +
+                                ", integrated by a group of lanes per trajectory)");
+}
+
+int coop_refuse_mixed() {
+  return fail(GS_ERR_PRECISION, "the float32-stage mode is not built for fields of more than 8 "
+                                "components");
+}
+
+template <class F>
+int launch_coop_record(const gs::RecordArgs& a_in, cudaStream_t s, bool mixed) {
+  constexpr int G = gs::group_of<F>::value;
+  if (mixed) return coop_refuse_mixed();
+  gs::RecordArgs a = a_in;
+  a.ctrl = gs::make_ctrl_consts(F::D, 10);
+  const unsigned grid = grid_for(a.n * G);
+  if (!a.rec && !a.ckpt)
+    gs::tsit5_coop_record_kernel<F, G, false><<<grid, kBlock, 0, s>>>(a);
+  else
+    gs::tsit5_coop_record_kernel<F, G, true><<<grid, kBlock, 0, s>>>(a);
+  return cuda_check("tsit5_coop_record_kernel");
+}
+
+template <class F>
+int launch_coop_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed) {
+  constexpr int G = gs::group_of<F>::value;
+  if (mixed) return coop_refuse_mixed();
+  gs::tsit5_coop_replay_kernel<F, G><<<grid_for(a.n * G), kBlock, 0, s>>>(a);
+  return cuda_check("tsit5_coop_replay_kernel");
+}
+
+template <class F>
+int launch_coop_adjoint(const gs::AdjointArgs& a, cudaStream_t s, bool mixed) {
+  constexpr int G = gs::group_of<F>::value;
+  constexpr int C = F::D / G;
+  if (mixed) return coop_refuse_mixed();
+  SegCfg c;
+  int rc;
+  if ((rc = occupancy_cfg(gs::tsit5_coop_adjoint_kernel<F, G>,
+                          gs::adjoint_smem_doubles<C>(a.ck_every), &c)))
+    return rc;
+  gs::tsit5_coop_adjoint_kernel<F, G><<<grid_for_block(a.n * G, c.block), c.block, c.smem, s>>>(a);
+  return cuda_check("tsit5_coop_adjoint_kernel");
+}
+
 // mixed = float32 stages (GS_PREC_MIXED, gs_mixed.cuh), else float64 throughout.
 template <class F>
 int launch_tsit5_record(const gs::RecordArgs& a_in, cudaStream_t s, bool mixed, int sched) {
+  if constexpr (kCoop<F>) {
+    (void)sched;
+    return launch_coop_record<F>(a_in, s, mixed);
+  } else {
   gs::RecordArgs a = a_in;
   a.ctrl = gs::make_ctrl_consts(F::D, 10);  // Tsit5: err^(-1/5) = m^(-1/10)
   if (sched == GS_SCHED_STATIC) {
@@ -304,19 +378,28 @@ int launch_tsit5_record(const gs::RecordArgs& a_in, cudaStream_t s, bool mixed, 
   const bool counter = sched == GS_SCHED_REFILL;
   return mixed ? launch_record_persistent<F, gs::LaneTsit5Mixed<F>>(a, s, counter)
                : launch_record_persistent<F, gs::LaneTsit5F64<F>>(a, s, counter);
+  }
 }
 template <class F>
 int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed) {
+  if constexpr (kCoop<F>) {
+    return launch_coop_replay<F>(a, s, mixed);
+  } else {
   if (mixed) {
     gs::tsit5_mixed_replay_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
     return cuda_check("tsit5_mixed_replay_kernel");
   }
   gs::tsit5_replay_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
   return cuda_check("tsit5_replay_kernel");
+  }
 }
 template <class F>
 int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool mixed,
                          int sched, int variant) {
+  if constexpr (kCoop<F>) {
+    (void)cap; (void)sched; (void)variant;
+    return launch_coop_adjoint<F>(a, s, mixed);
+  } else {
   if (sched == GS_SCHED_STATIC) {
     int rc;
     if (!mixed) {
@@ -329,12 +412,16 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
       const int sd = gs::adjoint_stages_smem_doubles<F::D>(a.ck_every);
       if (variant != GS_ADJ_RECOMPUTE) {
         if ((rc = occupancy_probe(stages, sd, &ck))) return rc;
-        if (a.ck_every == 2) {
-          SegCfg c2{0, 0, 0};
-          if ((rc = occupancy_probe(gs::tsit5_adjoint_stages_k2_kernel<F>, sd, &c2))) return rc;
-          if (c2.resident > 0 && c2.resident >= ck.resident) {
-            stages = gs::tsit5_adjoint_stages_k2_kernel<F>;
-            ck = c2;
+        // (only small states: the instance's register bound would spill an 8-state field's)
+        if constexpr (F::D <= 4) {
+          if (a.ck_every == 2) {
+            SegCfg c2{0, 0, 0};
+            if ((rc = occupancy_probe(gs::tsit5_adjoint_stages_k2_kernel<F>, sd, &c2)))
+              return rc;
+            if (c2.resident > 0 && c2.resident >= ck.resident) {
+              stages = gs::tsit5_adjoint_stages_k2_kernel<F>;
+              ck = c2;
+            }
           }
         }
       }
@@ -363,6 +450,7 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
   const bool counter = sched == GS_SCHED_REFILL;
   return mixed ? launch_adjoint_persistent<F, gs::Tsit5MixedStep>(a, cap, s, counter)
                : launch_adjoint_persistent<F, gs::Tsit5F64Step>(a, cap, s, counter);
+  }
 }
 template <class F>
 int launch_ros23_record(const gs::RecordArgs& a_in, cudaStream_t s, int sched) {
@@ -395,14 +483,18 @@ int launch_ros23_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, int 
       return rc;
     if (keeping_pays(ck, cr)) {
       auto keep = gs::ros23_adjoint_kernel<F, true>;
-      if (a.ck_every == 2) {  // the unrolled instance, where it keeps the residency
-        SegCfg c2{0, 0, 0};
-        if ((rc = occupancy_probe(gs::ros23_adjoint_k2_kernel<F>,
-                                  gs::ros23_adjoint_smem_doubles<F::D, true>(2), &c2)))
-          return rc;
-        if (c2.resident > 0 && c2.resident >= ck.resident) {
-          keep = gs::ros23_adjoint_k2_kernel<F>;
-          ck = c2;
+      // the unrolled instance, where it keeps the residency (small states only: its register
+      // bound would spill an 8-state field's)
+      if constexpr (F::D <= 4) {
+        if (a.ck_every == 2) {
+          SegCfg c2{0, 0, 0};
+          if ((rc = occupancy_probe(gs::ros23_adjoint_k2_kernel<F>,
+                                    gs::ros23_adjoint_smem_doubles<F::D, true>(2), &c2)))
+            return rc;
+          if (c2.resident > 0 && c2.resident >= ck.resident) {
+            keep = gs::ros23_adjoint_k2_kernel<F>;
+            ck = c2;
+          }
         }
       }
       if ((rc = allow_smem(keep, ck.smem))) return rc;
@@ -766,6 +858,9 @@ int launch_tsit5_vjp_static(long long n, long long S, long long ld, const double
                             const double* p, double t0, const double* dts, const double* ybar,
                             double* y_final, double* gy0, double* gp, unsigned char* base,
                             int cap, int K, size_t off_rec, size_t off_ckpt, cudaStream_t s) {
+  if constexpr (kCoop<F>) {
+    return coop_refuse<F>("gs_tsit5_vjp_static");
+  } else {
   int* n_steps = reinterpret_cast<int*>(base);
   double* rec = reinterpret_cast<double*>(base + off_rec);
   double* ckpt = reinterpret_cast<double*>(base + off_ckpt);
@@ -780,6 +875,7 @@ int launch_tsit5_vjp_static(long long n, long long S, long long ld, const double
   if ((rc = allow_smem(gs::tsit5_adjoint_kernel<F>, c.smem))) return rc;
   gs::tsit5_adjoint_kernel<F><<<grid_for_block(n, c.block), c.block, c.smem, s>>>(aa);
   return cuda_check("tsit5_adjoint_kernel");
+  }
 }
 
 }  // namespace
@@ -884,8 +980,12 @@ int launch_saveat_sched(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint, i
 template <class F>
 int launch_saveat_tsit5(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint, bool mixed,
                         int sched) {
-  return mixed ? launch_saveat_sched<F, gs::Tsit5MixedStep>(a, s, adjoint, sched)
-               : launch_saveat_sched<F, gs::Tsit5F64Step>(a, s, adjoint, sched);
+  if constexpr (kCoop<F>) {
+    return coop_refuse<F>("the dense output (saveat)");
+  } else {
+    return mixed ? launch_saveat_sched<F, gs::Tsit5MixedStep>(a, s, adjoint, sched)
+                 : launch_saveat_sched<F, gs::Tsit5F64Step>(a, s, adjoint, sched);
+  }
 }
 
 template <class F>
@@ -929,8 +1029,12 @@ int launch_fwd_lanes(const gs::RecordArgs& a_in, cudaStream_t s, FwdLanes lanes)
 
 template <class F>
 int launch_fwd_saveat_tsit5(const gs::RecordArgs& a, cudaStream_t s, bool mixed, FwdLanes lanes) {
-  return mixed ? launch_fwd_lanes<F, gs::LaneTsit5Mixed<F>>(a, s, lanes)
-               : launch_fwd_lanes<F, gs::LaneTsit5F64<F>>(a, s, lanes);
+  if constexpr (kCoop<F>) {
+    return coop_refuse<F>("the dense output (saveat)");
+  } else {
+    return mixed ? launch_fwd_lanes<F, gs::LaneTsit5Mixed<F>>(a, s, lanes)
+                 : launch_fwd_lanes<F, gs::LaneTsit5F64<F>>(a, s, lanes);
+  }
 }
 
 template <class F>

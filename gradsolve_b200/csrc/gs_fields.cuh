@@ -14,6 +14,20 @@
 //              counterpart of that generated field.
 //   Robertson  gradsolve/warp/_warp_rosenbrock.py:96-139 (p = [k1, k2, k3]); the analytic
 //              Jacobian is the one of _warp_rosenbrock.py:121-137.
+//   Lorenz96<D> gradsolve/warp/_warp_kernel.py:175-195: dy_i = (y_{i+1} - y_{i-2}) y_{i-1}
+//              - y_i + F, cyclic indices, p = [F], D >= 4 (the reference's lorenz96_<D>)
+//   Hires      gradsolve/warp/_warp_rosenbrock.py:142-216: HIRES-8 (Hairer & Wanner IV.10),
+//              autonomous, p ignored; analytic Jacobian as in :186-214.
+//
+// Fields that can be integrated by a group of lanes (D > 8: Linear<D>, Lorenz96<D>) also
+// give their right-hand side and VJP on a contiguous block of components, with the few
+// neighbouring components they read (a cyclic stencil) passed in beside the block:
+//   RHS_LO, RHS_HI                 components below / above the block rhs_block reads
+//   rhs_block<C>(yb, p, dy)        yb[RHS_LO + k] = y_{i0+k}, k in [-RHS_LO, C + RHS_HI);
+//                                  dy[k] = f_{i0+k}(y, p), k < C
+//   VJP_YLO, VJP_YHI, VJP_WLO, VJP_WHI, and
+//   vjp_block<C>(yb, wb, p, gy, gp) gy[k] += ((df/dy)^T w)_{i0+k}; gp += the block's share of
+//                                  (df/dp)^T w (the shares of all blocks sum to it)
 //
 // Contract of each field F (R = double or float):
 //   rhs(y, p, dy)                 dy = f(y, p)           (all fields are autonomous)
@@ -33,10 +47,32 @@ enum FieldId : int {
   FIELD_LORENZ = 1,
   FIELD_VDP = 2,
   FIELD_LOTKA_VOLTERRA = 3,
-  FIELD_LINEAR = 4,  // the ABI passes FIELD_LINEAR * 1000 + D
+  FIELD_LINEAR = 4,     // the ABI passes FIELD_LINEAR * 1000 + D
+  FIELD_LORENZ96 = 5,   // the ABI passes FIELD_LORENZ96 * 1000 + D
   FIELD_ROBERTSON = 10,
   FIELD_LORENZ3 = 11,
+  FIELD_HIRES = 12,
 };
+
+// Largest state dimension of the fused lanes (the reference refuses larger ones before
+// launch on the GPU: _GPU_VEC_DIM_CEILING, gradsolve/warp/warp_ode.py:75-81).
+constexpr int kMaxDim = 64;
+
+// Lanes that share one trajectory for a field of dimension D: 1 up to D = 8; above, the
+// smallest power of two G with D = G*C and C <= 4 components per lane, else the largest one
+// with C >= 2 (a stencil reaches two components into the neighbouring lane's block), else 1
+// (odd D: one thread per trajectory).
+constexpr int coop_group(int D) {
+  if (D <= 8) return 1;
+  int best = 1;
+  for (int g = 2; g <= 32; g *= 2) {
+    if (D % g == 0 && D / g >= 2) {
+      best = g;
+      if (D / g <= 4) return g;
+    }
+  }
+  return best;
+}
 
 struct Lorenz {
   static constexpr int D = 3, P = 1;
@@ -168,6 +204,19 @@ struct LotkaVolterra {
 template <int DD>
 struct Linear {
   static constexpr int D = DD, P = 1;
+  static constexpr int GROUP = coop_group(DD);
+  static constexpr int RHS_LO = 0, RHS_HI = 0, VJP_YLO = 0, VJP_YHI = 0, VJP_WLO = 0,
+                       VJP_WHI = 0;
+  template <int C, class R>
+  static GS_HD void rhs_block(const R* yb, const R*, R* dy) {
+#pragma unroll
+    for (int k = 0; k < C; ++k) dy[k] = R(1.01) * yb[k];
+  }
+  template <int C, class R>
+  static GS_HD void vjp_block(const R*, const R* wb, const R*, R* gy, R*) {
+#pragma unroll
+    for (int k = 0; k < C; ++k) gy[k] += R(1.01) * wb[k];
+  }
   template <class R>
   static GS_HD void rhs(const R* y, const R*, R* dy) {
 #pragma unroll
@@ -192,6 +241,130 @@ struct Linear {
   }
   template <class R>
   static GS_HD void jac_contract_grad(const R*, const R*, const R*, R*, R*) {}
+};
+
+template <int DD>
+struct Lorenz96 {
+  static_assert(DD >= 4, "lorenz96 needs D >= 4 (four distinct stencil components)");
+  static constexpr int D = DD, P = 1;
+  static constexpr int GROUP = coop_group(DD);
+  static constexpr int RHS_LO = 2, RHS_HI = 1, VJP_YLO = 2, VJP_YHI = 2, VJP_WLO = 1,
+                       VJP_WHI = 2;
+  // (y_{i+1} - y_{i-2}) * y_{i-1} - y_i + F, the reference's operation order
+  template <int C, class R>
+  static GS_HD void rhs_block(const R* yb, const R* p, R* dy) {
+#pragma unroll
+    for (int k = 0; k < C; ++k) dy[k] = (yb[k + 3] - yb[k]) * yb[k + 1] - yb[k + 2] + p[0];
+  }
+  // ((df/dy)^T w)_j = w_{j-1} y_{j-2} - w_{j+2} y_{j+1} + w_{j+1} (y_{j+2} - y_{j-1}) - w_j;
+  // d f_i / dF = 1
+  template <int C, class R>
+  static GS_HD void vjp_block(const R* yb, const R* wb, const R*, R* gy, R* gp) {
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+      const R* y = yb + k + 2;  // y[d] = y_{j+d}
+      const R* w = wb + k + 1;  // w[d] = w_{j+d}
+      gy[k] += w[-1] * y[-2] - w[2] * y[1] + w[1] * (y[2] - y[-1]) - w[0];
+      gp[0] += w[0];
+    }
+  }
+  template <class R>
+  static GS_HD void rhs(const R* y, const R* p, R* dy) {
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      dy[i] = (y[(i + 1) % D] - y[(i + D - 2) % D]) * y[(i + D - 1) % D] - y[i] + p[0];
+  }
+  // f(y + d) - f(y) = (d_{i+1} - d_{i-2}) (y_{i-1} + d_{i-1}) + (y_{i+1} - y_{i-2}) d_{i-1} - d_i
+  template <class R>
+  static GS_HD void rhs_delta(const R* y, const R*, const R* d, R* df) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      const int a = (i + 1) % D, b = (i + D - 2) % D, c = (i + D - 1) % D;
+      df[i] = (d[a] - d[b]) * (y[c] + d[c]) + (y[a] - y[b]) * d[c] - d[i];
+    }
+  }
+  template <class R>
+  static GS_HD void vjp(const R* y, const R*, const R* w, R* gy, R* gp) {
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      const int m1 = (j + D - 1) % D, m2 = (j + D - 2) % D, p1 = (j + 1) % D, p2 = (j + 2) % D;
+      gy[j] += w[m1] * y[m2] - w[p2] * y[p1] + w[p1] * (y[p2] - y[m1]) - w[j];
+      gp[0] += w[j];
+    }
+  }
+};
+
+struct Hires {
+  static constexpr int D = 8, P = 1;  // p is a placeholder: HIRES has no free parameters
+  template <class R>
+  static GS_HD void rhs(const R* y, const R*, R* dy) {
+    dy[0] = R(-1.71) * y[0] + R(0.43) * y[1] + R(8.32) * y[2] + R(0.0007);
+    dy[1] = R(1.71) * y[0] - R(8.75) * y[1];
+    dy[2] = R(-10.03) * y[2] + R(0.43) * y[3] + R(0.035) * y[4];
+    dy[3] = R(8.32) * y[1] + R(1.71) * y[2] - R(1.12) * y[3];
+    dy[4] = R(-1.745) * y[4] + R(0.43) * y[5] + R(0.43) * y[6];
+    dy[5] = R(-280.0) * y[5] * y[7] + R(0.69) * y[3] + R(1.71) * y[4] - R(0.43) * y[5] +
+            R(0.69) * y[6];
+    dy[6] = R(280.0) * y[5] * y[7] - R(1.81) * y[6];
+    dy[7] = R(-280.0) * y[5] * y[7] + R(1.81) * y[6];
+  }
+  // linear terms in d, and (y5 + d5)(y7 + d7) - y5 y7 = y5 d7 + d5 (y7 + d7)
+  template <class R>
+  static GS_HD void rhs_delta(const R* y, const R*, const R* d, R* df) {
+    const R q = y[5] * d[7] + d[5] * (y[7] + d[7]);
+    df[0] = R(-1.71) * d[0] + R(0.43) * d[1] + R(8.32) * d[2];
+    df[1] = R(1.71) * d[0] - R(8.75) * d[1];
+    df[2] = R(-10.03) * d[2] + R(0.43) * d[3] + R(0.035) * d[4];
+    df[3] = R(8.32) * d[1] + R(1.71) * d[2] - R(1.12) * d[3];
+    df[4] = R(-1.745) * d[4] + R(0.43) * d[5] + R(0.43) * d[6];
+    df[5] = R(-280.0) * q + R(0.69) * d[3] + R(1.71) * d[4] - R(0.43) * d[5] + R(0.69) * d[6];
+    df[6] = R(280.0) * q - R(1.81) * d[6];
+    df[7] = R(-280.0) * q + R(1.81) * d[6];
+  }
+  template <class R>
+  static GS_HD void vjp(const R* y, const R*, const R* w, R* gy, R*) {
+    gy[0] += R(-1.71) * w[0] + R(1.71) * w[1];
+    gy[1] += R(0.43) * w[0] - R(8.75) * w[1] + R(8.32) * w[3];
+    gy[2] += R(8.32) * w[0] - R(10.03) * w[2] + R(1.71) * w[3];
+    gy[3] += R(0.43) * w[2] - R(1.12) * w[3] + R(0.69) * w[5];
+    gy[4] += R(0.035) * w[2] - R(1.745) * w[4] + R(1.71) * w[5];
+    gy[5] += R(0.43) * w[4] + (R(-280.0) * y[7] - R(0.43)) * w[5] + R(280.0) * y[7] * w[6] -
+             R(280.0) * y[7] * w[7];
+    gy[6] += R(0.43) * w[4] + R(0.69) * w[5] - R(1.81) * w[6] + R(1.81) * w[7];
+    gy[7] += R(-280.0) * y[5] * w[5] + R(280.0) * y[5] * w[6] - R(280.0) * y[5] * w[7];
+  }
+  template <class R>
+  static GS_HD void jac(const R* y, const R*, R* J) {
+#pragma unroll
+    for (int a = 0; a < 64; ++a) J[a] = R(0.0);
+    J[0 * 8 + 0] = R(-1.71); J[0 * 8 + 1] = R(0.43); J[0 * 8 + 2] = R(8.32);
+    J[1 * 8 + 0] = R(1.71); J[1 * 8 + 1] = R(-8.75);
+    J[2 * 8 + 2] = R(-10.03); J[2 * 8 + 3] = R(0.43); J[2 * 8 + 4] = R(0.035);
+    J[3 * 8 + 1] = R(8.32); J[3 * 8 + 2] = R(1.71); J[3 * 8 + 3] = R(-1.12);
+    J[4 * 8 + 4] = R(-1.745); J[4 * 8 + 5] = R(0.43); J[4 * 8 + 6] = R(0.43);
+    J[5 * 8 + 3] = R(0.69); J[5 * 8 + 4] = R(1.71); J[5 * 8 + 5] = R(-280.0) * y[7] - R(0.43);
+    J[5 * 8 + 6] = R(0.69); J[5 * 8 + 7] = R(-280.0) * y[5];
+    J[6 * 8 + 5] = R(280.0) * y[7]; J[6 * 8 + 6] = R(-1.81); J[6 * 8 + 7] = R(280.0) * y[5];
+    J[7 * 8 + 5] = R(-280.0) * y[7]; J[7 * 8 + 6] = R(1.81); J[7 * 8 + 7] = R(-280.0) * y[5];
+  }
+  // only J[5][5], J[6][5], J[7][5] (through y7) and J[5][7], J[6][7], J[7][7] (through y5)
+  // depend on the state
+  template <class R>
+  static GS_HD void jac_contract_grad(const R*, const R*, const R* G, R* gy, R*) {
+    gy[5] += R(-280.0) * G[5 * 8 + 7] + R(280.0) * G[6 * 8 + 7] - R(280.0) * G[7 * 8 + 7];
+    gy[7] += R(-280.0) * G[5 * 8 + 5] + R(280.0) * G[6 * 8 + 5] - R(280.0) * G[7 * 8 + 5];
+  }
+};
+
+// Lanes per trajectory of a field: its GROUP where it declares one (the stencil fields),
+// else 1.
+template <class F, class = void>
+struct group_of {
+  static constexpr int value = 1;
+};
+template <class F>
+struct group_of<F, decltype(void(F::GROUP))> {
+  static constexpr int value = F::GROUP;
 };
 
 struct Robertson {

@@ -731,15 +731,10 @@ struct AdjBuf {
 // Start the copies of segment sg's checkpoint and dts into buffer b of buf.io (steps at or
 // past na read as 0).  Record addresses: step s of trajectory j at rec_index(j, s, n), so an
 // even s and s + 1 share a 16-byte aligned half sector.
-template <int D, class Buf>
-__device__ __forceinline__ void prefetch_segment(Buf& buf, int b, const double* ckpt,
-                                                 const double* rec, long long n, long long j,
-                                                 int sg, int K, int na) {
-  SegIO<D>& io = buf.io;
-  constexpr int CW = SegIO<D>::CW;
-  const double* src = ckpt + ((size_t)sg * (size_t)n + (size_t)j) * CW;
-#pragma unroll
-  for (int u = 0; u < CW / 2; ++u) cp_async16(io.unit(b, io.KU + u), src + 2 * u);
+// The dts of segment sg into buffer b (steps at or past na read as 0); the caller commits.
+template <int D>
+__device__ __forceinline__ void prefetch_dts(SegIO<D>& io, int b, const double* rec, long long n,
+                                             long long j, int sg, int K, int na) {
   const int start = sg * K;
   // (the loops stay rolled: unrolled, the copies of the pair loop raised the stage-keeping
   // kernel from 90 to 118 registers)
@@ -767,6 +762,18 @@ __device__ __forceinline__ void prefetch_segment(Buf& buf, int b, const double* 
         io.dt(b, q) = 0.0;
     }
   }
+}
+
+template <int D, class Buf>
+__device__ __forceinline__ void prefetch_segment(Buf& buf, int b, const double* ckpt,
+                                                 const double* rec, long long n, long long j,
+                                                 int sg, int K, int na) {
+  SegIO<D>& io = buf.io;
+  constexpr int CW = SegIO<D>::CW;
+  const double* src = ckpt + ((size_t)sg * (size_t)n + (size_t)j) * CW;
+#pragma unroll
+  for (int u = 0; u < CW / 2; ++u) cp_async16(io.unit(b, io.KU + u), src + 2 * u);
+  prefetch_dts<D>(io, b, rec, n, j, sg, K, na);
   cp_async_commit();
 }
 

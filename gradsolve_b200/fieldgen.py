@@ -529,12 +529,39 @@ def _sources_digest() -> str:
     return h.hexdigest()[:16]
 
 
+def library_path(header: str) -> Path:
+    """Where the library of a field header lives (named by the content of the header and of
+    the kernel sources), built or not."""
+    key = hashlib.sha256((header + _sources_digest()).encode()).hexdigest()[:20]
+    return GEN_DIR / f"libgsfield_{key}.so"
+
+
+# the built-in stencil families the core library carries at a few dimensions only; any other
+# dimension gets a library of its own, compiled on first use: kind -> (code base, template)
+FAMILIES = {"linear": (4000, "Linear"), "lorenz96": (5000, "Lorenz96")}
+
+
+def family_header(kind: str, dim: int) -> str:
+    """The field header of a built-in family member (Linear<D>, Lorenz96<D>) at dimension
+    ``dim``: the hand-written field of gs_fields.cuh, instantiated, not traced."""
+    base, tmpl = FAMILIES[kind]
+    return "\n".join([
+        f"// generated by gradsolve_b200.fieldgen: the built-in {kind} field at D = {dim}",
+        "#pragma once", "namespace gs {", f"using UserField = {tmpl}<{int(dim)}>;",
+        "}  // namespace gs", f"#define GS_USER_FIELD_CODE {base + int(dim)}",
+        "#define GS_USER_STIFF 0", ""])
+
+
+def family_library(kind: str, dim: int) -> Path:
+    return build_field_library(family_header(kind, dim))
+
+
 def build_field_library(header: str, *, force: bool = False) -> Path:
     """Compile the kernels and the C ABI for one generated field into its own library
     (cached by the content of the header and of the kernel sources)."""
-    key = hashlib.sha256((header + _sources_digest()).encode()).hexdigest()[:20]
     GEN_DIR.mkdir(exist_ok=True)
-    out = GEN_DIR / f"libgsfield_{key}.so"
+    out = library_path(header)
+    key = out.stem[len("libgsfield_"):]
     if out.exists() and not force:
         return out
     hdr = GEN_DIR / f"field_{key}.cuh"

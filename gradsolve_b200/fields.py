@@ -11,8 +11,17 @@ Routing (problem.name -> field):
                            from the params (all three columns get gradients)
   ``vdp``               -> vdp, params[:, 0] = mu
   ``lotka_volterra`` / ``lv`` -> Lotka-Volterra, params (n, 4) = [alpha, beta, gamma, delta]
-  ``linear_ladder_<D>`` -> linear_<D> (dy = 1.01 y), D in 1, 2, 3, 4, 8; params ignored
+  ``linear_ladder_<D>`` -> linear_<D> (dy = 1.01 y), any D > 0; params ignored
+  ``lorenz96_<D>``      -> lorenz96_<D>, any D >= 4, params (n, 1) = [F]
   ``robertson``         -> robertson, params (n, 3) = [k1, k2, k3] (stiff)
+  ``hires``             -> hires (stiff, D = 8, autonomous); params ignored
+  a name given to ``register_field`` / ``register_jax_field`` / ``register_linstiff``
+                        -> that generated field (``linstiff_*`` among them)
+
+The core library carries linear_<D> for D in LINEAR_DIMS and lorenz96_<D> for D in
+LORENZ96_DIMS; any other dimension of the two families gets a library of its own, compiled
+on first use (``fieldgen.family_library``).  Above MAX_DIM the fused lanes refuse before any
+launch, as the reference's GPU path does.
 
 Params with more columns than a field reads keep the extra columns; their gradient is 0
 (the field does not read them), as ``jax.grad`` through ``f_jax`` would give.
@@ -27,10 +36,22 @@ FIELD_LORENZ = 1
 FIELD_VDP = 2
 FIELD_LOTKA_VOLTERRA = 3
 FIELD_LINEAR = 4
+FIELD_LORENZ96 = 5
 FIELD_ROBERTSON = 10
 FIELD_LORENZ3 = 11
+FIELD_HIRES = 12
 
-LINEAR_DIMS = (1, 2, 3, 4, 8)
+LINEAR_DIMS = (1, 2, 3, 4, 8, 10, 32)   # linear_<D> in libgsolve.so
+STIFF_LINEAR_DIMS = (1, 2, 3, 4, 8)     # ... of which Rosenbrock23 serves these
+LORENZ96_DIMS = (4, 8, 32)              # lorenz96_<D> in libgsolve.so
+MAX_DIM = 64                            # gradsolve/warp/warp_ode.py:75-81 (_GPU_VEC_DIM_CEILING)
+
+
+def dim_limit_message(dim: int) -> str:
+    return (f"fused GPU register-vector limit: dim={dim} > {MAX_DIM}. The fused adaptive "
+            "kernels are low-NVAR GPU engines (state and stages in registers, a group of "
+            "lanes per trajectory above 8 components); larger systems are refused before "
+            "any launch (gradsolve/warp/warp_ode.py:649-664).")
 
 
 @dataclass(frozen=True)
@@ -40,7 +61,8 @@ class FieldSpec:
     dim: int      # state dimension D
     nparam: int   # parameters the kernel reads (P)
     stiff_ok: bool  # has an analytic Jacobian (Rosenbrock23 capable)
-    lib: str = ""   # the generated field's own library (empty: libgsolve.so)
+    lib: str = ""   # the field's own library (empty: libgsolve.so)
+    family: tuple = ()  # (kind, D) of a built-in family member whose library is built on use
 
 
 # problem name -> FieldSpec of a generated field (register_field)
@@ -53,7 +75,28 @@ _STATIC = {
     "vdp": FieldSpec("vdp", FIELD_VDP, 2, 1, True),
     "lv": FieldSpec("lv", FIELD_LOTKA_VOLTERRA, 2, 4, False),
     "robertson": FieldSpec("robertson", FIELD_ROBERTSON, 3, 3, True),
+    "hires": FieldSpec("hires", FIELD_HIRES, 8, 1, True),
 }
+
+
+def _family_spec(kind: str, d: int) -> FieldSpec:
+    """linear_<d> or lorenz96_<d>: in the core library at its built dimensions, else in a
+    library of its own (compiled by ``_lib.lib_for`` on first use)."""
+    base = FIELD_LINEAR if kind == "linear" else FIELD_LORENZ96
+    key, code = f"{kind}_{d}", base * 1000 + d
+    core = LINEAR_DIMS if kind == "linear" else LORENZ96_DIMS
+    if d in core:
+        return FieldSpec(key, code, d, 1, kind == "linear" and d in STIFF_LINEAR_DIMS)
+    from . import fieldgen
+    path = "" if d > MAX_DIM else str(fieldgen.library_path(fieldgen.family_header(kind, d)))
+    return FieldSpec(key, code, d, 1, False, path, (kind, d))
+
+
+def _suffix(name: str) -> int:
+    try:
+        return int(name.rsplit("_", 1)[1])
+    except ValueError:
+        return -1
 
 
 def field_spec(key: str) -> FieldSpec:
@@ -62,15 +105,12 @@ def field_spec(key: str) -> FieldSpec:
     for spec in _USER.values():
         if spec.key == key:
             return spec
-    if key.startswith("linear_"):
-        try:
-            d = int(key.split("_", 1)[1])
-        except ValueError:
-            d = -1
-        if d in LINEAR_DIMS:
-            return FieldSpec(key, FIELD_LINEAR * 1000 + d, d, 1, True)
-    raise KeyError(f"unknown field {key!r}; known: {sorted(_STATIC)} + linear_<D> for D in "
-                   f"{LINEAR_DIMS}")
+    if key.startswith("linear_") and _suffix(key) >= 1:
+        return _family_spec("linear", _suffix(key))
+    if key.startswith("lorenz96_") and _suffix(key) >= 4:
+        return _family_spec("lorenz96", _suffix(key))
+    raise KeyError(f"unknown field {key!r}; known: {sorted(_STATIC)} + linear_<D> (D >= 1) + "
+                   f"lorenz96_<D> (D >= 4)")
 
 
 def field_for(problem) -> FieldSpec | None:
@@ -86,15 +126,14 @@ def field_for(problem) -> FieldSpec | None:
         return _STATIC["vdp"]
     if nm in ("lotka_volterra", "lv"):
         return _STATIC["lv"]
-    if nm == "robertson":
-        return _STATIC["robertson"]
+    if nm in ("robertson", "hires"):
+        return _STATIC[nm]
     if nm.startswith("linear_ladder_"):
-        try:
-            d = int(nm.rsplit("_", 1)[1])
-        except ValueError:
-            return None
-        if d in LINEAR_DIMS:
-            return field_spec(f"linear_{d}")
+        d = _suffix(nm)
+        return _family_spec("linear", d) if d >= 1 else None
+    if nm.startswith("lorenz96_"):
+        d = _suffix(nm)
+        return _family_spec("lorenz96", d) if d >= 4 else None
     return None
 
 
@@ -113,7 +152,7 @@ def kernel_params(spec: FieldSpec, params: np.ndarray) -> np.ndarray:
     n = params.shape[0]
     if spec.lib and params.shape[1] == 0:  # a generated field without parameters
         return np.zeros((n, spec.nparam))
-    if spec.key.startswith("linear_"):
+    if spec.key.startswith("linear_") or spec.key == "hires":  # params read by nothing
         return np.zeros((n, 1)) if params.shape[1] == 0 else params[:, :1]
     if params.shape[1] < spec.nparam:
         raise ValueError(

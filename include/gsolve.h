@@ -23,8 +23,14 @@
  *   n_acc, n_rej, status : (n,) int32.
  * Field codes: GS_FIELD_LORENZ (D=3,P=1: rho), GS_FIELD_VDP (D=2,P=1: mu),
  *   GS_FIELD_LOTKA_VOLTERRA (D=2,P=4: alpha,beta,gamma,delta), GS_FIELD_LINEAR*1000 + D
- *   (D in 1,2,3,4,8; P=1, ignored), GS_FIELD_ROBERTSON (D=3,P=3: k1,k2,k3; stiff),
- *   GS_FIELD_LORENZ3 (D=3,P=3: sigma,beta,rho).
+ *   (D in 1,2,3,4,8,10,32; P=1, ignored; stiff-capable for D <= 8), GS_FIELD_LORENZ96*1000
+ *   + D (D in 4,8,32; P=1: F), GS_FIELD_ROBERTSON (D=3,P=3: k1,k2,k3; stiff),
+ *   GS_FIELD_LORENZ3 (D=3,P=3: sigma,beta,rho), GS_FIELD_HIRES (D=8,P=1 ignored; stiff).
+ *   Other dimensions of the linear and lorenz96 families, and registered fields, are served
+ *   by libraries of their own with this same ABI (gradsolve_b200/fieldgen.py).
+ * State dimensions above 8 are integrated by a group of lanes per trajectory (float64; the
+ *   float32-stage mode, the dense output and gs_tsit5_vjp_static refuse them); the fused
+ *   lanes stop at D = 64, the reference's GPU limit (gradsolve/warp/warp_ode.py:75-81).
  */
 #ifndef GSOLVE_H_
 #define GSOLVE_H_
@@ -45,8 +51,10 @@ extern "C" {
 #define GS_FIELD_VDP 2
 #define GS_FIELD_LOTKA_VOLTERRA 3
 #define GS_FIELD_LINEAR 4
+#define GS_FIELD_LORENZ96 5
 #define GS_FIELD_ROBERTSON 10
 #define GS_FIELD_LORENZ3 11
+#define GS_FIELD_HIRES 12
 
 #define GS_PREC_F64 0   /* everything float64 */
 #define GS_PREC_MIXED 1 /* float32 stages/RHS; float64 time, controller, error norm, state */

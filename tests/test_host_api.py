@@ -2,6 +2,8 @@
 mapping, checkpoint policy."""
 from __future__ import annotations
 
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -41,9 +43,46 @@ def test_field_routing_mirrors_reference_names():
     assert field_for(P("lotka_volterra")).key == "lv"
     assert field_for(P("robertson")).stiff_ok
     assert field_for(P("linear_ladder_3")).dim == 3
-    assert field_for(P("linear_ladder_5")) is None  # not built for D = 5
-    assert field_for(P("hires")) is None
+    assert field_for(P("hires")).stiff_ok and field_for(P("hires")).dim == 8
     assert field_for(P("my_rhs")) is None
+    # the families route for every dimension the reference routes (warp_ode.py:478-490):
+    # in the core library at its built dimensions, else in a library built on first use
+    s32, s5 = field_for(P("linear_ladder_32")), field_for(P("linear_ladder_5"))
+    assert (s32.key, s32.dim, s32.lib, s32.family) == ("linear_32", 32, "", ())
+    assert s5.dim == 5 and s5.family == ("linear", 5) and s5.lib.endswith(".so")
+    l96 = field_for(P("lorenz96_40"))
+    assert l96.code == 5040 and l96.family == ("lorenz96", 40) and not l96.stiff_ok
+    assert field_for(P("lorenz96_32")).family == ()
+    assert field_for(P("lorenz96_3")) is None  # D >= 4, as the reference requires
+    assert field_for(P("linear_ladder_0")) is None and field_for(P("lorenz96_x")) is None
+    # beyond the fused lanes' limit the name still routes, and use is refused before launch
+    big = field_for(P("lorenz96_65"))
+    assert big.dim == 65 and big.lib == ""
+    with pytest.raises(RuntimeError, match="dim=65 > 64"):
+        api._require_field(P("lorenz96_65"))
+
+
+def test_group_size_rule():
+    """Lanes per trajectory for a state of D components: 1 up to 8, then blocks of at most
+    4 components where D allows, at least 2 (the stencil reaches two components into the
+    next block), odd D on one thread -- the rule of coop_group in gs_fields.cuh, restated."""
+    src = (Path(__file__).resolve().parent.parent / "gradsolve_b200" / "csrc" /
+           "gs_fields.cuh").read_text()
+    assert "constexpr int coop_group(int D)" in src
+
+    def coop_group(D):
+        if D <= 8:
+            return 1
+        best, g = 1, 2
+        while g <= 32:
+            if D % g == 0 and D // g >= 2:
+                best = g
+                if D // g <= 4:
+                    return g
+            g *= 2
+        return best
+    assert [coop_group(d) for d in (3, 8, 9, 10, 12, 16, 20, 32, 40, 64)] == \
+        [1, 1, 1, 2, 4, 4, 4, 8, 8, 16]
 
 
 def test_kernel_params_leading_columns_and_errors():

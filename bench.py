@@ -649,11 +649,21 @@ def workload_groups(name: str, n: int, seed_shift: int):
                              cap=1024 if method == "tsit5" else 8192, loss="mse",
                              pilot_p=mu_t[sel, None]))
         return out
+    if name == "lorenz96_32":  # 32 components: eight lanes per trajectory
+        rng = np.random.default_rng(13 + seed_shift)
+        F = rng.uniform(7.5, 8.5, (n, 1))
+        y0 = F + rng.normal(0.0, 0.5, (n, 32))
+        return [Group("lorenz96_32", "tsit5", "lorenz96_32", y0, F, 2.0, 1e-8, 1e-8, cap=512)]
+    if name == "linear_32":
+        rng = np.random.default_rng(15 + seed_shift)
+        y0 = rng.uniform(-2.0, 2.0, (n, 32))
+        return [Group("linear_32", "tsit5", "linear_32", y0, np.zeros((n, 1)), 4.0, 1e-10,
+                      1e-10, cap=128)]
     raise ValueError(f"unknown workload {name!r}")
 
 
 WORKLOAD_N = {"lv_2e22": 1 << 22, "lorenz_2e22": 1 << 22, "robertson_2e18": 1 << 18,
-              "vdp_uneven_saveat": 1 << 20}
+              "vdp_uneven_saveat": 1 << 20, "lorenz96_32": 1 << 18, "linear_32": 1 << 18}
 
 
 def run_workload(args) -> None:
@@ -816,7 +826,8 @@ def run_workload(args) -> None:
 
     outs = r = gp = None  # the float64 records stay reachable through g.r64 only
     mixed = None
-    if not args.no_mixed and any(g.method == "tsit5" for g in groups):
+    # (the float32-stage mode is not built for the states integrated by a group of lanes)
+    if not args.no_mixed and any(g.method == "tsit5" for g in groups) and D <= 8:
         same = {}
         for g in groups:
             if g.method != "tsit5":

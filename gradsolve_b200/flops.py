@@ -15,6 +15,8 @@ COUNTS = {
     ("tsit5", "lorenz"): dict(F_att=269, F_step=198, F_vjp=228),
     ("tsit5", "lv"): dict(F_att=193, F_step=144, F_vjp=204),
     ("tsit5", "vdp"): dict(F_att=175, F_step=126, F_vjp=186),
+    ("tsit5", "lorenz96_32"): dict(F_att=3013, F_step=2304, F_vjp=3066),
+    ("tsit5", "linear_32"): dict(F_att=2437, F_step=1728, F_vjp=1728),
     ("rosenbrock23", "robertson"): dict(F_att=205, F_step=115, F_vjp=191),
     ("rosenbrock23", "vdp"): dict(F_att=108, F_step=54, F_vjp=97),
 }

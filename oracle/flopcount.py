@@ -148,10 +148,36 @@ def jcg_vdp(y, p, G):
     return gy, gp
 
 
+def f_l96(y, p):
+    """lorenz96_<D> in the reference's order (gradsolve/warp/_warp_kernel.py:175-195)."""
+    D = len(y)
+    return [(y[(i + 1) % D] - y[(i - 2) % D]) * y[(i - 1) % D] - y[i] + p[0] for i in range(D)]
+
+
+def vjp_l96(y, p, w):
+    D = len(y)
+    gy = [w[(j - 1) % D] * y[(j - 2) % D] - w[(j + 2) % D] * y[(j + 1) % D] +
+          w[(j + 1) % D] * (y[(j + 2) % D] - y[(j - 1) % D]) - w[j] for j in range(D)]
+    gF = w[0]
+    for j in range(1, D):
+        gF = gF + w[j]
+    return gy, [gF]
+
+
+def f_lin(y, p):
+    """linear_<D> (gradsolve/warp/_warp_kernel.py:133-155): 1.01 y, the parameter unread."""
+    return [1.01 * v for v in y]
+
+
+def vjp_lin(y, p, w):
+    return [1.01 * v for v in w], [0.0]
+
+
 STIFF = {"robertson": (jac_rob, jcg_rob, [0.04, 3e7, 1e4]), "vdp": (jac_vdp, jcg_vdp, [50.0])}
 
 FIELDS = {"lorenz": (f_lorenz, vjp_lorenz, 3, 1), "lv": (f_lv, vjp_lv, 2, 4),
-          "vdp": (f_vdp, vjp_vdp, 2, 1), "robertson": (f_rob, vjp_rob, 3, 3)}
+          "vdp": (f_vdp, vjp_vdp, 2, 1), "robertson": (f_rob, vjp_rob, 3, 3),
+          "lorenz96_32": (f_l96, vjp_l96, 32, 1), "linear_32": (f_lin, vjp_lin, 32, 1)}
 
 # Tsit5 tableau (values only matter for the arithmetic to run; counts are structural)
 A = [[0.161], [-0.0085, 0.3355], [2.897, -6.359, 4.362], [5.326, -11.749, 7.496, -0.0925],
@@ -317,7 +343,8 @@ def count_ros23(field="robertson"):
 
 
 def all_counts():
-    out = {("tsit5", k): count_tsit5(k) for k in ("lorenz", "lv", "vdp")}
+    out = {("tsit5", k): count_tsit5(k) for k in ("lorenz", "lv", "vdp", "lorenz96_32",
+                                                   "linear_32")}
     out[("rosenbrock23", "robertson")] = count_ros23("robertson")
     out[("rosenbrock23", "vdp")] = count_ros23("vdp")
     return out

@@ -60,7 +60,7 @@ def test_forward_record_matches_reference(gslib, cuda, case, field):
     check_dts(dts, g["dts"])
 
 
-def check_dts(dts, ref):
+def check_dts(dts, ref, rtol=1e-8):
     """Recorded steps vs the reference's.  The controller's input, the embedded error
     estimate e = h*sum(E_i k_i), cancels (sum E_i = 0), so its rounding -- and the kernel
     fuses multiply-adds where numpy does not -- moves dt = h*0.9*err^-0.2 by up to
@@ -70,13 +70,16 @@ def check_dts(dts, ref):
     # Typical size of that effect for these cases: |e| ~ 1e-8 |y| against h|k| ~ 1, i.e.
     # eps * 1e7 ~ 1e-9 on err and 0.2 of that on dt; measured on B200: median 2e-11..3e-10,
     # p99 2e-9..3.5e-9, max 1e-5 (one tiny error estimate in a chaotic Lorenz run).
+    # |e| scales with the tolerance (|e| ~ rtol |y| at acceptance), so the floor grows as
+    # 1/rtol: the bars below are for rtol = 1e-8 and widen by 1e-8 / rtol for tighter runs.
     m = ref > 0
     q = np.abs(dts[m] - ref[m]) / ref[m]
     assert np.all(dts[~m] == 0)
+    f = max(1.0, 1e-8 / rtol)
     p50, p99 = float(np.median(q)), float(np.quantile(q, 0.99))
-    msg = f"dt rel err p50 {p50:.2e} p99 {p99:.2e} max {q.max():.2e}"
-    assert p50 <= 1e-9, msg
-    assert p99 <= 1e-8, msg
+    msg = f"dt rel err p50 {p50:.2e} p99 {p99:.2e} max {q.max():.2e} (rtol {rtol:g})"
+    assert p50 <= 1e-9 * f, msg
+    assert p99 <= 1e-8 * f, msg
     assert q.max() <= 1e-4, msg
 
 

@@ -348,7 +348,8 @@ __all__ = ["solve", "grad_closure", "register_field", "register_jax_field", "reg
            "ENGINE_REGISTRY", "ALIASES", "FieldSpec"]
 
 
-def register_field(name: str, f, dim: int, n_params: int, *, stiff: bool = False) -> FieldSpec:
+def register_field(name: str, f, dim: int, n_params: int, *, stiff: bool = False,
+                   exprs=None) -> FieldSpec:
     """Register a Python right-hand side ``f(t, y, p) -> dy`` (autonomous: t unused) so that
     a Problem of that ``name`` routes to the B200 kernels like a built-in field.
 
@@ -364,7 +365,7 @@ def register_field(name: str, f, dim: int, n_params: int, *, stiff: bool = False
         return F._USER[name]
     if int(dim) > MAX_DIM:
         raise RuntimeError(dim_limit_message(int(dim)))
-    d = fieldgen.Derived(f, dim, n_params, stiff)
+    d = fieldgen.Derived(f, dim, n_params, stiff, exprs=exprs)
     code = fieldgen.USER_CODE_BASE + (sum(name.encode()) * 7919) % 90000
     path = fieldgen.build_field_library(fieldgen.emit_struct(d, name, code))
     spec = FieldSpec(f"user_{name}", code, d.D, d.P, bool(stiff), str(path))
@@ -372,9 +373,26 @@ def register_field(name: str, f, dim: int, n_params: int, *, stiff: bool = False
     return spec
 
 
-# the reference's name for the same registration (its f is a JAX function; here any
-# function of symbolic scalars: Python arithmetic, numpy ufuncs, gradsolve_b200.fieldgen)
-register_jax_field = register_field
+def register_jax_field(name: str, f_jax, dim: int, n_params: int, *,
+                       stiff: bool = False) -> FieldSpec:
+    """The reference's registration entry point (gradsolve/__init__.py:31-42,
+    gradsolve/warp/jax_field.py:517-560), same signature and contract as ``register_field``.
+    Where JAX is importable, ``f_jax`` is walked as its jaxpr (``jax.make_jaxpr``) through
+    ``fieldgen.JAXPR_PRIMITIVES``, as the reference's translator walks it; without JAX (this
+    image) the function is traced with symbolic scalars, which accepts the same expressions
+    written with Python arithmetic and numpy ufuncs."""
+    from . import fields as F
+    from . import fieldgen
+    if name in F._USER:
+        return F._USER[name]
+    try:
+        import jax
+        import jax.numpy as jnp
+    except ImportError:
+        return register_field(name, f_jax, dim, n_params, stiff=stiff)
+    closed = jax.make_jaxpr(f_jax)(0.0, jnp.zeros(int(dim)), jnp.zeros(int(n_params)))
+    exprs = fieldgen.trace_jaxpr(closed, int(dim), int(n_params))
+    return register_field(name, None, dim, n_params, stiff=stiff, exprs=exprs)
 
 
 def register_linstiff(key: str, A) -> FieldSpec:

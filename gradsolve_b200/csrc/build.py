@@ -51,12 +51,46 @@ def _compile(lib: Path, sources, log: str, verbose: bool) -> None:
         print(res.stderr)
 
 
+XLA_LIB = PKG / "libgsolve_xla.so"
+XLA_SOURCES = [CSRC / "gs_xla_ffi.cc"]
+
+
+def xla_ffi_include():
+    """XLA's FFI headers as JAX ships them, or None where JAX is not installed."""
+    try:
+        import jax.ffi
+        return jax.ffi.include_dir()
+    except Exception:
+        return None
+
+
+def build_xla_ffi(force: bool = False):
+    """The XLA FFI handlers (gs_xla_ffi.cc) as libgsolve_xla.so, linked to libgsolve.so;
+    skipped (returns None) where JAX is not installed, as in this image."""
+    inc = xla_ffi_include()
+    if inc is None:
+        return None
+    if not force and up_to_date(XLA_LIB, XLA_SOURCES + [LIB]):
+        return XLA_LIB
+    cxx = shutil.which("g++") or "c++"
+    cuda_inc = Path(nvcc()).resolve().parent.parent / "include"
+    cmd = [cxx, "-std=c++17", "-O2", "-shared", "-fPIC", f"-I{inc}", f"-I{cuda_inc}",
+           "-o", str(XLA_LIB), *map(str, XLA_SOURCES), f"-L{PKG}", "-lgsolve",
+           "-Wl,-rpath,$ORIGIN"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"building the XLA FFI handlers failed:\n{res.stderr[-4000:]}")
+    return XLA_LIB
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
-    """Build libgsolve.so (the solver) and libgsprobe.so (the FMA peak probes)."""
+    """Build libgsolve.so (the solver), libgsprobe.so (the FMA peak probes) and, where JAX is
+    installed, libgsolve_xla.so (the XLA FFI handlers)."""
     if force or not up_to_date(LIB, SOURCES):
         _compile(LIB, SOURCES, "ptxas.log", verbose)
     if force or not up_to_date(PROBE_LIB, PROBE_SOURCES):
         _compile(PROBE_LIB, PROBE_SOURCES, "ptxas_probe.log", verbose)
+    build_xla_ffi(force)
     return LIB
 
 

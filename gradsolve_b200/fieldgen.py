@@ -27,6 +27,8 @@ import tempfile
 from pathlib import Path
 from typing import Callable, Dict, List, Optional, Sequence
 
+import numpy as np
+
 HERE = Path(__file__).resolve().parent
 GEN_DIR = HERE / "_fields"
 USER_CODE_BASE = 9000
@@ -330,6 +332,156 @@ def trace(f: Callable, dim: int, n_params: int) -> List[Expr]:
     return out
 
 
+# ---- jaxpr walking: register_jax_field on a JAX function --------------------------------------
+# A jaxpr value is a numpy object array of Expr (a scalar is a 0-d array).  The table maps
+# jaxpr primitive names to what they do on such arrays -- the subset the reference's
+# translator accepts (gradsolve/warp/jax_field.py:75-95, :196-330): elementwise arithmetic
+# and transcendentals, integer_pow, element-type conversion, the shape primitives that
+# indexing and jnp.stack / jnp.array lower to, dot_general and reduce_sum for matrix-vector
+# fields, and call primitives (pjit / jit / closed_call), whose inner jaxpr is inlined.
+# Comparisons fold on constants only; a branch on the state (select_n, while, cond, ...) is
+# refused, as by the symbolic-scalar tracer.  trace_jaxpr reads only eqn.primitive.name,
+# eqn.invars, eqn.outvars, eqn.params and Literal.val, so it needs no JAX import.
+def _arr(x) -> np.ndarray:
+    a = np.empty(np.shape(x), dtype=object)
+    flat = np.asarray(x, dtype=object).reshape(-1)
+    a.reshape(-1)[:] = [v if isinstance(v, Expr) else _e(float(v)) for v in flat]
+    return a
+
+
+def _ew(fn: Callable, nargs: int):
+    uf = np.frompyfunc(fn, nargs, 1)
+
+    def h(params, *xs):
+        return _arr(uf(*xs))
+    return h
+
+
+def _folding_cmp(op: Callable[[float, float], bool]):
+    def f(a, b):
+        a, b = _e(a), _e(b)
+        if a.op == "c" and b.op == "c":
+            return const(1.0 if op(a.val, b.val) else 0.0)
+        raise UnsupportedRHS("a comparison of state-dependent values (a branch on the state) "
+                             "is not supported")
+    return _ew(f, 2)
+
+
+def _broadcast_in_dim(params, a):
+    shape = tuple(params["shape"])
+    inter = [1] * len(shape)
+    for i, d in enumerate(params["broadcast_dimensions"]):
+        inter[d] = a.shape[i]
+    return _arr(np.broadcast_to(a.reshape(inter), shape))
+
+
+def _slice(params, a):
+    strides = params.get("strides") or [1] * len(params["start_indices"])
+    idx = tuple(slice(b, e, st) for b, e, st in zip(params["start_indices"],
+                                                    params["limit_indices"], strides))
+    return _arr(a[idx])
+
+
+def _iota(params):
+    shape = tuple(params["shape"])
+    return _arr(np.indices(shape)[params["dimension"]].astype(float))
+
+
+def _dot_general(params, a, b):
+    (lc, rc), (lb, rb) = params["dimension_numbers"]
+    if len(lb) or len(rb):
+        raise UnsupportedRHS("dot_general with batch dimensions is not supported")
+    return _arr(np.tensordot(a, b, axes=(tuple(lc), tuple(rc))))
+
+
+def _reduce_sum(params, a):
+    return _arr(np.sum(a, axis=tuple(params["axes"])))
+
+
+JAXPR_PRIMITIVES: Dict[str, Callable] = {
+    "add": _ew(add, 2), "add_any": _ew(add, 2), "sub": _ew(sub, 2), "mul": _ew(mul, 2),
+    "div": _ew(div, 2), "max": _ew(maximum, 2), "min": _ew(minimum, 2), "pow": _ew(power, 2),
+    "neg": _ew(neg, 1), "abs": _ew(absolute, 1), "sign": _ew(sign, 1), "exp": _ew(exp, 1),
+    "log": _ew(log, 1), "sin": _ew(sin, 1), "cos": _ew(cos, 1), "tan": _ew(tan, 1),
+    "tanh": _ew(tanh, 1), "sqrt": _ew(sqrt, 1),
+    "rsqrt": _ew(lambda a: div(1.0, sqrt(a)), 1), "square": _ew(lambda a: mul(a, a), 1),
+    "integer_pow": lambda params, a: _arr(np.frompyfunc(
+        lambda v: power(v, float(params["y"])), 1, 1)(a)),
+    "lt": _folding_cmp(lambda a, b: a < b), "le": _folding_cmp(lambda a, b: a <= b),
+    "gt": _folding_cmp(lambda a, b: a > b), "ge": _folding_cmp(lambda a, b: a >= b),
+    "eq": _folding_cmp(lambda a, b: a == b), "ne": _folding_cmp(lambda a, b: a != b),
+    "convert_element_type": lambda params, a: a, "copy": lambda params, a: a,
+    "copy_p": lambda params, a: a,
+    "squeeze": lambda params, a: _arr(np.squeeze(a, axis=tuple(params["dimensions"]))),
+    "expand_dims": lambda params, a: _arr(np.expand_dims(a, tuple(params["dimensions"]))),
+    "reshape": lambda params, a: _arr(a.reshape(tuple(params["new_sizes"]))),
+    "broadcast_in_dim": _broadcast_in_dim,
+    "slice": _slice,
+    "concatenate": lambda params, *xs: _arr(np.concatenate(xs, axis=params["dimension"])),
+    "stack": lambda params, *xs: _arr(np.stack(xs, axis=params["axis"])),
+    "transpose": lambda params, a: _arr(np.transpose(a, tuple(params["permutation"]))),
+    "iota": _iota,
+    "dot_general": _dot_general,
+    "reduce_sum": _reduce_sum,
+}
+_CALL_PRIMITIVES = ("pjit", "jit", "closed_call", "core_call")
+
+
+def _walk_jaxpr(jaxpr, consts, args) -> list:
+    env: Dict[int, np.ndarray] = {}
+
+    def read(v):
+        if type(v).__name__ == "Literal":
+            return _arr(v.val)
+        return env[id(v)]
+
+    for v, c in zip(getattr(jaxpr, "constvars", ()), consts):
+        env[id(v)] = _arr(c)
+    for v, a in zip(jaxpr.invars, args):
+        env[id(v)] = a
+    for eqn in jaxpr.eqns:
+        name = eqn.primitive.name
+        ins = [read(v) for v in eqn.invars]
+        if name in _CALL_PRIMITIVES:
+            inner = eqn.params.get("jaxpr") or eqn.params.get("call_jaxpr")
+            if inner is None:
+                raise UnsupportedRHS(f"call primitive {name!r} without an inlinable jaxpr")
+            outs = _walk_jaxpr(getattr(inner, "jaxpr", inner), getattr(inner, "consts", ()),
+                               ins)
+        elif name in JAXPR_PRIMITIVES:
+            outs = [JAXPR_PRIMITIVES[name](eqn.params, *ins)]
+        else:
+            raise UnsupportedRHS(f"unsupported jaxpr primitive {name!r} in f_jax")
+        for v, o in zip(eqn.outvars, outs):
+            if type(v).__name__ != "DropVar":
+                env[id(v)] = o
+    return [read(v) for v in jaxpr.outvars]
+
+
+def trace_jaxpr(closed_jaxpr, dim: int, n_params: int) -> List[Expr]:
+    """The components of f(t, y, p) from the jaxpr of ``f_jax`` (what
+    ``jax.make_jaxpr(f_jax)(0.0, zeros(dim), zeros(n_params))`` returns), as expressions of
+    the symbolic state and parameters -- the same result ``trace`` gives for a function
+    written with Python arithmetic."""
+    jaxpr = getattr(closed_jaxpr, "jaxpr", closed_jaxpr)
+    consts = getattr(closed_jaxpr, "consts", ())
+    t = _arr(var("t", 0))
+    y = _arr([var("y", i) for i in range(dim)])
+    p = _arr([var("p", j) for j in range(max(n_params, 0))])
+    outs = _walk_jaxpr(jaxpr, consts, [t, y, p])
+    if len(outs) != 1:
+        raise UnsupportedRHS(f"f_jax returns {len(outs)} arrays; expected one of length {dim}")
+    flat = list(outs[0].reshape(-1))
+    if len(flat) != dim:
+        raise UnsupportedRHS(f"f_jax returns {len(flat)} components, expected dim={dim}")
+    out = [_e(o) for o in flat]
+    for o in out:
+        if _depends(o, "t"):
+            raise UnsupportedRHS("time-dependent field: the kernels integrate autonomous "
+                                 "systems f(y, p)")
+    return out
+
+
 def _depends(e: Expr, kind: str) -> bool:
     seen, stack = set(), [e]
     while stack:
@@ -383,9 +535,10 @@ def _eval1(n: Expr, a: list, env) -> float:
 class Derived:
     """f, its VJP, and (stiff) J and grad <G, J>, as expressions."""
 
-    def __init__(self, f: Callable, dim: int, n_params: int, stiff: bool):
+    def __init__(self, f: Optional[Callable], dim: int, n_params: int, stiff: bool,
+                 exprs: Optional[List[Expr]] = None):
         self.D, self.P, self.stiff = int(dim), max(int(n_params), 1), bool(stiff)
-        self.f = trace(f, self.D, int(n_params))
+        self.f = list(exprs) if exprs is not None else trace(f, self.D, int(n_params))
         ys = [var("y", i) for i in range(self.D)]
         ps = [var("p", j) for j in range(self.P)]
         s = const(0.0)

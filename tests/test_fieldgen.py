@@ -128,3 +128,116 @@ def test_register_field_builds_a_library_with_the_full_abi(gslib):
     assert (D.value, P.value) == (2, 2)
     assert L.gs_field_dims(1, ctypes.byref(D), ctypes.byref(P)) != 0  # serves its field only
     assert math.isfinite(spec.code)
+
+
+# ---- the jaxpr walker (register_jax_field where JAX is installed) ---------------------------
+# JAX is absent here, so the walker is driven with jaxprs built by hand in the shape
+# jax.make_jaxpr produces (the attributes it reads: primitive.name, invars, outvars, params,
+# Literal.val), written as JAX lowers these functions.
+class _Var:
+    pass
+
+
+class Literal:  # the walker recognises literals by this class name, as in JAX
+    def __init__(self, val):
+        self.val = val
+
+
+class _Prim:
+    def __init__(self, name):
+        self.name = name
+
+
+class _Eqn:
+    def __init__(self, name, invars, outvars, **params):
+        self.primitive, self.invars, self.outvars, self.params = (_Prim(name), invars, outvars,
+                                                                  params)
+
+
+class _Jaxpr:
+    def __init__(self, invars, eqns, outvars, constvars=()):
+        self.invars, self.eqns, self.outvars, self.constvars = invars, eqns, outvars, constvars
+
+
+class _Closed:
+    def __init__(self, jaxpr, consts=()):
+        self.jaxpr, self.consts = jaxpr, list(consts)
+
+
+def _lorenz_jaxpr():
+    """make_jaxpr of f(t, y, p) = jnp.stack([10*(y[1]-y[0]), p[0]*y[0]-y[1]-y[0]*y[2],
+    y[0]*y[1]-(8/3)*y[2]]): static indexing is slice + squeeze, jnp.stack the stack
+    primitive, and the arithmetic sits inside a pjit (jnp functions are jitted)."""
+    t, y, p = _Var(), _Var(), _Var()
+    eqns, v = [], {}
+
+    def take(src, i, name):
+        a, b = _Var(), _Var()
+        eqns.append(_Eqn("slice", [src], [a], start_indices=(i,), limit_indices=(i + 1,),
+                         strides=None))
+        eqns.append(_Eqn("squeeze", [a], [b], dimensions=(0,)))
+        v[name] = b
+
+    take(y, 0, "x"), take(y, 1, "u"), take(y, 2, "z"), take(p, 0, "rho")
+
+    def op(name, a, b):
+        o = _Var()
+        eqns.append(_Eqn(name, [a, b], [o]))
+        return o
+
+    f0 = op("mul", Literal(10.0), op("sub", v["u"], v["x"]))
+    f1 = op("sub", op("sub", op("mul", v["rho"], v["x"]), v["u"]), op("mul", v["x"], v["z"]))
+    f2 = op("sub", op("mul", v["x"], v["u"]), op("mul", Literal(8.0 / 3.0), v["z"]))
+    # the stack sits in a jitted helper: inlined through the pjit's inner jaxpr
+    a, b, c, o = _Var(), _Var(), _Var(), _Var()
+    inner = _Jaxpr([a, b, c], [_Eqn("stack", [a, b, c], [o], axis=0)], [o])
+    out = _Var()
+    eqns.append(_Eqn("pjit", [f0, f1, f2], [out], jaxpr=_Closed(inner)))
+    return _Closed(_Jaxpr([t, y, p], eqns, [out]))
+
+
+def test_jaxpr_walker_gives_the_traced_field():
+    ex = G.trace_jaxpr(_lorenz_jaxpr(), 3, 1)
+    ref = G.trace(lambda t, y, p: [10.0 * (y[1] - y[0]), p[0] * y[0] - y[1] - y[0] * y[2],
+                                   y[0] * y[1] - (8.0 / 3.0) * y[2]], 3, 1)
+    rng = np.random.default_rng(3)
+    for _ in range(5):
+        env = {"y": list(rng.normal(size=3)), "p": [float(rng.uniform(20, 30))]}
+        for a, b in zip(ex, ref):
+            assert G.evaluate(a, env) == G.evaluate(b, env)
+    d1 = G.Derived(None, 3, 1, True, exprs=ex)
+    d0 = G.Derived(lambda t, y, p: [10.0 * (y[1] - y[0]), p[0] * y[0] - y[1] - y[0] * y[2],
+                                    y[0] * y[1] - (8.0 / 3.0) * y[2]], 3, 1, True)
+    assert G.emit_struct(d1, "x", 1) == G.emit_struct(d0, "x", 1)
+
+
+def test_jaxpr_walker_matrix_field_and_refusals():
+    """f = A @ y (dot_general) + reduce_sum(y) * p[0], built from broadcast_in_dim; then the
+    refusals: a branch on the state and a primitive outside the table name themselves."""
+    A = np.array([[-2.0, 1.0, 0.0], [0.5, -3.0, 0.25], [0.0, 1.5, -4.0]])
+    t, y, p = _Var(), _Var(), _Var()
+    ay, s, s1, pb, sp, sb, out, p0 = (_Var() for _ in range(8))
+    Av = _Var()
+    eqns = [
+        _Eqn("dot_general", [Av, y], [ay], dimension_numbers=(((1,), (0,)), ((), ()))),
+        _Eqn("reduce_sum", [y], [s], axes=(0,)),
+        _Eqn("slice", [p], [p0], start_indices=(0,), limit_indices=(1,), strides=(1,)),
+        _Eqn("squeeze", [p0], [s1], dimensions=(0,)),
+        _Eqn("mul", [s, s1], [sp]),
+        _Eqn("broadcast_in_dim", [sp], [sb], shape=(3,), broadcast_dimensions=()),
+        _Eqn("add", [ay, sb], [out]),
+    ]
+    closed = _Closed(_Jaxpr([t, y, p], eqns, [out], constvars=[Av]), consts=[A])
+    ex = G.trace_jaxpr(closed, 3, 1)
+    yv = [0.3, -1.2, 2.0]
+    for i in range(3):
+        got = G.evaluate(ex[i], {"y": yv, "p": [0.7]})
+        assert abs(got - (A[i] @ yv + sum(yv) * 0.7)) < 1e-14
+    c = _Var()
+    bad = _Closed(_Jaxpr([t, y, p], [_Eqn("gt", [y, Literal(0.0)], [c])], [c]))
+    with pytest.raises(G.UnsupportedRHS, match="branch on the state"):
+        G.trace_jaxpr(bad, 3, 1)
+    w = _Var()
+    bad = _Closed(_Jaxpr([t, y, p], [_Eqn("while", [y], [w])], [w]))
+    with pytest.raises(G.UnsupportedRHS, match="'while'"):
+        G.trace_jaxpr(bad, 3, 1)

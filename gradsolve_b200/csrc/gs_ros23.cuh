@@ -72,7 +72,11 @@ __device__ __forceinline__ void lu_factor(LU<D>& f) {
   }
 }
 
-// x = W^-1 b
+// x = W^-1 b.  lu_factor exchanges whole rows, the multipliers of earlier columns included,
+// so L is stored in the final row order (W = P^T L U with P = P_{D-1} ... P_0): all row
+// exchanges are applied to b first, then L and U are solved.  (Interleaving each exchange with
+// its column's elimination would pair the multipliers, permuted by later pivots, with rows in
+// the wrong order whenever a pivot is taken after the first column.)
 template <int D>
 __device__ __forceinline__ void lu_solve(const LU<D>& f, const double* b, double* x) {
 #pragma unroll
@@ -89,6 +93,9 @@ __device__ __forceinline__ void lu_solve(const LU<D>& f, const double* b, double
       x[k] = sw ? xr : xk;
       x[r] = sw ? xk : xr;
     }
+  }
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
 #pragma unroll
     for (int r = k + 1; r < D; ++r) x[r] = x[r] - f.a[r * D + k] * x[k];
   }

@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <type_traits>
 
 #include "../../include/gsolve.h"
 #include "gs_coop.cuh"
@@ -319,49 +320,98 @@ int coop_refuse_mixed() {
                                 "components");
 }
 
+// The group sizes built for F: the default, then half and twice it where built.
 template <class F>
-int launch_coop_record(const gs::RecordArgs& a_in, cudaStream_t s, bool mixed) {
-  constexpr int G = gs::group_of<F>::value;
+int lane_choices(int* out, int cap) {
+  constexpr int G0 = gs::group_of<F>::value;
+  int k = 0;
+  if (cap > k) out[k] = G0;
+  ++k;
+  if constexpr (G0 > 1) {
+    if constexpr (gs::group_built<F::D, G0 / 2>()) {
+      if (cap > k) out[k] = G0 / 2;
+      ++k;
+    }
+    if constexpr (gs::group_built<F::D, 2 * G0>()) {
+      if (cap > k) out[k] = 2 * G0;
+      ++k;
+    }
+  }
+  return k;
+}
+
+// Launch `go` with the group size the precision flags ask for (GS_LANES; 0: the default):
+// go is called with an integral_constant of the size, so each kernel is instantiated only for
+// the built sizes.
+template <class F, class Go>
+int with_lanes(int precision, Go go) {
+  constexpr int G0 = gs::group_of<F>::value;
+  const int k = (precision & GS_LANES_MASK) >> GS_LANES_SHIFT;
+  const int G = k == 0 ? G0 : (1 << k);
+  if (G == G0) return go(std::integral_constant<int, G0>{});
+  if constexpr (gs::group_built<F::D, G0 / 2>()) {
+    if (G == G0 / 2) return go(std::integral_constant<int, G0 / 2>{});
+  }
+  if constexpr (gs::group_built<F::D, 2 * G0>()) {
+    if (G == 2 * G0) return go(std::integral_constant<int, 2 * G0>{});
+  }
+  return fail(GS_ERR_ARG, "a group of " + std::to_string(G) + " lanes per trajectory is not " +
+                              "built for D = " + std::to_string(F::D) + " (gs_lane_choices)");
+}
+
+template <class F>
+int launch_coop_record(const gs::RecordArgs& a_in, cudaStream_t s, bool mixed, int precision) {
   if (mixed) return coop_refuse_mixed();
   gs::RecordArgs a = a_in;
   a.ctrl = gs::make_ctrl_consts(F::D, 10);
-  const unsigned grid = grid_for(a.n * G);
-  if (!a.rec && !a.ckpt)
-    gs::tsit5_coop_record_kernel<F, G, false><<<grid, kBlock, 0, s>>>(a);
-  else
-    gs::tsit5_coop_record_kernel<F, G, true><<<grid, kBlock, 0, s>>>(a);
-  return cuda_check("tsit5_coop_record_kernel");
+  return with_lanes<F>(precision, [&](auto g) {
+    constexpr int G = decltype(g)::value;
+    const unsigned grid = grid_for(a.n * G);
+    if (!a.rec && !a.ckpt)
+      gs::tsit5_coop_record_kernel<F, G, false><<<grid, kBlock, 0, s>>>(a);
+    else
+      gs::tsit5_coop_record_kernel<F, G, true><<<grid, kBlock, 0, s>>>(a);
+    return cuda_check("tsit5_coop_record_kernel");
+  });
 }
 
 template <class F>
-int launch_coop_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed) {
-  constexpr int G = gs::group_of<F>::value;
+int launch_coop_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed, int precision) {
   if (mixed) return coop_refuse_mixed();
-  gs::tsit5_coop_replay_kernel<F, G><<<grid_for(a.n * G), kBlock, 0, s>>>(a);
-  return cuda_check("tsit5_coop_replay_kernel");
+  return with_lanes<F>(precision, [&](auto g) {
+    constexpr int G = decltype(g)::value;
+    gs::tsit5_coop_replay_kernel<F, G><<<grid_for(a.n * G), kBlock, 0, s>>>(a);
+    return cuda_check("tsit5_coop_replay_kernel");
+  });
 }
 
 template <class F>
-int launch_coop_adjoint(const gs::AdjointArgs& a, cudaStream_t s, bool mixed) {
-  constexpr int G = gs::group_of<F>::value;
-  constexpr int C = F::D / G;
+int launch_coop_adjoint(const gs::AdjointArgs& a, cudaStream_t s, bool mixed, int precision) {
   if (mixed) return coop_refuse_mixed();
-  SegCfg c;
-  int rc;
-  if ((rc = occupancy_cfg(gs::tsit5_coop_adjoint_kernel<F, G>,
-                          gs::adjoint_smem_doubles<C>(a.ck_every), &c)))
-    return rc;
-  gs::tsit5_coop_adjoint_kernel<F, G><<<grid_for_block(a.n * G, c.block), c.block, c.smem, s>>>(a);
-  return cuda_check("tsit5_coop_adjoint_kernel");
+  return with_lanes<F>(precision, [&](auto g) {
+    constexpr int G = decltype(g)::value;
+    constexpr int C = F::D / G;
+    SegCfg c;
+    int rc;
+    if ((rc = occupancy_cfg(gs::tsit5_coop_adjoint_kernel<F, G>,
+                            gs::adjoint_smem_doubles<C>(a.ck_every), &c)))
+      return rc;
+    gs::tsit5_coop_adjoint_kernel<F, G>
+        <<<grid_for_block(a.n * G, c.block), c.block, c.smem, s>>>(a);
+    return cuda_check("tsit5_coop_adjoint_kernel");
+  });
 }
 
 // mixed = float32 stages (GS_PREC_MIXED, gs_mixed.cuh), else float64 throughout.
 template <class F>
-int launch_tsit5_record(const gs::RecordArgs& a_in, cudaStream_t s, bool mixed, int sched) {
+int launch_tsit5_record(const gs::RecordArgs& a_in, cudaStream_t s, bool mixed, int sched,
+                        int precision) {
   if constexpr (kCoop<F>) {
     (void)sched;
-    return launch_coop_record<F>(a_in, s, mixed);
+    return launch_coop_record<F>(a_in, s, mixed, precision);
   } else {
+  if (precision & GS_LANES_MASK)
+    return fail(GS_ERR_ARG, "lanes per trajectory apply to fields of more than 8 components only");
   gs::RecordArgs a = a_in;
   a.ctrl = gs::make_ctrl_consts(F::D, 10);  // Tsit5: err^(-1/5) = m^(-1/10)
   if (sched == GS_SCHED_STATIC) {
@@ -381,10 +431,12 @@ int launch_tsit5_record(const gs::RecordArgs& a_in, cudaStream_t s, bool mixed, 
   }
 }
 template <class F>
-int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed) {
+int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed, int precision) {
   if constexpr (kCoop<F>) {
-    return launch_coop_replay<F>(a, s, mixed);
+    return launch_coop_replay<F>(a, s, mixed, precision);
   } else {
+  if (precision & GS_LANES_MASK)
+    return fail(GS_ERR_ARG, "lanes per trajectory apply to fields of more than 8 components only");
   if (mixed) {
     gs::tsit5_mixed_replay_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
     return cuda_check("tsit5_mixed_replay_kernel");
@@ -395,11 +447,13 @@ int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed) {
 }
 template <class F>
 int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool mixed,
-                         int sched, int variant) {
+                         int sched, int variant, int precision) {
   if constexpr (kCoop<F>) {
     (void)cap; (void)sched; (void)variant;
-    return launch_coop_adjoint<F>(a, s, mixed);
+    return launch_coop_adjoint<F>(a, s, mixed, precision);
   } else {
+  if (precision & GS_LANES_MASK)
+    return fail(GS_ERR_ARG, "lanes per trajectory apply to fields of more than 8 components only");
   if (sched == GS_SCHED_STATIC) {
     int rc;
     if (!mixed) {
@@ -678,13 +732,14 @@ int gs_tsit5_fwd_record(int field, int precision, long long n, const double* y0,
   gs::RecordArgs a{n, y0, p, t0, t1, rtol, atol, dt0, t1v, max_steps, cap, ckpt_every,
                    gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status};
   GS_TSIT5_DISPATCH(field, launch_tsit5_record, a, (cudaStream_t)stream,
-                    prec == GS_PREC_MIXED, forward_schedule(precision, t1v, ckpt))
+                    prec == GS_PREC_MIXED, forward_schedule(precision, t1v, ckpt), precision)
 }
 
 int gs_tsit5_replay(int field, int precision, long long n, const double* y0, const double* p,
                     double t0, const double* rec, const int* n_acc, int cap, int ckpt_every,
                     double* ckpt, double* y_final, void* stream) {
-  if (precision != GS_PREC_F64 && precision != GS_PREC_MIXED)
+  const int prec = precision & ~GS_LANES_MASK;
+  if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED)
     return fail(GS_ERR_PRECISION, "gs_tsit5_replay: unknown precision mode " + std::to_string(precision));
   if (n < 0) return fail(GS_ERR_ARG, "gs_tsit5_replay: n < 0");
   if (n == 0) return GS_OK;
@@ -699,7 +754,7 @@ int gs_tsit5_replay(int field, int precision, long long n, const double* y0, con
   gs::ReplayArgs a{n, y0, p, t0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every), ckpt,
                    y_final, cap};
   GS_TSIT5_DISPATCH(field, launch_tsit5_replay, a, (cudaStream_t)stream,
-                    precision == GS_PREC_MIXED)
+                    prec == GS_PREC_MIXED, precision)
 }
 
 int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, const double* rec,
@@ -715,7 +770,15 @@ int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, con
   if (n == 0) return GS_OK;
   gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp, cap};
   GS_TSIT5_DISPATCH(field, launch_tsit5_adjoint, a, cap, (cudaStream_t)stream,
-                    prec == GS_PREC_MIXED, adjoint_schedule(precision), precision & GS_ADJ_MASK)
+                    prec == GS_PREC_MIXED, adjoint_schedule(precision), precision & GS_ADJ_MASK,
+                    precision)
+}
+
+int gs_lane_choices(int field, int* out, int cap) {
+  int D, P, rc;
+  if ((rc = field_dims(field, &D, &P))) return rc;
+  if (!out && cap > 0) return fail(GS_ERR_ARG, "gs_lane_choices: null output");
+  GS_TSIT5_DISPATCH(field, lane_choices, out, cap)
 }
 
 int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,

@@ -356,6 +356,17 @@ struct Hires {
   }
 };
 
+// Group sizes built besides the default: half and twice it, where the lanes still hold equal
+// blocks of 2 to 8 components (a stencil reaches two components into a neighbour's block;
+// above 8 the lane's registers run out).
+template <int D, int G>
+constexpr bool group_built() {
+  return G == coop_group(D) ||
+         (G >= 2 && G <= 32 && coop_group(D) > 1 && (G == 2 * coop_group(D) ||
+                                                      2 * G == coop_group(D)) &&
+          D % G == 0 && D / G >= 2 && D / G <= 8);
+}
+
 // Lanes per trajectory of a field: its GROUP where it declares one (the stencil fields),
 // else 1.
 template <class F, class = void>

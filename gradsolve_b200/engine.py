@@ -14,6 +14,8 @@ reference's messages ("exhausted max_steps", "underflow").
 """
 from __future__ import annotations
 
+import ctypes
+
 import math
 from dataclasses import dataclass
 from typing import Optional
@@ -347,6 +349,76 @@ def _alloc_record(n: int, cap: int, dim: int, K: int, device) -> tuple:
     return rec, ckpt
 
 
+# ---- lanes per trajectory (fields of more than 8 components) -------------------------------
+# A group of G lanes integrates one trajectory of a field with D > 8 (gs_coop.cuh).  The
+# library builds the default G and, where the blocks stay 2..8 components, half and twice it
+# (gs_lane_choices); fewer lanes hold more of the state each (more registers, fewer resident
+# trajectories' worth of shuffles), more lanes fewer.  The autotuner times forward + reverse
+# pass for each on a sample of the caller's trajectories and keeps the fastest per field.
+_LANES: dict = {}  # field key -> lanes per trajectory chosen for it
+
+
+def lane_choices(spec: FieldSpec) -> list:
+    """Group sizes built for the field, the default first (one entry: [1] for the fields that
+    run one thread per trajectory)."""
+    L = _lib.lib_for(spec)
+    buf = (ctypes.c_int * 8)()
+    k = L.gs_lane_choices(spec.code, buf, 8)
+    if k < 0:
+        _lib.check(k, "gs_lane_choices", L)
+    return list(buf[: min(k, 8)])
+
+
+def set_lanes(spec: FieldSpec, lanes: Optional[int]) -> None:
+    """Pin the lanes per trajectory of a field (None: back to the default / autotuning)."""
+    if lanes is None:
+        _LANES.pop(spec.key, None)
+        return
+    if lanes not in lane_choices(spec):
+        raise ValueError(f"{lanes} lanes per trajectory are not built for {spec.key!r}; "
+                         f"built: {lane_choices(spec)}")
+    _LANES[spec.key] = int(lanes)
+
+
+def _lanes_flag(method: str, spec: FieldSpec) -> int:
+    G = _LANES.get(spec.key) if method == METHOD_TSIT5 else None
+    return 0 if not G or G == 1 else int(G).bit_length() - 1 << 12
+
+
+def autotune_lanes(spec: FieldSpec, y0: torch.Tensor, p: torch.Tensor, *, t0: float,
+                   t1: float, rtol: float, atol: float, t1v: Optional[torch.Tensor] = None,
+                   max_steps: int = 100000, sample: int = 1 << 16, reps: int = 2) -> int:
+    """Time forward + reverse pass for each built group size on up to ``sample`` of the
+    caller's trajectories; keep (and return) the fastest."""
+    choices = lane_choices(spec)
+    if len(choices) < 2:
+        _LANES[spec.key] = choices[0]
+        return choices[0]
+    m = min(y0.shape[0], sample)
+    ys, ps = y0[:m].contiguous(), p[:m].contiguous()
+    tv = None if t1v is None else t1v[:m].contiguous()
+    best, best_ms = choices[0], float("inf")
+    for G in choices:
+        _LANES[spec.key] = G
+        kw = dict(t0=t0, t1=t1, t1v=tv, rtol=rtol, atol=atol, max_steps=max_steps, checkpoint=4)
+        r = forward_record(METHOD_TSIT5, spec, ys, ps, **kw)
+        ybar = torch.ones_like(r.y_final)
+        adjoint(r, ps, ybar)
+        ms = float("inf")
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r = forward_record(METHOD_TSIT5, spec, ys, ps, workspace=r, **kw)
+            adjoint(r, ps, ybar)
+            e1.record()
+            e1.synchronize()
+            ms = min(ms, e0.elapsed_time(e1))
+        if ms < best_ms:
+            best, best_ms = G, ms
+    _LANES[spec.key] = best
+    return best
+
+
 def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tensor, *,
                    t0: float, t1: float, rtol: float, atol: float, dt0: Optional[float] = None,
                    t1v: Optional[torch.Tensor] = None, max_steps: int = 100000,
@@ -379,7 +451,8 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
         n_acc, n_rej, status = (
             (wsr.n_acc, wsr.n_rej, wsr.status) if wsr is not None else
             tuple(torch.empty(n, dtype=torch.int32, device=device) for _ in range(3)))
-        _lib.check(fn(spec.code, _PREC[precision] | _SCHED[schedule], n, _ptr(y0), _ptr(p),
+        _lib.check(fn(spec.code, _PREC[precision] | _SCHED[schedule] | _lanes_flag(method, spec),
+                      n, _ptr(y0), _ptr(p),
                       float(t0), _ptr(t1v), float(t1), float(rtol), float(atol),
                       -1.0 if dt0 is None else float(dt0), int(max_steps), 0, 1, None, None,
                       _ptr(yf), _ptr(n_acc), _ptr(n_rej), _ptr(status), _stream()),
@@ -387,6 +460,10 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
         empty = torch.empty(0, dtype=torch.float64, device=device)
         return Record(method, spec, n, float(t0), 0, 1, empty, empty, yf, n_acc, n_rej, status,
                       uneven=t1v is not None)
+    if (method == METHOD_TSIT5 and spec.dim > 8 and spec.key not in _LANES and n >= 4096 and
+            precision == "float64"):
+        autotune_lanes(spec, y0, p, t0=t0, t1=t1, t1v=t1v, rtol=rtol, atol=atol,
+                       max_steps=max_steps)
     if checkpoint == "auto" and tuned_ckpt_every(method, spec, precision) is None and n >= 4096:
         autotune_ckpt_every(method, spec, y0, p, t0=t0, t1=t1, t1v=t1v, rtol=rtol, atol=atol,
                             max_steps=max_steps, precision=precision)
@@ -418,7 +495,7 @@ def _forward_one(method, spec, y0, p, t1v, saveat_ts, cap, ws, kw) -> Record:
         rec, ckpt = ws.rec, ws.ckpt
     else:
         rec, ckpt = _alloc_record(n, cap, spec.dim, K, device)
-    mode = _PREC[precision] | _SCHED[kw["schedule"]]
+    mode = _PREC[precision] | _SCHED[kw["schedule"]] | _lanes_flag(method, spec)
     dt0_arg = -1.0 if kw["dt0"] is None else float(kw["dt0"])
     args = (float(kw["t0"]), _ptr(t1v), float(kw["t1"]), float(kw["rtol"]), float(kw["atol"]),
             dt0_arg, int(kw["max_steps"]), cap, K, _ptr(rec), _ptr(ckpt), _ptr(yf),
@@ -609,7 +686,8 @@ def _replay_one(r: Record, y0: torch.Tensor, p: torch.Tensor, *, write_ckpt: boo
     L = _lib.lib_for(r.spec)
     fn = L.gs_tsit5_replay if r.method == METHOD_TSIT5 else L.gs_ros23_replay
     yf = torch.empty_like(y0)
-    _lib.check(fn(r.spec.code, _PREC[precision], r.n, _ptr(y0), _ptr(p), float(r.t0),
+    _lib.check(fn(r.spec.code, _PREC[precision] | _lanes_flag(r.method, r.spec), r.n,
+                  _ptr(y0), _ptr(p), float(r.t0),
                   _ptr(r.rec), _ptr(r.n_acc), max(r.cap, 1), r.ckpt_every,
                   _ptr(r.ckpt) if write_ckpt else None, _ptr(yf), _stream()), fn.__name__, L)
     return yf
@@ -645,7 +723,7 @@ def _adjoint_one(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: boo
     ybar = ybar.contiguous()
     if schedule == "auto" and r.uneven:
         schedule = "refill"
-    flags = (_PREC[precision] | _SCHED[schedule] |
+    flags = (_PREC[precision] | _SCHED[schedule] | _lanes_flag(r.method, r.spec) |
              (_ADJ[variant] if r.method == METHOD_TSIT5 else 0))
     _lib.check(fn(r.spec.code, flags, r.n, _ptr(p), _ptr(r.rec), _ptr(r.n_acc),
                   max(r.cap, 1), _ptr(r.ckpt), r.ckpt_every, _ptr(ybar), _ptr(gy0), _ptr(gp),

@@ -85,6 +85,17 @@ extern "C" {
 #define GS_ADJ_STAGES 0x800
 #define GS_ADJ_MASK 0xC00
 
+/* Lanes per trajectory for the fields of more than 8 components (a group of G lanes
+ * integrates one trajectory, gs_coop.cuh), OR-ed into the precision argument of
+ * gs_tsit5_fwd_record, gs_tsit5_replay and gs_tsit5_adjoint: GS_LANES(k) asks for G = 2^k
+ * lanes; 0 takes the field's default.  gs_lane_choices lists the group sizes built for a
+ * field (the default first); any other is refused with GS_ERR_ARG.  Results do not depend
+ * on G beyond rounding (the error norm's and the parameter gradient's sums are grouped by
+ * lane). */
+#define GS_LANES_SHIFT 12
+#define GS_LANES_MASK 0x7000
+#define GS_LANES(log2_lanes) ((log2_lanes) << GS_LANES_SHIFT)
+
 /* per-trajectory status values written to status[] */
 #define GS_TRAJ_OK 0          /* reached t1 */
 #define GS_TRAJ_MAX_STEPS 1   /* max_steps attempts exhausted (or non-finite error) */
@@ -122,6 +133,13 @@ size_t gs_ckpt_bytes(int field, long long n, int cap, int ckpt_every);
 
 /* Largest checkpoint interval K the adjoint kernels accept. */
 int gs_max_ckpt_every(void);
+
+/* Lanes per trajectory built for a field: writes up to cap group sizes to out (the default
+ * first; 1 alone for fields integrated one thread per trajectory) and returns how many, or a
+ * negative GS_ERR_* for an unknown field.  No counterpart in the reference, whose fused lane
+ * is one thread per trajectory (gradsolve/warp/_warp_kernel.py:325-399); it serves the
+ * autotuner that picks the group size. */
+int gs_lane_choices(int field, int* out, int cap);
 
 /*
  * Adaptive Tsit5 forward solve that records the accepted step sizes.

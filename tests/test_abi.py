@@ -113,3 +113,17 @@ def test_argument_errors_are_status_codes(gslib):
     # padded-record conversion: S larger than the capacity
     rc = L.gs_record_from_padded(4, 9, a, 9, a, 8, ia, None)
     assert rc == -1
+
+
+def test_lane_choices_per_field(gslib):
+    """Host-only query: the group sizes built per field, the default first (the rule of
+    coop_group and group_built in gs_fields.cuh): one thread for D <= 8, 8 / 4 / 16 lanes for
+    D = 32, 2 lanes alone for D = 10 (5 components; neither 1 nor 4 lanes divide it well)."""
+    import ctypes
+    L = gslib.lib()
+    buf = (ctypes.c_int * 8)()
+    for code, want in ((1, [1]), (5008, [1]), (5032, [8, 4, 16]), (4032, [8, 4, 16]),
+                       (4010, [2]), (12, [1])):
+        k = L.gs_lane_choices(code, buf, 8)
+        assert list(buf[:k]) == want, code
+    assert L.gs_lane_choices(999, buf, 8) < 0

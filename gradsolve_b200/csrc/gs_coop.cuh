@@ -292,7 +292,9 @@ __global__ void __launch_bounds__(128) tsit5_coop_adjoint_kernel(const AdjointAr
   AdjBuf<C> buf(K);
   int b = 0;
   if (nseg > 0) coop_prefetch<F, G>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
-  for (int sg = nseg - 1; sg >= 0; --sg) {
+  const int top = warp_top_segments(nseg);
+  for (int sg = top - 1; sg >= 0; --sg) {
+    if (sg >= nseg) continue;  // in step with the warp's longest trajectory
     cp_async_wait_all();  // this segment's checkpoint block and dts have landed
     double y[C];
 #pragma unroll

@@ -384,7 +384,9 @@ __global__ void __launch_bounds__(128) tsit5_mixed_adjoint_kernel(const AdjointA
   AdjBuf<D> buf(K);
   int b = 0;
   if (nseg > 0) prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
-  for (int sg = nseg - 1; sg >= 0; --sg) {
+  const int top = warp_top_segments(nseg);
+  for (int sg = top - 1; sg >= 0; --sg) {
+    if (sg >= nseg) continue;  // in step with the warp's longest trajectory
     cp_async_wait_all();
     double y[D], c[D];
 #pragma unroll

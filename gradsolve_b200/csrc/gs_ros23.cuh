@@ -447,7 +447,9 @@ __device__ __forceinline__ void ros23_adjoint_body(const AdjointArgs& a) {
   AdjRosBuf<D, kKeep> buf(K);
   int b = 0;
   if (nseg > 0) prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
-  for (int sg = nseg - 1; sg >= 0; --sg) {
+  const int top = warp_top_segments(nseg);
+  for (int sg = top - 1; sg >= 0; --sg) {
+    if (sg >= nseg) continue;  // in step with the warp's longest trajectory
     cp_async_wait_all();  // this segment's checkpoint and dts have landed
     double y[D];
 #pragma unroll

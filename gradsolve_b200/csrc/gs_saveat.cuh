@@ -185,7 +185,9 @@ __global__ void __launch_bounds__(128) adjoint_saveat_kernel(const SaveatArgs a)
     prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
   }
   bool fin_done = false;  // cotangents of times >= t_fin joined lam
-  for (int sg = nseg - 1; sg >= 0; --sg) {
+  const int top = warp_top_segments(nseg);
+  for (int sg = top - 1; sg >= 0; --sg) {
+    if (sg >= nseg) continue;  // in step with the warp's longest trajectory
     cp_async_wait_all();
     double y[D], c[D];
 #pragma unroll

@@ -689,6 +689,18 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// The segment count of the warp's longest trajectory (over the lanes executing together
+// here).  The reverse passes sweep segments top-1 .. 0 in every lane, a lane idling while sg
+// lies beyond its own trajectory: the lanes then work on segment sg of adjacent trajectories
+// at the same time, so the checkpoint rows and dt sectors they fetch are neighbours in memory
+// and share DRAM bursts, where lanes each starting from their own last segment fetch
+// scattered sectors whose neighbours are evicted before their turn comes.  A warp takes as
+// long as before: it always ran until its longest trajectory was done (the idle time moves
+// from the end of the short trajectories to their start).
+__device__ __forceinline__ int warp_top_segments(int nseg) {
+  return __reduce_max_sync(__activemask(), nseg);
+}
+
 // Doubles per thread of the double-buffered dts + checkpoint area.
 template <int D>
 GS_HD int seg_io_doubles(int K) { return 2 * 2 * (((K + 1) >> 1) + ((D + 2) & ~1) / 2); }
@@ -796,7 +808,9 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a)
   AdjBuf<D> buf(K);
   int b = 0;
   if (nseg > 0) prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
-  for (int sg = nseg - 1; sg >= 0; --sg) {
+  const int top = warp_top_segments(nseg);
+  for (int sg = top - 1; sg >= 0; --sg) {
+    if (sg >= nseg) continue;  // in step with the warp's longest trajectory
     cp_async_wait_all();  // this segment's checkpoint and dts have landed
     double y[D];
 #pragma unroll
@@ -895,7 +909,9 @@ __device__ __forceinline__ void tsit5_adjoint_stages_body(const AdjointArgs& a) 
   AdjStageBuf<D> buf(K);
   int b = 0;
   if (nseg > 0) prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
-  for (int sg = nseg - 1; sg >= 0; --sg) {
+  const int top = warp_top_segments(nseg);
+  for (int sg = top - 1; sg >= 0; --sg) {
+    if (sg >= nseg) continue;  // in step with the warp's longest trajectory
     cp_async_wait_all();  // this segment's checkpoint and dts have landed
     double y[D];
 #pragma unroll

@@ -355,6 +355,33 @@ def headline_checks(torch, engine, spec, r, gp, y0_np, rho_np, inv, dev, m: int 
     }
 
 
+def mixed_precision_config(args, dev) -> dict:
+    """The mixed-precision configuration: Lotka-Volterra and Lorenz, n = 2^22 each, t in
+    [0, 20], rtol 1e-6 / atol 1e-8, float32 stages against plain float64 -- each workload's
+    float64 step rate and FP64 fraction, the float32-stage speed-up, and the float32-stage
+    gradient's error against float64 on the same mesh (`meets_1e-6` is the bar)."""
+    import copy
+
+    import torch
+    sub = copy.copy(args)
+    sub.steps, sub.warmup, sub.no_cpu, sub.no_mixed = 3, 2, True, False
+    sub.checkpoint, sub.schedule, sub.adjoint_variant = "auto", "auto", "auto"
+    out = {}
+    for name in ("lv_2e22", "lorenz_2e22"):
+        line = measure_workload(sub, name, WORKLOAD_N[name], dev)
+        g = line["groups"][0]
+        m = line["mixed"] or {}
+        err = (m.get("grad_rel_err_same_mesh") or {}).get(g["group"], {})
+        out[name] = {"n": g["n"], "f64_value": line["value"], "f64_ms_per_step": line["ms_per_step"],
+                     "f64_frac_of_fp64_peak": g["frac_of_fp64_peak"],
+                     "mixed_value": m.get("value"), "mixed_ms_per_step": m.get("ms_per_step"),
+                     "speedup_vs_f64": m.get("speedup_vs_f64"),
+                     "grad_rel_err_same_mesh": err, "meets_1e-6": m.get("meets_1e-6"),
+                     "oracle_parity_sample": line["oracle_parity_sample"].get(g["group"])}
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_b200(args) -> None:
     import torch
     import torch.distributed as dist
@@ -530,6 +557,15 @@ def run_b200(args) -> None:
                "ms_per_step": el * 1e3, "api": "gradsolve_b200.grad_closure + torch autograd",
                "ms_steps": [round((b - a) * 1e3, 3) for a, b in zip(marks, marks[1:])]}
 
+    # ---- the mixed-precision configuration (LV and Lorenz, 2^22 each, t in [0, 20]) -----
+    # float64 vs float32 stages, speed and gradient error, in the default run's line (one GPU)
+    config3 = None
+    if world == 1 and not args.no_config3:
+        clo = y0_h = rho_h = grad_h = None
+        gc.collect()
+        torch.cuda.empty_cache()
+        config3 = mixed_precision_config(args, dev)
+
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
@@ -596,7 +632,7 @@ def run_b200(args) -> None:
                    "l2": "flushed between timed steps (record traffic also >> L2)"},
         "gpu_launches": 2 * args.steps,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-        "parity_sample": checks,
+        "parity_sample": checks, "config3_mixed": config3,
         "fwd_ms": fwd_avg, "adj_ms": adj_avg, "mixed": mixed, "solve": solve or None,
         "fwd_ms_steps": [round(x, 3) for x in fwd_ms], "adj_ms_steps": [round(x, 3) for x in adj_ms],
     }
@@ -670,10 +706,6 @@ def run_workload(args) -> None:
     import torch
     import torch.distributed as dist
 
-    from gradsolve_b200 import engine, flops
-    from gradsolve_b200.fields import field_spec
-    from gradsolve_b200.sharding import max_over_ranks
-
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -683,9 +715,26 @@ def run_workload(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream()
     n = args.n if args.n != N_DEFAULT else WORKLOAD_N[args.workload]
-    groups = workload_groups(args.workload, n, 1000 * rank)
+    line = measure_workload(args, args.workload, n, dev, world, rank)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def measure_workload(args, name: str, n: int, dev, world: int = 1, rank: int = 0):
+    """One workload's JSON line (rank 0; None on the other ranks): the float64 step timed
+    over all groups, per-group FLOP rates, a 32-row oracle parity sample, the float32-stage
+    variant with its same-mesh and own-mesh gradient errors, and the CPU baseline."""
+    import torch
+
+    from gradsolve_b200 import engine, flops
+    from gradsolve_b200.fields import field_spec
+    from gradsolve_b200.sharding import max_over_ranks
+
+    stream = torch.cuda.current_stream()
+    groups = workload_groups(name, n, 1000 * rank)
     n_tot = n * world
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
     D = field_spec(groups[0].field).dim
@@ -845,13 +894,12 @@ def run_workload(args) -> None:
         mixed = {"value": n_tot / (m_ms * 1e-3), "ms_per_step": m_ms, "group_ms": m_groups,
                  "speedup_vs_f64": ms / m_ms, "grad_rel_err_same_mesh": same,
                  "grad_rel_err_own_mesh": own,
+                 "meets_1e-6": all(e["max"] <= 1e-6 for e in same.values()),
                  "note": "float32 stage increments on the tsit5 groups; rosenbrock23 groups "
                          "stay float64"}
     clk = clocks.stop()
     if rank != 0:
-        if world > 1:
-            dist.destroy_process_group()
-        return
+        return None
     fp64_peak = probe_fp64_tflops(torch, stream)
     for info in infos:
         info["frac_of_fp64_peak"] = info["tflops"] / fp64_peak
@@ -860,7 +908,7 @@ def run_workload(args) -> None:
     if world == 1 and not args.no_cpu:
         cpu = cpu_workload_rate(groups, args.cpu_seconds)
     line = {
-        "workload": args.workload, "metric": "trajectory grads/s (fwd+adjoint)",
+        "workload": name, "metric": "trajectory grads/s (fwd+adjoint)",
         "value": n_tot / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "dtype": "f64", "data": "synthetic (seeded numpy default_rng)", "groups": infos,
@@ -869,9 +917,7 @@ def run_workload(args) -> None:
         "config": {"n_per_gpu": n, "checkpoint_policy": str(args.checkpoint),
                    "schedule": args.schedule, "l2": "flushed between timed steps"},
     }
-    print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    return line
 
 
 def cpu_workload_rate(groups, target_s: float) -> dict:
@@ -995,6 +1041,8 @@ def main():
     ap.add_argument("--checkpoint", default="auto")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-config3", action="store_true",
+                    help="skip the mixed-precision configuration (LV and Lorenz at 2^22)")
     ap.add_argument("--no-checks", action="store_true",
                     help="skip the oracle/FD checks of 64 sampled trajectories (outside timing)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

@@ -6,8 +6,8 @@ A drop-in for the Tsit5 and Rosenbrock23 record-and-replay engines of gradsolve
 ABI of ``libgsolve.so`` (include/gsolve.h); PyTorch provides device memory, streams and
 autograd plumbing.
 """
-from .api import (ALIASES, ENGINE_REGISTRY, grad_closure, register_field,  # noqa: F401
-                  register_jax_field, register_linstiff, solve)
+from .api import (ALIASES, ENGINE_REGISTRY, grad_closure, record,  # noqa: F401
+                  register_field, register_jax_field, register_linstiff, solve)
 from .base import Problem, Route, SolveResult  # noqa: F401
 from .fields import field_for, field_spec  # noqa: F401
 

@@ -14,6 +14,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libgsolve.so"
 GS_OK = 0
 GS_PREC_F64 = 0
 GS_PREC_MIXED = 1
+GS_PREC_F32 = 2
 
 c_int, c_ll, c_double, c_size_t, c_void_p = (ctypes.c_int, ctypes.c_longlong, ctypes.c_double,
                                              ctypes.c_size_t, ctypes.c_void_p)
@@ -28,6 +29,8 @@ _SIGS = {
     "gs_record_bytes": (c_size_t, [c_ll, c_int]),
     "gs_ckpt_slots": (c_int, [c_int, c_int]),
     "gs_ckpt_bytes": (c_size_t, [c_int, c_ll, c_int, c_int]),
+    "gs_record_bytes_prec": (c_size_t, [c_int, c_ll, c_int]),
+    "gs_ckpt_bytes_prec": (c_size_t, [c_int, c_int, c_ll, c_int, c_int]),
     "gs_max_ckpt_every": (c_int, []),
     "gs_lane_choices": (c_int, [c_int, ctypes.POINTER(c_int), c_int]),
     "gs_tsit5_fwd_record": (c_int, [c_int, c_int, c_ll, c_void_p, c_void_p, c_double, c_void_p,

@@ -262,6 +262,32 @@ def build_replay_state(problem, y0, params, *, method: str, rtol: float, atol: f
     return state, y0_t, p_t
 
 
+def record(problem, y0, params, *, rtol: float = 1e-6, atol: float = 1e-9,
+           max_steps: Optional[int] = None, device: str = "cuda", precision: str = "float64",
+           engine: str = "auto"):
+    """The recording forward alone: ``(y_final (n, dim), n_acc (n,), dts_padded (n, S))`` as
+    host numpy arrays, ``S = max(n_acc)``, row j trajectory j's accepted dts zero-padded past
+    ``n_acc[j]`` -- the return of gradsolve/warp/warp_replay.py:120-182 (``record``, Tsit5) and
+    :295-337 (``record_rosenbrock``, for a stiff problem or ``engine="warp_rosenbrock"``).
+    ``precision="float32"`` records with the float32 kernels: the dts come back float32 and
+    y_final holds float32 values.  Trajectories that did not reach t1 raise."""
+    if precision not in ("float64", "float32"):
+        raise ValueError(f"unknown precision {precision!r}; known: ['float64', 'float32']")
+    spec = _require_field(problem)
+    if precision == "float32":
+        _check_float32_route(engine, spec, None)
+    name = _resolve(problem, engine, [])
+    ms = int(max_steps or DEFAULT_MAX_STEPS[name])
+    state, _y0, _p = build_replay_state(problem, y0, params, method=ENGINE_REGISTRY[name].method,
+                                        rtol=rtol, atol=atol, device=device, max_steps=ms,
+                                        checkpoint="auto", precision=precision)
+    r = state.record
+    yf = r.y_final.cpu().numpy()
+    if precision == "float32":
+        yf = yf.astype(np.float32)
+    return yf, r.n_acc.cpu().numpy(), r.padded_dts().cpu().numpy()
+
+
 def _make_reverse(name):
     method = ENGINE_REGISTRY[name].method
 
@@ -288,6 +314,10 @@ def _make_reverse(name):
 
             def kernel(z, p):  # the dense time series (n, k, dim), gradsolve/api.py:748-752
                 return saveat_apply(state, _as_tensor(z, dev), _as_tensor(p, dev), ts)
+        elif precision == "float32":
+            def kernel(z, p):  # float32 values; the closure's output is float32
+                return replay_apply(state, _as_tensor(z, dev),
+                                    _as_tensor(p, dev)).to(torch.float32)
         else:
             def kernel(z, p):
                 return replay_apply(state, _as_tensor(z, dev), _as_tensor(p, dev))
@@ -303,6 +333,31 @@ def _make_reverse(name):
     return reverse
 
 
+# Reference engine names whose lane has an f32 route (the registered-field record-and-replay
+# lanes, gradsolve/api.py:253-274); a general-RHS lane asked for float32 raises.
+F32_ENGINES = frozenset({"auto", ENGINE_TSIT5, ENGINE_ROS23, "warp_ode", "warp_replay",
+                         "warp_rosenbrock"})
+F32_MAX_DIM = 8
+
+
+def _check_float32_route(engine_name: str, spec: FieldSpec, saveat) -> None:
+    """precision="float32": the record, the replay and the reverse pass all in float32
+    (gradsolve/api.py:253-274, 876-887).  Refused, as the reference refuses it, on lanes
+    without an f32 route, and here also for fields above 8 components and for saveat, which
+    the float32 kernels do not cover."""
+    if engine_name not in F32_ENGINES:
+        raise ValueError(
+            f"precision='float32' is not supported on lane {engine_name!r}: the float32 "
+            "adjoint covers the registered-field record-and-replay lanes ('warp_replay', "
+            "'warp_ode', 'warp_rosenbrock'). Use one of those, or precision='float64'.")
+    if spec.dim > F32_MAX_DIM:
+        raise ValueError(f"precision='float32' is built for fields of at most {F32_MAX_DIM} "
+                         f"components; {spec.key!r} has {spec.dim}. Use precision='float64'.")
+    if saveat is not None:
+        raise ValueError("precision='float32' with saveat is not built; use "
+                         "precision='float64' for a dense time series.")
+
+
 def grad_closure(problem, y0, params, *, wrt="params", saveat=None, precision: str = "float64",
                  engine: str = "auto", rtol: float = 1e-6, atol: float = 1e-9,
                  device: str = "cuda", remat: Optional[bool] = None,
@@ -313,15 +368,12 @@ def grad_closure(problem, y0, params, *, wrt="params", saveat=None, precision: s
     The closure carries ``.route`` and ``.state`` (the device record)."""
     wrt_t = _normalize_wrt(wrt)
     reasons: list[str] = []
-    if precision == "float32":
-        # the reference's f32 route (record and replay all in float32, gradsolve/api.py:
-        # 253-274) is served by the mixed mode: float32 stages, float64 state/controller
-        precision = "mixed"
-        reasons.append("float32-served-by-mixed")
-    if precision not in ("float64", "mixed"):
+    if precision not in ("float64", "mixed", "float32"):
         raise ValueError(f"unknown precision {precision!r}; known: 'float64', 'mixed', "
                          "'float32'")
-    _require_field(problem)
+    fs = _require_field(problem)
+    if precision == "float32":
+        _check_float32_route(engine, fs, saveat)
     name = _resolve(problem, engine, reasons)
     spec = ENGINE_REGISTRY[name]
     if not spec.supports(problem):

@@ -13,6 +13,7 @@
 
 #include "../../include/gsolve.h"
 #include "gs_coop.cuh"
+#include "gs_f32.cuh"
 #include "gs_fields.cuh"
 #include "gs_mixed.cuh"
 #include "gs_ros23.cuh"
@@ -566,6 +567,89 @@ int launch_ros23_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, int 
   return launch_adjoint_persistent<F, gs::Ros23Step>(a, cap, s, sched == GS_SCHED_REFILL);
 }
 
+// ---- the float32 route (GS_PREC_F32, gs_f32.cuh) ----------------------------------------
+// One thread per trajectory, fields of at most 8 components; kMethod 0 = Tsit5, 1 =
+// Rosenbrock23.  AUTO is the static schedule here, per-trajectory end times included.
+int f32_schedule(int precision, const char* what) {
+  const int s = precision & GS_SCHED_MASK;
+  if (s != GS_SCHED_AUTO && s != GS_SCHED_STATIC)
+    return fail(GS_ERR_ARG, std::string(what) + ": the float32 route runs one thread per "
+                                                "trajectory (GS_SCHED_STATIC or AUTO)");
+  if (precision & (GS_LANES_MASK | GS_ADJ_MASK))
+    return fail(GS_ERR_ARG, std::string(what) + ": lanes and reverse-pass variants are "
+                                                "float64 options");
+  return GS_OK;
+}
+
+template <class F>
+constexpr bool kF32Built = F::D <= 8;
+
+int f32_refuse_dim() {
+  return fail(GS_ERR_PRECISION, "the float32 route is built for fields of at most 8 components");
+}
+
+template <class F, int kMethod>
+int launch_f32_record(const gs::RecordArgs& a, cudaStream_t s) {
+  if constexpr (!kF32Built<F>) {
+    (void)a; (void)s;
+    return f32_refuse_dim();
+  } else {
+    if (!a.rec && !a.ckpt)
+      gs::f32_record_kernel<F, kMethod, false><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    else
+      gs::f32_record_kernel<F, kMethod, true><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    return cuda_check("f32_record_kernel");
+  }
+}
+template <class F, int kMethod>
+int launch_f32_replay(const gs::ReplayArgs& a, cudaStream_t s) {
+  if constexpr (!kF32Built<F>) {
+    (void)a; (void)s;
+    return f32_refuse_dim();
+  } else {
+    gs::f32_replay_kernel<F, kMethod><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    return cuda_check("f32_replay_kernel");
+  }
+}
+template <class F, int kMethod>
+int launch_f32_adjoint(const gs::AdjointArgs& a, cudaStream_t s) {
+  if constexpr (!kF32Built<F>) {
+    (void)a; (void)s;
+    return f32_refuse_dim();
+  } else {
+    // K states of D floats per thread, counted in doubles for the occupancy helpers
+    SegCfg c;
+    int rc = occupancy_cfg(gs::f32_adjoint_kernel<F, kMethod>, (a.ck_every * F::D + 1) / 2, &c);
+    if (rc) return rc;
+    gs::f32_adjoint_kernel<F, kMethod><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+    return cuda_check("f32_adjoint_kernel");
+  }
+}
+template <class F>
+int launch_f32_tsit5_record(const gs::RecordArgs& a, cudaStream_t s) {
+  return launch_f32_record<F, 0>(a, s);
+}
+template <class F>
+int launch_f32_ros23_record(const gs::RecordArgs& a, cudaStream_t s) {
+  return launch_f32_record<F, 1>(a, s);
+}
+template <class F>
+int launch_f32_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s) {
+  return launch_f32_replay<F, 0>(a, s);
+}
+template <class F>
+int launch_f32_ros23_replay(const gs::ReplayArgs& a, cudaStream_t s) {
+  return launch_f32_replay<F, 1>(a, s);
+}
+template <class F>
+int launch_f32_tsit5_adjoint(const gs::AdjointArgs& a, cudaStream_t s) {
+  return launch_f32_adjoint<F, 0>(a, s);
+}
+template <class F>
+int launch_f32_ros23_adjoint(const gs::AdjointArgs& a, cudaStream_t s) {
+  return launch_f32_adjoint<F, 1>(a, s);
+}
+
 __global__ void device_tableau_kernel(double* out) {
   using T = gs::Tsit5;
   using C = gs::Ctrl;
@@ -713,6 +797,21 @@ size_t gs_ckpt_bytes(int field, long long n, int cap, int ckpt_every) {
          gs::kCtrlBytes;  // control block of the persistent kernels (work counters)
 }
 
+size_t gs_record_bytes_prec(int precision, long long n, int cap) {
+  if ((precision & GS_PREC_MASK) != GS_PREC_F32) return gs_record_bytes(n, cap);
+  if (n <= 0 || cap <= 0) return 0;
+  return (size_t)((cap + 3) / 4) * (size_t)n * 4u * sizeof(float);
+}
+
+size_t gs_ckpt_bytes_prec(int field, int precision, long long n, int cap, int ckpt_every) {
+  if ((precision & GS_PREC_MASK) != GS_PREC_F32) return gs_ckpt_bytes(field, n, cap, ckpt_every);
+  int D, P;
+  if (field_dims(field, &D, &P) != GS_OK || n <= 0) return 0;
+  return (size_t)gs_ckpt_slots(cap, ckpt_every) * (size_t)n * (size_t)gs::ckpt_width_f32(D) *
+             sizeof(float) +
+         gs::kCtrlBytes;
+}
+
 int gs_max_ckpt_every(void) { return gs::KMAX; }
 
 int gs_tsit5_fwd_record(int field, int precision, long long n, const double* y0,
@@ -721,7 +820,7 @@ int gs_tsit5_fwd_record(int field, int precision, long long n, const double* y0,
                         double* rec, double* ckpt, double* y_final, int* n_acc, int* n_rej,
                         int* status, void* stream) {
   const int prec = precision & GS_PREC_MASK;
-  if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED)
+  if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED && prec != GS_PREC_F32)
     return fail(GS_ERR_PRECISION, "gs_tsit5_fwd_record: unknown precision mode " + std::to_string(prec));
   int rc = check_record_args("gs_tsit5_fwd_record", n, y0, p, rtol, atol, max_steps, cap,
                              ckpt_every, rec, ckpt, y_final, n_acc, n_rej, status);
@@ -731,6 +830,10 @@ int gs_tsit5_fwd_record(int field, int precision, long long n, const double* y0,
   if (n == 0) return GS_OK;
   gs::RecordArgs a{n, y0, p, t0, t1, rtol, atol, dt0, t1v, max_steps, cap, ckpt_every,
                    gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status};
+  if (prec == GS_PREC_F32) {
+    if ((rc = f32_schedule(precision, "gs_tsit5_fwd_record"))) return rc;
+    GS_TSIT5_DISPATCH(field, launch_f32_tsit5_record, a, (cudaStream_t)stream)
+  }
   GS_TSIT5_DISPATCH(field, launch_tsit5_record, a, (cudaStream_t)stream,
                     prec == GS_PREC_MIXED, forward_schedule(precision, t1v, ckpt), precision)
 }
@@ -739,7 +842,7 @@ int gs_tsit5_replay(int field, int precision, long long n, const double* y0, con
                     double t0, const double* rec, const int* n_acc, int cap, int ckpt_every,
                     double* ckpt, double* y_final, void* stream) {
   const int prec = precision & ~GS_LANES_MASK;
-  if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED)
+  if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED && precision != GS_PREC_F32)
     return fail(GS_ERR_PRECISION, "gs_tsit5_replay: unknown precision mode " + std::to_string(precision));
   if (n < 0) return fail(GS_ERR_ARG, "gs_tsit5_replay: n < 0");
   if (n == 0) return GS_OK;
@@ -753,6 +856,9 @@ int gs_tsit5_replay(int field, int precision, long long n, const double* y0, con
   if (n == 0) return GS_OK;
   gs::ReplayArgs a{n, y0, p, t0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every), ckpt,
                    y_final, cap};
+  if (precision == GS_PREC_F32) {
+    GS_TSIT5_DISPATCH(field, launch_f32_tsit5_replay, a, (cudaStream_t)stream)
+  }
   GS_TSIT5_DISPATCH(field, launch_tsit5_replay, a, (cudaStream_t)stream,
                     prec == GS_PREC_MIXED, precision)
 }
@@ -761,7 +867,7 @@ int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, con
                      const int* n_acc, int cap, const double* ckpt, int ckpt_every,
                      const double* ybar, double* gy0, double* gp, void* stream) {
   const int prec = precision & GS_PREC_MASK;
-  if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED)
+  if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED && prec != GS_PREC_F32)
     return fail(GS_ERR_PRECISION, "gs_tsit5_adjoint: unknown precision mode " + std::to_string(prec));
   int rc = check_adjoint_args("gs_tsit5_adjoint", n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar);
   if (rc) return rc;
@@ -769,6 +875,10 @@ int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, con
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (n == 0) return GS_OK;
   gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp, cap};
+  if (prec == GS_PREC_F32) {
+    if ((rc = f32_schedule(precision, "gs_tsit5_adjoint"))) return rc;
+    GS_TSIT5_DISPATCH(field, launch_f32_tsit5_adjoint, a, (cudaStream_t)stream)
+  }
   GS_TSIT5_DISPATCH(field, launch_tsit5_adjoint, a, cap, (cudaStream_t)stream,
                     prec == GS_PREC_MIXED, adjoint_schedule(precision), precision & GS_ADJ_MASK,
                     precision)
@@ -786,8 +896,9 @@ int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,
                         double atol, double dt0, int max_steps, int cap, int ckpt_every,
                         double* rec, double* ckpt, double* y_final, int* n_acc, int* n_rej,
                         int* status, void* stream) {
-  if ((precision & GS_PREC_MASK) != GS_PREC_F64)
-    return fail(GS_ERR_PRECISION, "gs_ros23_fwd_record: Rosenbrock23 runs in float64 only");
+  const int prec = precision & GS_PREC_MASK;
+  if (prec != GS_PREC_F64 && prec != GS_PREC_F32)
+    return fail(GS_ERR_PRECISION, "gs_ros23_fwd_record: Rosenbrock23 runs in float64 or float32");
   int rc = check_record_args("gs_ros23_fwd_record", n, y0, p, rtol, atol, max_steps, cap,
                              ckpt_every, rec, ckpt, y_final, n_acc, n_rej, status);
   if (rc) return rc;
@@ -796,6 +907,10 @@ int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,
   if (n == 0) return GS_OK;
   gs::RecordArgs a{n, y0, p, t0, t1, rtol, atol, dt0, t1v, max_steps, cap, ckpt_every,
                    gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status};
+  if (prec == GS_PREC_F32) {
+    if ((rc = f32_schedule(precision, "gs_ros23_fwd_record"))) return rc;
+    GS_ROS23_DISPATCH(field, launch_f32_ros23_record, a, (cudaStream_t)stream)
+  }
   GS_ROS23_DISPATCH(field, launch_ros23_record, a, (cudaStream_t)stream,
                     forward_schedule(precision, t1v, ckpt))
 }
@@ -803,7 +918,7 @@ int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,
 int gs_ros23_replay(int field, int precision, long long n, const double* y0, const double* p,
                     double t0, const double* rec, const int* n_acc, int cap, int ckpt_every,
                     double* ckpt, double* y_final, void* stream) {
-  if (precision != GS_PREC_F64)
+  if (precision != GS_PREC_F64 && precision != GS_PREC_F32)
     return fail(GS_ERR_PRECISION, "gs_ros23_replay: precision mode not built");
   if (n < 0) return fail(GS_ERR_ARG, "gs_ros23_replay: n < 0");
   if (n == 0) return GS_OK;
@@ -817,20 +932,28 @@ int gs_ros23_replay(int field, int precision, long long n, const double* y0, con
   if (n == 0) return GS_OK;
   gs::ReplayArgs a{n, y0, p, t0, rec, n_acc, ckpt_every, gs_ckpt_slots(cap, ckpt_every), ckpt,
                    y_final, cap};
+  if (precision == GS_PREC_F32) {
+    GS_ROS23_DISPATCH(field, launch_f32_ros23_replay, a, (cudaStream_t)stream)
+  }
   GS_ROS23_DISPATCH(field, launch_ros23_replay, a, (cudaStream_t)stream)
 }
 
 int gs_ros23_adjoint(int field, int precision, long long n, const double* p, const double* rec,
                      const int* n_acc, int cap, const double* ckpt, int ckpt_every,
                      const double* ybar, double* gy0, double* gp, void* stream) {
-  if ((precision & GS_PREC_MASK) != GS_PREC_F64)
-    return fail(GS_ERR_PRECISION, "gs_ros23_adjoint: Rosenbrock23 runs in float64 only");
+  const int prec = precision & GS_PREC_MASK;
+  if (prec != GS_PREC_F64 && prec != GS_PREC_F32)
+    return fail(GS_ERR_PRECISION, "gs_ros23_adjoint: Rosenbrock23 runs in float64 or float32");
   int rc = check_adjoint_args("gs_ros23_adjoint", n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar);
   if (rc) return rc;
   int D, P;
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (n == 0) return GS_OK;
   gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp, cap};
+  if (prec == GS_PREC_F32) {
+    if ((rc = f32_schedule(precision, "gs_ros23_adjoint"))) return rc;
+    GS_ROS23_DISPATCH(field, launch_f32_ros23_adjoint, a, (cudaStream_t)stream)
+  }
   GS_ROS23_DISPATCH(field, launch_ros23_adjoint, a, cap, (cudaStream_t)stream,
                     adjoint_schedule(precision))
 }

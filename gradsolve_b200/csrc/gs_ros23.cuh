@@ -25,22 +25,22 @@
 
 namespace gs {
 
-template <int D>
+template <int D, class R = double>
 struct LU {
-  double a[D * D];  // L (unit, below diagonal) and U (on/above), row-swapped
-  double inv[D];    // 1 / U's diagonal
+  R a[D * D];  // L (unit, below diagonal) and U (on/above), row-swapped
+  R inv[D];         // 1 / U's diagonal
   int piv[D];
 };
 
-template <int D>
-__device__ __forceinline__ void lu_factor(LU<D>& f) {
+template <int D, class R>
+__device__ __forceinline__ void lu_factor(LU<D, R>& f) {
 #pragma unroll
   for (int col = 0; col < D; ++col) {
     int pv = col;
-    double big = fabs(f.a[col * D + col]);
+    R big = fabs(f.a[col * D + col]);
 #pragma unroll
     for (int r = col + 1; r < D; ++r) {
-      const double v = fabs(f.a[r * D + col]);
+      const R v = fabs(f.a[r * D + col]);
       if (v > big) {
         big = v;
         pv = r;
@@ -54,17 +54,17 @@ __device__ __forceinline__ void lu_factor(LU<D>& f) {
 #pragma unroll
         for (int r = col + 1; r < D; ++r) {
           const bool sw = r == pv;
-          const double u = f.a[col * D + c], v = f.a[r * D + c];
+          const R u = f.a[col * D + c], v = f.a[r * D + c];
           f.a[col * D + c] = sw ? v : u;
           f.a[r * D + c] = sw ? u : v;
         }
       }
     }
     // one reciprocal of the pivot serves the column's multipliers and the back substitutions
-    f.inv[col] = 1.0 / f.a[col * D + col];
+    f.inv[col] = R(1.0) / f.a[col * D + col];
 #pragma unroll
     for (int r = col + 1; r < D; ++r) {
-      const double factor = f.a[r * D + col] * f.inv[col];
+      const R factor = f.a[r * D + col] * f.inv[col];
       f.a[r * D + col] = factor;
 #pragma unroll
       for (int c = col + 1; c < D; ++c) f.a[r * D + c] = f.a[r * D + c] - factor * f.a[col * D + c];
@@ -77,8 +77,8 @@ __device__ __forceinline__ void lu_factor(LU<D>& f) {
 // exchanges are applied to b first, then L and U are solved.  (Interleaving each exchange with
 // its column's elimination would pair the multipliers, permuted by later pivots, with rows in
 // the wrong order whenever a pivot is taken after the first column.)
-template <int D>
-__device__ __forceinline__ void lu_solve(const LU<D>& f, const double* b, double* x) {
+template <int D, class R>
+__device__ __forceinline__ void lu_solve(const LU<D, R>& f, const R* b, R* x) {
 #pragma unroll
   for (int i = 0; i < D; ++i) x[i] = b[i];
 #pragma unroll
@@ -89,7 +89,7 @@ __device__ __forceinline__ void lu_solve(const LU<D>& f, const double* b, double
       // indexed access x[piv[k]] and moves x to local memory (a stack frame, L1/L2 traffic
       // every solve); as selects x stays in registers
       const bool sw = r == f.piv[k];
-      const double xk = x[k], xr = x[r];
+      const R xk = x[k], xr = x[r];
       x[k] = sw ? xr : xk;
       x[r] = sw ? xk : xr;
     }
@@ -102,7 +102,7 @@ __device__ __forceinline__ void lu_solve(const LU<D>& f, const double* b, double
 #pragma unroll
   for (int ii = 0; ii < D; ++ii) {
     const int i = D - 1 - ii;
-    double s = x[i];
+    R s = x[i];
 #pragma unroll
     for (int c = i + 1; c < D; ++c) s = s - f.a[i * D + c] * x[c];
     x[i] = s * f.inv[i];
@@ -110,11 +110,11 @@ __device__ __forceinline__ void lu_solve(const LU<D>& f, const double* b, double
 }
 
 // x = W^-T b   (W = P^T L U  =>  W^T = U^T L^T P)
-template <int D>
-__device__ __forceinline__ void lu_solve_t(const LU<D>& f, const double* b, double* x) {
+template <int D, class R>
+__device__ __forceinline__ void lu_solve_t(const LU<D, R>& f, const R* b, R* x) {
 #pragma unroll
   for (int i = 0; i < D; ++i) {
-    double s = b[i];
+    R s = b[i];
 #pragma unroll
     for (int jj = 0; jj < i; ++jj) s = s - f.a[jj * D + i] * x[jj];
     x[i] = s * f.inv[i];
@@ -122,7 +122,7 @@ __device__ __forceinline__ void lu_solve_t(const LU<D>& f, const double* b, doub
 #pragma unroll
   for (int ii = 0; ii < D; ++ii) {
     const int i = D - 1 - ii;
-    double s = x[i];
+    R s = x[i];
 #pragma unroll
     for (int r = i + 1; r < D; ++r) s = s - f.a[r * D + i] * x[r];
     x[i] = s;
@@ -136,61 +136,60 @@ __device__ __forceinline__ void lu_solve_t(const LU<D>& f, const double* b, doub
       // indexed access x[piv[k]] and moves x to local memory (a stack frame, L1/L2 traffic
       // every solve); as selects x stays in registers
       const bool sw = r == f.piv[k];
-      const double xk = x[k], xr = x[r];
+      const R xk = x[k], xr = x[r];
       x[k] = sw ? xr : xk;
       x[r] = sw ? xk : xr;
     }
   }
 }
 
-template <class F>
-__device__ __forceinline__ void ros23_build_w(const double* y, const double* p, double h,
-                                              LU<F::D>& W) {
+template <class F, class R = double>
+__device__ __forceinline__ void ros23_build_w(const R* y, const R* p, R h, LU<F::D, R>& W) {
   constexpr int D = F::D;
-  double J[D * D];
+  R J[D * D];
   F::jac(y, p, J);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
 #pragma unroll
-    for (int c = 0; c < D; ++c) W.a[i * D + c] = -Ros23::D * h * J[i * D + c];
-    W.a[i * D + i] = W.a[i * D + i] + 1.0;
+    for (int c = 0; c < D; ++c) W.a[i * D + c] = -R(Ros23::D) * h * J[i * D + c];
+    W.a[i * D + i] = W.a[i * D + i] + R(1.0);
   }
-  lu_factor<D>(W);
+  lu_factor(W);
 }
 
 // Shared part of the attempt and of the replay step: W factored, F0, k1, F1, k2, ynew.
-template <class F>
+template <class F, class R = double>
 struct RosCore {
   static constexpr int D = F::D;
-  LU<D> W;
-  double F0[D], k1[D], F1[D], k2p[D], k2[D];  // k2 = k2p + k1
+  LU<D, R> W;
+  R F0[D], k1[D], F1[D], k2p[D], k2[D];  // k2 = k2p + k1
 };
 
-template <class F>
-__device__ __forceinline__ void ros23_core(const double* y, const double* p, double h,
-                                           RosCore<F>& c, double* ynew) {
+template <class F, class R = double>
+__device__ __forceinline__ void ros23_core(const R* y, const R* p, R h, RosCore<F, R>& c,
+                                           R* ynew) {
   constexpr int D = F::D;
-  double s[D];
+  R s[D];
   ros23_build_w<F>(y, p, h, c.W);
   F::rhs(y, p, c.F0);
-  lu_solve<D>(c.W, c.F0, c.k1);
+  lu_solve(c.W, c.F0, c.k1);
 #pragma unroll
-  for (int i = 0; i < D; ++i) s[i] = y[i] + 0.5 * h * c.k1[i];
+  for (int i = 0; i < D; ++i) s[i] = y[i] + R(0.5) * h * c.k1[i];
   F::rhs(s, p, c.F1);
 #pragma unroll
   for (int i = 0; i < D; ++i) s[i] = c.F1[i] - c.k1[i];
-  lu_solve<D>(c.W, s, c.k2p);
+  lu_solve(c.W, s, c.k2p);
 #pragma unroll
   for (int i = 0; i < D; ++i) c.k2[i] = c.k2p[i] + c.k1[i];
 #pragma unroll
   for (int i = 0; i < D; ++i) ynew[i] = y[i] + h * c.k2[i];
 }
 
-template <class F>
-__device__ __forceinline__ void ros23_replay_step(double* y, const double* p, double dt) {
+template <class F, class R = double>
+__device__ __forceinline__ void ros23_replay_step(R* y, const R* p, R dt) {
   constexpr int D = F::D;
-  RosCore<F> c;
-  double yn[D];
+  RosCore<F, R> c;
+  R yn[D];
   ros23_core<F>(y, p, dt, c, yn);
 #pragma unroll
   for (int i = 0; i < D; ++i) y[i] = yn[i];
@@ -198,22 +197,21 @@ __device__ __forceinline__ void ros23_replay_step(double* y, const double* p, do
 
 // Reverse of one replay step from the step's forward quantities: the factors of W, k1, the
 // stage state s1 = y + dt/2 k1 and k2' = W \ (f(s1) - k1).
-template <class F>
-__device__ __forceinline__ void ros23_vjp_core(const double* y, const double* p, double dt,
-                                               const LU<F::D>& W, const double* k1,
-                                               const double* s1, const double* k2p, double* lam,
-                                               double* gp) {
+template <class F, class R = double>
+__device__ __forceinline__ void ros23_vjp_core(const R* y, const R* p, R dt, const LU<F::D, R>& W,
+                                               const R* k1, const R* s1, const R* k2p, R* lam,
+                                               R* gp) {
   constexpr int D = F::D;
-  double yb[D], k2b[D], k1b[D], r2b[D], s1b[D], r1b[D], G[D * D];
+  R yb[D], k2b[D], k1b[D], r2b[D], s1b[D], r1b[D], G[D * D];
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     yb[i] = lam[i];
     k2b[i] = dt * lam[i];
     k1b[i] = k2b[i];
-    s1b[i] = 0.0;
+    s1b[i] = R(0.0);
   }
-  lu_solve_t<D>(W, k2b, r2b);
-  const double scale = Ros23::D * dt;  // G = -d dt Wbar, Wbar = -(r2b k2p^T + r1b k1^T)
+  lu_solve_t(W, k2b, r2b);
+  const R scale = R(Ros23::D) * dt;  // G = -d dt Wbar, Wbar = -(r2b k2p^T + r1b k1^T)
 #pragma unroll
   for (int i = 0; i < D; ++i) {
 #pragma unroll
@@ -224,9 +222,9 @@ __device__ __forceinline__ void ros23_vjp_core(const double* y, const double* p,
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     yb[i] += s1b[i];
-    k1b[i] += 0.5 * dt * s1b[i];
+    k1b[i] += R(0.5) * dt * s1b[i];
   }
-  lu_solve_t<D>(W, k1b, r1b);
+  lu_solve_t(W, k1b, r1b);
 #pragma unroll
   for (int i = 0; i < D; ++i)
 #pragma unroll
@@ -239,15 +237,14 @@ __device__ __forceinline__ void ros23_vjp_core(const double* y, const double* p,
 
 // Reverse of one replay step at (y, dt), recomputing its forward quantities (the expressions
 // of ros23_core).
-template <class F>
-__device__ __forceinline__ void ros23_step_vjp(const double* y, const double* p, double dt,
-                                               double* lam, double* gp) {
+template <class F, class R = double>
+__device__ __forceinline__ void ros23_step_vjp(const R* y, const R* p, R dt, R* lam, R* gp) {
   constexpr int D = F::D;
-  RosCore<F> c;
-  double yn[D], s1[D];
+  RosCore<F, R> c;
+  R yn[D], s1[D];
   ros23_core<F>(y, p, dt, c, yn);
 #pragma unroll
-  for (int i = 0; i < D; ++i) s1[i] = y[i] + 0.5 * dt * c.k1[i];
+  for (int i = 0; i < D; ++i) s1[i] = y[i] + R(0.5) * dt * c.k1[i];
   ros23_vjp_core<F>(y, p, dt, c.W, c.k1, s1, c.k2p, lam, gp);
 }
 

@@ -213,59 +213,59 @@ __device__ __forceinline__ double wrms_sumsq(const double* e, const double* y, c
 // --- the shared stage arithmetic ------------------------------------------------------
 // Stages 2..6 inputs and k2..k6 from (y, k1, h).  Used by the forward, the replay and the
 // adjoint's recomputation so every kernel evaluates the same expressions.
-template <class F>
+template <class F, class R = double>
 struct Stages {
   static constexpr int D = F::D;
-  double k2[D], k3[D], k4[D], k5[D], k6[D];
+  R k2[D], k3[D], k4[D], k5[D], k6[D];
 };
 
-template <class F>
-__device__ __forceinline__ void tsit5_k2_to_k6(const double* y, const double* p, const double* k1,
-                                               double h, Stages<F>& S) {
+template <class F, class R = double>
+__device__ __forceinline__ void tsit5_k2_to_k6(const R* y, const R* p, const R* k1, R h,
+                                               Stages<F, R>& S) {
   constexpr int D = F::D;
   using T = Tsit5;
-  double s[D];
+  R s[D];
 #pragma unroll
-  for (int i = 0; i < D; ++i) s[i] = y[i] + h * (T::A21 * k1[i]);
+  for (int i = 0; i < D; ++i) s[i] = y[i] + h * (R(T::A21) * k1[i]);
   F::rhs(s, p, S.k2);
 #pragma unroll
-  for (int i = 0; i < D; ++i) s[i] = y[i] + h * (T::A31 * k1[i] + T::A32 * S.k2[i]);
+  for (int i = 0; i < D; ++i) s[i] = y[i] + h * (R(T::A31) * k1[i] + R(T::A32) * S.k2[i]);
   F::rhs(s, p, S.k3);
 #pragma unroll
   for (int i = 0; i < D; ++i)
-    s[i] = y[i] + h * (T::A41 * k1[i] + T::A42 * S.k2[i] + T::A43 * S.k3[i]);
+    s[i] = y[i] + h * (R(T::A41) * k1[i] + R(T::A42) * S.k2[i] + R(T::A43) * S.k3[i]);
   F::rhs(s, p, S.k4);
 #pragma unroll
   for (int i = 0; i < D; ++i)
-    s[i] = y[i] + h * (T::A51 * k1[i] + T::A52 * S.k2[i] + T::A53 * S.k3[i] + T::A54 * S.k4[i]);
+    s[i] = y[i] + h * (R(T::A51) * k1[i] + R(T::A52) * S.k2[i] + R(T::A53) * S.k3[i] + R(T::A54) * S.k4[i]);
   F::rhs(s, p, S.k5);
 #pragma unroll
   for (int i = 0; i < D; ++i)
-    s[i] = y[i] + h * (T::A61 * k1[i] + T::A62 * S.k2[i] + T::A63 * S.k3[i] + T::A64 * S.k4[i] +
-                       T::A65 * S.k5[i]);
+    s[i] = y[i] + h * (R(T::A61) * k1[i] + R(T::A62) * S.k2[i] + R(T::A63) * S.k3[i] + R(T::A64) * S.k4[i] +
+                       R(T::A65) * S.k5[i]);
   F::rhs(s, p, S.k6);
 }
 
-template <class F>
-__device__ __forceinline__ void tsit5_y5(const double* y, const double* k1, const Stages<F>& S,
-                                         double h, double* y5) {
+template <class F, class R = double>
+__device__ __forceinline__ void tsit5_y5(const R* y, const R* k1, const Stages<F, R>& S, R h,
+                                         R* y5) {
   using T = Tsit5;
 #pragma unroll
   for (int i = 0; i < F::D; ++i)
-    y5[i] = y[i] + h * (T::B1 * k1[i] + T::B2 * S.k2[i] + T::B3 * S.k3[i] + T::B4 * S.k4[i] +
-                        T::B5 * S.k5[i] + T::B6 * S.k6[i]);
+    y5[i] = y[i] + h * (R(T::B1) * k1[i] + R(T::B2) * S.k2[i] + R(T::B3) * S.k3[i] + R(T::B4) * S.k4[i] +
+                        R(T::B5) * S.k5[i] + R(T::B6) * S.k6[i]);
 }
 
 // One replay step (gradsolve/solvers/tsit5_step.py:80-102).  The B7*k7 term of the
 // reference is an exact +0 (B7 == 0), so k7 is not evaluated here.
-template <class F>
-__device__ __forceinline__ void tsit5_replay_step(double* y, const double* p, double dt) {
+template <class F, class R = double>
+__device__ __forceinline__ void tsit5_replay_step(R* y, const R* p, R dt) {
   constexpr int D = F::D;
-  double k1[D], yn[D];
-  Stages<F> S;
+  R k1[D], yn[D];
+  Stages<F, R> S;
   F::rhs(y, p, k1);
-  tsit5_k2_to_k6<F>(y, p, k1, dt, S);
-  tsit5_y5<F>(y, k1, S, dt, yn);
+  tsit5_k2_to_k6<F, R>(y, p, k1, dt, S);
+  tsit5_y5<F, R>(y, k1, S, dt, yn);
 #pragma unroll
   for (int i = 0; i < D; ++i) y[i] = yn[i];
 }
@@ -273,137 +273,137 @@ __device__ __forceinline__ void tsit5_replay_step(double* y, const double* p, do
 // Stage inputs s2..s6 of one step at (y, dt) -- the expressions of tsit5_k2_to_k6 -- and,
 // with kNext, the step's result (tsit5_y5), so a pass that keeps the stages for the reverse
 // sweep produces the same states as tsit5_replay_step.
-template <class F>
+template <class F, class R = double>
 struct StageStates {
   static constexpr int D = F::D;
-  double s2[D], s3[D], s4[D], s5[D], s6[D];
+  R s2[D], s3[D], s4[D], s5[D], s6[D];
   template <int M>
-  __device__ __forceinline__ void get(double* out) const {
-    const double* src = M == 2 ? s2 : M == 3 ? s3 : M == 4 ? s4 : M == 5 ? s5 : s6;
+  __device__ __forceinline__ void get(R* out) const {
+    const R* src = M == 2 ? s2 : M == 3 ? s3 : M == 4 ? s4 : M == 5 ? s5 : s6;
 #pragma unroll
     for (int i = 0; i < D; ++i) out[i] = src[i];
   }
 };
 
-template <class F, bool kNext>
-__device__ __forceinline__ void tsit5_stage_states(const double* y, const double* p, double dt,
-                                                   StageStates<F>& S, double* ynext) {
+template <class F, bool kNext, class R = double>
+__device__ __forceinline__ void tsit5_stage_states(const R* y, const R* p, R dt,
+                                                   StageStates<F, R>& S, R* ynext) {
   constexpr int D = F::D;
   using T = Tsit5;
-  double k1[D], k2[D], k3[D], k4[D], k5[D];
+  R k1[D], k2[D], k3[D], k4[D], k5[D];
   F::rhs(y, p, k1);
 #pragma unroll
-  for (int i = 0; i < D; ++i) S.s2[i] = y[i] + dt * (T::A21 * k1[i]);
+  for (int i = 0; i < D; ++i) S.s2[i] = y[i] + dt * (R(T::A21) * k1[i]);
   F::rhs(S.s2, p, k2);
 #pragma unroll
-  for (int i = 0; i < D; ++i) S.s3[i] = y[i] + dt * (T::A31 * k1[i] + T::A32 * k2[i]);
+  for (int i = 0; i < D; ++i) S.s3[i] = y[i] + dt * (R(T::A31) * k1[i] + R(T::A32) * k2[i]);
   F::rhs(S.s3, p, k3);
 #pragma unroll
   for (int i = 0; i < D; ++i)
-    S.s4[i] = y[i] + dt * (T::A41 * k1[i] + T::A42 * k2[i] + T::A43 * k3[i]);
+    S.s4[i] = y[i] + dt * (R(T::A41) * k1[i] + R(T::A42) * k2[i] + R(T::A43) * k3[i]);
   F::rhs(S.s4, p, k4);
 #pragma unroll
   for (int i = 0; i < D; ++i)
-    S.s5[i] = y[i] + dt * (T::A51 * k1[i] + T::A52 * k2[i] + T::A53 * k3[i] + T::A54 * k4[i]);
+    S.s5[i] = y[i] + dt * (R(T::A51) * k1[i] + R(T::A52) * k2[i] + R(T::A53) * k3[i] + R(T::A54) * k4[i]);
   F::rhs(S.s5, p, k5);
 #pragma unroll
   for (int i = 0; i < D; ++i)
-    S.s6[i] = y[i] + dt * (T::A61 * k1[i] + T::A62 * k2[i] + T::A63 * k3[i] + T::A64 * k4[i] +
-                           T::A65 * k5[i]);
+    S.s6[i] = y[i] + dt * (R(T::A61) * k1[i] + R(T::A62) * k2[i] + R(T::A63) * k3[i] + R(T::A64) * k4[i] +
+                           R(T::A65) * k5[i]);
   if (kNext) {
-    double k6[D];
+    R k6[D];
     F::rhs(S.s6, p, k6);
 #pragma unroll
     for (int i = 0; i < D; ++i)
-      ynext[i] = y[i] + dt * (T::B1 * k1[i] + T::B2 * k2[i] + T::B3 * k3[i] + T::B4 * k4[i] +
-                              T::B5 * k5[i] + T::B6 * k6[i]);
+      ynext[i] = y[i] + dt * (R(T::B1) * k1[i] + R(T::B2) * k2[i] + R(T::B3) * k3[i] + R(T::B4) * k4[i] +
+                              R(T::B5) * k5[i] + R(T::B6) * k6[i]);
   }
 }
 
 // Reverse of one replay step at (y, dt) given its stage inputs (Src::get<M> yields s_M):
 // lam <- (dy'/dy)^T lam, gp += (dy'/dp)^T lam.  Stage 7 carries weight B7 == 0, so its
 // cotangent is exactly zero and it is skipped.
-template <class F, class Src>
-__device__ __forceinline__ void tsit5_vjp_core(const double* y, const Src& src, const double* p,
-                                               double dt, double* lam, double* gp) {
+template <class F, class Src, class R = double>
+__device__ __forceinline__ void tsit5_vjp_core(const R* y, const Src& src, const R* p, R dt,
+                                               R* lam, R* gp) {
   constexpr int D = F::D;
   using T = Tsit5;
-  double st[D];
-  double g[D], kb1[D], kb2[D], kb3[D], kb4[D], kb5[D], kb6[D], sb[D], yb[D];
+  R st[D];
+  R g[D], kb1[D], kb2[D], kb3[D], kb4[D], kb5[D], kb6[D], sb[D], yb[D];
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     g[i] = dt * lam[i];
     yb[i] = lam[i];
-    kb1[i] = T::B1 * g[i];
-    kb2[i] = T::B2 * g[i];
-    kb3[i] = T::B3 * g[i];
-    kb4[i] = T::B4 * g[i];
-    kb5[i] = T::B5 * g[i];
-    kb6[i] = T::B6 * g[i];
+    kb1[i] = R(T::B1) * g[i];
+    kb2[i] = R(T::B2) * g[i];
+    kb3[i] = R(T::B3) * g[i];
+    kb4[i] = R(T::B4) * g[i];
+    kb5[i] = R(T::B5) * g[i];
+    kb6[i] = R(T::B6) * g[i];
   }
   // stage 6
   src.template get<6>(st);
 #pragma unroll
-  for (int i = 0; i < D; ++i) sb[i] = 0.0;
+  for (int i = 0; i < D; ++i) sb[i] = R(0.0);
   F::vjp(st, p, kb6, sb, gp);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     yb[i] += sb[i];
-    const double u = dt * sb[i];
-    kb1[i] += T::A61 * u;
-    kb2[i] += T::A62 * u;
-    kb3[i] += T::A63 * u;
-    kb4[i] += T::A64 * u;
-    kb5[i] += T::A65 * u;
+    const R u = dt * sb[i];
+    kb1[i] += R(T::A61) * u;
+    kb2[i] += R(T::A62) * u;
+    kb3[i] += R(T::A63) * u;
+    kb4[i] += R(T::A64) * u;
+    kb5[i] += R(T::A65) * u;
   }
   // stage 5
   src.template get<5>(st);
 #pragma unroll
-  for (int i = 0; i < D; ++i) sb[i] = 0.0;
+  for (int i = 0; i < D; ++i) sb[i] = R(0.0);
   F::vjp(st, p, kb5, sb, gp);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     yb[i] += sb[i];
-    const double u = dt * sb[i];
-    kb1[i] += T::A51 * u;
-    kb2[i] += T::A52 * u;
-    kb3[i] += T::A53 * u;
-    kb4[i] += T::A54 * u;
+    const R u = dt * sb[i];
+    kb1[i] += R(T::A51) * u;
+    kb2[i] += R(T::A52) * u;
+    kb3[i] += R(T::A53) * u;
+    kb4[i] += R(T::A54) * u;
   }
   // stage 4
   src.template get<4>(st);
 #pragma unroll
-  for (int i = 0; i < D; ++i) sb[i] = 0.0;
+  for (int i = 0; i < D; ++i) sb[i] = R(0.0);
   F::vjp(st, p, kb4, sb, gp);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     yb[i] += sb[i];
-    const double u = dt * sb[i];
-    kb1[i] += T::A41 * u;
-    kb2[i] += T::A42 * u;
-    kb3[i] += T::A43 * u;
+    const R u = dt * sb[i];
+    kb1[i] += R(T::A41) * u;
+    kb2[i] += R(T::A42) * u;
+    kb3[i] += R(T::A43) * u;
   }
   // stage 3
   src.template get<3>(st);
 #pragma unroll
-  for (int i = 0; i < D; ++i) sb[i] = 0.0;
+  for (int i = 0; i < D; ++i) sb[i] = R(0.0);
   F::vjp(st, p, kb3, sb, gp);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     yb[i] += sb[i];
-    const double u = dt * sb[i];
-    kb1[i] += T::A31 * u;
-    kb2[i] += T::A32 * u;
+    const R u = dt * sb[i];
+    kb1[i] += R(T::A31) * u;
+    kb2[i] += R(T::A32) * u;
   }
   // stage 2
   src.template get<2>(st);
 #pragma unroll
-  for (int i = 0; i < D; ++i) sb[i] = 0.0;
+  for (int i = 0; i < D; ++i) sb[i] = R(0.0);
   F::vjp(st, p, kb2, sb, gp);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     yb[i] += sb[i];
-    kb1[i] += T::A21 * (dt * sb[i]);
+    kb1[i] += R(T::A21) * (dt * sb[i]);
   }
   // stage 1 (s1 = y)
   F::vjp(y, p, kb1, yb, gp);
@@ -412,11 +412,10 @@ __device__ __forceinline__ void tsit5_vjp_core(const double* y, const Src& src, 
 }
 
 // Reverse of one replay step, recomputing its stages from y.
-template <class F>
-__device__ __forceinline__ void tsit5_step_vjp(const double* y, const double* p, double dt,
-                                               double* lam, double* gp) {
-  StageStates<F> S;
-  tsit5_stage_states<F, false>(y, p, dt, S, nullptr);
+template <class F, class R = double>
+__device__ __forceinline__ void tsit5_step_vjp(const R* y, const R* p, R dt, R* lam, R* gp) {
+  StageStates<F, R> S;
+  tsit5_stage_states<F, false, R>(y, p, dt, S, nullptr);
   tsit5_vjp_core<F>(y, S, p, dt, lam, gp);
 }
 

@@ -27,7 +27,8 @@ from .fields import FieldSpec
 
 METHOD_TSIT5 = "tsit5"
 METHOD_ROS23 = "rosenbrock23"
-_PREC = {"float64": _lib.GS_PREC_F64, "mixed": _lib.GS_PREC_MIXED}
+_PREC = {"float64": _lib.GS_PREC_F64, "mixed": _lib.GS_PREC_MIXED,
+         "float32": _lib.GS_PREC_F32}
 # scheduling flags (include/gsolve.h GS_SCHED_*): one thread per trajectory, persistent lanes
 # refilled from a work counter, or persistent lanes with strided assignment
 _SCHED = {"auto": 0x000, "static": 0x100, "refill": 0x200, "strided": 0x300}
@@ -47,6 +48,19 @@ def _stream() -> int:
 
 def ckpt_width(dim: int) -> int:
     return (dim + 2) & ~1
+
+
+def ckpt_width_f32(dim: int) -> int:
+    """Floats per checkpoint row of the float32 route: the state and the time, rounded up
+    to 16 bytes."""
+    return (dim + 4) & ~3
+
+
+def record_dtype(precision: str) -> torch.dtype:
+    """Element type of the dt record and the checkpoints: float32 on the float32 route (the
+    reference's f32 lane records float32 dts, gradsolve/warp/warp_replay.py:87-94), float64
+    otherwise (the mixed mode keeps float64 time and state)."""
+    return torch.float32 if precision == "float32" else torch.float64
 
 
 def choose_ckpt_every(policy, dim: int, n: int, cap: int, budget_bytes: Optional[int],
@@ -140,8 +154,8 @@ class Record:
     t0: float
     cap: int
     ckpt_every: int
-    rec: torch.Tensor        # chunked dt record (flat float64)
-    ckpt: torch.Tensor       # checkpoints (flat float64)
+    rec: torch.Tensor        # chunked dt record (flat; float32 on the float32 route)
+    ckpt: torch.Tensor       # checkpoints (flat; float32 on the float32 route)
     y_final: torch.Tensor    # (n, D)
     n_acc: torch.Tensor      # (n,) int32
     n_rej: torch.Tensor      # (n,) int32
@@ -150,9 +164,11 @@ class Record:
     ys: Optional[torch.Tensor] = None  # (n, K, D) dense output of the forward, if asked for
 
     def padded_dts(self, S: Optional[int] = None) -> torch.Tensor:
-        """The record in the reference's (n, S) zero-padded layout."""
+        """The record in the reference's (n, S) zero-padded layout, in the record's type."""
         if S is None:
             S = int(self.n_acc.max().item()) if self.n else 0
+        if self.rec.dtype != torch.float64:
+            return self.dts_rows(torch.arange(self.n, device=self.rec.device), S)
         out = torch.zeros((self.n, S), dtype=torch.float64, device=self.rec.device)
         L = _lib.lib_for(self.spec)
         _lib.check(L.gs_record_to_padded(self.n, self.cap, _ptr(self.rec), _ptr(self.n_acc), S,
@@ -221,7 +237,8 @@ class RecordSet:
 
     @property
     def nbytes(self) -> int:
-        return sum(r.rec.numel() * 8 + r.ckpt.numel() * 8 for _, r in self.parts)
+        return sum(r.rec.numel() * r.rec.element_size() + r.ckpt.numel() * r.ckpt.element_size()
+                   for _, r in self.parts)
 
     def plan_rows(self) -> list:
         """For each part, the rows whose final tier it is, longest first (by this record's
@@ -242,10 +259,14 @@ class RecordSet:
             out.append(rows)
         return out
 
+    @property
+    def rec_dtype(self) -> torch.dtype:
+        return self.parts[0][1].rec.dtype
+
     def padded_dts(self, S: Optional[int] = None) -> torch.Tensor:
         if S is None:
             S = int(self.n_acc.max().item()) if self.n else 0
-        out = torch.zeros((self.n, S), dtype=torch.float64, device=self.y_final.device)
+        out = torch.zeros((self.n, S), dtype=self.rec_dtype, device=self.y_final.device)
         for rows, r in self.parts:
             w = min(S, r.cap)  # a tier holds at most its capacity
             part = r.padded_dts(w)
@@ -260,7 +281,7 @@ class RecordSet:
         rows = rows.to(device=self.y_final.device, dtype=torch.int64)
         if S is None:
             S = int(self.n_acc[rows].max().item()) if rows.numel() else 0
-        out = torch.zeros((rows.numel(), S), dtype=torch.float64, device=rows.device)
+        out = torch.zeros((rows.numel(), S), dtype=self.rec_dtype, device=rows.device)
         for prow, r in self.parts:
             if prow is None:
                 out.copy_(r.dts_rows(rows, S))
@@ -338,10 +359,19 @@ def _over_parts(r, fn) -> list:
     return [(parts[k][0], out[k]) for k in range(len(parts))]
 
 
-def _alloc_record(n: int, cap: int, dim: int, K: int, device) -> tuple:
+def _alloc_record(n: int, cap: int, dim: int, K: int, device,
+                  precision: str = "float64") -> tuple:
     L = _lib.lib()
-    rec_elems = L.gs_record_bytes(n, cap) // 8
     slots = L.gs_ckpt_slots(cap, K)
+    if precision == "float32":
+        # half the float64 record (gs_record_bytes_prec); float32 checkpoint rows + the
+        # 256-byte control block
+        rec = torch.empty(max(L.gs_record_bytes_prec(_lib.GS_PREC_F32, n, cap) // 4, 4),
+                          dtype=torch.float32, device=device)
+        ckpt = torch.empty(slots * n * ckpt_width_f32(dim) + 2 * CTRL_DOUBLES,
+                           dtype=torch.float32, device=device)
+        return rec, ckpt
+    rec_elems = L.gs_record_bytes(n, cap) // 8
     rec = torch.empty(max(rec_elems, 2), dtype=torch.float64, device=device)
     # checkpoint slots + the persistent kernels' 256-byte control block (gs_ckpt_bytes)
     ckpt = torch.empty(slots * n * ckpt_width(dim) + CTRL_DOUBLES, dtype=torch.float64,
@@ -491,10 +521,11 @@ def _forward_one(method, spec, y0, p, t1v, saveat_ts, cap, ws, kw) -> Record:
     n_acc, n_rej, status = ((ws.n_acc, ws.n_rej, ws.status) if ok else
                             tuple(torch.empty(n, dtype=torch.int32, device=device)
                                   for _ in range(3)))
-    if ok and ws.cap == cap and ws.ckpt_every == K and ws.rec.numel() > 2:
+    if (ok and ws.cap == cap and ws.ckpt_every == K and ws.rec.numel() > 2 and
+            ws.rec.dtype == record_dtype(precision)):
         rec, ckpt = ws.rec, ws.ckpt
     else:
-        rec, ckpt = _alloc_record(n, cap, spec.dim, K, device)
+        rec, ckpt = _alloc_record(n, cap, spec.dim, K, device, precision)
     mode = _PREC[precision] | _SCHED[kw["schedule"]] | _lanes_flag(method, spec)
     dt0_arg = -1.0 if kw["dt0"] is None else float(kw["dt0"])
     args = (float(kw["t0"]), _ptr(t1v), float(kw["t1"]), float(kw["rtol"]), float(kw["atol"]),
@@ -706,8 +737,8 @@ def adjoint(r, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
     the segment's replay evaluates, "recompute" re-evaluates every step's stages in the
     reverse sweep; "auto" is "stages" while its buffer leaves it at least 3/5 of the
     recomputing kernel's resident threads, else "recompute"."""
-    if schedule == "auto" and r.uneven:
-        schedule = "refill"
+    if schedule == "auto" and r.uneven and precision != "float32":
+        schedule = "refill"  # (the float32 route runs one thread per trajectory)
     res = _over_parts(r, lambda rr, rows: _adjoint_one(
         rr, _take(p, rows), _take(ybar, rows), want_y0=want_y0, want_p=want_p,
         precision=precision, schedule=schedule, variant=variant))
@@ -721,7 +752,7 @@ def _adjoint_one(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: boo
     gy0 = torch.empty((r.n, r.spec.dim), dtype=torch.float64, device=p.device) if want_y0 else None
     gp = torch.empty((r.n, p.shape[1]), dtype=torch.float64, device=p.device) if want_p else None
     ybar = ybar.contiguous()
-    if schedule == "auto" and r.uneven:
+    if schedule == "auto" and r.uneven and precision != "float32":
         schedule = "refill"
     flags = (_PREC[precision] | _SCHED[schedule] | _lanes_flag(r.method, r.spec) |
              (_ADJ[variant] if r.method == METHOD_TSIT5 else 0))

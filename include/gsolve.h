@@ -58,6 +58,13 @@ extern "C" {
 
 #define GS_PREC_F64 0   /* everything float64 */
 #define GS_PREC_MIXED 1 /* float32 stages/RHS; float64 time, controller, error norm, state */
+/* Everything float32 (state, stages, time, error norm, controller): the reference's
+ * precision="float32" lane (gradsolve/api.py:253-274, gradsolve/warp/warp_replay.py:87-94, 140-160, 200-219).
+ * rec and ckpt then hold float32 data -- size them with gs_record_bytes_prec /
+ * gs_ckpt_bytes_prec (half the float64 record) -- while y0, p, y_final, cotangents and
+ * gradients stay float64 arrays holding float32 values.  Tsit5 and Rosenbrock23, fields of
+ * at most 8 components, one thread per trajectory (STATIC or AUTO schedule), no saveat. */
+#define GS_PREC_F32 2
 #define GS_PREC_MASK 0xff
 
 /* Scheduling flags, OR-ed into the precision argument of the forward and adjoint entry
@@ -130,6 +137,12 @@ int gs_ckpt_slots(int cap, int ckpt_every);
 
 /* Bytes of the checkpoint buffer for (field, n, cap, K); 0 for an unknown field. */
 size_t gs_ckpt_bytes(int field, long long n, int cap, int ckpt_every);
+
+/* The two sizes above for a precision mode: GS_PREC_F32 records 4-byte steps (the record
+ * is exactly half the float64 one) and 4-byte checkpoint rows of D+1 values rounded up to a
+ * multiple of 4; any other mode gives the float64 sizes.  0 for an unknown field. */
+size_t gs_record_bytes_prec(int precision, long long n, int cap);
+size_t gs_ckpt_bytes_prec(int field, int precision, long long n, int cap, int ckpt_every);
 
 /* Largest checkpoint interval K the adjoint kernels accept. */
 int gs_max_ckpt_every(void);

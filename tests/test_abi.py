@@ -70,6 +70,14 @@ def test_workspace_sizes(gslib):
     assert L.gs_ckpt_bytes(2, 7, 100, 1) == 101 * 7 * 4 * 8 + ctrl     # vdp: CW = 4
     assert L.gs_ckpt_bytes(4008, 7, 100, 1) == 101 * 7 * 10 * 8 + ctrl  # linear_8: CW = 10
     assert L.gs_max_ckpt_every() == 64
+    # the float32 route: 4-byte steps (exactly half the record) and 16-byte checkpoint rows
+    F32 = gslib.GS_PREC_F32
+    for n, cap in ((10, 5), (3, 1), (1000, 4099)):
+        assert 2 * L.gs_record_bytes_prec(F32, n, cap) == L.gs_record_bytes(n, cap)
+        assert L.gs_record_bytes_prec(0, n, cap) == L.gs_record_bytes(n, cap)
+    assert L.gs_ckpt_bytes_prec(1, F32, 7, 100, 10) == 11 * 7 * 4 * 4 + ctrl     # lorenz: 4
+    assert L.gs_ckpt_bytes_prec(4008, F32, 7, 100, 1) == 101 * 7 * 12 * 4 + ctrl  # linear_8: 12
+    assert L.gs_ckpt_bytes_prec(4008, 0, 7, 100, 1) == L.gs_ckpt_bytes(4008, 7, 100, 1)
 
 
 def test_argument_errors_are_status_codes(gslib):
@@ -105,6 +113,17 @@ def test_argument_errors_are_status_codes(gslib):
     assert rc == -2 and b"Jacobian" in L.gs_last_error()
     # precision not built
     rc = L.gs_tsit5_adjoint(1, 7, 4, a, a, ia, 8, a, 2, a, a, a, None)
+    assert rc == -4
+    # the float32 route: one thread per trajectory only, no lanes or reverse-pass variants,
+    # Rosenbrock23 included; fields above 8 components refused
+    rc = L.gs_tsit5_fwd_record(1, 2 | 0x200, 4, a, a, 0.0, None, 1.0, 1e-6, 1e-9, -1.0, 10, 8,
+                               2, a, a, a, ia, ia, ia, None)
+    assert rc == -1 and b"one thread per trajectory" in L.gs_last_error()
+    rc = L.gs_tsit5_adjoint(1, 2 | 0x800, 4, a, a, ia, 8, a, 2, a, a, a, None)
+    assert rc == -1 and b"float64 options" in L.gs_last_error()
+    rc = L.gs_ros23_adjoint(10, 2 | 0x300, 4, a, a, ia, 8, a, 2, a, a, a, None)
+    assert rc == -1
+    rc = L.gs_tsit5_replay(5032, 2 | 0x1000, 4, a, a, 0.0, a, ia, 8, 2, a, a, None)
     assert rc == -4
     # empty ensemble is a no-op success
     rc = L.gs_tsit5_fwd_record(1, 0, 0, a, a, 0.0, None, 1.0, 1e-6, 1e-9, -1.0, 10, 8, 2,

@@ -81,7 +81,7 @@ def test_own_mesh_mixed_forward(gslib, cuda, case, field):
     assert ey <= 1e-5
 
 
-def test_grad_closure_mixed_and_float32_route(gslib, oracle, cuda):
+def test_grad_closure_mixed_and_float32_routes(gslib, oracle, cuda):
     import gradsolve_b200 as gsb
 
     class LV:
@@ -94,10 +94,11 @@ def test_grad_closure_mixed_and_float32_route(gslib, oracle, cuda):
     g = load_golden("lv_mixed")
     for prec in ("mixed", "float32"):
         clo = gsb.grad_closure(LV(), g["y0"], g["params"], rtol=1e-6, atol=1e-8, precision=prec)
-        if prec == "float32":
-            assert "float32-served-by-mixed" in clo.route.reason
+        assert clo.route.reason is None  # float32 is its own route, not the mixed mode
         p = torch.tensor(g["params"], device="cuda", requires_grad=True)
-        (clo(p) ** 2).sum().backward()
+        out = clo(p)
+        assert out.dtype == (torch.float32 if prec == "float32" else torch.float64)
+        (out ** 2).sum().backward()
         assert torch.isfinite(p.grad).all()
     with pytest.raises(ValueError, match="unknown precision"):
         gsb.grad_closure(LV(), g["y0"], g["params"], precision="float16")

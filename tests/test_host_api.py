@@ -116,6 +116,34 @@ def test_engine_resolution_and_aliases():
         api._resolve(S(), "diffrax", [])
 
 
+def test_float32_route_refusals():
+    """precision="float32" is refused, before anything runs, where it has no float32 kernels:
+    reference lanes without an f32 route (tests/test_f32_replay.py:171-192), fields above 8
+    components, saveat; an unknown precision names the known ones."""
+    class Lz:
+        name = "diffeqgpu_lorenz"
+        dim = 3
+        t0 = 0.0
+        t1 = 1.0
+        is_stiff = False
+
+    class L96(Lz):
+        name = "lorenz96_32"
+        dim = 32
+
+    y0, p = np.ones((4, 3)), np.full((4, 1), 28.0)
+    with pytest.raises(ValueError, match="float32"):
+        api.grad_closure(Lz(), y0, p, engine="tsit5_replay", precision="float32")
+    with pytest.raises(ValueError, match="precision"):
+        api.grad_closure(Lz(), y0, p, engine="warp_replay", precision="float16")
+    with pytest.raises(ValueError, match="at most 8 components"):
+        api.grad_closure(L96(), np.ones((4, 32)), np.full((4, 1), 8.0), precision="float32")
+    with pytest.raises(ValueError, match="saveat"):
+        api.grad_closure(Lz(), y0, p, precision="float32", saveat=[0.5, 1.0])
+    with pytest.raises(ValueError, match="precision"):
+        api.record(Lz(), y0, p, precision="mixed")
+
+
 def test_checkpoint_policy(gslib):
     from gradsolve_b200.engine import choose_ckpt_every
     assert choose_ckpt_every("all", 3, 10, 700, None) == 1

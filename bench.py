@@ -382,6 +382,74 @@ def mixed_precision_config(args, dev) -> dict:
     return out
 
 
+def float32_route_config(args, dev, n: int = 1 << 20) -> dict:
+    """The float32 route on the reference's f32 nonstiff cell (tests/test_f32_replay.py:84-117:
+    diffeqgpu_lorenz, y0 = [1, 0, 0] + 0.01 N(0, 1) seed 0, rho = 28, t in [0, 1], rtol 1e-6 /
+    atol 1e-9, loss sum(y_final**2)) at n = 2^20: float64 and float32 gradient steps (record
+    + reverse pass), the record bytes of each, and the float32 gradient against the float64
+    reverse pass over the same float32-recorded mesh (rel-L2 <= 1e-3 and cosine >= 1 - 1e-6
+    are the reference's bars)."""
+    import torch
+
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    spec = field_spec("lorenz")
+    rng = np.random.default_rng(0)
+    y0 = torch.tensor(np.tile([1.0, 0.0, 0.0], (n, 1)) + 0.01 * rng.standard_normal((n, 3)),
+                      device=dev)
+    rho = torch.full((n, 1), 28.0, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    out = {"workload": "lorenz f32 cell, n=2^20, t in [0, 1], rtol 1e-6, atol 1e-9"}
+    recs = {}
+    for prec in ("float64", "float32"):
+        ws = {"r": None}
+
+        def step(events=None, prec=prec, ws=ws):
+            if events:
+                events[0].record(stream)
+            r = engine.forward_record("tsit5", spec, y0, rho, t0=0.0, t1=1.0, rtol=1e-6,
+                                      atol=1e-9, max_steps=100000, checkpoint="auto",
+                                      precision=prec, workspace=ws["r"])
+            ws["r"] = r
+            if events:
+                events[1].record(stream)
+            ybar = 2.0 * r.y_final
+            if events:
+                events[2].record(stream)
+            _g, gp = engine.adjoint(r, rho, ybar, want_y0=False, precision=prec)
+            if events:
+                events[3].record(stream)
+            return r, gp
+
+        for _ in range(3):
+            step()
+        torch.cuda.synchronize()
+        fwd, adj, whole, (r, gp) = _time_steps(torch, step, 5, flush, stream)
+        ms = float(np.mean(whole))
+        recs[prec] = (r, gp)
+        out[prec] = {"value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                     "fwd_ms": float(np.mean(fwd)), "adj_ms": float(np.mean(adj)),
+                     "record_bytes": int(r.rec.numel() * r.rec.element_size()),
+                     "accepted_steps": int(r.n_acc.to(torch.int64).sum().item())}
+    out["speedup_vs_f64"] = out["float64"]["ms_per_step"] / out["float32"]["ms_per_step"]
+    out["record_bytes_ratio"] = out["float32"]["record_bytes"] / out["float64"]["record_bytes"]
+    # same mesh: the float32 record's dts replayed and differentiated in float64
+    r32, g32 = recs["float32"]
+    r64 = engine.record_from_padded("tsit5", spec, r32.padded_dts().double(), 0.0,
+                                    checkpoint=r32.ckpt_every)
+    y64 = engine.replay(r64, y0, rho, write_ckpt=True)
+    _g, g64 = engine.adjoint(r64, rho, 2.0 * y64, want_y0=False)
+    a, b = g32.double().flatten(), g64.flatten()
+    err = _grad_err(g32.double(), g64)
+    err["cosine"] = float((a @ b / (a.norm() * b.norm())).item())
+    err["meets_reference_bars"] = bool(err["rel_l2"] <= 1e-3 and err["cosine"] >= 1 - 1e-6)
+    out["grad_vs_f64_same_mesh"] = err
+    recs = r64 = None
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_b200(args) -> None:
     import torch
     import torch.distributed as dist
@@ -565,6 +633,9 @@ def run_b200(args) -> None:
         gc.collect()
         torch.cuda.empty_cache()
         config3 = mixed_precision_config(args, dev)
+    f32_route = None
+    if world == 1 and not args.no_config3:
+        f32_route = float32_route_config(args, dev)
 
     if rank != 0:
         if world > 1:
@@ -632,7 +703,7 @@ def run_b200(args) -> None:
                    "l2": "flushed between timed steps (record traffic also >> L2)"},
         "gpu_launches": 2 * args.steps,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-        "parity_sample": checks, "config3_mixed": config3,
+        "parity_sample": checks, "config3_mixed": config3, "float32_route": f32_route,
         "fwd_ms": fwd_avg, "adj_ms": adj_avg, "mixed": mixed, "solve": solve or None,
         "fwd_ms_steps": [round(x, 3) for x in fwd_ms], "adj_ms_steps": [round(x, 3) for x in adj_ms],
     }
@@ -825,7 +896,7 @@ def measure_workload(args, name: str, n: int, dev, world: int = 1, rank: int = 0
         time_variant.steps_ms = [round(x, 3) for x in steps_ms]
         return whole, per_group, outs
 
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(dev.index if dev.index is not None else 0)
     clocks.start()
     ms, per_group, outs = time_variant("float64")
     steps_ms = time_variant.steps_ms
@@ -1042,7 +1113,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-config3", action="store_true",
-                    help="skip the mixed-precision configuration (LV and Lorenz at 2^22)")
+                    help="skip the mixed-precision configuration (LV and Lorenz at 2^22) and "
+                         "the float32-route leg (the reference's f32 Lorenz cell at 2^20)")
     ap.add_argument("--no-checks", action="store_true",
                     help="skip the oracle/FD checks of 64 sampled trajectories (outside timing)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

@@ -9,12 +9,22 @@
 //   err = sqrt(mean((e / sc)^2)),  sc = atol + rtol * max(|y|, |y5|)
 //         (one division per component; the mean summed in numpy's add.reduce order:
 //          sequential below 8 terms, 8 accumulators combined pairwise from 8 to 128)
-//   dt  = h * min(max(0.9 * max(err, 1e-10)^-0.2, 0.2), 5)      (CUDA's pow)
+//   dt  = h * min(max(0.9 * max(err, 1e-10)^-0.2, 0.2), 5)
 // where the tuned kernel uses a shared reciprocal, the sum S against a threshold and a
-// series root.  With these, the recorded dts and y_final of the reference's own goldens are
-// reproduced bit for bit (tests/test_gpu_exact.py), which pins the product's stage
-// arithmetic and fields to the reference's association; the tuned kernel's measured
-// distance from this instance is the dt tolerance its own tests use.
+// series root.
+//
+// The one operation that cannot match by construction is the power: the reference's is the
+// host libm's pow (Python float **), which is not correctly rounded (nor is CUDA's pow), and
+// the two differ in the last bit for some arguments.  So the power can be supplied: with
+// pow_table (n, A) given, attempt `it` of trajectory j uses pow_table[j*A + it] -- the host
+// libm's value of max(err, 1e-10)^-0.2 for that attempt's err (NaN: not known; CUDA's pow is
+// used) -- and err_log (n, 2A) receives each attempt's floored err and the power it used.
+// The test feeds
+// the log back through the host's pow until the table is a fixed point; with it the recorded
+// dts and y_final of the reference's own goldens are reproduced bit for bit
+// (tests/test_gpu_exact.py), which pins the product's stage arithmetic and fields to the
+// reference's association.  The tuned kernel's measured distance from this instance is the
+// dt tolerance its own tests use.
 //
 // Output layout: dts row-major (n, cap), zero past n_acc[j] (the reference's padded form).
 
@@ -55,7 +65,8 @@ template <class F>
 __global__ void exact_tsit5_record_kernel(long long n, const double* y0, const double* p,
                                           double t0, double t1, double rtol, double atol,
                                           double dt0, int max_steps, int cap, double* dts,
-                                          double* yf, int* n_acc, int* n_rej, int* status) {
+                                          double* yf, int* n_acc, int* n_rej, int* status,
+                                          const double* pow_table, double* err_log, int A) {
   constexpr int D = F::D, P = F::P;
   using T = gs::Tsit5;
   using C = gs::Ctrl;
@@ -101,7 +112,16 @@ __global__ void exact_tsit5_record_kernel(long long n, const double* y0, const d
       ++rej;
     }
     const double e = err > C::ERR_FLOOR ? err : C::ERR_FLOOR;
-    const double fac = C::SAFETY * pow(e, T::ORDER_EXP);
+    double pw = pow(e, T::ORDER_EXP);
+    if (pow_table && it < A) {  // the host libm's power, where the table has it (not NaN)
+      const double v = pow_table[j * A + it];
+      if (v == v) pw = v;
+    }
+    if (err_log && it < A) {
+      err_log[(j * A + it) * 2] = e;
+      err_log[(j * A + it) * 2 + 1] = pw;
+    }
+    const double fac = C::SAFETY * pw;
     const double lo = fac > C::FAC_MIN ? fac : C::FAC_MIN;
     dt = h * (C::FAC_MAX < lo ? C::FAC_MAX : lo);
   }
@@ -116,31 +136,34 @@ __global__ void exact_tsit5_record_kernel(long long n, const double* y0, const d
 template <class F>
 int launch(long long n, const double* y0, const double* p, double t0, double t1, double rtol,
            double atol, double dt0, int max_steps, int cap, double* dts, double* yf, int* n_acc,
-           int* n_rej, int* status, cudaStream_t s) {
+           int* n_rej, int* status, const double* pow_table, double* err_log, int A,
+           cudaStream_t s) {
   const unsigned block = 64;
   exact_tsit5_record_kernel<F><<<(unsigned)((n + block - 1) / block), block, 0, s>>>(
-      n, y0, p, t0, t1, rtol, atol, dt0, max_steps, cap, dts, yf, n_acc, n_rej, status);
+      n, y0, p, t0, t1, rtol, atol, dt0, max_steps, cap, dts, yf, n_acc, n_rej, status,
+      pow_table, err_log, A);
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 
 }  // namespace gx
 
 // Field codes: those of include/gsolve.h; Linear<D> = 4000 + D and Lorenz96<D> = 5000 + D
-// for the sizes the goldens hold.  Returns 0, -1 (bad argument), -2 (field not built here) or
-// -3 (launch failed).
+// for the sizes the goldens hold.  pow_table and err_log may be null (A is then ignored).
+// Returns 0, -1 (bad argument), -2 (field not built here) or -3 (launch failed).
 extern "C" int gx_tsit5_record(int field, long long n, const double* y0, const double* p,
                                double t0, double t1, double rtol, double atol, double dt0,
                                int max_steps, int cap, double* dts, double* yf, int* n_acc,
-                               int* n_rej, int* status, void* stream) {
+                               int* n_rej, int* status, const double* pow_table,
+                               double* err_log, int A, void* stream) {
   if (n < 0 || cap < 1 || max_steps < 1 || !y0 || !p || !dts || !yf || !n_acc || !n_rej ||
-      !status)
+      !status || ((pow_table || err_log) && A < 1))
     return -1;
   if (n == 0) return 0;
   cudaStream_t s = (cudaStream_t)stream;
 #define GX_CASE(code, Fld)                                                                 \
   case code:                                                                               \
     return gx::launch<Fld>(n, y0, p, t0, t1, rtol, atol, dt0, max_steps, cap, dts, yf,     \
-                           n_acc, n_rej, status, s);
+                           n_acc, n_rej, status, pow_table, err_log, A, s);
   switch (field) {
     GX_CASE(gs::FIELD_LORENZ, gs::Lorenz)
     GX_CASE(gs::FIELD_VDP, gs::VdP)

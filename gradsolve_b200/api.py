@@ -256,9 +256,13 @@ def build_replay_state(problem, y0, params, *, method: str, rtol: float, atol: f
     ms = int(max_steps or 100000)
     r = engine.forward_record(method, spec, y0_t, pk, t0=float(problem.t0), t1=t1s, t1v=t1v,
                               rtol=rtol, atol=atol, max_steps=ms, checkpoint=checkpoint,
-                              precision=precision, saveat_ts=saveat)
+                              precision=precision,
+                              # the float32 route records without dense output: its closure
+                              # replays the saved states at the recording point
+                              saveat_ts=None if precision == "float32" else saveat)
     engine.raise_on_failed(r, ms, t1s)
-    state = ReplayState(r, y0_t, pk, spec.nparam, precision=precision, ts_rec=saveat)
+    state = ReplayState(r, y0_t, pk, spec.nparam, precision=precision,
+                        ts_rec=None if precision == "float32" else saveat)
     return state, y0_t, p_t
 
 
@@ -275,7 +279,7 @@ def record(problem, y0, params, *, rtol: float = 1e-6, atol: float = 1e-9,
         raise ValueError(f"unknown precision {precision!r}; known: ['float64', 'float32']")
     spec = _require_field(problem)
     if precision == "float32":
-        _check_float32_route(engine, spec, None)
+        _check_float32_route(engine, spec)
     name = _resolve(problem, engine, [])
     ms = int(max_steps or DEFAULT_MAX_STEPS[name])
     state, _y0, _p = build_replay_state(problem, y0, params, method=ENGINE_REGISTRY[name].method,
@@ -313,7 +317,8 @@ def _make_reverse(name):
         if saveat is not None:
 
             def kernel(z, p):  # the dense time series (n, k, dim), gradsolve/api.py:748-752
-                return saveat_apply(state, _as_tensor(z, dev), _as_tensor(p, dev), ts)
+                ys = saveat_apply(state, _as_tensor(z, dev), _as_tensor(p, dev), ts)
+                return ys.to(torch.float32) if precision == "float32" else ys
         elif precision == "float32":
             def kernel(z, p):  # float32 values; the closure's output is float32
                 return replay_apply(state, _as_tensor(z, dev),
@@ -340,11 +345,11 @@ F32_ENGINES = frozenset({"auto", ENGINE_TSIT5, ENGINE_ROS23, "warp_ode", "warp_r
 F32_MAX_DIM = 8
 
 
-def _check_float32_route(engine_name: str, spec: FieldSpec, saveat) -> None:
-    """precision="float32": the record, the replay and the reverse pass all in float32
-    (gradsolve/api.py:253-274, 876-887).  Refused, as the reference refuses it, on lanes
-    without an f32 route, and here also for fields above 8 components and for saveat, which
-    the float32 kernels do not cover."""
+def _check_float32_route(engine_name: str, spec: FieldSpec) -> None:
+    """precision="float32": the record, the replay (dense output included) and the reverse
+    pass all in float32 (gradsolve/api.py:253-274, 876-887).  Refused, as the reference
+    refuses it, on lanes without an f32 route, and here also for fields above 8 components,
+    which the float32 kernels do not cover."""
     if engine_name not in F32_ENGINES:
         raise ValueError(
             f"precision='float32' is not supported on lane {engine_name!r}: the float32 "
@@ -353,9 +358,6 @@ def _check_float32_route(engine_name: str, spec: FieldSpec, saveat) -> None:
     if spec.dim > F32_MAX_DIM:
         raise ValueError(f"precision='float32' is built for fields of at most {F32_MAX_DIM} "
                          f"components; {spec.key!r} has {spec.dim}. Use precision='float64'.")
-    if saveat is not None:
-        raise ValueError("precision='float32' with saveat is not built; use "
-                         "precision='float64' for a dense time series.")
 
 
 def grad_closure(problem, y0, params, *, wrt="params", saveat=None, precision: str = "float64",
@@ -373,7 +375,7 @@ def grad_closure(problem, y0, params, *, wrt="params", saveat=None, precision: s
                          "'float32'")
     fs = _require_field(problem)
     if precision == "float32":
-        _check_float32_route(engine, fs, saveat)
+        _check_float32_route(engine, fs)
     name = _resolve(problem, engine, reasons)
     spec = ENGINE_REGISTRY[name]
     if not spec.supports(problem):

@@ -1182,11 +1182,51 @@ int launch_saveat_ros23(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint, i
 // precision carries GS_PREC_* and, for the reverse pass, GS_SCHED_* (AUTO = one thread per
 // trajectory; REFILL / STRIDED = persistent lanes).  The forward replay runs one thread per
 // trajectory.
+// The float32 route's dense output: one thread per trajectory, fields of at most 8 components.
+template <class F, int kMethod>
+int launch_f32_saveat(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint) {
+  if constexpr (!kF32Built<F>) {
+    (void)a; (void)s; (void)adjoint;
+    return f32_refuse_dim();
+  } else {
+    if (!adjoint) {
+      gs::f32_replay_saveat_kernel<F, kMethod><<<grid_for(a.n), kBlock, 0, s>>>(a);
+      return cuda_check("f32_replay_saveat_kernel");
+    }
+    // K rows of D + 1 floats per thread, counted in doubles for the occupancy helpers
+    SegCfg c;
+    int rc = occupancy_cfg(gs::f32_adjoint_saveat_kernel<F, kMethod>,
+                           (a.ck_every * (F::D + 1) + 1) / 2, &c);
+    if (rc) return rc;
+    gs::f32_adjoint_saveat_kernel<F, kMethod><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+    return cuda_check("f32_adjoint_saveat_kernel");
+  }
+}
+template <class F>
+int launch_f32_saveat_tsit5(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint) {
+  return launch_f32_saveat<F, 0>(a, s, adjoint);
+}
+template <class F>
+int launch_f32_saveat_ros23(const gs::SaveatArgs& a, cudaStream_t s, bool adjoint) {
+  return launch_f32_saveat<F, 1>(a, s, adjoint);
+}
+
 int saveat_dispatch(int method, int field, int precision, const gs::SaveatArgs& a, void* stream,
                     bool adjoint) {
   const cudaStream_t s = (cudaStream_t)stream;
   const int prec = precision & GS_PREC_MASK;
   const int sched = adjoint ? adjoint_schedule(precision) : GS_SCHED_STATIC;
+  if (prec == GS_PREC_F32) {
+    int rc = f32_schedule(precision, adjoint ? "gs_adjoint_saveat" : "gs_replay_saveat");
+    if (rc) return rc;
+    if (method == GS_METHOD_TSIT5) {
+      GS_TSIT5_DISPATCH(field, launch_f32_saveat_tsit5, a, s, adjoint)
+    }
+    if (method == GS_METHOD_ROS23) {
+      GS_ROS23_DISPATCH(field, launch_f32_saveat_ros23, a, s, adjoint)
+    }
+    return fail(GS_ERR_ARG, "saveat: unknown method " + std::to_string(method));
+  }
   if (method == GS_METHOD_TSIT5) {
     if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED)
       return fail(GS_ERR_PRECISION, "saveat: unknown precision mode " + std::to_string(prec));
@@ -1292,6 +1332,10 @@ extern "C" int gs_fwd_record_saveat(int method, int field, int precision, long l
                    gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status,
                    gs::CtrlConsts{}, ts, ts_ld, K, K > 0 ? ys : nullptr};
   const cudaStream_t s = (cudaStream_t)stream;
+  if (prec == GS_PREC_F32)
+    return fail(GS_ERR_PRECISION, std::string(who) + ": the float32 route records without dense "
+                                                     "output; replay its record with "
+                                                     "gs_replay_saveat");
   if (method == GS_METHOD_TSIT5) {
     if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED)
       return fail(GS_ERR_PRECISION, std::string(who) + ": unknown precision mode " + std::to_string(prec));

@@ -17,7 +17,10 @@
 // err <= 1, dt = h * clip(0.9 * max(err, 1e-10)^(-1/q), 0.2, 5) after accept and reject.
 #pragma once
 
+#include <math_constants.h>
+
 #include "gs_ros23.cuh"
+#include "gs_saveat.cuh"
 #include "gs_tsit5.cuh"
 
 namespace gs {
@@ -272,6 +275,187 @@ __global__ void __launch_bounds__(128) f32_adjoint_kernel(const AdjointArgs a) {
         ros23_step_vjp<F>(ys, p, dt, lam, gp);
     }
   }
+  if (a.gy0) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) a.gy0[j * D + i] = (double)lam[i];
+  }
+  if (a.gp) {
+#pragma unroll
+    for (int i = 0; i < P; ++i) a.gp[j * P + i] = (double)gp[i];
+  }
+}
+
+// --- dense output (saveat) on the float32 route --------------------------------------------
+// The semantics of replay_saveat_kernel / adjoint_saveat_kernel (gs_saveat.cuh,
+// gradsolve/solvers/dense.py:106-163) in float: the reference's f32 closure casts the
+// requested times to float32 with the rest (gradsolve/warp/warp_replay.py:213-217), so the
+// times, the accumulated step times, the bracket tests and the re-step sizes ts_k - t are all
+// float32 here.  The checkpoint rows carry each segment start's time (float32), from which the
+// adjoint rebuilds the step times with the replay's own additions.
+template <int D>
+__device__ __forceinline__ void store_row_f32(double* dst, const float* v) {
+#pragma unroll
+  for (int i = 0; i < D; ++i) dst[i] = (double)v[i];
+}
+
+template <int D>
+__device__ __forceinline__ float load_ckpt_time_f32(const float* ckpt, long long n, long long j,
+                                                    int slot) {
+  constexpr int CW = (D + 4) & ~3;
+  return __ldg(ckpt + ((size_t)slot * (size_t)n + (size_t)j) * CW + D);
+}
+
+template <class F, int kMethod>
+__global__ void __launch_bounds__(128) f32_replay_saveat_kernel(const SaveatArgs a) {
+  constexpr int D = F::D, P = F::P;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  float y[D], p[P];
+#pragma unroll
+  for (int i = 0; i < D; ++i) y[i] = (float)a.y0[j * D + i];
+#pragma unroll
+  for (int i = 0; i < P; ++i) p[i] = (float)a.p[j * P + i];
+  const float* rec = reinterpret_cast<const float*>(a.rec);
+  float* ckpt = reinterpret_cast<float*>(a.ckpt);
+  const double* ts = a.ts + j * a.ts_ld;
+  double* ys = a.ys + j * (long long)a.K * D;
+  const int na = steps_in_record(a.n_acc, j, a.cap);
+  float t = (float)a.t0;
+  int kk = 0;
+  while (kk < a.K && (float)ts[kk] <= t) {  // never bracketed: y0
+    store_row_f32<D>(ys + (long long)kk * D, y);
+    ++kk;
+  }
+  const bool ck_on = ckpt != nullptr;
+  if (ck_on) store_ckpt_f32<D>(ckpt, a.n, j, 0, y, t);
+  int ck_cnt = 0, ck_slot = 0;
+  for (int s = 0; s < na; ++s) {
+    const float dt = load_rec_f32(rec, a.n, j, s);
+    if (dt > 0.0f) {
+      const float tn = t + dt;
+      while (kk < a.K && (float)ts[kk] <= tn) {  // bracketed by this step: re-step to ts
+        float yk[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) yk[i] = y[i];
+        f32_step<F, kMethod>(yk, p, (float)ts[kk] - t);
+        store_row_f32<D>(ys + (long long)kk * D, yk);
+        ++kk;
+      }
+      f32_step<F, kMethod>(y, p, dt);
+      t = tn;
+    }
+    if (ck_on && ++ck_cnt == a.ck_every) {
+      ck_cnt = 0;
+      if (++ck_slot < a.ck_slots) store_ckpt_f32<D>(ckpt, a.n, j, ck_slot, y, t);
+    }
+  }
+  // times at or past the final accumulated time take y_final itself
+  for (int k = a.K - 1; k >= 0 && (float)ts[k] >= t; --k) store_row_f32<D>(ys + (long long)k * D, y);
+  for (int k = kk; k < a.K; ++k) store_row_f32<D>(ys + (long long)k * D, y);
+  store_row_f32<D>(a.yf + j * D, y);
+}
+
+// Segment buffer in dynamic shared memory: K rows of D + 1 floats (state, step start time)
+// per thread, element e of thread t at e * blockDim + t.
+template <class F, int kMethod>
+__global__ void __launch_bounds__(128) f32_adjoint_saveat_kernel(const SaveatArgs a) {
+  constexpr int D = F::D, P = F::P;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  float p[P], lam[D], gp[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    p[i] = (float)a.p[j * P + i];
+    gp[i] = 0.0f;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) lam[i] = a.ybar ? (float)a.ybar[j * D + i] : 0.0f;
+  const float* rec = reinterpret_cast<const float*>(a.rec);
+  const float* ckpt = reinterpret_cast<const float*>(a.ckpt);
+  const double* ts = a.ts + j * a.ts_ld;
+  const double* ysb = a.ysbar + j * (long long)a.K * D;
+  float* st = gs_seg_smem_f32 + threadIdx.x;
+  const int stride = blockDim.x;
+  const int na = steps_in_record(a.n_acc, j, a.cap);
+  const int K = a.ck_every;
+  const int nseg = (na + K - 1) / K;
+  int kk = a.K;  // times [0, kk) not yet assigned to a step
+  float tlast = kk > 0 ? (float)ts[kk - 1] : -CUDART_INF_F;
+  auto pop = [&]() {
+    --kk;
+    tlast = kk > 0 ? (float)ts[kk - 1] : -CUDART_INF_F;
+  };
+  auto add_row = [&](float* acc, int k) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) acc[i] += (float)ysb[(long long)k * D + i];
+  };
+  if (nseg == 0) {
+    const float tfin = (float)a.t0;
+    while (tlast >= tfin) {
+      add_row(lam, kk - 1);
+      pop();
+    }
+  }
+  bool fin_done = false;  // cotangents of times >= t_fin joined lam
+  const int top = warp_top_segments(nseg);
+  for (int sg = top - 1; sg >= 0; --sg) {
+    if (sg >= nseg) continue;  // in step with the warp's longest trajectory
+    float y[D];
+    load_ckpt_f32<D>(ckpt, a.n, j, sg, y);
+    float t = load_ckpt_time_f32<D>(ckpt, a.n, j, sg);
+    const int start = sg * K;
+    for (int q = 0; q < K; ++q) {  // states y_{start+q} with their times; t ends at the segment end
+#pragma unroll
+      for (int i = 0; i < D; ++i) st[(q * (D + 1) + i) * stride] = y[i];
+      st[(q * (D + 1) + D) * stride] = t;
+      const int s = start + q;
+      const float dt = s < na ? load_rec_f32(rec, a.n, j, s) : 0.0f;
+      if (dt > 0.0f) {
+        if (q + 1 < K) f32_step<F, kMethod>(y, p, dt);
+        t = t + dt;
+      }
+    }
+    if (!fin_done) {  // first processed segment: t is t_fin
+      fin_done = true;
+      while (tlast >= t) {
+        add_row(lam, kk - 1);
+        pop();
+      }
+    }
+    for (int q = K - 1; q >= 0; --q) {
+      const int s = start + q;
+      const float dt = s < na ? load_rec_f32(rec, a.n, j, s) : 0.0f;
+      if (!(dt > 0.0f)) continue;
+      float ys[D], add[D];
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        ys[i] = st[(q * (D + 1) + i) * stride];
+        add[i] = 0.0f;
+      }
+      const float ts0 = st[(q * (D + 1) + D) * stride];
+      while (tlast > ts0) {  // re-steps bracketed by this step
+        const float tk = tlast;
+        float w[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) w[i] = (float)ysb[(long long)(kk - 1) * D + i];
+        pop();
+        if constexpr (kMethod == 0)
+          tsit5_step_vjp<F>(ys, p, tk - ts0, w, gp);
+        else
+          ros23_step_vjp<F>(ys, p, tk - ts0, w, gp);
+#pragma unroll
+        for (int i = 0; i < D; ++i) add[i] += w[i];
+      }
+      if constexpr (kMethod == 0)
+        tsit5_step_vjp<F>(ys, p, dt, lam, gp);
+      else
+        ros23_step_vjp<F>(ys, p, dt, lam, gp);
+#pragma unroll
+      for (int i = 0; i < D; ++i) lam[i] += add[i];
+    }
+  }
+  // remaining times were never bracketed (ts <= t0): their value is y0
+  for (int k = 0; k < kk; ++k) add_row(lam, k);
   if (a.gy0) {
 #pragma unroll
     for (int i = 0; i < D; ++i) a.gy0[j * D + i] = (double)lam[i];

@@ -244,6 +244,9 @@ class RecordSet:
         """For each part, the rows whose final tier it is, longest first (by this record's
         step counts): lanes refilled from a work counter then take the long trajectories
         first, and the short ones fill in around them instead of the long ones ending last."""
+        if len(self.parts) == 1 and self.parts[0][0] is None:  # one tier: no host sync
+            cost = (self.n_acc + self.n_rej).to(torch.int64)
+            return [torch.argsort(cost, descending=True, stable=True)]
         owner = torch.zeros(self.n, dtype=torch.int64, device=self.y_final.device)
         for k, (rows, _r) in enumerate(self.parts):
             if rows is None:
@@ -499,6 +502,13 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
                             max_steps=max_steps, precision=precision)
     if isinstance(ws, RecordSet):
         return _forward_planned(method, spec, y0, p, t1v, saveat_ts, ws, kw)
+    if isinstance(ws, Record) and n > 32 and ws.rec.numel() > 2:
+        # a record of the same batch: its step counts order the lanes (one tier, trajectories
+        # sorted by last time's attempts, so a warp's lanes take similar numbers of steps and
+        # none idles while the longest finishes)
+        plan = RecordSet(method, spec, n, ws.t0, [(None, ws)], None, ws.y_final, ws.n_acc,
+                         ws.n_rej, ws.status, uneven=ws.uneven, ys=ws.ys, streams=[None])
+        return _forward_planned(method, spec, y0, p, t1v, saveat_ts, plan, kw)
     cap = max(1, min(int(cap0), int(max_steps)))
     r0 = _forward_one(method, spec, y0, p, t1v, saveat_ts, cap, ws, kw)
     return _grow(method, spec, y0, p, t1v, saveat_ts, r0, None, kw)

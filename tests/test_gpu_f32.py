@@ -212,7 +212,7 @@ def test_replay_reproduces_the_recording_pass(gslib, cuda, method, field, proble
 
 def test_float32_refusals(gslib, cuda):
     """Refused rather than served another way: other schedules, lanes and reverse-pass
-    variants at the C ABI; fields above 8 components and saveat at the API."""
+    variants at the C ABI; fields above 8 components at the API."""
     import gradsolve_b200 as gsb
     from gradsolve_b200 import _lib, engine
     from gradsolve_b200.fields import field_spec
@@ -237,5 +237,43 @@ def test_float32_refusals(gslib, cuda):
 
     with pytest.raises(ValueError, match="at most 8 components"):
         gsb.grad_closure(L96(), np.ones((4, 32)), np.full((4, 1), 8.0), precision="float32")
-    with pytest.raises(ValueError, match="saveat"):
-        gsb.grad_closure(Lorenz(), y0, params, precision="float32", saveat=[0.5, 1.0])
+
+
+@pytest.mark.parametrize("method,field,problem,batch,kw,ts", [
+    ("tsit5", "lorenz", Lorenz(), lorenz_batch, dict(rtol=1e-6, atol=1e-9),
+     np.linspace(0.0, 1.0, 17)),
+    ("rosenbrock23", "robertson", Robertson(), robertson_batch, dict(rtol=1e-5, atol=1e-8),
+     np.array([0.0, 1.0, 10.0, 100.0, 1000.0, 1.0e4]))])
+def test_saveat_matches_f64_oracle_on_the_same_mesh(gslib, oracle, cuda, method, field,
+                                                     problem, batch, kw, ts):
+    """The float32 closure with saveat (the times float32, as the reference's f32 replay
+    casts them): the saved states and dL/dparams of sum(ys**2) against the float64 oracle's
+    dense-output replay and reverse pass over the same float32 mesh, at the reference's f32
+    bars; the last saved state equals y_final bit for bit."""
+    import gradsolve_b200 as gsb
+    y0, params = batch(256)
+    clo = gsb.grad_closure(problem, y0, params, precision="float32", saveat=ts, **kw)
+    p = torch.tensor(params, dtype=torch.float32, device="cuda", requires_grad=True)
+    ys = clo(p)
+    assert ys.dtype == torch.float32 and ys.shape == (256, len(ts), 3)
+    (ys.double() ** 2).sum().backward()
+    g32 = p.grad.cpu().numpy().astype(np.float64)
+    dts = clo.state.record.padded_dts().cpu().numpy().astype(np.float64)
+    _yf, ys64 = oracle.replay_saveat(method, field, y0, params, dts, ts, nthreads=8)
+    _gy, g64 = oracle.replay_saveat_vjp(method, field, y0, params, dts, ts, 2.0 * ys64,
+                                        nthreads=8)
+    y32 = ys.detach().cpu().numpy().astype(np.float64)
+    scale = np.abs(ys64).max(axis=(1, 2), keepdims=True)
+    ey = float(np.max(np.abs(y32 - ys64) / scale))
+    rel, cos = rel_l2(g32, g64), cosine(g32, g64)
+    print(f"{field} f32 saveat: ys row error {ey:.2e}, grad rel-L2 {rel:.3e}, "
+          f"cosine 1 - {1 - cos:.2e}")
+    assert ey <= 1e-4
+    assert rel <= GRAD_REL_L2_TOL
+    assert cos >= 1 - GRAD_COSINE_TOL
+    # the final saved time is t1: its state is y_final itself
+    from gradsolve_b200 import engine
+    yf = engine.replay(clo.state.record, torch.tensor(y0, device="cuda"),
+                       torch.tensor(params, device="cuda"), write_ckpt=False,
+                       precision="float32")
+    assert torch.equal(ys[:, -1].detach().double(), yf)

@@ -118,8 +118,8 @@ def test_engine_resolution_and_aliases():
 
 def test_float32_route_refusals():
     """precision="float32" is refused, before anything runs, where it has no float32 kernels:
-    reference lanes without an f32 route (tests/test_f32_replay.py:171-192), fields above 8
-    components, saveat; an unknown precision names the known ones."""
+    reference lanes without an f32 route (tests/test_f32_replay.py:171-192) and fields above 8
+    components; an unknown precision names the known ones."""
     class Lz:
         name = "diffeqgpu_lorenz"
         dim = 3
@@ -138,8 +138,6 @@ def test_float32_route_refusals():
         api.grad_closure(Lz(), y0, p, engine="warp_replay", precision="float16")
     with pytest.raises(ValueError, match="at most 8 components"):
         api.grad_closure(L96(), np.ones((4, 32)), np.full((4, 1), 8.0), precision="float32")
-    with pytest.raises(ValueError, match="saveat"):
-        api.grad_closure(Lz(), y0, p, precision="float32", saveat=[0.5, 1.0])
     with pytest.raises(ValueError, match="precision"):
         api.record(Lz(), y0, p, precision="mixed")
 

@@ -495,11 +495,38 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
       gs::tsit5_adjoint_kernel<F><<<grid_for_block(a.n, cr.block), cr.block, cr.smem, s>>>(a);
       return cuda_check("tsit5_adjoint_kernel");
     }
-    SegCfg c;
-    if ((rc = occupancy_cfg(gs::tsit5_mixed_adjoint_kernel<F>,
-                            gs::adjoint_smem_doubles<F::D>(a.ck_every), &c)))
+    // float32 stages: the same choice between keeping the replayed steps' stage inputs (6*D
+    // floats per step) and recomputing them, with the same K = 2 instance for small states
+    auto mstages = gs::tsit5_mixed_adjoint_stages_kernel<F>;
+    SegCfg ck{0, 0, 0}, cr{0, 0, 0};
+    const int msd = gs::mixed_stages_smem_doubles<F::D>(a.ck_every);
+    if (variant != GS_ADJ_RECOMPUTE) {
+      if ((rc = occupancy_probe(mstages, msd, &ck))) return rc;
+      if constexpr (F::D <= 4) {
+        if (a.ck_every == 2) {
+          SegCfg c2{0, 0, 0};
+          if ((rc = occupancy_probe(gs::tsit5_mixed_adjoint_stages_k2_kernel<F>, msd, &c2)))
+            return rc;
+          if (c2.resident > 0 && c2.resident >= ck.resident) {
+            mstages = gs::tsit5_mixed_adjoint_stages_k2_kernel<F>;
+            ck = c2;
+          }
+        }
+      }
+    }
+    if ((rc = occupancy_probe(gs::tsit5_mixed_adjoint_kernel<F>,
+                              gs::adjoint_smem_doubles<F::D>(a.ck_every), &cr)))
       return rc;
-    gs::tsit5_mixed_adjoint_kernel<F><<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+    if (ck.resident > 0 && (variant == GS_ADJ_STAGES || keeping_pays(ck, cr))) {
+      if ((rc = allow_smem(mstages, ck.smem))) return rc;
+      mstages<<<grid_for_block(a.n, ck.block), ck.block, ck.smem, s>>>(a);
+      return cuda_check("tsit5_mixed_adjoint_stages_kernel");
+    }
+    if (cr.resident <= 0)
+      return fail(GS_ERR_ARG, "segment buffer does not fit shared memory (checkpoint "
+                              "interval too large for this state dimension)");
+    if ((rc = allow_smem(gs::tsit5_mixed_adjoint_kernel<F>, cr.smem))) return rc;
+    gs::tsit5_mixed_adjoint_kernel<F><<<grid_for_block(a.n, cr.block), cr.block, cr.smem, s>>>(a);
     return cuda_check("tsit5_mixed_adjoint_kernel");
   }
   const bool counter = sched == GS_SCHED_REFILL;

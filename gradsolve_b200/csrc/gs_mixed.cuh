@@ -121,48 +121,78 @@ __device__ __forceinline__ void mixed_replay_step(double* y, double* c, const do
   kahan_add<D>(y, c, inc);
 }
 
-// Reverse of one step at (y, dt): lam (float64) <- (dy'/dy)^T lam; gp += (dy'/dp)^T lam.
+// Float32 inputs of one step's stages: yf = y and the stage states s_m = y + d_m (m = 2..6).
+// With kNext the step's result is also produced (the expressions of mixed_replay_step, so a
+// replay that keeps the stages lands on the same states).
 template <class F>
-__device__ __forceinline__ void mixed_step_vjp(const double* y, const double* p, const float* pf,
-                                               double dt, double* lam, double* gp) {
-  constexpr int D = F::D, P = F::P;
+struct MixedStageStates {
+  static constexpr int D = F::D;
+  float yf[D], s2[D], s3[D], s4[D], s5[D], s6[D];
+  template <int M>
+  __device__ __forceinline__ void get(float* out) const {
+    const float* src = M == 1 ? yf : M == 2 ? s2 : M == 3 ? s3 : M == 4 ? s4 : M == 5 ? s5 : s6;
+#pragma unroll
+    for (int i = 0; i < D; ++i) out[i] = src[i];
+  }
+};
+
+template <class F, bool kNext>
+__device__ __forceinline__ void mixed_stage_states(const double* y, const double* p,
+                                                   const float* pf, double dt,
+                                                   MixedStageStates<F>& S, double* yn,
+                                                   double* cn) {
+  constexpr int D = F::D;
   using T = Tsit5f;
   double k1[D];
-  float yf[D], k1f[D];
+  float k1f[D];
   F::rhs(y, p, k1);
-  to_float<F>(y, yf);
+  to_float<F>(y, S.yf);
   to_float<F>(k1, k1f);
   const float hf = (float)dt;
-  // stage states s_m = y + d_m (m = 2..6), float32
-  float s2[D], s3[D], s4[D], s5[D], s6[D];
-  {
-    float d[D], dk2[D], dk3[D], dk4[D], dk5[D];
+  MixedStages<F> K;
+  float d[D];
 #pragma unroll
-    for (int i = 0; i < D; ++i) { d[i] = hf * (T::C2 * k1f[i]); s2[i] = yf[i] + d[i]; }
-    F::rhs_delta(yf, pf, d, dk2);
+  for (int i = 0; i < D; ++i) { d[i] = hf * (T::C2 * k1f[i]); S.s2[i] = S.yf[i] + d[i]; }
+  F::rhs_delta(S.yf, pf, d, K.dk2);
 #pragma unroll
-    for (int i = 0; i < D; ++i) { d[i] = hf * (T::C3 * k1f[i] + T::A32 * dk2[i]); s3[i] = yf[i] + d[i]; }
-    F::rhs_delta(yf, pf, d, dk3);
+  for (int i = 0; i < D; ++i) { d[i] = hf * (T::C3 * k1f[i] + T::A32 * K.dk2[i]); S.s3[i] = S.yf[i] + d[i]; }
+  F::rhs_delta(S.yf, pf, d, K.dk3);
 #pragma unroll
-    for (int i = 0; i < D; ++i) {
-      d[i] = hf * (T::C4 * k1f[i] + T::A42 * dk2[i] + T::A43 * dk3[i]);
-      s4[i] = yf[i] + d[i];
-    }
-    F::rhs_delta(yf, pf, d, dk4);
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      d[i] = hf * (T::C5 * k1f[i] + T::A52 * dk2[i] + T::A53 * dk3[i] + T::A54 * dk4[i]);
-      s5[i] = yf[i] + d[i];
-    }
-    F::rhs_delta(yf, pf, d, dk5);
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      d[i] = hf * (T::C6 * k1f[i] + T::A62 * dk2[i] + T::A63 * dk3[i] + T::A64 * dk4[i] +
-                   T::A65 * dk5[i]);
-      s6[i] = yf[i] + d[i];
-    }
+  for (int i = 0; i < D; ++i) {
+    d[i] = hf * (T::C4 * k1f[i] + T::A42 * K.dk2[i] + T::A43 * K.dk3[i]);
+    S.s4[i] = S.yf[i] + d[i];
   }
-  float g[D], kb1[D], kb2[D], kb3[D], kb4[D], kb5[D], kb6[D], sb[D], acc[D], gpf[P];
+  F::rhs_delta(S.yf, pf, d, K.dk4);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    d[i] = hf * (T::C5 * k1f[i] + T::A52 * K.dk2[i] + T::A53 * K.dk3[i] + T::A54 * K.dk4[i]);
+    S.s5[i] = S.yf[i] + d[i];
+  }
+  F::rhs_delta(S.yf, pf, d, K.dk5);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    d[i] = hf * (T::C6 * k1f[i] + T::A62 * K.dk2[i] + T::A63 * K.dk3[i] + T::A64 * K.dk4[i] +
+                 T::A65 * K.dk5[i]);
+    S.s6[i] = S.yf[i] + d[i];
+  }
+  if constexpr (kNext) {
+    F::rhs_delta(S.yf, pf, d, K.dk6);
+    double inc[D];
+    mixed_increment<F>(k1, K, dt, hf, inc);
+    kahan_add<D>(yn, cn, inc);
+  }
+}
+
+// Reverse of one step given its float32 stage inputs (Src::get<1> yields y as float, get<M>
+// s_M): lam (float64) <- (dy'/dy)^T lam; gp += (dy'/dp)^T lam.  The stage VJPs run in float32
+// and their sums join lam and gp in float64.
+template <class F, class Src>
+__device__ __forceinline__ void mixed_vjp_core(const Src& src, const float* pf, double dt,
+                                               double* lam, double* gp) {
+  constexpr int D = F::D, P = F::P;
+  using T = Tsit5f;
+  const float hf = (float)dt;
+  float st[D], g[D], kb1[D], kb2[D], kb3[D], kb4[D], kb5[D], kb6[D], sb[D], acc[D], gpf[P];
 #pragma unroll
   for (int k = 0; k < P; ++k) gpf[k] = 0.0f;
 #pragma unroll
@@ -176,9 +206,10 @@ __device__ __forceinline__ void mixed_step_vjp(const double* y, const double* p,
     kb5[i] = T::B5 * g[i];
     kb6[i] = T::B6 * g[i];
   }
+  src.template get<6>(st);
 #pragma unroll
   for (int i = 0; i < D; ++i) sb[i] = 0.0f;
-  F::vjp(s6, pf, kb6, sb, gpf);
+  F::vjp(st, pf, kb6, sb, gpf);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     acc[i] += sb[i];
@@ -186,46 +217,60 @@ __device__ __forceinline__ void mixed_step_vjp(const double* y, const double* p,
     kb1[i] += T::A61 * u; kb2[i] += T::A62 * u; kb3[i] += T::A63 * u;
     kb4[i] += T::A64 * u; kb5[i] += T::A65 * u;
   }
+  src.template get<5>(st);
 #pragma unroll
   for (int i = 0; i < D; ++i) sb[i] = 0.0f;
-  F::vjp(s5, pf, kb5, sb, gpf);
+  F::vjp(st, pf, kb5, sb, gpf);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     acc[i] += sb[i];
     const float u = hf * sb[i];
     kb1[i] += T::A51 * u; kb2[i] += T::A52 * u; kb3[i] += T::A53 * u; kb4[i] += T::A54 * u;
   }
+  src.template get<4>(st);
 #pragma unroll
   for (int i = 0; i < D; ++i) sb[i] = 0.0f;
-  F::vjp(s4, pf, kb4, sb, gpf);
+  F::vjp(st, pf, kb4, sb, gpf);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     acc[i] += sb[i];
     const float u = hf * sb[i];
     kb1[i] += T::A41 * u; kb2[i] += T::A42 * u; kb3[i] += T::A43 * u;
   }
+  src.template get<3>(st);
 #pragma unroll
   for (int i = 0; i < D; ++i) sb[i] = 0.0f;
-  F::vjp(s3, pf, kb3, sb, gpf);
+  F::vjp(st, pf, kb3, sb, gpf);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     acc[i] += sb[i];
     const float u = hf * sb[i];
     kb1[i] += T::A31 * u; kb2[i] += T::A32 * u;
   }
+  src.template get<2>(st);
 #pragma unroll
   for (int i = 0; i < D; ++i) sb[i] = 0.0f;
-  F::vjp(s2, pf, kb2, sb, gpf);
+  F::vjp(st, pf, kb2, sb, gpf);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     acc[i] += sb[i];
     kb1[i] += T::A21 * (hf * sb[i]);
   }
-  F::vjp(yf, pf, kb1, acc, gpf);
+  src.template get<1>(st);
+  F::vjp(st, pf, kb1, acc, gpf);
 #pragma unroll
   for (int i = 0; i < D; ++i) lam[i] += (double)acc[i];
 #pragma unroll
   for (int k = 0; k < P; ++k) gp[k] += (double)gpf[k];
+}
+
+// Reverse of one step at (y, dt), recomputing its stages.
+template <class F>
+__device__ __forceinline__ void mixed_step_vjp(const double* y, const double* p, const float* pf,
+                                               double dt, double* lam, double* gp) {
+  MixedStageStates<F> S;
+  mixed_stage_states<F, false>(y, p, pf, dt, S, nullptr, nullptr);
+  mixed_vjp_core<F>(S, pf, dt, lam, gp);
 }
 
 // --- forward adaptive solve with record, float32 stages ----------------------------------
@@ -419,6 +464,139 @@ __global__ void __launch_bounds__(128) tsit5_mixed_adjoint_kernel(const AdjointA
 #pragma unroll
     for (int i = 0; i < P; ++i) a.gp[j * P + i] = gp[i];
   }
+}
+
+
+// --- float32-stage reverse pass that keeps the stage inputs ---------------------------------
+// The counterpart of tsit5_adjoint_stages_body: the segment's replay keeps, for each of its
+// first K-1 steps, the float32 stage inputs (y and s2..s6: 6*D floats, packed two to a
+// double of the shared-memory buffer), so those steps' VJPs skip the recomputation; only the
+// segment's last step evaluates its stages in the reverse sweep.  Same states as
+// tsit5_mixed_adjoint_kernel (mixed_stage_states<F, true> evaluates mixed_replay_step's
+// expressions) and the same VJP code (mixed_vjp_core).
+template <int D>
+GS_HD int mixed_stages_smem_doubles(int K) {
+  return K * D + (K - 1) * 3 * D + seg_io_doubles<D>(K);
+}
+
+template <int D>
+struct MixedStageBuf {
+  double* base;
+  int stride, K;
+  SegIO<D> io;
+  __device__ __forceinline__ MixedStageBuf(int k)
+      : base(gs_seg_smem + threadIdx.x), stride(blockDim.x), K(k),
+        io(k * D + (k - 1) * 3 * D, k) {}
+  __device__ __forceinline__ double& st(int q, int i) { return base[(q * D + i) * stride]; }
+  // float m*D + i of step q's kept inputs (m = 0: y, m = 1..5: s2..s6), q < K-1
+  __device__ __forceinline__ float& stg(int q, int m, int i) {
+    const int f = m * D + i;
+    return reinterpret_cast<float*>(&base[(K * D + q * 3 * D + (f >> 1)) * stride])[f & 1];
+  }
+  __device__ __forceinline__ double& dt(int b, int q) { return io.dt(b, q); }
+  __device__ __forceinline__ double& ck(int b, int i) { return io.ck(b, i); }
+};
+
+template <class F>
+struct MixedKeptStages {  // mixed_vjp_core's stage source: the kept inputs of step q
+  static constexpr int D = F::D;
+  MixedStageBuf<D>* buf;
+  int q;
+  template <int M>
+  __device__ __forceinline__ void get(float* out) const {
+#pragma unroll
+    for (int i = 0; i < D; ++i) out[i] = buf->stg(q, M - 1, i);
+  }
+};
+
+template <class F, int KC>
+__device__ __forceinline__ void tsit5_mixed_adjoint_stages_body(const AdjointArgs& a) {
+  constexpr int D = F::D, P = F::P;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.n) return;
+  double p[P], lam[D], gp[P];
+  float pf[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    p[i] = a.p[j * P + i];
+    pf[i] = (float)p[i];
+    gp[i] = 0.0;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) lam[i] = a.ybar[j * D + i];
+  const int na = steps_in_record(a.n_acc, j, a.cap);
+  const int K = KC > 0 ? KC : a.ck_every;
+  const int nseg = (na + K - 1) / K;
+  MixedStageBuf<D> buf(K);
+  int b = 0;
+  if (nseg > 0) prefetch_segment<D>(buf, b, a.ckpt, a.rec, a.n, j, nseg - 1, K, na);
+  const int top = warp_top_segments(nseg);
+  for (int sg = top - 1; sg >= 0; --sg) {
+    if (sg >= nseg) continue;  // in step with the warp's longest trajectory
+    cp_async_wait_all();  // this segment's checkpoint and dts have landed
+    double y[D], c[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) { y[i] = buf.ck(b, i); c[i] = 0.0; }
+    if (sg > 0) prefetch_segment<D>(buf, b ^ 1, a.ckpt, a.rec, a.n, j, sg - 1, K, na);
+#pragma unroll
+    for (int i = 0; i < D; ++i) buf.st(0, i) = y[i];
+    for (int q = 1; q < K; ++q) {  // replay steps 0..K-2, keeping their stage inputs
+      const double dt = buf.dt(b, q - 1);
+      if (dt != 0.0) {
+        MixedStageStates<F> S;
+        mixed_stage_states<F, true>(y, p, pf, dt, S, y, c);
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          buf.stg(q - 1, 0, i) = S.yf[i];
+          buf.stg(q - 1, 1, i) = S.s2[i];
+          buf.stg(q - 1, 2, i) = S.s3[i];
+          buf.stg(q - 1, 3, i) = S.s4[i];
+          buf.stg(q - 1, 4, i) = S.s5[i];
+          buf.stg(q - 1, 5, i) = S.s6[i];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < D; ++i) buf.st(q, i) = y[i];
+    }
+    {  // the segment's last step: its stages were not evaluated by the replay
+      const double dt = buf.dt(b, K - 1);
+      if (dt != 0.0) {
+        double ys[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) ys[i] = buf.st(K - 1, i);
+        mixed_step_vjp<F>(ys, p, pf, dt, lam, gp);
+      }
+    }
+    for (int q = K - 2; q >= 0; --q) {
+      const double dt = buf.dt(b, q);
+      if (dt != 0.0) {
+        const MixedKeptStages<F> src{&buf, q};
+        mixed_vjp_core<F>(src, pf, dt, lam, gp);
+      }
+    }
+    b ^= 1;
+  }
+  if (a.gy0) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) a.gy0[j * D + i] = lam[i];
+  }
+  if (a.gp) {
+#pragma unroll
+    for (int i = 0; i < P; ++i) a.gp[j * P + i] = gp[i];
+  }
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) tsit5_mixed_adjoint_stages_kernel(const AdjointArgs a) {
+  tsit5_mixed_adjoint_stages_body<F, 0>(a);
+}
+
+// K = 2 with the segment loops unrolled (the autotuned interval of the small built-in fields),
+// bounded to 6 blocks of 128 per SM: unbounded, Lorenz's instance takes 94 registers (5 blocks)
+// where the general stage-keeping kernel holds 6
+template <class F>
+__global__ void __launch_bounds__(128, 6) tsit5_mixed_adjoint_stages_k2_kernel(const AdjointArgs a) {
+  tsit5_mixed_adjoint_stages_body<F, 2>(a);
 }
 
 }  // namespace gs

@@ -79,10 +79,11 @@ extern "C" {
 #define GS_SCHED_STRIDED 0x300
 #define GS_SCHED_MASK 0x300
 
-/* Reverse-pass variant flags, OR-ed into the precision argument of gs_tsit5_adjoint (float64,
- * one thread per trajectory).  RECOMPUTE: the reverse sweep re-evaluates each step's stages
- * from the segment's states.  STAGES: the segment's replay keeps the stage inputs of the steps
- * it evaluates (5*D doubles per step of shared memory), so only each segment's last step
+/* Reverse-pass variant flags, OR-ed into the precision argument of gs_tsit5_adjoint (float64
+ * and float32-stage modes, one thread per trajectory).  RECOMPUTE: the reverse sweep
+ * re-evaluates each step's stages from the segment's states.  STAGES: the segment's replay
+ * keeps the stage inputs of the steps it evaluates (5*D doubles per step of shared memory;
+ * 6*D floats in the float32-stage mode), so only each segment's last step
  * evaluates its stages twice; falls back to RECOMPUTE where that buffer would not fit.  AUTO
  * (0): STAGES while its shared memory leaves it at least 3/5 of RECOMPUTE's resident threads
  * per SM (the autotuned K = 2 of the built-in fields: equal residency, 4-6% faster), else

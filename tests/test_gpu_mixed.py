@@ -102,3 +102,26 @@ def test_grad_closure_mixed_and_float32_routes(gslib, oracle, cuda):
         assert torch.isfinite(p.grad).all()
     with pytest.raises(ValueError, match="unknown precision"):
         gsb.grad_closure(LV(), g["y0"], g["params"], precision="float16")
+
+
+@pytest.mark.parametrize("case,field", CASES[:3])
+def test_mixed_reverse_variants_agree(gslib, cuda, case, field):
+    """The float32-stage reverse pass that keeps the replayed steps' stage inputs (and its
+    unrolled K = 2 instance) against the one that recomputes them: the same float32 stage
+    states and VJP code, so the gradients agree to rounding; K = 64 exceeds the kept buffer for
+    D = 3 and takes the recomputing kernel."""
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    g = load_golden(case)
+    spec = field_spec(field)
+    y0 = torch.tensor(g["y0"], device=cuda)
+    p = torch.tensor(g["params"][:, : spec.nparam], device=cuda).contiguous()
+    for K in (2, 3, 5, 64):
+        r = engine.forward_record("tsit5", spec, y0, p, t0=0.0, t1=float(g["t1"]),
+                                  rtol=float(g["rtol"]), atol=float(g["atol"]), checkpoint=K,
+                                  precision="mixed")
+        ybar = 2.0 * r.y_final
+        a = engine.adjoint(r, p, ybar, precision="mixed", variant="stages")
+        b = engine.adjoint(r, p, ybar, precision="mixed", variant="recompute")
+        for x, y in zip(a, b):
+            assert rowrel(x.cpu().numpy(), y.cpu().numpy()) <= 1e-13, (case, K)

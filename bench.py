@@ -430,7 +430,7 @@ def float32_route_config(args, dev, n: int = 1 << 20) -> dict:
         recs[prec] = (r, gp)
         out[prec] = {"value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
                      "fwd_ms": float(np.mean(fwd)), "adj_ms": float(np.mean(adj)),
-                     "record_bytes": int(r.rec.numel() * r.rec.element_size()),
+                     "record_bytes": int(r.record_bytes),
                      "accepted_steps": int(r.n_acc.to(torch.int64).sum().item())}
     out["speedup_vs_f64"] = out["float64"]["ms_per_step"] / out["float32"]["ms_per_step"]
     out["record_bytes_ratio"] = out["float32"]["record_bytes"] / out["float64"]["record_bytes"]

@@ -167,6 +167,11 @@ class Record:
     uneven: bool = False     # per-trajectory end times: the reverse pass refills lanes
     ys: Optional[torch.Tensor] = None  # (n, K, D) dense output of the forward, if asked for
 
+    @property
+    def record_bytes(self) -> int:
+        """Bytes of the dt record buffer (float32 on the float32 route)."""
+        return self.rec.numel() * self.rec.element_size()
+
     def padded_dts(self, S: Optional[int] = None) -> torch.Tensor:
         """The record in the reference's (n, S) zero-padded layout, in the record's type."""
         if S is None:
@@ -265,6 +270,10 @@ class RecordSet:
                 rows = rows.index_select(0, torch.argsort(cost, descending=True, stable=True))
             out.append(rows)
         return out
+
+    @property
+    def record_bytes(self) -> int:
+        return sum(r.record_bytes for _, r in self.parts)
 
     @property
     def rec_dtype(self) -> torch.dtype:

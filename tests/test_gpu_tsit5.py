@@ -356,3 +356,30 @@ def test_adjoint_variants_agree(gslib, cuda, case, field):
             x, y = x.cpu().numpy(), y.cpu().numpy()
             den = np.maximum(np.abs(y).max(axis=1, keepdims=True), 1e-300)
             assert float((np.abs(x - y) / den).max()) <= 1e-13, (case, K)
+
+
+def test_reused_record_orders_lanes_by_cost(gslib, cuda):
+    """A solve given the previous record of the same batch as its workspace runs its lanes in
+    the order of that record's attempts, longest first (one tier), so a warp's lanes take
+    similar numbers of steps.  Values do not depend on the order: y_final, the step counts,
+    the padded dts and the gradient equal those of a solve in batch order bit for bit."""
+    from gradsolve_b200 import engine
+    g = load_golden("lorenz_small")
+    kw = dict(checkpoint=2)
+    spec, y0, p, ref = _record(gslib, cuda, "lorenz", g, **kw)
+    ybar = 2.0 * ref.y_final
+    gref = engine.adjoint(ref, p, ybar)
+    _, _, _, r0 = _record(gslib, cuda, "lorenz", g, **kw)
+    r1 = engine.forward_record("tsit5", spec, y0, p, t0=float(g["t0"]), t1=float(g["t1"]),
+                               rtol=float(g["rtol"]), atol=float(g["atol"]), max_steps=100000,
+                               workspace=r0, **kw)
+    assert isinstance(r1, engine.RecordSet) and len(r1.parts) == 1
+    rows = r1.parts[0][0]
+    cost = (ref.n_acc + ref.n_rej)[rows].cpu().numpy()
+    assert np.all(np.diff(cost) <= 0) and not np.array_equal(rows.cpu().numpy(),
+                                                             np.arange(ref.n))
+    for a, b in ((r1.y_final, ref.y_final), (r1.n_acc, ref.n_acc), (r1.n_rej, ref.n_rej),
+                 (r1.padded_dts(), ref.padded_dts())):
+        assert torch.equal(a, b)
+    for a, b in zip(engine.adjoint(r1, p, ybar), gref):
+        assert torch.equal(a, b)

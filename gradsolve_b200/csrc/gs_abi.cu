@@ -734,6 +734,29 @@ __global__ void record_to_padded_kernel(long long n, const double* rec, const in
   dts[idx] = s < n_acc[j] ? rec[gs::rec_index(j, s, n)] : 0.0;
 }
 
+// Rows of `width` elements of T: gather dst[r] = src[idx[r]] or scatter dst[idx[r]] = src[r].
+// One thread per element, so the plain side is read or written contiguously and the indexed
+// side a row at a time.  Indices outside [0, src_rows) (gather) or [0, dst_rows) (scatter) are
+// skipped and counted in *bad (the host turns a count into an error).
+template <class T, bool kScatter>
+__global__ void move_rows_kernel(const T* src, const long long* idx, long long rows, int width,
+                                 long long limit, T* dst, unsigned long long* bad) {
+  const long long total = rows * (long long)width;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long r = i / width, c = i - r * width;
+    const long long k = idx[r];
+    if (k < 0 || k >= limit) {
+      if (c == 0) atomicAdd(bad, 1ull);
+      continue;
+    }
+    if (kScatter)
+      dst[k * width + c] = src[i];
+    else
+      dst[i] = src[k * width + c];
+  }
+}
+
 int check_record_args(const char* who, long long n, const double* y0, const double* p,
                       double rtol, double atol, int max_steps, int cap, int ckpt_every,
                       const double* rec, const double* ckpt, const double* yf, const int* n_acc,
@@ -996,6 +1019,40 @@ int gs_record_from_padded(long long n, long long S, const double* dts, long long
   record_from_padded_kernel<<<grid_rows(n), kBlock, 0, (cudaStream_t)stream>>>(n, S, dts, ld, rec,
                                                                                 n_steps);
   return cuda_check("record_from_padded_kernel");
+}
+
+int gs_move_rows(int scatter, int elem_bytes, const void* src, const long long* idx,
+                 long long rows, int width, long long limit, void* dst,
+                 unsigned long long* bad, void* stream) {
+  if (rows < 0 || width < 1 || limit < 0 || (elem_bytes != 4 && elem_bytes != 8))
+    return fail(GS_ERR_ARG, "gs_move_rows: bad sizes");
+  if (rows == 0) return GS_OK;
+  if (!src || !idx || !dst || !bad) return fail(GS_ERR_ARG, "gs_move_rows: null buffer");
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess)
+    return fail(GS_ERR_CUDA, std::string("CUDA: device query: ") + cudaGetErrorString(e));
+  const long long total = rows * (long long)width;
+  const long long want = (total + 255) / 256, cap = 8LL * sms;  // a few waves of 256-thread blocks
+  const unsigned grid = (unsigned)(want < cap ? want : cap);
+  const cudaStream_t s = (cudaStream_t)stream;
+  if (elem_bytes == 8) {
+    if (scatter)
+      move_rows_kernel<unsigned long long, true><<<grid, 256, 0, s>>>(
+          (const unsigned long long*)src, idx, rows, width, limit, (unsigned long long*)dst, bad);
+    else
+      move_rows_kernel<unsigned long long, false><<<grid, 256, 0, s>>>(
+          (const unsigned long long*)src, idx, rows, width, limit, (unsigned long long*)dst, bad);
+  } else {
+    if (scatter)
+      move_rows_kernel<unsigned, true><<<grid, 256, 0, s>>>((const unsigned*)src, idx, rows,
+                                                           width, limit, (unsigned*)dst, bad);
+    else
+      move_rows_kernel<unsigned, false><<<grid, 256, 0, s>>>((const unsigned*)src, idx, rows,
+                                                            width, limit, (unsigned*)dst, bad);
+  }
+  return cuda_check("move_rows_kernel");
 }
 
 int gs_record_to_padded(long long n, int cap, const double* rec, const int* n_acc, long long S,

@@ -323,12 +323,67 @@ def _parts(r):
     return r.parts if isinstance(r, RecordSet) else [(None, r)]
 
 
+# Row moves of the tier plan (gather into a tier's order, scatter back) run in libgsolve's
+# gs_move_rows: one thread per element, the contiguous side streamed.  (torch's index_select
+# took 2.2 ms for the 4M parameter rows of a 2^22 Lotka-Volterra batch; this kernel is
+# HBM-bound.)  Out-of-range indices are skipped and counted in a per-device counter, which
+# the forward checks after its own synchronisation (_check_moves).
+_ELEM_BYTES = {torch.float64: 8, torch.int64: 8, torch.float32: 4, torch.int32: 4}
+_BAD_MOVES: dict = {}
+
+
+def _bad_counter(device) -> torch.Tensor:
+    key = device.index
+    if key not in _BAD_MOVES:
+        _BAD_MOVES[key] = torch.zeros(1, dtype=torch.int64, device=device)
+    return _BAD_MOVES[key]
+
+
+def _check_moves(device) -> None:
+    c = _BAD_MOVES.get(device.index)
+    if c is not None and int(c.item()) != 0:
+        n = int(c.item())
+        c.zero_()
+        raise RuntimeError(f"gs_move_rows skipped {n} out-of-range row indices (a tier plan "
+                           "referenced rows outside its batch)")
+
+
+def _movable(t: torch.Tensor) -> bool:
+    return t.is_cuda and t.dtype in _ELEM_BYTES and t.is_contiguous() and t.ndim >= 1
+
+
+def _move_rows(src: torch.Tensor, idx: torch.Tensor, dst: torch.Tensor, scatter: bool) -> None:
+    width = 1
+    for d in src.shape[1:]:
+        width *= int(d)
+    if idx.numel() == 0 or width == 0:
+        return
+    idx = idx.to(device=src.device, dtype=torch.int64).contiguous()
+    L = _lib.lib()
+    _lib.check(L.gs_move_rows(int(scatter), _ELEM_BYTES[src.dtype], _ptr(src), _ptr(idx),
+                              idx.numel(), width, dst.shape[0] if scatter else src.shape[0],
+                              _ptr(dst), _ptr(_bad_counter(src.device)), _stream()),
+               "gs_move_rows", L)
+
+
+def _put_rows(dst: torch.Tensor, rows: torch.Tensor, src: torch.Tensor) -> None:
+    """dst[rows] = src along the leading dimension, on the current stream."""
+    if _movable(dst) and _movable(src) and src.dtype == dst.dtype:
+        _move_rows(src, rows, dst, scatter=True)
+    else:
+        dst.index_copy_(0, rows, src)
+
+
 def _take(t: Optional[torch.Tensor], rows: Optional[torch.Tensor]):
     """Rows of t on the current stream (t stays alive until this stream has read it)."""
     if t is None or rows is None:
         return t
     if t.is_cuda:
         t.record_stream(torch.cuda.current_stream())
+    if _movable(t):
+        out = torch.empty((rows.numel(),) + tuple(t.shape[1:]), dtype=t.dtype, device=t.device)
+        _move_rows(t, rows, out, scatter=False)
+        return out
     return t.index_select(0, rows).contiguous()
 
 
@@ -585,10 +640,10 @@ def _assemble(method, spec, n, device, parts, t1v, saveat_ts, streams, sub=None)
             yf.copy_(rr.y_final), n_acc.copy_(rr.n_acc), n_rej.copy_(rr.n_rej)
             status.copy_(rr.status)
         else:
-            yf.index_copy_(0, rows, rr.y_final)
-            n_acc.index_copy_(0, rows, rr.n_acc)
-            n_rej.index_copy_(0, rows, rr.n_rej)
-            status.index_copy_(0, rows, rr.status)
+            _put_rows(yf, rows, rr.y_final)
+            _put_rows(n_acc, rows, rr.n_acc)
+            _put_rows(n_rej, rows, rr.n_rej)
+            _put_rows(status, rows, rr.status)
         if rr.ys is not None:
             if ys is None:
                 ys = torch.empty((n,) + tuple(rr.ys.shape[1:]), dtype=torch.float64,
@@ -596,7 +651,7 @@ def _assemble(method, spec, n, device, parts, t1v, saveat_ts, streams, sub=None)
             if rows is None:
                 ys.copy_(rr.ys)
             else:
-                ys.index_copy_(0, rows, rr.ys)
+                _put_rows(ys, rows, rr.ys)
     return RecordSet(method, spec, n, float(parts[0][1].t0), parts, sub, yf, n_acc, n_rej,
                      status, uneven=t1v is not None, ys=ys, streams=streams)
 
@@ -667,6 +722,7 @@ def _forward_planned(method, spec, y0, p, t1v, saveat_ts, ws: RecordSet, kw):
     res = _assemble(method, spec, n, y0.device, out, t1v, saveat_ts, streams)
     # trajectories that outgrew their planned tier: solved again with more capacity
     over = torch.nonzero(res.status == 3).squeeze(1)
+    _check_moves(y0.device)  # (after the synchronisation nonzero makes)
     if over.numel() == 0:
         return res
     cap_of_row = torch.zeros(n, dtype=torch.int64, device=y0.device)
@@ -731,7 +787,7 @@ def _scatter(r, res, i):
         if rows is None:
             out.copy_(outs[i])
         else:
-            out.index_copy_(0, rows, outs[i])
+            _put_rows(out, rows, outs[i])
     return out
 
 

@@ -290,6 +290,18 @@ int gs_record_from_padded(long long n, long long S, const double* dts, long long
 int gs_record_to_padded(long long n, int cap, const double* rec, const int* n_acc, long long S,
                         double* dts, void* stream);
 
+/*
+ * Row moves for batches split into tiers or reordered (the host side's tier plan): rows of
+ * `width` elements of elem_bytes (4 or 8) bytes.  scatter = 0: dst[r] = src[idx[r]] for r <
+ * rows (idx into `limit` source rows); scatter = 1: dst[idx[r]] = src[r] (idx into `limit`
+ * destination rows).  Indices outside [0, limit) are skipped and counted into *bad (a device
+ * counter the caller zeroes and reads).  No counterpart in the reference, which re-solves the
+ * whole batch instead of planning tiers (gradsolve/solvers/record_jax.py:192-199).
+ */
+int gs_move_rows(int scatter, int elem_bytes, const void* src, const long long* idx,
+                 long long rows, int width, long long limit, void* dst,
+                 unsigned long long* bad, void* stream);
+
 /* Size of the library's own device scratch used by gs_tsit5_vjp_static: 64 MiB, held by
  * every GPU that loads libgsolve.so until the process exits.  Only libgsolve.so carries it:
  * the libraries built for generated fields (gradsolve_b200/fieldgen.py) export

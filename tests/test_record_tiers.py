@@ -249,3 +249,27 @@ def test_planned_tier_outgrown(fake):
     assert np.all(r2.status.numpy() == 0)
     yf = engine.replay(r2, y0, torch.tensor(steps2[:, None]))
     np.testing.assert_array_equal(yf[:, 0].numpy(), steps2 + 1000.0 * np.array([8, 32, 128]))
+
+
+def test_reused_single_record_orders_lanes_by_cost(fake):
+    """A record reused as the next solve's workspace becomes a one-tier plan whose rows run
+    longest first (by the previous record's attempts); its results come back in batch order."""
+    spec = field_spec("lorenz")
+    rng = np.random.default_rng(3)
+    steps = rng.integers(1, 8, 40).astype(np.float64)
+    p = torch.tensor(steps[:, None])
+    y0 = torch.zeros((40, 3), dtype=torch.float64)
+    kw = dict(t0=0.0, t1=1.0, rtol=1e-6, atol=1e-6, cap0=8, checkpoint=4, budget_bytes=1 << 40)
+    r1 = engine.forward_record("tsit5", spec, y0, p, **kw)
+    assert isinstance(r1, engine.Record)
+    r2 = engine.forward_record("tsit5", spec, y0, p, workspace=r1, **kw)
+    assert isinstance(r2, engine.RecordSet) and len(r2.parts) == 1
+    rows = r2.parts[0][0].numpy()
+    assert np.all(np.diff(steps[rows]) <= 0)           # longest first
+    np.testing.assert_array_equal(r2.n_acc.numpy(), steps.astype(np.int32))
+    np.testing.assert_array_equal(r2.y_final.numpy(), y0.numpy() + steps[:, None])
+    gy0, gp = engine.adjoint(r2, p, torch.ones((40, 3), dtype=torch.float64))
+    np.testing.assert_array_equal(gp[:, 0].numpy(), steps + 1e6 * 8)
+    d = r2.padded_dts().numpy()
+    for j in range(40):
+        np.testing.assert_array_equal(d[j, : int(steps[j])], 1.0 / steps[j])

@@ -118,8 +118,8 @@ def autotune_ckpt_every(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch
     cache the fastest (best of ``reps`` timings).  The sample spans many waves of the GPU:
     the candidates' reverse passes hold different numbers of blocks per SM (their shared
     memory grows with K), and on a few waves the partial last wave, not the kernel, decides
-    (on 2^19 Lotka-Volterra rows K = 4 won by noise where the full 2^22 batch runs 5% faster
-    at K = 2)."""
+    (a 2^19-row sample of a 2^22 Lotka-Volterra batch chose K = 4, where the full batch runs
+    5% faster at K = 2)."""
     m = min(y0.shape[0], sample)
     ys, ps = y0[:m].contiguous(), p[:m].contiguous()
     tv = None if t1v is None else t1v[:m].contiguous()

@@ -32,6 +32,9 @@ _SIGS = {
     "gs_record_bytes_prec": (c_size_t, [c_int, c_ll, c_int]),
     "gs_move_rows": (c_int, [c_int, c_int, c_void_p, c_void_p, c_ll, c_int, c_ll, c_void_p,
                              c_void_p, c_void_p]),
+    "gs_adjoint_ordered": (c_int, [c_int, c_int, c_int, c_ll, c_void_p, c_void_p, c_void_p,
+                                   c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                                   c_void_p, c_void_p]),
     "gs_ckpt_bytes_prec": (c_size_t, [c_int, c_int, c_ll, c_int, c_int]),
     "gs_max_ckpt_every": (c_int, []),
     "gs_lane_choices": (c_int, [c_int, ctypes.POINTER(c_int), c_int]),

@@ -913,9 +913,10 @@ int gs_tsit5_replay(int field, int precision, long long n, const double* y0, con
                     prec == GS_PREC_MIXED, precision)
 }
 
-int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, const double* rec,
-                     const int* n_acc, int cap, const double* ckpt, int ckpt_every,
-                     const double* ybar, double* gy0, double* gp, void* stream) {
+static int tsit5_adjoint_impl(int field, int precision, long long n, const double* p,
+                              const double* rec, const int* n_acc, int cap, const double* ckpt,
+                              int ckpt_every, const double* ybar, double* gy0, double* gp,
+                              const long long* order, void* stream) {
   const int prec = precision & GS_PREC_MASK;
   if (prec != GS_PREC_F64 && prec != GS_PREC_MIXED && prec != GS_PREC_F32)
     return fail(GS_ERR_PRECISION, "gs_tsit5_adjoint: unknown precision mode " + std::to_string(prec));
@@ -924,7 +925,7 @@ int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, con
   int D, P;
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (n == 0) return GS_OK;
-  gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp, cap};
+  gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp, cap, order};
   if (prec == GS_PREC_F32) {
     if ((rc = f32_schedule(precision, "gs_tsit5_adjoint"))) return rc;
     GS_TSIT5_DISPATCH(field, launch_f32_tsit5_adjoint, a, (cudaStream_t)stream)
@@ -932,6 +933,13 @@ int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, con
   GS_TSIT5_DISPATCH(field, launch_tsit5_adjoint, a, cap, (cudaStream_t)stream,
                     prec == GS_PREC_MIXED, adjoint_schedule(precision), precision & GS_ADJ_MASK,
                     precision)
+}
+
+int gs_tsit5_adjoint(int field, int precision, long long n, const double* p, const double* rec,
+                     const int* n_acc, int cap, const double* ckpt, int ckpt_every,
+                     const double* ybar, double* gy0, double* gp, void* stream) {
+  return tsit5_adjoint_impl(field, precision, n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar,
+                            gy0, gp, nullptr, stream);
 }
 
 int gs_lane_choices(int field, int* out, int cap) {
@@ -988,9 +996,10 @@ int gs_ros23_replay(int field, int precision, long long n, const double* y0, con
   GS_ROS23_DISPATCH(field, launch_ros23_replay, a, (cudaStream_t)stream)
 }
 
-int gs_ros23_adjoint(int field, int precision, long long n, const double* p, const double* rec,
-                     const int* n_acc, int cap, const double* ckpt, int ckpt_every,
-                     const double* ybar, double* gy0, double* gp, void* stream) {
+static int ros23_adjoint_impl(int field, int precision, long long n, const double* p,
+                              const double* rec, const int* n_acc, int cap, const double* ckpt,
+                              int ckpt_every, const double* ybar, double* gy0, double* gp,
+                              const long long* order, void* stream) {
   const int prec = precision & GS_PREC_MASK;
   if (prec != GS_PREC_F64 && prec != GS_PREC_F32)
     return fail(GS_ERR_PRECISION, "gs_ros23_adjoint: Rosenbrock23 runs in float64 or float32");
@@ -999,13 +1008,39 @@ int gs_ros23_adjoint(int field, int precision, long long n, const double* p, con
   int D, P;
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (n == 0) return GS_OK;
-  gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp, cap};
+  gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp, cap, order};
   if (prec == GS_PREC_F32) {
     if ((rc = f32_schedule(precision, "gs_ros23_adjoint"))) return rc;
     GS_ROS23_DISPATCH(field, launch_f32_ros23_adjoint, a, (cudaStream_t)stream)
   }
   GS_ROS23_DISPATCH(field, launch_ros23_adjoint, a, cap, (cudaStream_t)stream,
                     adjoint_schedule(precision))
+}
+
+int gs_ros23_adjoint(int field, int precision, long long n, const double* p, const double* rec,
+                     const int* n_acc, int cap, const double* ckpt, int ckpt_every,
+                     const double* ybar, double* gy0, double* gp, void* stream) {
+  return ros23_adjoint_impl(field, precision, n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar, gy0,
+                            gp, nullptr, stream);
+}
+
+int gs_adjoint_ordered(int method, int field, int precision, long long n, const double* p,
+                       const double* rec, const int* n_acc, int cap, const double* ckpt,
+                       int ckpt_every, const double* ybar, double* gy0, double* gp,
+                       const long long* order, void* stream) {
+  if (!order || !aligned8(order))
+    return fail(GS_ERR_ARG, "gs_adjoint_ordered: order must be an 8-byte aligned device array");
+  if (adjoint_schedule(precision) != GS_SCHED_STATIC)
+    return fail(GS_ERR_ARG, "gs_adjoint_ordered: the lane order applies to one thread per "
+                            "trajectory (GS_SCHED_STATIC or AUTO); persistent lanes balance "
+                            "themselves");
+  if (method == GS_METHOD_TSIT5)
+    return tsit5_adjoint_impl(field, precision, n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar,
+                              gy0, gp, order, stream);
+  if (method == GS_METHOD_ROS23)
+    return ros23_adjoint_impl(field, precision, n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar,
+                              gy0, gp, order, stream);
+  return fail(GS_ERR_ARG, "gs_adjoint_ordered: unknown method " + std::to_string(method));
 }
 
 int gs_record_from_padded(long long n, long long S, const double* dts, long long ld,

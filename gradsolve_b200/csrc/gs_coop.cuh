@@ -275,8 +275,10 @@ template <class F, int G>
 __global__ void __launch_bounds__(128) tsit5_coop_adjoint_kernel(const AdjointArgs a) {
   using L = Lane<F, G>;
   constexpr int C = L::C, D = F::D, P = F::P;
-  const long long j = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / G;
-  if (j >= a.n) return;
+  const long long g = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  if (g >= a.n) return;
+  const long long j = lane_traj(a, g);  // the group's trajectory (one entry for all G lanes)
+  if (j < 0) return;
   const int l = L::lane();
   double p[P], lam[C], gp[P];
 #pragma unroll

@@ -232,8 +232,10 @@ extern __shared__ float gs_seg_smem_f32[];
 template <class F, int kMethod>
 __global__ void __launch_bounds__(128) f32_adjoint_kernel(const AdjointArgs a) {
   constexpr int D = F::D, P = F::P;
-  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= a.n) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  const long long j = lane_traj(a, t);
+  if (j < 0) return;
   float p[P], lam[D], gp[P];
 #pragma unroll
   for (int i = 0; i < P; ++i) {

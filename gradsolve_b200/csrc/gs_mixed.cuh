@@ -410,8 +410,10 @@ __global__ void __launch_bounds__(128) tsit5_mixed_replay_kernel(const ReplayArg
 template <class F>
 __global__ void __launch_bounds__(128) tsit5_mixed_adjoint_kernel(const AdjointArgs a) {
   constexpr int D = F::D, P = F::P;
-  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= a.n) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  const long long j = lane_traj(a, t);
+  if (j < 0) return;
   double p[P], lam[D], gp[P];
   float pf[P];
 #pragma unroll
@@ -512,8 +514,10 @@ struct MixedKeptStages {  // mixed_vjp_core's stage source: the kept inputs of s
 template <class F, int KC>
 __device__ __forceinline__ void tsit5_mixed_adjoint_stages_body(const AdjointArgs& a) {
   constexpr int D = F::D, P = F::P;
-  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= a.n) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  const long long j = lane_traj(a, t);
+  if (j < 0) return;
   double p[P], lam[D], gp[P];
   float pf[P];
 #pragma unroll

@@ -428,8 +428,10 @@ struct AdjRosBuf {
 template <class F, bool kKeep, int KC>
 __device__ __forceinline__ void ros23_adjoint_body(const AdjointArgs& a) {
   constexpr int D = F::D, P = F::P;
-  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= a.n) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  const long long j = lane_traj(a, t);
+  if (j < 0) return;
   double p[P], lam[D], gp[P];
 #pragma unroll
   for (int i = 0; i < P; ++i) {

@@ -453,7 +453,18 @@ struct AdjointArgs {
   double* gy0;
   double* gp;
   int cap;  // record capacity: step counts are clamped to [0, cap] before any record read
+  // lane t integrates trajectory order[t] (a permutation of [0, n): lanes ordered by step
+  // count keep a warp's lanes in step), or trajectory t when null
+  const long long* order = nullptr;
 };
+
+// The trajectory of reverse-pass lane t; -1 (the lane idles) for an entry of `order` outside
+// [0, n), so a bad permutation cannot send a lane outside the batch's arrays.
+__device__ __forceinline__ long long lane_traj(const AdjointArgs& a, long long t) {
+  if (!a.order) return t;
+  const long long j = __ldg(a.order + t);
+  return (j >= 0 && j < a.n) ? j : -1;
+}
 
 struct ReplayArgs {
   long long n;
@@ -791,8 +802,10 @@ __device__ __forceinline__ void prefetch_segment(Buf& buf, int b, const double* 
 template <class F>
 __global__ void __launch_bounds__(128) tsit5_adjoint_kernel(const AdjointArgs a) {
   constexpr int D = F::D, P = F::P;
-  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= a.n) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  const long long j = lane_traj(a, t);
+  if (j < 0) return;
   double p[P], lam[D], gp[P];
 #pragma unroll
   for (int i = 0; i < P; ++i) {
@@ -892,8 +905,10 @@ struct KeptStages {  // tsit5_vjp_core's stage source: the kept inputs of step q
 template <class F, int KC>
 __device__ __forceinline__ void tsit5_adjoint_stages_body(const AdjointArgs& a) {
   constexpr int D = F::D, P = F::P;
-  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= a.n) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  const long long j = lane_traj(a, t);
+  if (j < 0) return;
   double p[P], lam[D], gp[P];
 #pragma unroll
   for (int i = 0; i < P; ++i) {

@@ -226,6 +226,19 @@ int gs_ros23_adjoint(int field, int precision, long long n, const double* p, con
                      const int* n_acc, int cap, const double* ckpt, int ckpt_every,
                      const double* ybar, double* gy0, double* gp, void* stream);
 
+/* gs_tsit5_adjoint (method GS_METHOD_TSIT5) or gs_ros23_adjoint (GS_METHOD_ROS23) with the
+ * lanes in a given order: lane t integrates trajectory order[t], a device array of n int64
+ * forming a permutation of [0, n) (an entry outside [0, n) leaves its lane idle).  Every
+ * input and output keeps the batch's own order; only the assignment of trajectories to
+ * threads changes, so the results equal the unordered call's bit for bit.  Ordered by step
+ * count (longest first), a warp's lanes take similar numbers of steps: the reverse pass of a
+ * record whose step counts spread widely then wastes no lanes on finished trajectories.  One
+ * thread per trajectory only (GS_SCHED_STATIC or AUTO).  No counterpart in the reference. */
+int gs_adjoint_ordered(int method, int field, int precision, long long n, const double* p,
+                       const double* rec, const int* n_acc, int cap, const double* ckpt,
+                       int ckpt_every, const double* ybar, double* gy0, double* gp,
+                       const long long* order, void* stream);
+
 #define GS_METHOD_TSIT5 0
 #define GS_METHOD_ROS23 1
 

@@ -383,3 +383,30 @@ def test_reused_record_orders_lanes_by_cost(gslib, cuda):
         assert torch.equal(a, b)
     for a, b in zip(engine.adjoint(r1, p, ybar), gref):
         assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("method,field,case,precision", [
+    ("tsit5", "lorenz", "lorenz_small", "float64"), ("tsit5", "lorenz", "lorenz_small", "mixed"),
+    ("tsit5", "lorenz", "lorenz_small", "float32"), ("rosenbrock23", "robertson",
+                                                      "robertson_stiff", "float64"),
+    ("tsit5", "lorenz96_32", "lorenz96_32", "float64")])
+def test_ordered_reverse_lanes_equal_batch_order(gslib, cuda, monkeypatch, method, field, case,
+                                                 precision):
+    """gs_adjoint_ordered (lanes assigned longest trajectory first) against the reverse pass in
+    batch order: every gradient bit for bit, for the float64, float32-stage, float32,
+    Rosenbrock23 and group-of-lanes kernels."""
+    from gradsolve_b200 import engine
+    g = load_golden(case)
+    spec = _spec(field)
+    y0 = torch.tensor(g["y0"], device=cuda)
+    p = torch.tensor(g["params"][:, : spec.nparam], device=cuda).contiguous()
+    r = engine.forward_record(method, spec, y0, p, t0=float(g["t0"]), t1=float(g["t1"]),
+                              rtol=float(g["rtol"]), atol=float(g["atol"]), max_steps=100000,
+                              checkpoint=3, precision=precision)
+    ybar = 2.0 * r.y_final
+    kw = dict(want_y0=True, want_p=True, precision=precision, schedule="auto", variant="auto")
+    monkeypatch.setattr(engine, "ORDER_LANES_MIN", 1)
+    a = engine._adjoint_one(r, p, ybar, in_batch_order=True, **kw)
+    b = engine._adjoint_one(r, p, ybar, in_batch_order=False, **kw)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)

@@ -77,8 +77,12 @@ def _device(device) -> torch.device:
 
 
 def _as_tensor(x, dev: torch.device) -> torch.Tensor:
+    """x as a float64 tensor on dev.  A pinned host tensor is copied asynchronously on the
+    current stream (the kernels that read it follow on the same stream), so the host goes on
+    to launch them while the copy runs; as with any asynchronous copy, the caller keeps the
+    host buffer unchanged until the stream has passed it."""
     if isinstance(x, torch.Tensor):
-        return x.to(device=dev, dtype=torch.float64)
+        return x.to(device=dev, dtype=torch.float64, non_blocking=x.is_pinned())
     return torch.as_tensor(np.asarray(x, dtype=np.float64), device=dev)
 
 
@@ -103,7 +107,7 @@ def _prepare(problem, y0, params, dev):
     if y0_np.shape[-1] != spec.dim:
         raise ValueError(f"y0 must be (n, {spec.dim}) for {problem.name!r}; got {tuple(y0_np.shape)}")
     if isinstance(params, torch.Tensor):
-        p_t = params.to(device=dev, dtype=torch.float64)
+        p_t = params.to(device=dev, dtype=torch.float64, non_blocking=params.is_pinned())
         if p_t.ndim == 1:
             p_t = p_t[:, None]
     else:

@@ -19,6 +19,31 @@ import torch
 from . import engine
 
 
+def _point(y0: torch.Tensor, pk: torch.Tensor) -> tuple:
+    """A replay point: the tensors and their version counters at capture."""
+    return (y0, pk, y0._version, pk._version)
+
+
+def _same(a: torch.Tensor, b: torch.Tensor) -> bool:
+    """a equals b elementwise.  The same view of the same storage answers without a device
+    synchronisation (the caller has checked b's version counter, which a shares)."""
+    if (a.data_ptr() == b.data_ptr() and a.shape == b.shape and a.stride() == b.stride()
+            and a.dtype == b.dtype and a.device == b.device):
+        return True
+    return torch.equal(a, b)
+
+
+def _at_point(y0: torch.Tensor, pk: torch.Tensor, point) -> bool:
+    """(y0, pk) is the stored point, and the point's tensors were not modified in place since
+    it was taken."""
+    if point is None:
+        return False
+    y0r, pr, v0, v1 = point
+    if y0r._version != v0 or pr._version != v1:
+        return False
+    return _same(y0, y0r) and _same(pk, pr)
+
+
 class ReplayState:
     """The frozen record plus bookkeeping shared by every call of one closure."""
 
@@ -31,13 +56,12 @@ class ReplayState:
         self.nparam = nparam
         self.precision = precision
         self.version = 0           # bumps whenever the checkpoints are rewritten
-        self.ckpt_point = (y0_rec, p_rec) if reuse_recording else None
+        self.ckpt_point = _point(y0_rec, p_rec) if reuse_recording else None
         self.ts_rec = ts_rec       # the saveat times the recording pass also saved at
 
     def at_recording(self, y0: torch.Tensor, pk: torch.Tensor) -> bool:
         """The checkpoints are the recording pass's own and (y0, pk) is its point."""
-        return (self.version == 0 and self.ckpt_point is not None
-                and torch.equal(y0, self.ckpt_point[0]) and torch.equal(pk, self.ckpt_point[1]))
+        return self.version == 0 and _at_point(y0, pk, self.ckpt_point)
 
     def kernel_p(self, p: torch.Tensor) -> torch.Tensor:
         if p.shape[1] < self.nparam:  # only fields that ignore their parameter get here
@@ -46,12 +70,11 @@ class ReplayState:
 
     def run_forward(self, y0: torch.Tensor, p: torch.Tensor) -> torch.Tensor:
         pk = self.kernel_p(p)
-        if (self.ckpt_point is not None and torch.equal(y0, self.ckpt_point[0])
-                and torch.equal(pk, self.ckpt_point[1])):
+        if _at_point(y0, pk, self.ckpt_point):
             return self.record.y_final.clone()
         yf = engine.replay(self.record, y0.contiguous(), pk, write_ckpt=True,
                            precision=self.precision)
-        self.ckpt_point = (y0.detach().clone(), pk.detach().clone())
+        self.ckpt_point = _point(y0.detach().clone(), pk.detach().clone())
         self.version += 1
         return yf
 
@@ -72,11 +95,10 @@ class _ReplayFn(torch.autograd.Function):
         state: ReplayState = ctx.state
         y0, p = ctx.saved_tensors
         pk = state.kernel_p(p)
-        if state.version != ctx.version or state.ckpt_point is None or not (
-                torch.equal(y0, state.ckpt_point[0]) and torch.equal(pk, state.ckpt_point[1])):
+        if state.version != ctx.version or not _at_point(y0, pk, state.ckpt_point):
             # another forward of the same closure rewrote the checkpoints: rebuild ours
             engine.replay(state.record, y0, pk, write_ckpt=True, precision=state.precision)
-            state.ckpt_point = (y0.detach().clone(), pk.detach().clone())
+            state.ckpt_point = _point(y0.detach().clone(), pk.detach().clone())
             state.version += 1
         need_y0, need_p = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
         gy0, gpk = engine.adjoint(state.record, pk, ybar.to(torch.float64),
@@ -111,7 +133,7 @@ class _SaveatFn(torch.autograd.Function):
         else:
             _yf, ys = engine.replay_saveat(rec, y0, pk, ts, write_ckpt=True,
                                            precision=state.precision)
-            state.ckpt_point = (y0.detach().clone(), pk.detach().clone())
+            state.ckpt_point = _point(y0.detach().clone(), pk.detach().clone())
             state.version += 1
         ctx.state, ctx.ts, ctx.version = state, ts, state.version
         ctx.save_for_backward(y0, p)
@@ -125,7 +147,7 @@ class _SaveatFn(torch.autograd.Function):
         if state.version != ctx.version:
             engine.replay_saveat(state.record, y0, pk, ctx.ts, write_ckpt=True,
                                  precision=state.precision)
-            state.ckpt_point = (y0.detach().clone(), pk.detach().clone())
+            state.ckpt_point = _point(y0.detach().clone(), pk.detach().clone())
             state.version += 1
         need_y0, need_p = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
         gy0, gpk = engine.adjoint_saveat(state.record, pk, ctx.ts, ysbar, None,

@@ -511,7 +511,10 @@ def run_b200(args) -> None:
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    from gradsolve_b200 import _lib
+    launches0 = _lib.launch_count()
     fwd_ms, adj_ms, step_ms, (r, gp) = _time_steps(torch, step, args.steps, flush, stream)
+    gpu_launches = _lib.launch_count() - launches0  # this library's kernels in the timed steps
     if world > 1:
         dist.barrier()
     ms_per_step = float(np.mean(step_ms))
@@ -609,7 +612,7 @@ def run_b200(args) -> None:
         for _ in range(max(1, args.warmup)):
             e2e_step()
         torch.cuda.synchronize()
-        ke = max(1, min(args.steps, 5))
+        ke = max(1, min(args.steps, 10))
         with _NoGC():
             t0 = time.perf_counter()
             marks = [t0]
@@ -701,7 +704,7 @@ def run_b200(args) -> None:
                    "n_per_gpu": n, "record_len_max": S, "checkpoint_every": K,
                    "attempts": att, "accepted": acc, "parallelism": f"shard{world}",
                    "l2": "flushed between timed steps (record traffic also >> L2)"},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": gpu_launches,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
         "parity_sample": checks, "config3_mixed": config3, "float32_route": f32_route,
         "fwd_ms": fwd_avg, "adj_ms": adj_avg, "mixed": mixed, "solve": solve or None,
@@ -878,6 +881,8 @@ def measure_workload(args, name: str, n: int, dev, world: int = 1, rank: int = 0
         evs = [[torch.cuda.Event(enable_timing=True) for _ in range(len(groups) + 1)]
                for _ in range(args.steps)]
         outs = None
+        from gradsolve_b200 import _lib
+        launches0 = _lib.launch_count()
         nogc = _NoGC()
         nogc.__enter__()
         for e in evs:
@@ -889,6 +894,7 @@ def measure_workload(args, name: str, n: int, dev, world: int = 1, rank: int = 0
                 e[k + 1].record(stream)
         torch.cuda.synchronize()
         nogc.__exit__(None, None, None)
+        time_variant.launches = _lib.launch_count() - launches0
         per_group = [float(np.mean([e[k].elapsed_time(e[k + 1]) for e in evs]))
                      for k in range(len(groups))]
         steps_ms = [e[0].elapsed_time(e[-1]) for e in evs]
@@ -900,6 +906,7 @@ def measure_workload(args, name: str, n: int, dev, world: int = 1, rank: int = 0
     clocks.start()
     ms, per_group, outs = time_variant("float64")
     steps_ms = time_variant.steps_ms
+    gpu_launches = time_variant.launches
     infos = []
     for g, t_ms, (r, gp) in zip(groups, per_group, outs):
         assert int((r.status != 0).sum().item()) == 0, f"{g.name}: solve failed"
@@ -984,7 +991,7 @@ def measure_workload(args, name: str, n: int, dev, world: int = 1, rank: int = 0
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "dtype": "f64", "data": "synthetic (seeded numpy default_rng)", "groups": infos,
         "fp64_peak_tflops": fp64_peak, "oracle_parity_sample": parity, "mixed": mixed,
-        "cpu_baseline": cpu, "clocks": clk, "ms_steps": steps_ms,
+        "cpu_baseline": cpu, "clocks": clk, "ms_steps": steps_ms, "gpu_launches": gpu_launches,
         "config": {"n_per_gpu": n, "checkpoint_policy": str(args.checkpoint),
                    "schedule": args.schedule, "l2": "flushed between timed steps"},
     }

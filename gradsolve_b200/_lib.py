@@ -22,6 +22,7 @@ c_int, c_ll, c_double, c_size_t, c_void_p = (ctypes.c_int, ctypes.c_longlong, ct
 # name -> (restype, argtypes).  Pointers to device memory travel as c_void_p integers.
 _SIGS = {
     "gs_version": (c_int, []),
+    "gs_launch_count": (ctypes.c_ulonglong, []),
     "gs_last_error": (ctypes.c_char_p, []),
     "gs_field_dims": (c_int, [c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
     "gs_tableau": (c_int, [ctypes.POINTER(c_double), c_int]),
@@ -123,6 +124,12 @@ def lib_for(spec):
                 raise RuntimeError(f"field library {built} is not the expected {path}")
         L = _FIELD_LIBS[path] = _load(path)
     return L
+
+
+def launch_count() -> int:
+    """Kernel launches issued so far by libgsolve.so and every field library loaded."""
+    return int(lib().gs_launch_count()) + sum(int(L.gs_launch_count())
+                                               for L in _FIELD_LIBS.values())
 
 
 def check(rc: int, what: str, L=None) -> None:

@@ -37,7 +37,12 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+// Kernel launches this library has issued in the process (every launch is followed by a
+// cuda_check, which counts it); read through gs_launch_count.
+std::atomic<unsigned long long> g_launches{0};
+
 int cuda_check(const char* what) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(GS_ERR_CUDA, std::string("CUDA: ") + what + ": " + cudaGetErrorString(e));
   return GS_OK;
@@ -801,6 +806,8 @@ int check_adjoint_args(const char* who, long long n, const double* p, const doub
 extern "C" {
 
 int gs_version(void) { return 100; }
+
+unsigned long long gs_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 const char* gs_last_error(void) { return g_err.c_str(); }
 

@@ -113,6 +113,10 @@ extern "C" {
 /* Library version (major*10000 + minor*100 + patch). */
 int gs_version(void);
 
+/* Kernel launches this library has issued in the process so far (all entry points,
+ * counted as they are made): a measurement aid, e.g. the launches inside a timed region. */
+unsigned long long gs_launch_count(void);
+
 /* Message of the last failed call on this thread ("" if none). */
 const char* gs_last_error(void);
 

@@ -38,12 +38,12 @@ L2_BYTES = 126 * 1024 * 1024
 
 # DRAM bytes per trajectory of each kernel on this workload, from ncu captures at n = 2^18
 # (dram__bytes_read.sum + dram__bytes_write.sum per launch / 2^18), by checkpoint interval;
-# profiles/reverse_passes_warp_aligned_segments.md (the reverse pass with warp-aligned
-# segment sweeps) and profiles/tsit5_f64_lorenz_bench_n2e20_launches_n2e18_K2.md.  Traffic
-# grows with the trajectory count.
+# profiles/tsit5_f64_lorenz_bench_n2e20_launches_n2e18_K2.md (the timed step's launches:
+# lanes ordered by cost, segments swept in step with the warp's longest trajectory).
+# Traffic grows with the trajectory count.
 DRAM_BYTES_PER_TRAJ = {
-    "tsit5_adjoint_stages_k2_kernel": {2: (4.390491136e9 + 2.427392e6) / 2**18},
-    "tsit5_record_kernel": {2: (0.178603264e9 + 4.341853440e9) / 2**18},
+    "tsit5_adjoint_stages_k2_kernel": {2: (4.268379e9 + 6.600e6) / 2**18},
+    "tsit5_record_kernel": {2: (0.170665e9 + 4.326640e9) / 2**18},
 }
 
 

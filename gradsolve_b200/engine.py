@@ -63,6 +63,30 @@ def record_dtype(precision: str) -> torch.dtype:
     return torch.float32 if precision == "float32" else torch.float64
 
 
+# The checkpoint budget, a quarter of the memory free for the checkpoints (the device's free
+# memory plus what the caching allocator holds unused).  cudaMemGetInfo took 0.1-1 ms per
+# call on B200, inside every solve; the answer is kept while the allocator's reservation is
+# unchanged (the steady state of a training loop) and for at most BUDGET_TTL seconds, so a
+# solve re-queries after its own process allocated or released device memory.
+BUDGET_TTL = 5.0
+_BUDGET: dict = {}
+
+
+def _checkpoint_budget() -> int:
+    import time
+    dev = torch.cuda.current_device()
+    reserved = torch.cuda.memory_reserved()
+    hit = _BUDGET.get(dev)
+    now = time.monotonic()
+    if hit is not None and hit[1] == reserved and now - hit[2] < BUDGET_TTL:
+        return hit[0]
+    free, _total = torch.cuda.mem_get_info()
+    cached = reserved - torch.cuda.memory_allocated()
+    budget = (free + max(cached, 0)) // 4
+    _BUDGET[dev] = (budget, reserved, now)
+    return budget
+
+
 def choose_ckpt_every(policy, dim: int, n: int, cap: int, budget_bytes: Optional[int],
                       tuned: Optional[int] = None) -> int:
     """Checkpoint interval K (the segment length of the reverse pass).
@@ -85,10 +109,7 @@ def choose_ckpt_every(policy, dim: int, n: int, cap: int, budget_bytes: Optional
     if policy != "auto":
         raise ValueError(f"checkpoint policy must be 'auto', 'all', 'sqrt' or an int; got {policy!r}")
     if budget_bytes is None:
-        free, _total = torch.cuda.mem_get_info()
-        # memory the caching allocator holds but does not use is free for this purpose too
-        cached = torch.cuda.memory_reserved() - torch.cuda.memory_allocated()
-        budget_bytes = (free + max(cached, 0)) // 4
+        budget_bytes = _checkpoint_budget()
     K = tuned or 8
     while K < kmax and (cap // K + 2) * n * ckpt_width(dim) * 8 > budget_bytes:
         K *= 2

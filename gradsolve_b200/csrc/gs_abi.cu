@@ -1183,10 +1183,9 @@ int launch_tsit5_vjp_static(long long n, long long S, long long ld, const double
   gs::tsit5_replay_kernel<F><<<grid_for(n), kBlock, 0, s>>>(ra);
   if ((rc = cuda_check("tsit5_replay_kernel"))) return rc;
   gs::AdjointArgs aa{n, p, rec, n_steps, ckpt, K, ybar, gy0, gp, cap};
-  const SegCfg c = seg_cfg_doubles(gs::adjoint_smem_doubles<F::D>(K));
-  if ((rc = allow_smem(gs::tsit5_adjoint_kernel<F>, c.smem))) return rc;
-  gs::tsit5_adjoint_kernel<F><<<grid_for_block(n, c.block), c.block, c.smem, s>>>(aa);
-  return cuda_check("tsit5_adjoint_kernel");
+  // the reverse pass gs_tsit5_adjoint would run (stage-keeping or recomputing by residency,
+  // the unrolled K = 2 instance where it applies)
+  return launch_tsit5_adjoint<F>(aa, cap, s, false, GS_SCHED_STATIC, GS_ADJ_AUTO, GS_PREC_F64);
   }
 }
 
@@ -1215,12 +1214,16 @@ extern "C" int gs_tsit5_vjp_static(int field, long long n, const double* y0, con
                                 " bytes (use gs_tsit5_replay + gs_tsit5_adjoint with "
                                 "caller-allocated buffers for larger ensembles)");
   const int cap = S > 0 ? (int)S : 1;
-  int K = 1;
-  while ((long long)K * K < cap && K < gs::KMAX) ++K;  // ceil(sqrt(S)), at most KMAX
+  // the shortest segments that fit: K = 2 where it can (the interval the autotuner picks
+  // for the built-in fields), longer ones as the checkpoints outgrow the scratch
   const size_t b_steps = round256((size_t)n * sizeof(int));
   const size_t b_rec = round256(gs_record_bytes(n, cap));
-  const size_t b_ckpt = round256(gs_ckpt_bytes(field, n, cap, K));
-  const size_t need = b_steps + b_rec + b_ckpt;
+  int K = cap > 1 ? 2 : 1;
+  size_t need = b_steps + b_rec + round256(gs_ckpt_bytes(field, n, cap, K));
+  while (need > (size_t)GS_STATIC_SCRATCH_BYTES && K < gs::KMAX && K < cap) {
+    ++K;
+    need = b_steps + b_rec + round256(gs_ckpt_bytes(field, n, cap, K));
+  }
   if (need > (size_t)GS_STATIC_SCRATCH_BYTES)
     return fail(GS_ERR_ARG, "gs_tsit5_vjp_static: n=" + std::to_string(n) + ", S=" +
                                 std::to_string(S) + " needs " + std::to_string(need) +

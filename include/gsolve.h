@@ -335,9 +335,11 @@ int gs_move_rows(int scatter, int elem_bytes, const void* src, const long long* 
  * be NULL) for the cotangent ybar = dL/dy_final: the result of gs_record_from_padded +
  * gs_tsit5_replay + gs_tsit5_adjoint, computed with the dt record, checkpoints and step
  * counts in a static device array inside the library instead of caller buffers.
- * Limits: the record + checkpoints + counts must fit GS_STATIC_SCRATCH_BYTES (roughly
- * n * S <= 7.5e6 steps for the 3-state fields); larger problems return GS_ERR_ARG with the
- * numbers -- use the allocating entry points for them.
+ * Checkpoints every K steps, the shortest K >= 2 for which the record + checkpoints + counts
+ * fit GS_STATIC_SCRATCH_BYTES, and the reverse pass gs_tsit5_adjoint would choose for it.
+ * Limits: those must fit at K = 64 at least (roughly n * S <= 7.5e6 steps for the 3-state
+ * fields); larger problems return GS_ERR_ARG with the numbers -- use the allocating entry
+ * points for them.
  * The first call on each device looks up the array's device address (cudaGetSymbolAddress,
  * with that device current); make that first call before any stream capture.  The address
  * is kept until the process exits, so resetting the device (cudaDeviceReset) after that

@@ -92,21 +92,32 @@ def test_static_vjp_with_one_gradient_left_out(gslib, cuda, want):
         assert s_gy0 is None and _rel(s_gp, a_gp) <= 1e-9
 
 
-def test_static_vjp_long_record_takes_the_largest_interval(gslib, cuda):
-    """A record of more than 4096 steps: the entry point checkpoints every 64 steps (its
-    largest interval, ceil(sqrt(S)) capped), the shared-memory sizing of that segment length
-    included; twice in a row, the second call with another cotangent."""
+@pytest.mark.parametrize("n", [48, 1024])
+def test_static_vjp_long_record_intervals(gslib, cuda, n):
+    """Records of more than 4096 steps.  At n = 48 the checkpoints fit the scratch at the
+    shortest interval, K = 2 (the unrolled stage-keeping reverse pass); at n = 1024 they do
+    not, and the entry point lengthens the segments until they fit (checked here with the
+    library's own size functions), the shared-memory sizing of the longer segments included.
+    Twice in a row, the second call with another cotangent."""
     from gradsolve_b200 import engine
     from gradsolve_b200.fields import field_spec
     spec = field_spec("lorenz")
     rng = np.random.default_rng(7)
-    n = 48
     y0 = torch.tensor(np.array([1.0, 0.0, 0.0]) + rng.normal(0.0, 0.1, (n, 3)), device=cuda)
     p = torch.tensor(rng.uniform(20.0, 30.0, (n, 1)), device=cuda)
     r = engine.forward_record("tsit5", spec, y0, p, t0=0.0, t1=70.0, rtol=1e-8, atol=1e-8,
                               max_steps=100000)
     dts = r.padded_dts().contiguous()
-    assert dts.shape[1] >= 4096
+    S = dts.shape[1]
+    assert S >= 4096
+    L = gslib.lib()
+
+    def need(K):
+        return L.gs_record_bytes(n, S) + L.gs_ckpt_bytes(spec.code, n, S, K)
+    if n == 48:
+        assert need(2) < (64 << 20)
+    else:
+        assert need(2) > (64 << 20) and need(64) < (64 << 20)
     for scale in (1.0, -3.0):
         ybar = scale * torch.linspace(-1.0, 2.0, y0.numel(), dtype=torch.float64,
                                       device=cuda).reshape(y0.shape)

@@ -271,6 +271,11 @@ def build_replay_state(problem, y0, params, *, method: str, rtol: float, atol: f
     return state, y0_t, p_t
 
 
+def _lib_max_ckpt_every() -> int:
+    from . import _lib
+    return _lib.lib().gs_max_ckpt_every()
+
+
 def record(problem, y0, params, *, rtol: float = 1e-6, atol: float = 1e-9,
            max_steps: Optional[int] = None, device: str = "cuda", precision: str = "float64",
            engine: str = "auto"):
@@ -287,9 +292,11 @@ def record(problem, y0, params, *, rtol: float = 1e-6, atol: float = 1e-9,
         _check_float32_route(engine, spec)
     name = _resolve(problem, engine, [])
     ms = int(max_steps or DEFAULT_MAX_STEPS[name])
+    # (the checkpoints are not returned: the longest interval keeps them smallest)
     state, _y0, _p = build_replay_state(problem, y0, params, method=ENGINE_REGISTRY[name].method,
                                         rtol=rtol, atol=atol, device=device, max_steps=ms,
-                                        checkpoint="auto", precision=precision)
+                                        checkpoint=int(_lib_max_ckpt_every()),
+                                        precision=precision)
     r = state.record
     yf = r.y_final.cpu().numpy()
     if precision == "float32":

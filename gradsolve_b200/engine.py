@@ -686,6 +686,7 @@ def _grow(method, spec, y0, p, t1v, saveat_ts, r0, streams, kw):
     if n == 0 or r0.cap >= max_steps:
         return r0
     rows = torch.nonzero(r0.status == 3).squeeze(1)
+    _check_moves(y0.device)  # (after the synchronisation nonzero makes)
     if rows.numel() == 0:
         return r0
     sub = forward_record(method, spec, _take(y0, rows), _take(p, rows), t1v=_take(t1v, rows),

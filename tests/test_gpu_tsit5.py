@@ -410,3 +410,30 @@ def test_ordered_reverse_lanes_equal_batch_order(gslib, cuda, monkeypatch, metho
     b = engine._adjoint_one(r, p, ybar, in_batch_order=False, **kw)
     for x, y in zip(a, b):
         assert torch.equal(x, y)
+
+
+def test_row_mover_matches_torch_and_counts_bad_indices(gslib, cuda):
+    """gs_move_rows (the tier plan's gathers and scatters) against torch indexing, for 8- and
+    4-byte rows of several widths; indices outside the batch are skipped and counted."""
+    from gradsolve_b200 import engine
+    g = torch.Generator(device="cpu").manual_seed(5)
+    for dtype, width in ((torch.float64, 3), (torch.int32, 1), (torch.float32, 4),
+                         (torch.int64, 2)):
+        src = torch.randn(1000, width, generator=g).to(dtype).to(cuda)
+        idx = torch.randperm(1000, generator=g)[:700].to(cuda)
+        out = torch.empty((700, width), dtype=dtype, device=cuda)
+        engine._move_rows(src, idx, out, scatter=False)
+        assert torch.equal(out, src[idx])
+        dst = torch.zeros((1000, width), dtype=dtype, device=cuda)
+        engine._move_rows(out, idx, dst, scatter=True)
+        ref = torch.zeros_like(dst)
+        ref[idx] = src[idx]
+        assert torch.equal(dst, ref)
+    bad = torch.tensor([0, 5, 1000, -1, 7], device=cuda)
+    out = torch.full((5, 3), -9.0, dtype=torch.float64, device=cuda)
+    src = torch.arange(3000, dtype=torch.float64, device=cuda).reshape(1000, 3)
+    engine._move_rows(src, bad, out, scatter=False)
+    assert torch.equal(out[[0, 1, 4]], src[[0, 5, 7]])
+    assert torch.equal(out[[2, 3]], torch.full((2, 3), -9.0, dtype=torch.float64, device=cuda))
+    with pytest.raises(RuntimeError, match="skipped 2 out-of-range"):
+        engine._check_moves(torch.device(cuda))

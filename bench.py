@@ -382,6 +382,32 @@ def mixed_precision_config(args, dev) -> dict:
     return out
 
 
+def other_configs(args, dev) -> dict:
+    """The other workloads at their bench sizes, float64, in the default run's line (one
+    GPU): the stiff Robertson batch (Rosenbrock23, 2^18), the uneven VdP batch with dense
+    output (2^20), and the two 32-component fields integrated by groups of lanes (2^18
+    each) -- per group the step time, the FP64 fraction and the 32-row oracle parity sample
+    (the full lines: `bench.py --workload <name>`)."""
+    import copy
+
+    import torch
+    sub = copy.copy(args)
+    sub.steps, sub.warmup, sub.no_cpu, sub.no_mixed = 3, 2, True, True
+    sub.checkpoint, sub.schedule, sub.adjoint_variant = "auto", "auto", "auto"
+    out = {}
+    for name in ("robertson_2e18", "vdp_uneven_saveat", "lorenz96_32", "linear_32"):
+        line = measure_workload(sub, name, WORKLOAD_N[name], dev)
+        out[name] = {"value": line["value"], "unit": UNIT, "ms_per_step": line["ms_per_step"],
+                     "groups": [{k: g[k] for k in ("group", "method", "n", "ms",
+                                                   "frac_of_fp64_peak", "checkpoint_every",
+                                                   "record_len_max")}
+                                for g in line["groups"]],
+                     "oracle_parity_sample": line["oracle_parity_sample"],
+                     "gpu_launches": line["gpu_launches"]}
+        torch.cuda.empty_cache()
+    return out
+
+
 def float32_route_config(args, dev, n: int = 1 << 20) -> dict:
     """The float32 route on the reference's f32 nonstiff cell (tests/test_f32_replay.py:84-117:
     diffeqgpu_lorenz, y0 = [1, 0, 0] + 0.01 N(0, 1) seed 0, rho = 28, t in [0, 1], rtol 1e-6 /
@@ -639,6 +665,9 @@ def run_b200(args) -> None:
     f32_route = None
     if world == 1 and not args.no_config3:
         f32_route = float32_route_config(args, dev)
+    others = None
+    if world == 1 and not args.no_config3:
+        others = other_configs(args, dev)
 
     if rank != 0:
         if world > 1:
@@ -707,6 +736,7 @@ def run_b200(args) -> None:
         "gpu_launches": gpu_launches,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
         "parity_sample": checks, "config3_mixed": config3, "float32_route": f32_route,
+        "other_configs": others,
         "fwd_ms": fwd_avg, "adj_ms": adj_avg, "mixed": mixed, "solve": solve or None,
         "fwd_ms_steps": [round(x, 3) for x in fwd_ms], "adj_ms_steps": [round(x, 3) for x in adj_ms],
     }
@@ -1120,8 +1150,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-config3", action="store_true",
-                    help="skip the mixed-precision configuration (LV and Lorenz at 2^22) and "
-                         "the float32-route leg (the reference's f32 Lorenz cell at 2^20)")
+                    help="skip the mixed-precision configuration (LV and Lorenz at 2^22), "
+                         "the float32-route leg (the reference's f32 Lorenz cell at 2^20) and "
+                         "the other workloads' summaries")
     ap.add_argument("--no-checks", action="store_true",
                     help="skip the oracle/FD checks of 64 sampled trajectories (outside timing)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

@@ -265,6 +265,7 @@ def build_replay_state(problem, y0, params, *, method: str, rtol: float, atol: f
                               # the float32 route records without dense output: its closure
                               # replays the saved states at the recording point
                               saveat_ts=None if precision == "float32" else saveat)
+    engine.prepare_lane_order(r)  # queued behind the forward; the reverse pass will use it
     engine.raise_on_failed(r, ms, t1s)
     state = ReplayState(r, y0_t, pk, spec.nparam, precision=precision,
                         ts_rec=None if precision == "float32" else saveat)

@@ -188,6 +188,7 @@ class Record:
     status: torch.Tensor     # (n,) int32
     uneven: bool = False     # per-trajectory end times: the reverse pass refills lanes
     ys: Optional[torch.Tensor] = None  # (n, K, D) dense output of the forward, if asked for
+    lane_order: Optional[torch.Tensor] = None  # the reverse pass's lane order, if prepared
 
     @property
     def record_bytes(self) -> int:
@@ -847,6 +848,16 @@ def adjoint(r, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
     return _scatter(r, res, 0), _scatter(r, res, 1)
 
 
+def prepare_lane_order(r) -> Optional[torch.Tensor]:
+    """Queue the sort that orders a batch-order record's reverse lanes by step count (longest
+    first) on the current stream, so it runs while the host prepares the cotangent; the
+    reverse pass picks it up.  Planned records (already ordered by cost) need none."""
+    if isinstance(r, Record) and r.n >= ORDER_LANES_MIN:
+        r.lane_order = torch.argsort(r.n_acc, descending=True, stable=True)
+        return r.lane_order
+    return None
+
+
 # A record in batch order (a fresh forward; a planned tier is already ordered by cost) runs its
 # reverse pass with the lanes ordered by step count, longest first, from this many
 # trajectories up (the sort costs ~0.1 ms at 2^20 and saves the idle lanes of warps whose
@@ -867,7 +878,7 @@ def _adjoint_one(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: boo
     flags = (_PREC[precision] | _SCHED[schedule] | _lanes_flag(r.method, r.spec) |
              (_ADJ[variant] if r.method == METHOD_TSIT5 else 0))
     if in_batch_order and r.n >= ORDER_LANES_MIN and schedule in ("auto", "static"):
-        order = torch.argsort(r.n_acc, descending=True, stable=True)
+        order = r.lane_order if r.lane_order is not None else prepare_lane_order(r)
         _lib.check(L.gs_adjoint_ordered(_METHOD_CODE[r.method], r.spec.code, flags, r.n, _ptr(p),
                                         _ptr(r.rec), _ptr(r.n_acc), max(r.cap, 1), _ptr(r.ckpt),
                                         r.ckpt_every, _ptr(ybar), _ptr(gy0), _ptr(gp),

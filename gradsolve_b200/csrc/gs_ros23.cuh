@@ -13,27 +13,79 @@
 //   multipliers and the back substitutions multiply by the pivot's reciprocal, computed once
 //   per column, where the reference divides by the pivot in each (within an ulp of the
 //   division each time; it takes the dependent divisions off each attempt's critical path:
-//   D divisions per factorisation instead of D (D + 1) / 2 + D per solve).
+//   D divisions per factorisation instead of D (D + 1) / 2 + D per solve).  Float64 fields of
+//   up to 3 components (Robertson, VdP) hold W as its explicit inverse instead (kInverseW
+//   below): one division per attempt and matrix-vector products for the solves.
 // Replay: gradsolve/solvers/rosenbrock23_step.py:47-66 (no k3) with the analytic Jacobian.
 // Adjoint: reverse of that step, including the second-order term through W = I - d dt J(y,p):
 //   Wbar = -(W^-T k2bar) k2'^T - (W^-T k1bar) k1^T,  then  d<-d dt Wbar, J(y,p)>/d(y,p).
 // Record, checkpoint and segment scheme: as the Tsit5 kernels (gs_tsit5.cuh).
 #pragma once
+#include <type_traits>
+
 #include "gs_fields.cuh"
 #include "gs_tableau.cuh"
 #include "gs_tsit5.cuh"
 
 namespace gs {
 
+// For float64 fields of up to 3 components W is held as its explicit inverse (cofactors over
+// the determinant): the cofactors are independent products, so the factorisation has one
+// reciprocal on its dependent chain instead of one pivot search and reciprocal per column,
+// and each solve is a matrix-vector product instead of two substitution sweeps -- the
+// Rosenbrock23 kernels are latency-bound, and this shortens every attempt's critical path.
+// Against the partial-pivoting elimination the numbers agree to rounding (on the reference's
+// Robertson goldens: the same accepted and rejected counts, dts within 1e-8 relative).  Larger
+// fields and the float32 route keep the pivoted LU.
+template <int D, class R>
+constexpr bool kInverseW = D <= 3 && std::is_same<R, double>::value;
+
 template <int D, class R = double>
 struct LU {
-  R a[D * D];  // L (unit, below diagonal) and U (on/above), row-swapped
-  R inv[D];         // 1 / U's diagonal
-  int piv[D];
+  R a[D * D];  // L (unit, below diagonal) and U (on/above), row-swapped; or W^-1 (kInverseW)
+  R inv[D];         // 1 / U's diagonal (LU only)
+  int piv[D];       // (LU only)
 };
 
 template <int D, class R>
+__device__ __forceinline__ void inverse_factor(LU<D, R>& f) {
+  R* a = f.a;
+  if constexpr (D == 1) {
+    a[0] = R(1.0) / a[0];
+  } else if constexpr (D == 2) {
+    const R r = R(1.0) / (a[0] * a[3] - a[1] * a[2]);
+    const R a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3];
+    a[0] = a3 * r;
+    a[1] = -a1 * r;
+    a[2] = -a2 * r;
+    a[3] = a0 * r;
+  } else {
+    // cofactors c_ij of W; W^-1 = adj(W) / det = (c_ji) / det
+    const R c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8],
+            c02 = a[3] * a[7] - a[4] * a[6];
+    const R c10 = a[2] * a[7] - a[1] * a[8], c11 = a[0] * a[8] - a[2] * a[6],
+            c12 = a[1] * a[6] - a[0] * a[7];
+    const R c20 = a[1] * a[5] - a[2] * a[4], c21 = a[2] * a[3] - a[0] * a[5],
+            c22 = a[0] * a[4] - a[1] * a[3];
+    const R r = R(1.0) / (a[0] * c00 + a[1] * c01 + a[2] * c02);
+    a[0] = c00 * r;
+    a[1] = c10 * r;
+    a[2] = c20 * r;
+    a[3] = c01 * r;
+    a[4] = c11 * r;
+    a[5] = c21 * r;
+    a[6] = c02 * r;
+    a[7] = c12 * r;
+    a[8] = c22 * r;
+  }
+}
+
+template <int D, class R>
 __device__ __forceinline__ void lu_factor(LU<D, R>& f) {
+  if constexpr (kInverseW<D, R>) {
+    inverse_factor(f);
+    return;
+  }
 #pragma unroll
   for (int col = 0; col < D; ++col) {
     int pv = col;
@@ -79,6 +131,16 @@ __device__ __forceinline__ void lu_factor(LU<D, R>& f) {
 // the wrong order whenever a pivot is taken after the first column.)
 template <int D, class R>
 __device__ __forceinline__ void lu_solve(const LU<D, R>& f, const R* b, R* x) {
+  if constexpr (kInverseW<D, R>) {  // x = W^-1 b
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      R s = f.a[i * D] * b[0];
+#pragma unroll
+      for (int c = 1; c < D; ++c) s = s + f.a[i * D + c] * b[c];
+      x[i] = s;
+    }
+    return;
+  }
 #pragma unroll
   for (int i = 0; i < D; ++i) x[i] = b[i];
 #pragma unroll
@@ -112,6 +174,16 @@ __device__ __forceinline__ void lu_solve(const LU<D, R>& f, const R* b, R* x) {
 // x = W^-T b   (W = P^T L U  =>  W^T = U^T L^T P)
 template <int D, class R>
 __device__ __forceinline__ void lu_solve_t(const LU<D, R>& f, const R* b, R* x) {
+  if constexpr (kInverseW<D, R>) {  // x = W^-T b
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      R s = f.a[i] * b[0];
+#pragma unroll
+      for (int r = 1; r < D; ++r) s = s + f.a[r * D + i] * b[r];
+      x[i] = s;
+    }
+    return;
+  }
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     R s = b[i];

@@ -951,8 +951,8 @@ def adjoint_saveat(r, p: torch.Tensor, ts: torch.Tensor, ysbar: torch.Tensor,
     """(dL/dy0, dL/dp) for cotangents ysbar = dL/dys (n, K, D) and ybar = dL/dy_final.
     ``schedule="auto"`` refills lanes from a work counter for an uneven batch (per-trajectory
     end times), else runs one thread per trajectory."""
-    if schedule == "auto" and r.uneven:
-        schedule = "refill"
+    if schedule == "auto" and r.uneven and precision != "float32":
+        schedule = "refill"  # (the float32 route runs one thread per trajectory)
     res = _over_parts(r, lambda rr, rows: _adjoint_saveat_one(
         rr, _take(p, rows), _take_ts(ts, rows), _take(ysbar, rows), _take(ybar, rows),
         want_y0=want_y0, want_p=want_p, precision=precision, schedule=schedule))

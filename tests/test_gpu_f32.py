@@ -277,3 +277,36 @@ def test_saveat_matches_f64_oracle_on_the_same_mesh(gslib, oracle, cuda, method,
                        torch.tensor(params, device="cuda"), write_ckpt=False,
                        precision="float32")
     assert torch.equal(ys[:, -1].detach().double(), yf)
+
+
+def test_uneven_end_times_per_row_saveat_and_wrt_y0(gslib, oracle, cuda):
+    """The float32 route with per-trajectory end times, a row of saved times per trajectory
+    (ending at its own t1) and the gradient with respect to y0 and the parameters together:
+    against the float64 oracle's dense-output replay and reverse pass over the same float32
+    mesh, at the reference's f32 bars."""
+    import gradsolve_b200 as gsb
+    n = 256
+    y0, params = lorenz_batch(n)
+    rng = np.random.default_rng(3)
+    t1v = rng.uniform(0.5, 1.0, n)
+    ts = t1v[:, None] * np.linspace(0.0, 1.0, 9)[None, :]
+    clo = gsb.grad_closure(Lorenz(), y0, params, precision="float32", t1=t1v, saveat=ts,
+                           wrt=("y0", "params"), rtol=1e-6, atol=1e-9)
+    z = torch.tensor(y0, dtype=torch.float32, device="cuda", requires_grad=True)
+    p = torch.tensor(params, dtype=torch.float32, device="cuda", requires_grad=True)
+    ys = clo(z, p)
+    assert ys.dtype == torch.float32 and ys.shape == (n, 9, 3)
+    (ys.double() ** 2).sum().backward()
+    dts = clo.state.record.padded_dts().cpu().numpy().astype(np.float64)
+    _yf, ys64 = oracle.replay_saveat("tsit5", "lorenz", y0, params, dts, ts, nthreads=8)
+    gy64, gp64 = oracle.replay_saveat_vjp("tsit5", "lorenz", y0, params, dts, ts, 2.0 * ys64,
+                                          nthreads=8)
+    y32 = ys.detach().cpu().numpy().astype(np.float64)
+    ey = float(np.max(np.abs(y32 - ys64) / np.abs(ys64).max(axis=(1, 2), keepdims=True)))
+    g32 = np.concatenate([z.grad.cpu().numpy().ravel(), p.grad.cpu().numpy().ravel()])
+    g64 = np.concatenate([gy64.ravel(), gp64.ravel()])
+    rel, cos = rel_l2(g32.astype(np.float64), g64), cosine(g32.astype(np.float64), g64)
+    print(f"uneven f32 saveat: ys row error {ey:.2e}, grad rel-L2 {rel:.3e}, 1 - cos {1 - cos:.2e}")
+    assert ey <= 1e-4
+    assert rel <= GRAD_REL_L2_TOL
+    assert cos >= 1 - GRAD_COSINE_TOL

@@ -553,8 +553,9 @@ def run_b200(args) -> None:
     S = int(r.n_acc.max().item())
     K = r.ckpt_every
     # the timed run's own gradients, checked on 64 sampled trajectories (oracle + FD)
-    checks = None if args.no_checks else headline_checks(torch, engine, spec, r, gp, y0_np,
-                                                         rho_np, inv, dev)
+    # (rank 0 alone: only its line is printed, and the checks run no collective)
+    checks = None if (args.no_checks or rank != 0) else headline_checks(
+        torch, engine, spec, r, gp, y0_np, rho_np, inv, dev)
 
     # ---- the float32-stage variant on the same workload, and its accuracy ---------------
     mixed = None

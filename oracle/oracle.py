@@ -54,8 +54,16 @@ def set_linstiff(A) -> str:
 
 
 def build() -> Path:
-    """Compile the oracle (make in this directory); returns the library path."""
-    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    """Compile the oracle (make in this directory); returns the library path.  Concurrent
+    callers (one process per GPU, parallel test workers) take an exclusive lock first, so one
+    of them runs make and the others find the library up to date."""
+    import fcntl
+    with open(HERE / ".build.lock", "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        try:
+            subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+        finally:
+            fcntl.flock(lock, fcntl.LOCK_UN)
     return LIB_PATH
 
 

@@ -271,8 +271,10 @@ def build_replay_state(problem, y0, params, *, method: str, rtol: float, atol: f
                               # the float32 route records without dense output: its closure
                               # replays the saved states at the recording point
                               saveat_ts=None if precision == "float32" else saveat)
-    engine.prepare_lane_order(r)  # queued behind the forward; the reverse pass will use it
     engine.raise_on_failed(r, ms, t1s)
+    # queued after the checks' synchronisation, so the sort runs on the device while the host
+    # goes on to the closure call and the cotangent; the reverse pass picks it up
+    engine.prepare_lane_order(r)
     state = ReplayState(r, y0_t, pk, spec.nparam, precision=precision,
                         ts_rec=None if precision == "float32" else saveat)
     return state, y0_t, p_t

@@ -602,14 +602,18 @@ int launch_ros23_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, int 
 // ---- the float32 route (GS_PREC_F32, gs_f32.cuh) ----------------------------------------
 // One thread per trajectory, fields of at most 8 components; kMethod 0 = Tsit5, 1 =
 // Rosenbrock23.  AUTO is the static schedule here, per-trajectory end times included.
-int f32_schedule(int precision, const char* what) {
+// pairs_ok: the caller is the Tsit5 reverse pass, which takes GS_ADJ_RECOMPUTE (one trajectory
+// per thread) and GS_ADJ_PAIRS (two per thread, packed float32x2) besides AUTO.
+int f32_schedule(int precision, const char* what, bool pairs_ok = false) {
   const int s = precision & GS_SCHED_MASK;
   if (s != GS_SCHED_AUTO && s != GS_SCHED_STATIC)
     return fail(GS_ERR_ARG, std::string(what) + ": the float32 route runs one thread per "
                                                 "trajectory (GS_SCHED_STATIC or AUTO)");
-  if (precision & (GS_LANES_MASK | GS_ADJ_MASK))
-    return fail(GS_ERR_ARG, std::string(what) + ": lanes and reverse-pass variants are "
-                                                "float64 options");
+  const int v = precision & GS_ADJ_MASK;
+  if ((precision & GS_LANES_MASK) || v == GS_ADJ_STAGES ||
+      (v != GS_ADJ_AUTO && !pairs_ok))
+    return fail(GS_ERR_ARG, std::string(what) + ": lanes and this reverse-pass variant are "
+                                                "not float32-route options");
   return GS_OK;
 }
 
@@ -626,10 +630,12 @@ int launch_f32_record(const gs::RecordArgs& a, cudaStream_t s) {
     (void)a; (void)s;
     return f32_refuse_dim();
   } else {
-    if (!a.rec && !a.ckpt)
-      gs::f32_record_kernel<F, kMethod, false><<<grid_for(a.n), kBlock, 0, s>>>(a);
+    gs::RecordArgs b = a;
+    b.ctrlf = gs::make_ctrl_consts_f32(F::D, kMethod == 0 ? 10 : 6);  // err^(-1/q) = m^(-1/2q)
+    if (!b.rec && !b.ckpt)
+      gs::f32_record_kernel<F, kMethod, false><<<grid_for(b.n), kBlock, 0, s>>>(b);
     else
-      gs::f32_record_kernel<F, kMethod, true><<<grid_for(a.n), kBlock, 0, s>>>(a);
+      gs::f32_record_kernel<F, kMethod, true><<<grid_for(b.n), kBlock, 0, s>>>(b);
     return cuda_check("f32_record_kernel");
   }
 }
@@ -673,9 +679,25 @@ template <class F>
 int launch_f32_ros23_replay(const gs::ReplayArgs& a, cudaStream_t s) {
   return launch_f32_replay<F, 1>(a, s);
 }
+// variant AUTO: two trajectories per thread where the field is built for it (gs::Packable),
+// else one; GS_ADJ_RECOMPUTE: one; GS_ADJ_PAIRS: two, refused for other fields.
 template <class F>
-int launch_f32_tsit5_adjoint(const gs::AdjointArgs& a, cudaStream_t s) {
-  return launch_f32_adjoint<F, 0>(a, s);
+int launch_f32_tsit5_adjoint(const gs::AdjointArgs& a, cudaStream_t s, int variant) {
+  if constexpr (!kF32Built<F> || !gs::Packable<F>::value) {
+    if (variant == GS_ADJ_PAIRS)
+      return fail(GS_ERR_ARG, "gs_tsit5_adjoint: GS_ADJ_PAIRS is built for the built-in "
+                              "nonstiff fields only");
+    return launch_f32_adjoint<F, 0>(a, s);
+  } else {
+    if (variant == GS_ADJ_RECOMPUTE) return launch_f32_adjoint<F, 0>(a, s);
+    // K states of D float pairs (8 bytes each) per thread, counted in doubles
+    SegCfg c;
+    int rc = occupancy_cfg(gs::f32_adjoint_pairs_kernel<F>, a.ck_every * F::D, &c);
+    if (rc) return rc;
+    const long long threads = (a.n + 1) / 2;
+    gs::f32_adjoint_pairs_kernel<F><<<grid_for_block(threads, c.block), c.block, c.smem, s>>>(a);
+    return cuda_check("f32_adjoint_pairs_kernel");
+  }
 }
 template <class F>
 int launch_f32_ros23_adjoint(const gs::AdjointArgs& a, cudaStream_t s) {
@@ -934,8 +956,9 @@ static int tsit5_adjoint_impl(int field, int precision, long long n, const doubl
   if (n == 0) return GS_OK;
   gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp, cap, order};
   if (prec == GS_PREC_F32) {
-    if ((rc = f32_schedule(precision, "gs_tsit5_adjoint"))) return rc;
-    GS_TSIT5_DISPATCH(field, launch_f32_tsit5_adjoint, a, (cudaStream_t)stream)
+    if ((rc = f32_schedule(precision, "gs_tsit5_adjoint", true))) return rc;
+    GS_TSIT5_DISPATCH(field, launch_f32_tsit5_adjoint, a, (cudaStream_t)stream,
+                      precision & GS_ADJ_MASK)
   }
   GS_TSIT5_DISPATCH(field, launch_tsit5_adjoint, a, cap, (cudaStream_t)stream,
                     prec == GS_PREC_MIXED, adjoint_schedule(precision), precision & GS_ADJ_MASK,

@@ -152,6 +152,39 @@ __host__ inline CtrlConsts make_ctrl_consts(int D, int K) {
   return c;
 }
 
+// The same controller in float (the float32 route; the reference kernel's err = sqrtf(S / D),
+// accept iff err <= 1, dt = h * clip(0.9 * max(err, 1e-10)^(-1/q), 0.2, 5), all in float):
+//  * sqrtf is correctly rounded and sqrt(1 + 2^-23) = 1 + 2^-24 - 2^-49 rounds to 1 while
+//    sqrt(1 + 2^-22) rounds to 1 + 2^-23, so err <= 1 <=> fl(S / D) <= 1 + 2^-23 <=>
+//    S <= accept_sum, the largest float whose quotient by D still rounds to <= 1 + 2^-23;
+//  * 0.9 * err^(-1/q) = scale * S^(-1/K), K = 2q, scale = 0.9 D^(1/K), from the hardware's
+//    approximate lg2 / ex2 directly (a few float ulp; no refinement is needed at float
+//    precision); S = 0 or below the 1e-10 floor gives a factor at or above 5 and S = +inf
+//    gives 0, which the clip turns into 5 and 0.2 as the reference's max/clip does.
+struct CtrlConstsF {
+  float accept_sum, scale, inv_k;
+};
+
+__host__ inline CtrlConstsF make_ctrl_consts_f32(int D, int K) {
+  const float A = 1.0f + 1.1920928955078125e-7f;  // 1 + 2^-23
+  const float dd = (float)D;
+  float x = A * dd;
+  while (x / dd > A) x = std::nextafterf(x, 0.0f);
+  while (std::nextafterf(x, 1e30f) / dd <= A) x = std::nextafterf(x, 1e30f);
+  CtrlConstsF c;
+  c.accept_sum = x;
+  c.scale = (float)(Ctrl::SAFETY * std::pow((double)D, 1.0 / K));
+  c.inv_k = -1.0f / (float)K;
+  return c;
+}
+
+__device__ __forceinline__ float step_from_sum_f32(float S, float h, const CtrlConstsF& c) {
+  float fac = c.scale * ex2_approx(lg2_approx(S) * c.inv_k);
+  fac = fac > (float)Ctrl::FAC_MIN ? fac : (float)Ctrl::FAC_MIN;
+  fac = (float)Ctrl::FAC_MAX < fac ? (float)Ctrl::FAC_MAX : fac;
+  return h * fac;
+}
+
 // K = 10 for Tsit5 (q = 5), K = 6 for Rosenbrock23 (q = 3).  Returns the new dt from the sum
 // of squares S.
 template <int K>
@@ -440,6 +473,7 @@ struct RecordArgs {
   long long ts_ld = 0;
   int K = 0;
   double* ys = nullptr;
+  CtrlConstsF ctrlf{};  // the float32 route's controller constants (set by its launcher)
 };
 
 struct AdjointArgs {

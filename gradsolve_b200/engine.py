@@ -124,6 +124,10 @@ def choose_ckpt_every(policy, dim: int, n: int, cap: int, budget_bytes: Optional
 # process on a sample of the caller's own trajectories and cached.
 _TUNED: dict = {}
 TUNE_CANDIDATES = (2, 3, 4, 6, 8, 12, 16)
+# On the float32 route a checkpoint row is 16 bytes for D <= 3 (against 32 in float64), and
+# storing every state (K = 1) can win: the Lorenz f32 cell at 2^20 measured 1.37 ms per
+# gradient step at K = 1 against 1.43 at K = 2 and 1.45 at K = 4.
+TUNE_CANDIDATES_F32 = (1,) + TUNE_CANDIDATES
 
 
 def tuned_ckpt_every(method: str, spec: FieldSpec, precision: str) -> Optional[int]:
@@ -134,7 +138,7 @@ def autotune_ckpt_every(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch
                         t0: float, t1: float, rtol: float, atol: float,
                         t1v: Optional[torch.Tensor] = None, max_steps: int = 100000,
                         precision: str = "float64", sample: int = 1 << 21,
-                        candidates=TUNE_CANDIDATES, reps: int = 3) -> int:
+                        candidates=None, reps: int = 3) -> int:
     """Time forward + reverse pass for each candidate K on up to ``sample`` trajectories and
     cache the fastest (best of ``reps`` timings).  The sample spans many waves of the GPU:
     the candidates' reverse passes hold different numbers of blocks per SM (their shared
@@ -144,8 +148,14 @@ def autotune_ckpt_every(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch
     m = min(y0.shape[0], sample)
     ys, ps = y0[:m].contiguous(), p[:m].contiguous()
     tv = None if t1v is None else t1v[:m].contiguous()
+    if candidates is None:
+        candidates = TUNE_CANDIDATES_F32 if precision == "float32" else TUNE_CANDIDATES
+    budget = _checkpoint_budget()
+    row = 4 * ckpt_width_f32(spec.dim) if precision == "float32" else 8 * ckpt_width(spec.dim)
     best, best_ms = None, float("inf")
     for K in candidates:
+        if (DEFAULT_CAP0 // K + 2) * m * row > budget and K != candidates[-1]:
+            continue  # this interval's checkpoints would not fit beside the caller's data
         kw = dict(t0=t0, t1=t1, t1v=tv, rtol=rtol, atol=atol, max_steps=max_steps,
                   checkpoint=K, precision=precision)
         r = forward_record(method, spec, ys, ps, **kw)
@@ -189,6 +199,7 @@ class Record:
     uneven: bool = False     # per-trajectory end times: the reverse pass refills lanes
     ys: Optional[torch.Tensor] = None  # (n, K, D) dense output of the forward, if asked for
     lane_order: Optional[torch.Tensor] = None  # the reverse pass's lane order, if prepared
+    status_max: Optional[int] = None  # largest status code, once a check has read it
 
     @property
     def record_bytes(self) -> int:
@@ -258,6 +269,7 @@ class RecordSet:
     uneven: bool = False
     ys: Optional[torch.Tensor] = None
     streams: Optional[list] = None  # per part: None (the caller's stream) or a side stream
+    status_max: Optional[int] = None  # largest status code, once a check has read it
 
     @property
     def cap(self) -> int:
@@ -350,7 +362,7 @@ def _parts(r):
 # gs_move_rows: one thread per element, the contiguous side streamed.  (torch's index_select
 # took 2.2 ms for the 4M parameter rows of a 2^22 Lotka-Volterra batch; this kernel is
 # HBM-bound.)  Out-of-range indices are skipped and counted in a per-device counter, which
-# the forward checks after its own synchronisation (_check_moves).
+# the forward reads with its status codes in its one synchronisation (_status_max).
 _ELEM_BYTES = {torch.float64: 8, torch.int64: 8, torch.float32: 4, torch.int32: 4}
 _BAD_MOVES: dict = {}
 
@@ -362,13 +374,30 @@ def _bad_counter(device) -> torch.Tensor:
     return _BAD_MOVES[key]
 
 
+def _raise_bad_moves(c: torch.Tensor, n: int) -> None:
+    c.zero_()
+    raise RuntimeError(f"gs_move_rows skipped {n} out-of-range row indices (a tier plan "
+                       "referenced rows outside its batch)")
+
+
 def _check_moves(device) -> None:
     c = _BAD_MOVES.get(device.index)
-    if c is not None and int(c.item()) != 0:
+    if c is not None:
         n = int(c.item())
-        c.zero_()
-        raise RuntimeError(f"gs_move_rows skipped {n} out-of-range row indices (a tier plan "
-                           "referenced rows outside its batch)")
+        if n != 0:
+            _raise_bad_moves(c, n)
+
+
+def _status_max(status: torch.Tensor, device) -> int:
+    """The largest status code of a forward's trajectories (0 ok, 1 not finished, 2 step-size
+    underflow, 3 record full), read together with the row-move counter in one device-to-host
+    copy: the forward's one synchronisation when nothing went wrong."""
+    c = _BAD_MOVES.get(device.index)
+    smax = status.max().to(torch.int64).reshape(1)
+    vals = (torch.cat([smax, c]) if c is not None else smax).tolist()
+    if c is not None and vals[1] != 0:
+        _raise_bad_moves(c, int(vals[1]))
+    return int(vals[0])
 
 
 def _movable(t: torch.Tensor) -> bool:
@@ -686,10 +715,10 @@ def _grow(method, spec, y0, p, t1v, saveat_ts, r0, streams, kw):
     max_steps = int(kw["max_steps"])
     if n == 0 or r0.cap >= max_steps:
         return r0
-    rows = torch.nonzero(r0.status == 3).squeeze(1)
-    _check_moves(y0.device)  # (after the synchronisation nonzero makes)
-    if rows.numel() == 0:
+    r0.status_max = _status_max(r0.status, y0.device)
+    if r0.status_max < 3:  # no row overflowed the record
         return r0
+    rows = torch.nonzero(r0.status == 3).squeeze(1)
     sub = forward_record(method, spec, _take(y0, rows), _take(p, rows), t1v=_take(t1v, rows),
                          cap0=min(TIER_GROWTH * r0.cap, max_steps),
                          saveat_ts=_take_ts(saveat_ts, rows), **kw)
@@ -745,10 +774,10 @@ def _forward_planned(method, spec, y0, p, t1v, saveat_ts, ws: RecordSet, kw):
                     t.record_stream(main)
     res = _assemble(method, spec, n, y0.device, out, t1v, saveat_ts, streams)
     # trajectories that outgrew their planned tier: solved again with more capacity
-    over = torch.nonzero(res.status == 3).squeeze(1)
-    _check_moves(y0.device)  # (after the synchronisation nonzero makes)
-    if over.numel() == 0:
+    res.status_max = _status_max(res.status, y0.device)
+    if res.status_max < 3:
         return res
+    over = torch.nonzero(res.status == 3).squeeze(1)
     cap_of_row = torch.zeros(n, dtype=torch.int64, device=y0.device)
     for rows, rr in out:
         cap_of_row.index_fill_(0, rows, rr.cap)
@@ -771,7 +800,7 @@ def _forward_planned(method, spec, y0, p, t1v, saveat_ts, ws: RecordSet, kw):
 def raise_on_failed(r: Record, max_steps: int, t1) -> None:
     """Refuse an incomplete mesh, with the reference's messages
     (gradsolve/warp/warp_replay.py:167-173, gradsolve/solvers/record_jax.py:201-211)."""
-    if r.n == 0:
+    if r.n == 0 or r.status_max == 0:  # (the forward's own check read every status)
         return
     bad = torch.nonzero(r.status != 0).flatten()
     if bad.numel() == 0:
@@ -827,7 +856,7 @@ def _replay_one(r: Record, y0: torch.Tensor, p: torch.Tensor, *, write_ckpt: boo
     return yf
 
 
-_ADJ = {"auto": 0x000, "recompute": 0x400, "stages": 0x800}
+_ADJ = {"auto": 0x000, "recompute": 0x400, "stages": 0x800, "pairs": 0xC00}
 
 
 def adjoint(r, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
@@ -839,7 +868,9 @@ def adjoint(r, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: bool = True,
     ``variant`` (Tsit5, float64, one thread per trajectory): "stages" keeps the stage inputs
     the segment's replay evaluates, "recompute" re-evaluates every step's stages in the
     reverse sweep; "auto" is "stages" while its buffer leaves it at least 3/5 of the
-    recomputing kernel's resident threads, else "recompute"."""
+    recomputing kernel's resident threads, else "recompute".  On the float32 route (Tsit5)
+    "pairs" runs two trajectories per thread in packed float32x2 arithmetic (built-in
+    nonstiff fields), "recompute" one per thread, and "auto" is "pairs" where it is built."""
     if schedule == "auto" and r.uneven and precision != "float32":
         schedule = "refill"  # (the float32 route runs one thread per trajectory)
     res = _over_parts(r, lambda rr, rows: _adjoint_one(

@@ -91,6 +91,13 @@ extern "C" {
 #define GS_ADJ_AUTO 0x000
 #define GS_ADJ_RECOMPUTE 0x400
 #define GS_ADJ_STAGES 0x800
+/* The float32 route's Tsit5 reverse pass (GS_PREC_F32): PAIRS runs two trajectories per thread
+ * (lanes 2u and 2u + 1, in packed float32x2 arithmetic: one instruction for both), built for
+ * the built-in nonstiff fields and refused for others; RECOMPUTE runs one per thread; AUTO is
+ * PAIRS where it is built, else RECOMPUTE.  The two agree to float rounding (the packed
+ * expressions fuse their own choice of products).  STAGES is a float64 / float32-stage
+ * option. */
+#define GS_ADJ_PAIRS 0xC00
 #define GS_ADJ_MASK 0xC00
 
 /* Lanes per trajectory for the fields of more than 8 components (a group of G lanes

@@ -114,13 +114,16 @@ def test_argument_errors_are_status_codes(gslib):
     # precision not built
     rc = L.gs_tsit5_adjoint(1, 7, 4, a, a, ia, 8, a, 2, a, a, a, None)
     assert rc == -4
-    # the float32 route: one thread per trajectory only, no lanes or reverse-pass variants,
-    # Rosenbrock23 included; fields above 8 components refused
+    # the float32 route: one thread per trajectory only, no lanes, and of the reverse-pass
+    # variants only the Tsit5 ones (pairs, one per thread), Rosenbrock23 included; fields
+    # above 8 components refused
     rc = L.gs_tsit5_fwd_record(1, 2 | 0x200, 4, a, a, 0.0, None, 1.0, 1e-6, 1e-9, -1.0, 10, 8,
                                2, a, a, a, ia, ia, ia, None)
     assert rc == -1 and b"one thread per trajectory" in L.gs_last_error()
     rc = L.gs_tsit5_adjoint(1, 2 | 0x800, 4, a, a, ia, 8, a, 2, a, a, a, None)
-    assert rc == -1 and b"float64 options" in L.gs_last_error()
+    assert rc == -1 and b"not float32-route options" in L.gs_last_error()
+    rc = L.gs_ros23_adjoint(10, 2 | 0xC00, 4, a, a, ia, 8, a, 2, a, a, a, None)
+    assert rc == -1 and b"not float32-route options" in L.gs_last_error()
     rc = L.gs_ros23_adjoint(10, 2 | 0x300, 4, a, a, ia, 8, a, 2, a, a, a, None)
     assert rc == -1
     rc = L.gs_tsit5_replay(5032, 2 | 0x1000, 4, a, a, 0.0, a, ia, 8, 2, a, a, None)

@@ -225,8 +225,16 @@ def test_float32_refusals(gslib, cuda):
                               precision="float32", schedule="refill")
     r = engine.forward_record("tsit5", spec, y0t, pt, t0=0.0, t1=1.0, rtol=1e-6, atol=1e-9,
                               precision="float32", checkpoint=4)
-    with pytest.raises(_lib.GsolveError, match="float64 options"):
+    with pytest.raises(_lib.GsolveError, match="not float32-route options"):
         engine.adjoint(r, pt, y0t, precision="float32", variant="stages")
+    spec8 = field_spec("lorenz96_8")
+    y8 = torch.full((64, 8), 8.0, dtype=torch.float64, device="cuda")
+    y8[:, 0] += 0.01
+    p8 = torch.full((64, 1), 8.0, dtype=torch.float64, device="cuda")
+    r8 = engine.forward_record("tsit5", spec8, y8, p8, t0=0.0, t1=0.5, rtol=1e-6, atol=1e-9,
+                               precision="float32", checkpoint=4)
+    with pytest.raises(_lib.GsolveError, match="GS_ADJ_PAIRS is built for"):
+        engine.adjoint(r8, p8, y8, precision="float32", variant="pairs")
 
     class L96:
         name = "lorenz96_32"
@@ -310,3 +318,34 @@ def test_uneven_end_times_per_row_saveat_and_wrt_y0(gslib, oracle, cuda):
     assert ey <= 1e-4
     assert rel <= GRAD_REL_L2_TOL
     assert cos >= 1 - GRAD_COSINE_TOL
+
+
+@pytest.mark.parametrize("n,K,uneven", [(1, 2, False), (5, 3, True), (2048, 2, False),
+                                        (4099, 1, True), (4099, 2, True), (4099, 8, False)])
+def test_pairs_agree_with_one_trajectory_per_thread(gslib, cuda, n, K, uneven):
+    """The float32 reverse pass two trajectories per thread (packed float32x2, the default for
+    the built-in nonstiff fields) against one per thread on the same record: bit for bit
+    equal (both evaluate each step with the same explicit contractions), for odd batches (a
+    half without a trajectory), lanes ordered by step count (from 4096 trajectories),
+    neighbours with different step counts (per-trajectory end times) and several checkpoint
+    intervals."""
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    spec = field_spec("lorenz")
+    rng = np.random.default_rng(n + K)
+    y0 = torch.tensor(np.tile([1.0, 0.0, 0.0], (n, 1)) + 0.1 * rng.standard_normal((n, 3)),
+                      device="cuda")
+    p = torch.tensor(rng.uniform(20.0, 30.0, (n, 1)), device="cuda")
+    t1v = torch.tensor(rng.uniform(0.2, 1.0, n), device="cuda") if uneven else None
+    r = engine.forward_record("tsit5", spec, y0, p, t0=0.0, t1=1.0, t1v=t1v, rtol=1e-6,
+                              atol=1e-9, precision="float32", checkpoint=K)
+    ybar = 2.0 * r.y_final
+    out = {}
+    for variant in ("pairs", "recompute"):
+        out[variant] = engine.adjoint(r, p, ybar, precision="float32", variant=variant)
+    auto = engine.adjoint(r, p, ybar, precision="float32")
+    for a, b, c in zip(out["pairs"], out["recompute"], auto):
+        a, b, c = a.cpu().numpy(), b.cpu().numpy(), c.cpu().numpy()
+        assert np.array_equal(a, c)  # auto is pairs for this field
+        assert np.all(np.isfinite(a))
+        assert np.array_equal(a, b), f"pairs vs one per thread: rel-L2 {rel_l2(a, b):.3e}"

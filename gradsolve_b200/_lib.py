@@ -39,6 +39,7 @@ _SIGS = {
     "gs_ckpt_bytes_prec": (c_size_t, [c_int, c_int, c_ll, c_int, c_int]),
     "gs_max_ckpt_every": (c_int, []),
     "gs_lane_choices": (c_int, [c_int, ctypes.POINTER(c_int), c_int]),
+    "gs_occ_choices": (c_int, [c_int, c_int, ctypes.POINTER(c_int), c_int]),
     "gs_tsit5_fwd_record": (c_int, [c_int, c_int, c_ll, c_void_p, c_void_p, c_double, c_void_p,
                                     c_double, c_double, c_double, c_double, c_int, c_int, c_int,
                                     c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,

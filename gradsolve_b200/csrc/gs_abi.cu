@@ -346,6 +346,73 @@ int lane_choices(int* out, int cap) {
   return k;
 }
 
+// Occupancy instances (GS_OCC) for fields of up to 4 components.  The float64 recording
+// forward, whose default instance is bounded for 6 blocks per SM, also has instances bounded
+// for 4 and 5 (more registers: longer-range scheduling, no spills where the default spills),
+// 7 and 8 (fewer registers, more resident warps); the float64 reverse pass's K = 2
+// stage-keeping instance (default 5 blocks) has 3, 4 and 6.  Larger fields keep the compiler's
+// allocation alone.
+template <class F>
+int occ_choices(int pass, int* out, int cap) {
+  int k = 0;
+  if (cap > k) out[k] = 0;
+  ++k;
+  if constexpr (F::D <= 4) {
+    const std::initializer_list<int> fwd = {4, 5, 7, 8}, rev = {3, 4, 6};
+    for (int b : (pass == GS_OCC_REVERSE ? rev : fwd)) {
+      if (cap > k) out[k] = b;
+      ++k;
+    }
+  }
+  return k;
+}
+
+template <class F>
+int launch_adjoint_k2_occ(const gs::AdjointArgs& a, cudaStream_t s, int occ) {
+  if constexpr (F::D <= 4) {
+    const int sd = gs::adjoint_stages_smem_doubles<F::D>(2);
+    auto go = [&](auto kern) -> int {
+      SegCfg c{0, 0, 0};
+      int rc;
+      if ((rc = occupancy_probe(kern, sd, &c))) return rc;
+      if (c.resident <= 0)
+        return fail(GS_ERR_ARG, "GS_OCC: the K = 2 segment buffer does not fit shared memory");
+      if ((rc = allow_smem(kern, c.smem))) return rc;
+      kern<<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+      return cuda_check("tsit5_adjoint_stages_kernel");
+    };
+    switch (occ) {
+      case 3: return go(gs::tsit5_adjoint_stages_k2_kernel<F, 3>);
+      case 4: return go(gs::tsit5_adjoint_stages_k2_kernel<F, 4>);
+      case 6: return go(gs::tsit5_adjoint_stages_k2_kernel<F, 6>);
+      default: break;
+    }
+  }
+  return fail(GS_ERR_ARG, "GS_OCC: no reverse-pass instance bounded for " + std::to_string(occ) +
+                              " blocks per SM is built for D = " + std::to_string(F::D) +
+                              " (gs_occ_choices)");
+}
+
+template <class F>
+int launch_record_occ(const gs::RecordArgs& a, cudaStream_t s, int occ) {
+  if constexpr (F::D <= 4) {
+    switch (occ) {
+      case 4: gs::tsit5_record_kernel<F, true, 4><<<grid_for(a.n), kBlock, 0, s>>>(a);
+        return cuda_check("tsit5_record_kernel");
+      case 5: gs::tsit5_record_kernel<F, true, 5><<<grid_for(a.n), kBlock, 0, s>>>(a);
+        return cuda_check("tsit5_record_kernel");
+      case 7: gs::tsit5_record_kernel<F, true, 7><<<grid_for(a.n), kBlock, 0, s>>>(a);
+        return cuda_check("tsit5_record_kernel");
+      case 8: gs::tsit5_record_kernel<F, true, 8><<<grid_for(a.n), kBlock, 0, s>>>(a);
+        return cuda_check("tsit5_record_kernel");
+      default: break;
+    }
+  }
+  return fail(GS_ERR_ARG, "GS_OCC: no recording-forward instance bounded for " +
+                              std::to_string(occ) + " blocks per SM is built for D = " +
+                              std::to_string(F::D) + " (gs_occ_choices)");
+}
+
 // Launch `go` with the group size the precision flags ask for (GS_LANES; 0: the default):
 // go is called with an integral_constant of the size, so each kernel is instantiated only for
 // the built sizes.
@@ -414,17 +481,25 @@ int launch_tsit5_record(const gs::RecordArgs& a_in, cudaStream_t s, bool mixed, 
                         int precision) {
   if constexpr (kCoop<F>) {
     (void)sched;
+    if (precision & GS_OCC_MASK)
+      return fail(GS_ERR_ARG, "GS_OCC: fields of more than 8 components have no occupancy "
+                              "instances (gs_occ_choices)");
     return launch_coop_record<F>(a_in, s, mixed, precision);
   } else {
   if (precision & GS_LANES_MASK)
     return fail(GS_ERR_ARG, "lanes per trajectory apply to fields of more than 8 components only");
   gs::RecordArgs a = a_in;
   a.ctrl = gs::make_ctrl_consts(F::D, 10);  // Tsit5: err^(-1/5) = m^(-1/10)
+  const int occ = (precision & GS_OCC_MASK) >> GS_OCC_SHIFT;
+  if (occ && (mixed || sched != GS_SCHED_STATIC || (!a.rec && !a.ckpt)))
+    return fail(GS_ERR_ARG, "GS_OCC applies to the float64 recording forward, one thread per "
+                            "trajectory");
   if (sched == GS_SCHED_STATIC) {
     if (mixed) {
       gs::tsit5_mixed_record_kernel<F><<<grid_for(a.n), kBlock, 0, s>>>(a);
       return cuda_check("tsit5_mixed_record_kernel");
     }
+    if (occ) return launch_record_occ<F>(a, s, occ);
     if (!a.rec && !a.ckpt)
       gs::tsit5_record_kernel<F, false><<<grid_for(a.n), kBlock, 0, s>>>(a);
     else
@@ -454,12 +529,18 @@ int launch_tsit5_replay(const gs::ReplayArgs& a, cudaStream_t s, bool mixed, int
 template <class F>
 int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool mixed,
                          int sched, int variant, int precision) {
+  const int occ = (precision & GS_OCC_MASK) >> GS_OCC_SHIFT;
+  if (occ && (kCoop<F> || mixed || sched != GS_SCHED_STATIC || variant == GS_ADJ_RECOMPUTE ||
+              a.ck_every != 2))
+    return fail(GS_ERR_ARG, "GS_OCC applies to the float64 reverse pass's K = 2 stage-keeping "
+                            "instance, one thread per trajectory");
   if constexpr (kCoop<F>) {
     (void)cap; (void)sched; (void)variant;
     return launch_coop_adjoint<F>(a, s, mixed, precision);
   } else {
   if (precision & GS_LANES_MASK)
     return fail(GS_ERR_ARG, "lanes per trajectory apply to fields of more than 8 components only");
+  if (occ) return launch_adjoint_k2_occ<F>(a, s, occ);
   if (sched == GS_SCHED_STATIC) {
     int rc;
     if (!mixed) {
@@ -910,6 +991,8 @@ int gs_tsit5_fwd_record(int field, int precision, long long n, const double* y0,
   gs::RecordArgs a{n, y0, p, t0, t1, rtol, atol, dt0, t1v, max_steps, cap, ckpt_every,
                    gs_ckpt_slots(cap, ckpt_every), rec, ckpt, y_final, n_acc, n_rej, status};
   if (prec == GS_PREC_F32) {
+    if (precision & GS_OCC_MASK)
+      return fail(GS_ERR_ARG, "GS_OCC applies to the float64 recording forward only");
     if ((rc = f32_schedule(precision, "gs_tsit5_fwd_record"))) return rc;
     GS_TSIT5_DISPATCH(field, launch_f32_tsit5_record, a, (cudaStream_t)stream)
   }
@@ -956,6 +1039,8 @@ static int tsit5_adjoint_impl(int field, int precision, long long n, const doubl
   if (n == 0) return GS_OK;
   gs::AdjointArgs a{n, p, rec, n_acc, ckpt, ckpt_every, ybar, gy0, gp, cap, order};
   if (prec == GS_PREC_F32) {
+    if (precision & GS_OCC_MASK)
+      return fail(GS_ERR_ARG, "GS_OCC applies to the float64 reverse pass only");
     if ((rc = f32_schedule(precision, "gs_tsit5_adjoint", true))) return rc;
     GS_TSIT5_DISPATCH(field, launch_f32_tsit5_adjoint, a, (cudaStream_t)stream,
                       precision & GS_ADJ_MASK)
@@ -979,6 +1064,15 @@ int gs_lane_choices(int field, int* out, int cap) {
   GS_TSIT5_DISPATCH(field, lane_choices, out, cap)
 }
 
+int gs_occ_choices(int field, int pass, int* out, int cap) {
+  int D, P, rc;
+  if ((rc = field_dims(field, &D, &P))) return rc;
+  if (!out && cap > 0) return fail(GS_ERR_ARG, "gs_occ_choices: null output");
+  if (pass != GS_OCC_FORWARD && pass != GS_OCC_REVERSE)
+    return fail(GS_ERR_ARG, "gs_occ_choices: pass is GS_OCC_FORWARD or GS_OCC_REVERSE");
+  GS_TSIT5_DISPATCH(field, occ_choices, pass, out, cap)
+}
+
 int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,
                         const double* p, double t0, const double* t1v, double t1, double rtol,
                         double atol, double dt0, int max_steps, int cap, int ckpt_every,
@@ -987,6 +1081,8 @@ int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,
   const int prec = precision & GS_PREC_MASK;
   if (prec != GS_PREC_F64 && prec != GS_PREC_F32)
     return fail(GS_ERR_PRECISION, "gs_ros23_fwd_record: Rosenbrock23 runs in float64 or float32");
+  if (precision & GS_OCC_MASK)
+    return fail(GS_ERR_ARG, "GS_OCC applies to the Tsit5 entry points only");
   int rc = check_record_args("gs_ros23_fwd_record", n, y0, p, rtol, atol, max_steps, cap,
                              ckpt_every, rec, ckpt, y_final, n_acc, n_rej, status);
   if (rc) return rc;
@@ -1033,6 +1129,8 @@ static int ros23_adjoint_impl(int field, int precision, long long n, const doubl
   const int prec = precision & GS_PREC_MASK;
   if (prec != GS_PREC_F64 && prec != GS_PREC_F32)
     return fail(GS_ERR_PRECISION, "gs_ros23_adjoint: Rosenbrock23 runs in float64 or float32");
+  if (precision & GS_OCC_MASK)
+    return fail(GS_ERR_ARG, "GS_OCC applies to the Tsit5 entry points only");
   int rc = check_adjoint_args("gs_ros23_adjoint", n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar);
   if (rc) return rc;
   int D, P;

@@ -635,9 +635,11 @@ __device__ __forceinline__ bool tsit5_attempt(const RecordArgs& a, long long j,
 // bytes it spills at 80 cost less than the lost warps (11.63 vs 11.73 ms on the Lorenz 2^20
 // bench forward; 7 blocks at 72 registers: 11.35 ms).  Larger states keep their registers.
 // kStore = false: the forward-only solve (no record, no checkpoints), with the store paths
-// compiled out.
-template <class F, bool kStore = true>
-__global__ void __launch_bounds__(128, (F::D <= 4 ? 6 : 1)) tsit5_record_kernel(const RecordArgs a) {
+// compiled out.  kMinB > 0 bounds the registers for kMinB resident blocks per SM instead
+// (the instances the occupancy autotuner chooses among; same arithmetic, bit for bit).
+template <class F, bool kStore = true, int kMinB = 0>
+__global__ void __launch_bounds__(128, (kMinB > 0 ? kMinB : (F::D <= 4 ? 6 : 1)))
+    tsit5_record_kernel(const RecordArgs a) {
   constexpr int D = F::D, P = F::P;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.n) return;
@@ -1023,9 +1025,11 @@ __global__ void __launch_bounds__(128) tsit5_adjoint_stages_kernel(const Adjoint
 }
 
 // K = 2, bounded to 5 blocks of 128 per SM: unrolled without the bound, the segment's two
-// steps interleave into 128 registers (4 blocks)
-template <class F>
-__global__ void __launch_bounds__(128, 5) tsit5_adjoint_stages_k2_kernel(const AdjointArgs a) {
+// steps interleave into 128 registers (4 blocks).  kMinB > 0 bounds it for kMinB blocks
+// instead (the instances the occupancy autotuner chooses among; same arithmetic, bit for bit).
+template <class F, int kMinB = 0>
+__global__ void __launch_bounds__(128, (kMinB > 0 ? kMinB : 5))
+    tsit5_adjoint_stages_k2_kernel(const AdjointArgs a) {
   tsit5_adjoint_stages_body<F, 2>(a);
 }
 

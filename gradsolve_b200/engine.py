@@ -124,6 +124,19 @@ def choose_ckpt_every(policy, dim: int, n: int, cap: int, budget_bytes: Optional
 # process on a sample of the caller's own trajectories and cached.
 _TUNED: dict = {}
 TUNE_CANDIDATES = (2, 3, 4, 6, 8, 12, 16)
+_IN_TUNER = [0]  # nonzero while an autotuner runs its own forwards (no nested tuning)
+
+
+def _tuner(fn):
+    """Mark the autotuner's own forwards, so they start no other autotuner."""
+    def run(*args, **kwargs):
+        _IN_TUNER[0] += 1
+        try:
+            return fn(*args, **kwargs)
+        finally:
+            _IN_TUNER[0] -= 1
+    run.__name__, run.__doc__, run.__wrapped__ = fn.__name__, fn.__doc__, fn
+    return run
 # On the float32 route a checkpoint row is 16 bytes for D <= 3 (against 32 in float64), and
 # storing every state (K = 1) can win: the Lorenz f32 cell at 2^20 measured 1.37 ms per
 # gradient step at K = 1 against 1.43 at K = 2 and 1.45 at K = 4.
@@ -134,6 +147,7 @@ def tuned_ckpt_every(method: str, spec: FieldSpec, precision: str) -> Optional[i
     return _TUNED.get((method, spec.key, precision))
 
 
+@_tuner
 def autotune_ckpt_every(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tensor, *,
                         t0: float, t1: float, rtol: float, atol: float,
                         t1v: Optional[torch.Tensor] = None, max_steps: int = 100000,
@@ -538,6 +552,127 @@ def _lanes_flag(method: str, spec: FieldSpec) -> int:
     return 0 if not G or G == 1 else int(G).bit_length() - 1 << 12
 
 
+# ---- registers and occupancy of the float64 Tsit5 forward and reverse pass ---------------
+# For each field of up to 4 components the library builds the recording forward with its
+# registers bounded for 6 resident blocks of 128 threads per SM (the default) and for 4, 5, 7
+# and 8, and the K = 2 stage-keeping reverse pass for 5 (the default), 3, 4 and 6
+# (gs_occ_choices): more registers (longer-range scheduling, no spills) against more resident
+# warps to hide the FP64 pipe's latency.  The instances compute the same values bit for bit;
+# which runs fastest depends on the field and is measured once per process on a sample of
+# the caller's trajectories.
+_OCC: dict = {}      # field key -> GS_OCC blocks per SM of the forward (0: default instance)
+_OCC_REV: dict = {}  # field key -> the same for the reverse pass at K = 2
+OCC_MARGIN = 0.01    # another instance replaces the default only when faster by more than 1%
+_OCC_PASS = {"forward": 0, "reverse": 1}
+
+
+def occ_choices(spec: FieldSpec, pass_: str = "forward") -> list:
+    """GS_OCC values built for the field's float64 Tsit5 recording forward ("forward") or
+    K = 2 reverse pass ("reverse"), 0 (the default instance) first."""
+    L = _lib.lib_for(spec)
+    buf = (ctypes.c_int * 8)()
+    k = L.gs_occ_choices(spec.code, _OCC_PASS[pass_], buf, 8)
+    if k < 0:
+        _lib.check(k, "gs_occ_choices", L)
+    return list(buf[: min(k, 8)])
+
+
+def set_occupancy(spec: FieldSpec, blocks: Optional[int], pass_: str = "forward") -> None:
+    """Pin the occupancy instance of a field's forward or reverse pass (None: back to
+    autotuning)."""
+    table = _OCC if pass_ == "forward" else _OCC_REV
+    if blocks is None:
+        table.pop(spec.key, None)
+        return
+    if blocks not in occ_choices(spec, pass_):
+        raise ValueError(f"no {pass_} instance for {blocks} blocks per SM is built for "
+                         f"{spec.key!r}; built: {occ_choices(spec, pass_)}")
+    table[spec.key] = int(blocks)
+
+
+def _occ_applies(method, precision, schedule, t1v, saveat_ts) -> bool:
+    """The recording forward that GS_OCC selects among: float64 Tsit5, one thread per
+    trajectory (the static schedule, which "auto" is without per-trajectory end times)."""
+    return (method == METHOD_TSIT5 and precision == "float64" and saveat_ts is None and
+            (schedule == "static" or (schedule == "auto" and t1v is None)))
+
+
+def _occ_flag(method, spec, precision, schedule, t1v, saveat_ts) -> int:
+    if not _occ_applies(method, precision, schedule, t1v, saveat_ts):
+        return 0
+    return int(_OCC.get(spec.key) or 0) << 15
+
+
+def _occ_rev_flag(r, precision: str, schedule: str, variant: str) -> int:
+    """The reverse pass's GS_OCC: float64 Tsit5 at K = 2, stage-keeping, one thread per
+    trajectory."""
+    if (r.method != METHOD_TSIT5 or precision != "float64" or r.ckpt_every != 2 or
+            variant == "recompute" or schedule not in ("auto", "static")):
+        return 0
+    return int(_OCC_REV.get(r.spec.key) or 0) << 15
+
+
+def _time_ms(fn, reps: int) -> float:
+    best = float("inf")
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return best
+
+
+def _pick(times: dict) -> int:
+    best = min(times, key=times.get)
+    return 0 if times[best] > times[0] * (1.0 - OCC_MARGIN) else best
+
+
+@_tuner
+def autotune_occupancy(spec: FieldSpec, y0: torch.Tensor, p: torch.Tensor, *, t0: float,
+                       t1: float, rtol: float, atol: float, max_steps: int = 100000,
+                       checkpoint="auto", sample: int = 1 << 20, reps: int = 3) -> tuple:
+    """Time the float64 recording forward of each built occupancy instance on up to
+    ``sample`` of the caller's trajectories (buffers reused, lanes ordered by cost as in a
+    training loop's steady state; best of ``reps``), then, where the record's checkpoint
+    interval is 2, the reverse pass's instances on that record; keep the fastest of each per
+    field (the default unless another is faster by more than ``OCC_MARGIN``).  Returns
+    (forward, reverse) GS_OCC values."""
+    fwd, rev = occ_choices(spec, "forward"), occ_choices(spec, "reverse")
+    _OCC[spec.key] = 0
+    _OCC_REV[spec.key] = 0
+    if len(fwd) < 2:
+        return 0, 0
+    m = min(y0.shape[0], sample)
+    ys, ps = y0[:m].contiguous(), p[:m].contiguous()
+    kw = dict(t0=t0, t1=t1, rtol=rtol, atol=atol, max_steps=max_steps, checkpoint=checkpoint)
+    box = {"r": None}
+
+    def fwd_once():
+        box["r"] = forward_record(METHOD_TSIT5, spec, ys, ps, workspace=box["r"], **kw)
+
+    times = {}
+    for b in fwd:
+        _OCC[spec.key] = b
+        for _ in range(2):  # warm: the record sized, the lanes ordered by cost
+            fwd_once()
+        times[b] = _time_ms(fwd_once, reps)
+    _OCC[spec.key] = _pick(times)
+    r = box["r"]
+    if r.ckpt_every == 2 and len(rev) > 1:
+        ybar = torch.ones_like(r.y_final)
+        times = {}
+        for b in rev:
+            _OCC_REV[spec.key] = b
+            adjoint(r, ps, ybar)  # warm
+            times[b] = _time_ms(lambda: adjoint(r, ps, ybar), reps)
+        _OCC_REV[spec.key] = _pick(times)
+    return _OCC[spec.key], _OCC_REV[spec.key]
+
+
+@_tuner
 def autotune_lanes(spec: FieldSpec, y0: torch.Tensor, p: torch.Tensor, *, t0: float,
                    t1: float, rtol: float, atol: float, t1v: Optional[torch.Tensor] = None,
                    max_steps: int = 100000, sample: int = 1 << 16, reps: int = 2) -> int:
@@ -620,6 +755,10 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
     if checkpoint == "auto" and tuned_ckpt_every(method, spec, precision) is None and n >= 4096:
         autotune_ckpt_every(method, spec, y0, p, t0=t0, t1=t1, t1v=t1v, rtol=rtol, atol=atol,
                             max_steps=max_steps, precision=precision)
+    if (spec.key not in _OCC and not _IN_TUNER[0] and n >= 4096 and
+            _occ_applies(method, precision, schedule, t1v, saveat_ts)):
+        autotune_occupancy(spec, y0, p, t0=t0, t1=t1, rtol=rtol, atol=atol,
+                           max_steps=max_steps, checkpoint=checkpoint)
     if isinstance(ws, RecordSet):
         return _forward_planned(method, spec, y0, p, t1v, saveat_ts, ws, kw)
     if isinstance(ws, Record) and n > 32 and ws.rec.numel() > 2:
@@ -656,7 +795,8 @@ def _forward_one(method, spec, y0, p, t1v, saveat_ts, cap, ws, kw) -> Record:
         rec, ckpt = ws.rec, ws.ckpt
     else:
         rec, ckpt = _alloc_record(n, cap, spec.dim, K, device, precision)
-    mode = _PREC[precision] | _SCHED[kw["schedule"]] | _lanes_flag(method, spec)
+    mode = (_PREC[precision] | _SCHED[kw["schedule"]] | _lanes_flag(method, spec) |
+            _occ_flag(method, spec, precision, kw["schedule"], t1v, saveat_ts))
     dt0_arg = -1.0 if kw["dt0"] is None else float(kw["dt0"])
     args = (float(kw["t0"]), _ptr(t1v), float(kw["t1"]), float(kw["rtol"]), float(kw["atol"]),
             dt0_arg, int(kw["max_steps"]), cap, K, _ptr(rec), _ptr(ckpt), _ptr(yf),
@@ -907,7 +1047,8 @@ def _adjoint_one(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: boo
     if schedule == "auto" and r.uneven and precision != "float32":
         schedule = "refill"
     flags = (_PREC[precision] | _SCHED[schedule] | _lanes_flag(r.method, r.spec) |
-             (_ADJ[variant] if r.method == METHOD_TSIT5 else 0))
+             (_ADJ[variant] if r.method == METHOD_TSIT5 else 0) |
+             _occ_rev_flag(r, precision, schedule, variant))
     if in_batch_order and r.n >= ORDER_LANES_MIN and schedule in ("auto", "static"):
         order = r.lane_order if r.lane_order is not None else prepare_lane_order(r)
         _lib.check(L.gs_adjoint_ordered(_METHOD_CODE[r.method], r.spec.code, flags, r.n, _ptr(p),

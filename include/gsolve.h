@@ -111,6 +111,22 @@ extern "C" {
 #define GS_LANES_MASK 0x7000
 #define GS_LANES(log2_lanes) ((log2_lanes) << GS_LANES_SHIFT)
 
+/* Registers and occupancy, OR-ed into the precision argument of gs_tsit5_fwd_record (the
+ * float64 recording forward, one thread per trajectory) and of gs_tsit5_adjoint /
+ * gs_adjoint_ordered (the float64 reverse pass's K = 2 stage-keeping instance, one thread
+ * per trajectory): GS_OCC(b) runs the kernel instance whose registers are bounded for b
+ * resident blocks of 128 threads per SM; 0 takes the default instance.  gs_occ_choices
+ * lists the values built for a field and pass (0 first); any other value, and any nonzero
+ * value on another path (float32 stages, the float32 route, the forward without a record,
+ * persistent schedules, another checkpoint interval or reverse-pass variant, Rosenbrock23),
+ * is refused with GS_ERR_ARG.  The instances run the same arithmetic: results are bit for
+ * bit those of the default. */
+#define GS_OCC_SHIFT 15
+#define GS_OCC_MASK 0x78000
+#define GS_OCC(blocks) ((blocks) << GS_OCC_SHIFT)
+#define GS_OCC_FORWARD 0
+#define GS_OCC_REVERSE 1
+
 /* per-trajectory status values written to status[] */
 #define GS_TRAJ_OK 0          /* reached t1 */
 #define GS_TRAJ_MAX_STEPS 1   /* max_steps attempts exhausted (or non-finite error) */
@@ -165,6 +181,16 @@ int gs_max_ckpt_every(void);
  * is one thread per trajectory (gradsolve/warp/_warp_kernel.py:325-399); it serves the
  * autotuner that picks the group size. */
 int gs_lane_choices(int field, int* out, int cap);
+
+/* Occupancy choices built for a field, pass = GS_OCC_FORWARD (the float64 Tsit5 recording
+ * forward; default instance bounded for 6 blocks per SM at up to 4 components, unbounded
+ * above) or GS_OCC_REVERSE (the float64 Tsit5 reverse pass at K = 2; default 5 blocks):
+ * writes up to cap GS_OCC values to out (0, the default instance, first) and returns how
+ * many, or a negative GS_ERR_* for an unknown field or pass.  No counterpart in the
+ * reference, whose kernels take the compiler's register allocation
+ * (gradsolve/warp/_warp_kernel.py:325-399); it serves the autotuner that picks registers and
+ * occupancy per field. */
+int gs_occ_choices(int field, int pass, int* out, int cap);
 
 /*
  * Adaptive Tsit5 forward solve that records the accepted step sizes.

@@ -42,8 +42,8 @@ L2_BYTES = 126 * 1024 * 1024
 # lanes ordered by cost, segments swept in step with the warp's longest trajectory).
 # Traffic grows with the trajectory count.
 DRAM_BYTES_PER_TRAJ = {
-    "tsit5_adjoint_stages_k2_kernel": {2: (4.268379e9 + 6.600e6) / 2**18},
-    "tsit5_record_kernel": {2: (0.170665e9 + 4.326640e9) / 2**18},
+    "tsit5_adjoint_stages_k2_kernel": {2: (4.266209e9 + 5.998e6) / 2**18},
+    "tsit5_record_kernel": {2: (0.146856e9 + 4.304376e9) / 2**18},
 }
 
 
@@ -496,6 +496,10 @@ def run_b200(args) -> None:
     stream = torch.cuda.current_stream()
     n = args.n
     spec = field_spec("lorenz")
+    if args.occupancy != "auto":  # pinned instances (a profile of a known kernel)
+        f_occ, r_occ = (int(x) for x in args.occupancy.split(","))
+        engine.set_occupancy(spec, f_occ, "forward")
+        engine.set_occupancy(spec, r_occ, "reverse")
     y0_np, rho_np = make_inputs(n, shard_seed(rank))
     y0 = torch.tensor(y0_np, device=dev)
     rho = torch.tensor(rho_np, device=dev)
@@ -552,6 +556,10 @@ def run_b200(args) -> None:
     acc = int(r.n_acc.to(torch.int64).sum().item())
     S = int(r.n_acc.max().item())
     K = r.ckpt_every
+    # the occupancy instances the timed steps ran (GS_OCC blocks per SM; 0 = default: 6 for
+    # the forward, 5 for the K = 2 reverse pass)
+    occ_f = engine._OCC.get(spec.key, 0)
+    occ_r = engine._OCC_REV.get(spec.key, 0) if K == 2 else None
     # the timed run's own gradients, checked on 64 sampled trajectories (oracle + FD)
     # (rank 0 alone: only its line is printed, and the checks run no collective)
     checks = None if (args.no_checks or rank != 0) else headline_checks(
@@ -703,8 +711,9 @@ def run_b200(args) -> None:
         "frac": achieved / fp64_peak,
         "traffic": (DRAM_BYTES_PER_TRAJ[dom][K] * n if K in DRAM_BYTES_PER_TRAJ.get(dom, {})
                     else None),
-        "traffic_source": (f"ncu capture of {dom} at n=2^18, K={K}, scaled to n={n} "
-                           "(bytes grow with the trajectory count)"
+        "traffic_source": (f"ncu capture of {dom} at n=2^18, K={K} (occupancy instances "
+                           f"GS_OCC 5 / 4), scaled to n={n} (bytes grow with the trajectory "
+                           "count)"
                            if K in DRAM_BYTES_PER_TRAJ.get(dom, {}) else
                            f"no ncu capture at K={K}"),
         "kernel": dom,
@@ -733,6 +742,8 @@ def run_b200(args) -> None:
                    "checkpoint_policy": str(args.checkpoint),
                    "n_per_gpu": n, "record_len_max": S, "checkpoint_every": K,
                    "attempts": att, "accepted": acc, "parallelism": f"shard{world}",
+                   "occupancy": {"forward_blocks_per_sm": occ_f, "reverse_blocks_per_sm": occ_r,
+                                 "policy": args.occupancy},
                    "l2": "flushed between timed steps (record traffic also >> L2)"},
         "gpu_launches": gpu_launches,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
@@ -1161,6 +1172,9 @@ def main():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--schedule", default="auto", choices=["auto", "static", "refill", "strided"])
     ap.add_argument("--adjoint-variant", default="auto", choices=["auto", "stages", "recompute"])
+    ap.add_argument("--occupancy", default="auto",
+                    help="'auto' (autotuned per field) or 'F,R': the GS_OCC blocks per SM of "
+                         "the Lorenz forward and K = 2 reverse-pass instances (0 = default)")
     ap.add_argument("--workload", default="lorenz_2e20",
                     choices=["lorenz_2e20", "published_h200"] + sorted(WORKLOAD_N))
     args = ap.parse_args()

@@ -408,6 +408,56 @@ def other_configs(args, dev) -> dict:
     return out
 
 
+def replay_graph_config(dev, calls: int = 50) -> dict:
+    """The small plain-method Lorenz case (n = 1024, y0 = (1, 0, 0), rho = linspace(20, 30),
+    t in [0, 1], rtol = atol = 1e-8): the frozen-mesh replay + cotangent + reverse pass at a
+    new point, launched one by one (replay, adjoint) and as the captured CUDA graph
+    (engine.ReplayGraph) -- mean ms per gradient evaluation over ``calls`` calls each: queued
+    back to back (CUDA events around the loop: the device's rate) and one at a time with the
+    result waited for (host clock: the latency an optimiser that reads each gradient sees);
+    results bit for bit equal."""
+    import torch
+
+    from gradsolve_b200 import engine
+    from gradsolve_b200.fields import field_spec
+    n = 1024
+    spec = field_spec("lorenz")
+    y0 = torch.tensor(np.tile([1.0, 0.0, 0.0], (n, 1)), device=dev)
+    p = torch.linspace(20.0, 30.0, n, dtype=torch.float64, device=dev).reshape(n, 1)
+    r = engine.forward_record("tsit5", spec, y0, p, t0=0.0, t1=1.0, rtol=1e-8, atol=1e-8,
+                              checkpoint=2)
+    cot = lambda yf: 2.0 * yf  # noqa: E731
+    pts = [p * (1.0 + 1e-3 * k) for k in range(4)]
+
+    def eager(pk):
+        yf = engine.replay(r, y0, pk, write_ckpt=True)
+        return engine.adjoint(r, pk, cot(yf))
+
+    g = engine.ReplayGraph(r, y0, p, cot)
+    same = all(torch.equal(eager(pk)[1], g(None, pk)[2]) for pk in pts)
+    out = {}
+    for name, fn in (("eager", eager), ("graph", lambda pk: g(None, pk))):
+        for pk in pts:
+            fn(pk)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(calls):
+            fn(pts[k % len(pts)])
+        e1.record()
+        e1.synchronize()
+        out[f"{name}_queued_ms"] = e0.elapsed_time(e1) / calls
+        t0 = time.perf_counter()
+        for k in range(calls):
+            fn(pts[k % len(pts)])
+            torch.cuda.synchronize()
+        out[f"{name}_latency_ms"] = (time.perf_counter() - t0) * 1e3 / calls
+    return {"workload": "lorenz n=1024, y0=(1,0,0), rho=linspace(20,30), t in [0,1], "
+                        "rtol=atol=1e-8: replay + cotangent + reverse pass at a new point",
+            **out, "latency_speedup": out["eager_latency_ms"] / out["graph_latency_ms"],
+            "bitwise_equal": bool(same)}
+
+
 def float32_route_config(args, dev, n: int = 1 << 20) -> dict:
     """The float32 route on the reference's f32 nonstiff cell (tests/test_f32_replay.py:84-117:
     diffeqgpu_lorenz, y0 = [1, 0, 0] + 0.01 N(0, 1) seed 0, rho = 28, t in [0, 1], rtol 1e-6 /
@@ -677,6 +727,9 @@ def run_b200(args) -> None:
     others = None
     if world == 1 and not args.no_config3:
         others = other_configs(args, dev)
+    graph_cfg = None
+    if world == 1 and not args.no_config3:
+        graph_cfg = replay_graph_config(dev)
 
     if rank != 0:
         if world > 1:
@@ -748,7 +801,7 @@ def run_b200(args) -> None:
         "gpu_launches": gpu_launches,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
         "parity_sample": checks, "config3_mixed": config3, "float32_route": f32_route,
-        "other_configs": others,
+        "other_configs": others, "replay_graph": graph_cfg,
         "fwd_ms": fwd_avg, "adj_ms": adj_avg, "mixed": mixed, "solve": solve or None,
         "fwd_ms_steps": [round(x, 3) for x in fwd_ms], "adj_ms_steps": [round(x, 3) for x in adj_ms],
     }

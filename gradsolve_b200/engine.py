@@ -1062,6 +1062,61 @@ def _adjoint_one(r: Record, p: torch.Tensor, ybar: torch.Tensor, *, want_y0: boo
     return gy0, gp
 
 
+class ReplayGraph:
+    """The frozen-mesh replay, a cotangent and the reverse pass, captured once as a CUDA
+    graph and re-launched as one unit (gradsolve/warp/warp_replay.py:30-55 and 186-237, the
+    replay and its gradient, which the reference runs as one jitted computation).
+
+    For loops that evaluate the same recorded mesh at many points -- an optimiser stepping
+    the parameters of a fixed mesh, a finite-difference or Newton iteration -- the per-call
+    host work (argument checks, the reverse pass's occupancy queries, the launches) is paid
+    once at capture.  ``cotangent(y_final) -> ybar`` is the loss's derivative written with
+    torch operations; it is captured with the kernels.  ``graph(y0, p)`` copies the point
+    into the graph's input buffers, re-launches, and returns (y_final, gy0, gp): the graph's
+    own output buffers, overwritten by the next call (clone what must be kept).  Results are
+    bit for bit those of ``replay`` + ``adjoint`` called one by one.
+
+    Float64, one Record (a RecordSet's tiers run on side streams and are not captured); the
+    record's buffers must stay alive and unmodified while the graph is used (a new forward
+    into the same record changes the mesh the graph replays)."""
+
+    def __init__(self, r, y0: torch.Tensor, p: torch.Tensor, cotangent, *,
+                 want_y0: bool = True, want_p: bool = True):
+        if not isinstance(r, Record):
+            raise TypeError("ReplayGraph captures a single Record (not the tiers of a RecordSet)")
+        if r.rec.dtype != torch.float64:
+            raise TypeError("ReplayGraph captures the float64 replay only")
+        self.r = r
+        self.y0 = y0.detach().clone().contiguous()
+        self.p = p.detach().clone().contiguous()
+        self.cotangent = cotangent
+        self.want_y0, self.want_p = want_y0, want_p
+        prepare_lane_order(r)  # the sort stays outside the graph
+        main = torch.cuda.current_stream()
+        side = torch.cuda.Stream(device=self.y0.device)
+        side.wait_stream(main)
+        with torch.cuda.stream(side):  # one eager pass first: kernel attributes set, caches warm
+            self._run()
+        main.wait_stream(side)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.out = self._run()
+
+    def _run(self):
+        yf = replay(self.r, self.y0, self.p, write_ckpt=True)
+        gy0, gp = adjoint(self.r, self.p, self.cotangent(yf), want_y0=self.want_y0,
+                          want_p=self.want_p)
+        return yf, gy0, gp
+
+    def __call__(self, y0: Optional[torch.Tensor] = None, p: Optional[torch.Tensor] = None):
+        if y0 is not None:
+            self.y0.copy_(y0)
+        if p is not None:
+            self.p.copy_(p)
+        self.graph.replay()
+        return self.out
+
+
 def record_from_padded(method: str, spec: FieldSpec, dts: torch.Tensor, t0: float,
                        checkpoint="auto", budget_bytes: Optional[int] = None) -> Record:
     """A Record built from a padded (n, S) dt array (e.g. the reference's own record).

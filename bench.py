@@ -608,8 +608,8 @@ def run_b200(args) -> None:
     K = r.ckpt_every
     # the occupancy instances the timed steps ran (GS_OCC blocks per SM; 0 = default: 6 for
     # the forward, 5 for the K = 2 reverse pass)
-    occ_f = engine._OCC.get(spec.key, 0)
-    occ_r = engine._OCC_REV.get(spec.key, 0) if K == 2 else None
+    occ_f = engine._OCC.get(("tsit5", spec.key), 0)
+    occ_r = engine._OCC_REV.get(("tsit5", spec.key), 0) if K == 2 else None
     # the timed run's own gradients, checked on 64 sampled trajectories (oracle + FD)
     # (rank 0 alone: only its line is printed, and the checks run no collective)
     checks = None if (args.no_checks or rank != 0) else headline_checks(

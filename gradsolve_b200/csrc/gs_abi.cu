@@ -346,7 +346,9 @@ int lane_choices(int* out, int cap) {
   return k;
 }
 
-// Occupancy instances (GS_OCC) for fields of up to 4 components.  The float64 recording
+// Occupancy instances (GS_OCC) for fields of up to 4 components.  Rosenbrock23: the
+// recording forward (unbounded by default) also bounded for 4 and 6 blocks per SM, the K = 2
+// kept-factor reverse pass (default 4 blocks) for 3 and 5.  Tsit5: the float64 recording
 // forward, whose default instance is bounded for 6 blocks per SM, also has instances bounded
 // for 4 and 5 (more registers: longer-range scheduling, no spills where the default spills),
 // 7 and 8 (fewer registers, more resident warps); the float64 reverse pass's K = 2
@@ -358,8 +360,10 @@ int occ_choices(int pass, int* out, int cap) {
   if (cap > k) out[k] = 0;
   ++k;
   if constexpr (F::D <= 4) {
-    const std::initializer_list<int> fwd = {4, 5, 7, 8}, rev = {3, 4, 6};
-    for (int b : (pass == GS_OCC_REVERSE ? rev : fwd)) {
+    const std::initializer_list<int> fwd = {4, 5, 7, 8}, rev = {3, 4, 6}, rfwd = {4, 6},
+                                     rrev = {3, 5};
+    for (int b : (pass == GS_OCC_REVERSE ? rev : pass == GS_OCC_ROS23_FORWARD ? rfwd
+                  : pass == GS_OCC_ROS23_REVERSE ? rrev : fwd)) {
       if (cap > k) out[k] = b;
       ++k;
     }
@@ -621,9 +625,26 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
   }
 }
 template <class F>
-int launch_ros23_record(const gs::RecordArgs& a_in, cudaStream_t s, int sched) {
+int launch_ros23_record(const gs::RecordArgs& a_in, cudaStream_t s, int sched, int occ) {
   gs::RecordArgs a = a_in;
   a.ctrl = gs::make_ctrl_consts(F::D, 6);  // Rosenbrock23: err^(-1/3) = m^(-1/6)
+  if (occ && (sched != GS_SCHED_STATIC || (!a.rec && !a.ckpt)))
+    return fail(GS_ERR_ARG, "GS_OCC applies to the float64 recording forward, one thread per "
+                            "trajectory");
+  if (occ) {
+    if constexpr (F::D <= 4) {
+      switch (occ) {
+        case 4: gs::ros23_record_occ_kernel<F, 4><<<grid_for(a.n), kBlock, 0, s>>>(a);
+          return cuda_check("ros23_record_occ_kernel");
+        case 6: gs::ros23_record_occ_kernel<F, 6><<<grid_for(a.n), kBlock, 0, s>>>(a);
+          return cuda_check("ros23_record_occ_kernel");
+        default: break;
+      }
+    }
+    return fail(GS_ERR_ARG, "GS_OCC: no Rosenbrock23 forward instance bounded for " +
+                                std::to_string(occ) + " blocks per SM is built for D = " +
+                                std::to_string(F::D) + " (gs_occ_choices)");
+  }
   if (sched == GS_SCHED_STATIC) {
     if (!a.rec && !a.ckpt)
       gs::ros23_record_kernel<F, false><<<grid_for(a.n), kBlock, 0, s>>>(a);
@@ -639,7 +660,33 @@ int launch_ros23_replay(const gs::ReplayArgs& a, cudaStream_t s) {
   return cuda_check("ros23_replay_kernel");
 }
 template <class F>
-int launch_ros23_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, int sched) {
+int launch_ros23_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, int sched, int occ) {
+  if (occ) {
+    if (sched != GS_SCHED_STATIC || a.ck_every != 2)
+      return fail(GS_ERR_ARG, "GS_OCC applies to the Rosenbrock23 reverse pass's K = 2 "
+                              "kept-factor instance, one thread per trajectory");
+    if constexpr (F::D <= 4) {
+      auto go = [&](auto kern) -> int {
+        SegCfg c{0, 0, 0};
+        int rc;
+        if ((rc = occupancy_probe(kern, gs::ros23_adjoint_smem_doubles<F::D, true>(2), &c)))
+          return rc;
+        if (c.resident <= 0)
+          return fail(GS_ERR_ARG, "GS_OCC: the K = 2 segment buffer does not fit shared memory");
+        if ((rc = allow_smem(kern, c.smem))) return rc;
+        kern<<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
+        return cuda_check("ros23_adjoint_kernel");
+      };
+      switch (occ) {
+        case 3: return go(gs::ros23_adjoint_k2_kernel<F, 3>);
+        case 5: return go(gs::ros23_adjoint_k2_kernel<F, 5>);
+        default: break;
+      }
+    }
+    return fail(GS_ERR_ARG, "GS_OCC: no Rosenbrock23 reverse-pass instance bounded for " +
+                                std::to_string(occ) + " blocks per SM is built for D = " +
+                                std::to_string(F::D) + " (gs_occ_choices)");
+  }
   if (sched == GS_SCHED_STATIC) {
     SegCfg ck{0, 0, 0}, cr{0, 0, 0};
     int rc;
@@ -1068,8 +1115,11 @@ int gs_occ_choices(int field, int pass, int* out, int cap) {
   int D, P, rc;
   if ((rc = field_dims(field, &D, &P))) return rc;
   if (!out && cap > 0) return fail(GS_ERR_ARG, "gs_occ_choices: null output");
+  if (pass == GS_OCC_ROS23_FORWARD || pass == GS_OCC_ROS23_REVERSE) {
+    GS_ROS23_DISPATCH(field, occ_choices, pass, out, cap)
+  }
   if (pass != GS_OCC_FORWARD && pass != GS_OCC_REVERSE)
-    return fail(GS_ERR_ARG, "gs_occ_choices: pass is GS_OCC_FORWARD or GS_OCC_REVERSE");
+    return fail(GS_ERR_ARG, "gs_occ_choices: unknown pass " + std::to_string(pass));
   GS_TSIT5_DISPATCH(field, occ_choices, pass, out, cap)
 }
 
@@ -1081,8 +1131,8 @@ int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,
   const int prec = precision & GS_PREC_MASK;
   if (prec != GS_PREC_F64 && prec != GS_PREC_F32)
     return fail(GS_ERR_PRECISION, "gs_ros23_fwd_record: Rosenbrock23 runs in float64 or float32");
-  if (precision & GS_OCC_MASK)
-    return fail(GS_ERR_ARG, "GS_OCC applies to the Tsit5 entry points only");
+  if ((precision & GS_OCC_MASK) && prec != GS_PREC_F64)
+    return fail(GS_ERR_ARG, "GS_OCC applies to the float64 recording forward only");
   int rc = check_record_args("gs_ros23_fwd_record", n, y0, p, rtol, atol, max_steps, cap,
                              ckpt_every, rec, ckpt, y_final, n_acc, n_rej, status);
   if (rc) return rc;
@@ -1096,7 +1146,8 @@ int gs_ros23_fwd_record(int field, int precision, long long n, const double* y0,
     GS_ROS23_DISPATCH(field, launch_f32_ros23_record, a, (cudaStream_t)stream)
   }
   GS_ROS23_DISPATCH(field, launch_ros23_record, a, (cudaStream_t)stream,
-                    forward_schedule(precision, t1v, ckpt))
+                    forward_schedule(precision, t1v, ckpt),
+                    (precision & GS_OCC_MASK) >> GS_OCC_SHIFT)
 }
 
 int gs_ros23_replay(int field, int precision, long long n, const double* y0, const double* p,
@@ -1129,8 +1180,8 @@ static int ros23_adjoint_impl(int field, int precision, long long n, const doubl
   const int prec = precision & GS_PREC_MASK;
   if (prec != GS_PREC_F64 && prec != GS_PREC_F32)
     return fail(GS_ERR_PRECISION, "gs_ros23_adjoint: Rosenbrock23 runs in float64 or float32");
-  if (precision & GS_OCC_MASK)
-    return fail(GS_ERR_ARG, "GS_OCC applies to the Tsit5 entry points only");
+  if ((precision & GS_OCC_MASK) && prec != GS_PREC_F64)
+    return fail(GS_ERR_ARG, "GS_OCC applies to the float64 reverse pass only");
   int rc = check_adjoint_args("gs_ros23_adjoint", n, p, rec, n_acc, cap, ckpt, ckpt_every, ybar);
   if (rc) return rc;
   int D, P;
@@ -1142,7 +1193,7 @@ static int ros23_adjoint_impl(int field, int precision, long long n, const doubl
     GS_ROS23_DISPATCH(field, launch_f32_ros23_adjoint, a, (cudaStream_t)stream)
   }
   GS_ROS23_DISPATCH(field, launch_ros23_adjoint, a, cap, (cudaStream_t)stream,
-                    adjoint_schedule(precision))
+                    adjoint_schedule(precision), (precision & GS_OCC_MASK) >> GS_OCC_SHIFT)
 }
 
 int gs_ros23_adjoint(int field, int precision, long long n, const double* p, const double* rec,

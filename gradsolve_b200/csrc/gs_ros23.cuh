@@ -376,8 +376,8 @@ __device__ __forceinline__ bool ros23_attempt(const RecordArgs& a, long long j, 
 }
 
 // kStore = false: the forward-only solve (no record, no checkpoints), stores compiled out.
-template <class F, bool kStore = true>
-__global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
+template <class F, bool kStore>
+__device__ __forceinline__ void ros23_record_body(const RecordArgs& a) {
   constexpr int D = F::D, P = F::P;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.n) return;
@@ -413,6 +413,18 @@ __global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
   a.n_acc[j] = c.acc;
   a.n_rej[j] = c.rej;
   a.status[j] = c.st;
+}
+
+template <class F, bool kStore = true>
+__global__ void __launch_bounds__(128) ros23_record_kernel(const RecordArgs a) {
+  ros23_record_body<F, kStore>(a);
+}
+
+// The recording forward with its registers bounded for kMinB resident blocks of 128 per SM
+// (the instances the occupancy autotuner chooses among; same arithmetic, bit for bit).
+template <class F, int kMinB>
+__global__ void __launch_bounds__(128, kMinB) ros23_record_occ_kernel(const RecordArgs a) {
+  ros23_record_body<F, true>(a);
 }
 
 template <class F>
@@ -583,9 +595,10 @@ __global__ void __launch_bounds__(128) ros23_adjoint_kernel(const AdjointArgs a)
   ros23_adjoint_body<F, kKeep, 0>(a);
 }
 
-// K = 2 with the kept factors, unrolled; bounded to 4 blocks of 128 per SM
-template <class F>
-__global__ void __launch_bounds__(128, 4) ros23_adjoint_k2_kernel(const AdjointArgs a) {
+// K = 2 with the kept factors, unrolled; bounded to 4 blocks of 128 per SM (kMinB = 0), or
+// for kMinB blocks (the occupancy instances; same arithmetic, bit for bit)
+template <class F, int kMinB = 0>
+__global__ void __launch_bounds__(128, (kMinB > 0 ? kMinB : 4)) ros23_adjoint_k2_kernel(const AdjointArgs a) {
   ros23_adjoint_body<F, true, 2>(a);
 }
 

@@ -552,64 +552,67 @@ def _lanes_flag(method: str, spec: FieldSpec) -> int:
     return 0 if not G or G == 1 else int(G).bit_length() - 1 << 12
 
 
-# ---- registers and occupancy of the float64 Tsit5 forward and reverse pass ---------------
-# For each field of up to 4 components the library builds the recording forward with its
+# ---- registers and occupancy of the float64 forward and reverse pass ---------------------
+# For each field of up to 4 components the library builds the Tsit5 recording forward with its
 # registers bounded for 6 resident blocks of 128 threads per SM (the default) and for 4, 5, 7
-# and 8, and the K = 2 stage-keeping reverse pass for 5 (the default), 3, 4 and 6
-# (gs_occ_choices): more registers (longer-range scheduling, no spills) against more resident
-# warps to hide the FP64 pipe's latency.  The instances compute the same values bit for bit;
-# which runs fastest depends on the field and is measured once per process on a sample of
-# the caller's trajectories.
-_OCC: dict = {}      # field key -> GS_OCC blocks per SM of the forward (0: default instance)
-_OCC_REV: dict = {}  # field key -> the same for the reverse pass at K = 2
+# and 8, the Tsit5 K = 2 stage-keeping reverse pass for 5 (the default), 3, 4 and 6, the
+# Rosenbrock23 forward unbounded (the default) and for 4 and 6, and its K = 2 kept-factor
+# reverse pass for 4 (the default), 3 and 5 (gs_occ_choices): more registers (longer-range
+# scheduling, no spills) against more resident warps to hide the FP64 pipe's latency.  The
+# instances compute the same values bit for bit; which runs fastest depends on the method and
+# the field and is measured once per process on a sample of the caller's trajectories.
+_OCC: dict = {}      # (method, field key) -> GS_OCC blocks per SM of the forward (0: default)
+_OCC_REV: dict = {}  # (method, field key) -> the same for the reverse pass at K = 2
 OCC_MARGIN = 0.01    # another instance replaces the default only when faster by more than 1%
-_OCC_PASS = {"forward": 0, "reverse": 1}
+_OCC_PASS = {(METHOD_TSIT5, "forward"): 0, (METHOD_TSIT5, "reverse"): 1,
+             (METHOD_ROS23, "forward"): 2, (METHOD_ROS23, "reverse"): 3}
 
 
-def occ_choices(spec: FieldSpec, pass_: str = "forward") -> list:
-    """GS_OCC values built for the field's float64 Tsit5 recording forward ("forward") or
-    K = 2 reverse pass ("reverse"), 0 (the default instance) first."""
+def occ_choices(spec: FieldSpec, pass_: str = "forward", method: str = METHOD_TSIT5) -> list:
+    """GS_OCC values built for the field's float64 recording forward ("forward") or K = 2
+    reverse pass ("reverse") of ``method``, 0 (the default instance) first."""
     L = _lib.lib_for(spec)
     buf = (ctypes.c_int * 8)()
-    k = L.gs_occ_choices(spec.code, _OCC_PASS[pass_], buf, 8)
+    k = L.gs_occ_choices(spec.code, _OCC_PASS[(method, pass_)], buf, 8)
     if k < 0:
         _lib.check(k, "gs_occ_choices", L)
     return list(buf[: min(k, 8)])
 
 
-def set_occupancy(spec: FieldSpec, blocks: Optional[int], pass_: str = "forward") -> None:
+def set_occupancy(spec: FieldSpec, blocks: Optional[int], pass_: str = "forward",
+                  method: str = METHOD_TSIT5) -> None:
     """Pin the occupancy instance of a field's forward or reverse pass (None: back to
     autotuning)."""
     table = _OCC if pass_ == "forward" else _OCC_REV
     if blocks is None:
-        table.pop(spec.key, None)
+        table.pop((method, spec.key), None)
         return
-    if blocks not in occ_choices(spec, pass_):
+    if blocks not in occ_choices(spec, pass_, method):
         raise ValueError(f"no {pass_} instance for {blocks} blocks per SM is built for "
-                         f"{spec.key!r}; built: {occ_choices(spec, pass_)}")
-    table[spec.key] = int(blocks)
+                         f"{spec.key!r} ({method}); built: {occ_choices(spec, pass_, method)}")
+    table[(method, spec.key)] = int(blocks)
 
 
 def _occ_applies(method, precision, schedule, t1v, saveat_ts) -> bool:
-    """The recording forward that GS_OCC selects among: float64 Tsit5, one thread per
-    trajectory (the static schedule, which "auto" is without per-trajectory end times)."""
-    return (method == METHOD_TSIT5 and precision == "float64" and saveat_ts is None and
+    """The recording forward that GS_OCC selects among: float64, one thread per trajectory
+    (the static schedule, which "auto" is without per-trajectory end times)."""
+    return (precision == "float64" and saveat_ts is None and
             (schedule == "static" or (schedule == "auto" and t1v is None)))
 
 
 def _occ_flag(method, spec, precision, schedule, t1v, saveat_ts) -> int:
     if not _occ_applies(method, precision, schedule, t1v, saveat_ts):
         return 0
-    return int(_OCC.get(spec.key) or 0) << 15
+    return int(_OCC.get((method, spec.key)) or 0) << 15
 
 
 def _occ_rev_flag(r, precision: str, schedule: str, variant: str) -> int:
-    """The reverse pass's GS_OCC: float64 Tsit5 at K = 2, stage-keeping, one thread per
-    trajectory."""
-    if (r.method != METHOD_TSIT5 or precision != "float64" or r.ckpt_every != 2 or
-            variant == "recompute" or schedule not in ("auto", "static")):
+    """The reverse pass's GS_OCC: float64 at K = 2, the instance that keeps the replayed
+    steps' stage inputs (Tsit5) or factors (Rosenbrock23), one thread per trajectory."""
+    if (precision != "float64" or r.ckpt_every != 2 or schedule not in ("auto", "static") or
+            (r.method == METHOD_TSIT5 and variant == "recompute")):
         return 0
-    return int(_OCC_REV.get(r.spec.key) or 0) << 15
+    return int(_OCC_REV.get((r.method, r.spec.key)) or 0) << 15
 
 
 def _time_ms(fn, reps: int) -> float:
@@ -633,43 +636,49 @@ def _pick(times: dict) -> int:
 @_tuner
 def autotune_occupancy(spec: FieldSpec, y0: torch.Tensor, p: torch.Tensor, *, t0: float,
                        t1: float, rtol: float, atol: float, max_steps: int = 100000,
-                       checkpoint="auto", sample: int = 1 << 20, reps: int = 3) -> tuple:
+                       checkpoint="auto", sample: int = 1 << 20, reps: int = 3,
+                       method: str = METHOD_TSIT5, t1v: Optional[torch.Tensor] = None,
+                       dt0: Optional[float] = None) -> tuple:
     """Time the float64 recording forward of each built occupancy instance on up to
     ``sample`` of the caller's trajectories (buffers reused, lanes ordered by cost as in a
     training loop's steady state; best of ``reps``), then, where the record's checkpoint
     interval is 2, the reverse pass's instances on that record; keep the fastest of each per
     field (the default unless another is faster by more than ``OCC_MARGIN``).  Returns
     (forward, reverse) GS_OCC values."""
-    fwd, rev = occ_choices(spec, "forward"), occ_choices(spec, "reverse")
-    _OCC[spec.key] = 0
-    _OCC_REV[spec.key] = 0
+    key = (method, spec.key)
+    fwd, rev = occ_choices(spec, "forward", method), occ_choices(spec, "reverse", method)
+    _OCC[key] = 0
+    _OCC_REV[key] = 0
     if len(fwd) < 2:
         return 0, 0
     m = min(y0.shape[0], sample)
     ys, ps = y0[:m].contiguous(), p[:m].contiguous()
-    kw = dict(t0=t0, t1=t1, rtol=rtol, atol=atol, max_steps=max_steps, checkpoint=checkpoint)
+    tv = None if t1v is None else t1v[:m].contiguous()
+    kw = dict(t0=t0, t1=t1, t1v=tv, dt0=dt0, rtol=rtol, atol=atol, max_steps=max_steps,
+              checkpoint=checkpoint)
     box = {"r": None}
 
     def fwd_once():
-        box["r"] = forward_record(METHOD_TSIT5, spec, ys, ps, workspace=box["r"], **kw)
+        box["r"] = forward_record(method, spec, ys, ps, workspace=box["r"], **kw)
 
     times = {}
     for b in fwd:
-        _OCC[spec.key] = b
+        _OCC[key] = b
         for _ in range(2):  # warm: the record sized, the lanes ordered by cost
             fwd_once()
         times[b] = _time_ms(fwd_once, reps)
-    _OCC[spec.key] = _pick(times)
+    _OCC[key] = _pick(times)
     r = box["r"]
-    if r.ckpt_every == 2 and len(rev) > 1:
+    parts = [rr for _rows, rr in _parts(r)]
+    if all(rr.ckpt_every == 2 for rr in parts) and len(rev) > 1:
         ybar = torch.ones_like(r.y_final)
         times = {}
         for b in rev:
-            _OCC_REV[spec.key] = b
+            _OCC_REV[key] = b
             adjoint(r, ps, ybar)  # warm
             times[b] = _time_ms(lambda: adjoint(r, ps, ybar), reps)
-        _OCC_REV[spec.key] = _pick(times)
-    return _OCC[spec.key], _OCC_REV[spec.key]
+        _OCC_REV[key] = _pick(times)
+    return _OCC[key], _OCC_REV[key]
 
 
 @_tuner
@@ -755,10 +764,13 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
     if checkpoint == "auto" and tuned_ckpt_every(method, spec, precision) is None and n >= 4096:
         autotune_ckpt_every(method, spec, y0, p, t0=t0, t1=t1, t1v=t1v, rtol=rtol, atol=atol,
                             max_steps=max_steps, precision=precision)
-    if (spec.key not in _OCC and not _IN_TUNER[0] and n >= 4096 and
-            _occ_applies(method, precision, schedule, t1v, saveat_ts)):
+    occ_sched = "static" if method == METHOD_ROS23 and schedule == "auto" and isinstance(
+        ws, RecordSet) else schedule  # (planned Rosenbrock23 tiers run one thread per row)
+    if ((method, spec.key) not in _OCC and not _IN_TUNER[0] and n >= 4096 and
+            _occ_applies(method, precision, occ_sched, t1v, saveat_ts)):
         autotune_occupancy(spec, y0, p, t0=t0, t1=t1, rtol=rtol, atol=atol,
-                           max_steps=max_steps, checkpoint=checkpoint)
+                           max_steps=max_steps, checkpoint=checkpoint, method=method,
+                           t1v=t1v, dt0=dt0)
     if isinstance(ws, RecordSet):
         return _forward_planned(method, spec, y0, p, t1v, saveat_ts, ws, kw)
     if isinstance(ws, Record) and n > 32 and ws.rec.numel() > 2:

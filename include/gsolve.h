@@ -111,21 +111,24 @@ extern "C" {
 #define GS_LANES_MASK 0x7000
 #define GS_LANES(log2_lanes) ((log2_lanes) << GS_LANES_SHIFT)
 
-/* Registers and occupancy, OR-ed into the precision argument of gs_tsit5_fwd_record (the
- * float64 recording forward, one thread per trajectory) and of gs_tsit5_adjoint /
- * gs_adjoint_ordered (the float64 reverse pass's K = 2 stage-keeping instance, one thread
- * per trajectory): GS_OCC(b) runs the kernel instance whose registers are bounded for b
- * resident blocks of 128 threads per SM; 0 takes the default instance.  gs_occ_choices
- * lists the values built for a field and pass (0 first); any other value, and any nonzero
- * value on another path (float32 stages, the float32 route, the forward without a record,
- * persistent schedules, another checkpoint interval or reverse-pass variant, Rosenbrock23),
- * is refused with GS_ERR_ARG.  The instances run the same arithmetic: results are bit for
- * bit those of the default. */
+/* Registers and occupancy, OR-ed into the precision argument of gs_tsit5_fwd_record /
+ * gs_ros23_fwd_record (the float64 recording forward, one thread per trajectory) and of
+ * gs_tsit5_adjoint / gs_ros23_adjoint / gs_adjoint_ordered (the float64 reverse pass's K = 2
+ * instance that keeps the replayed steps' stage inputs or factors, one thread per
+ * trajectory): GS_OCC(b) runs the kernel instance whose registers are bounded for b resident
+ * blocks of 128 threads per SM; 0 takes the default instance.  gs_occ_choices lists the
+ * values built for a field and pass (0 first); any other value, and any nonzero value on
+ * another path (float32 stages, the float32 route, the forward without a record, persistent
+ * schedules, another checkpoint interval or reverse-pass variant), is refused with
+ * GS_ERR_ARG.  The instances run the same arithmetic: results are bit for bit those of the
+ * default. */
 #define GS_OCC_SHIFT 15
 #define GS_OCC_MASK 0x78000
 #define GS_OCC(blocks) ((blocks) << GS_OCC_SHIFT)
-#define GS_OCC_FORWARD 0
-#define GS_OCC_REVERSE 1
+#define GS_OCC_FORWARD 0       /* Tsit5 recording forward */
+#define GS_OCC_REVERSE 1       /* Tsit5 reverse pass at K = 2 */
+#define GS_OCC_ROS23_FORWARD 2 /* Rosenbrock23 recording forward */
+#define GS_OCC_ROS23_REVERSE 3 /* Rosenbrock23 reverse pass at K = 2 */
 
 /* per-trajectory status values written to status[] */
 #define GS_TRAJ_OK 0          /* reached t1 */
@@ -184,9 +187,11 @@ int gs_lane_choices(int field, int* out, int cap);
 
 /* Occupancy choices built for a field, pass = GS_OCC_FORWARD (the float64 Tsit5 recording
  * forward; default instance bounded for 6 blocks per SM at up to 4 components, unbounded
- * above) or GS_OCC_REVERSE (the float64 Tsit5 reverse pass at K = 2; default 5 blocks):
- * writes up to cap GS_OCC values to out (0, the default instance, first) and returns how
- * many, or a negative GS_ERR_* for an unknown field or pass.  No counterpart in the
+ * above), GS_OCC_REVERSE (the float64 Tsit5 reverse pass at K = 2; default 5 blocks),
+ * GS_OCC_ROS23_FORWARD (Rosenbrock23 forward; default unbounded) or GS_OCC_ROS23_REVERSE
+ * (Rosenbrock23 reverse pass at K = 2; default 4 blocks): writes up to cap GS_OCC values to
+ * out (0, the default instance, first) and returns how many, or a negative GS_ERR_* for an
+ * unknown field or pass (or a field without a Jacobian for the Rosenbrock23 passes).  No counterpart in the
  * reference, whose kernels take the compiler's register allocation
  * (gradsolve/warp/_warp_kernel.py:325-399); it serves the autotuner that picks registers and
  * occupancy per field. */

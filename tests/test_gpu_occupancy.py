@@ -92,17 +92,17 @@ def test_occupancy_refusals(gslib, cuda):
             engine.set_occupancy(spec, 3)
         with pytest.raises(ValueError, match=r"reverse instance for 5 blocks .* \[0, 3, 4, 6\]"):
             engine.set_occupancy(spec, 5, "reverse")
-        engine._OCC[spec.key] = 3  # bypass the check: the library itself refuses
+        engine._OCC[("tsit5", spec.key)] = 3  # bypass the check: the library itself refuses
         with pytest.raises(GsolveError, match="GS_OCC"):
             engine.forward_record("tsit5", spec, y0, p, t0=0.0, t1=0.5, rtol=1e-6, atol=1e-6,
                                   checkpoint=2)
-        engine._OCC[spec.key] = 0
-        engine._OCC_REV[spec.key] = 7
+        engine._OCC[("tsit5", spec.key)] = 0
+        engine._OCC_REV[("tsit5", spec.key)] = 7
         r = engine.forward_record("tsit5", spec, y0, p, t0=0.0, t1=0.5, rtol=1e-6, atol=1e-6,
                                   checkpoint=2)
         with pytest.raises(GsolveError, match="GS_OCC"):
             engine.adjoint(r, p, torch.ones_like(r.y_final))
-        engine._OCC_REV[spec.key] = 4  # applies at K = 2 only: other intervals ignore it
+        engine._OCC_REV[("tsit5", spec.key)] = 4  # applies at K = 2 only: other intervals ignore it
         r = engine.forward_record("tsit5", spec, y0, p, t0=0.0, t1=0.5, rtol=1e-6, atol=1e-6,
                                   checkpoint=3)
         engine.adjoint(r, p, torch.ones_like(r.y_final))
@@ -147,11 +147,11 @@ def test_occupancy_autotuner(gslib, cuda):
     kw = dict(t0=0.0, t1=1.0, rtol=1e-8, atol=1e-8, checkpoint=2)
     saved = dict(engine._OCC), dict(engine._OCC_REV)
     try:
-        engine._OCC.pop(spec.key, None)
-        engine._OCC_REV.pop(spec.key, None)
+        engine._OCC.pop(("tsit5", spec.key), None)
+        engine._OCC_REV.pop(("tsit5", spec.key), None)
         r = engine.forward_record("tsit5", spec, y0, p, **kw)
-        assert engine._OCC.get(spec.key) in engine.occ_choices(spec, "forward")
-        assert engine._OCC_REV.get(spec.key) in engine.occ_choices(spec, "reverse")
+        assert engine._OCC.get(("tsit5", spec.key)) in engine.occ_choices(spec, "forward")
+        assert engine._OCC_REV.get(("tsit5", spec.key)) in engine.occ_choices(spec, "reverse")
         f, b = engine.autotune_occupancy(spec, y0, p, t0=0.0, t1=1.0, rtol=1e-8, atol=1e-8,
                                          checkpoint=2)
         assert f in engine.occ_choices(spec, "forward")
@@ -168,3 +168,47 @@ def test_occupancy_autotuner(gslib, cuda):
             assert torch.equal(x, y)
     finally:
         _restore(engine, saved)
+
+
+@pytest.mark.parametrize("case", ["robertson_toy", "robertson_stiff"])
+def test_ros23_occupancy_instances_bitwise(gslib, cuda, case):
+    """Rosenbrock23: the forward's and the K = 2 reverse pass's instances against the
+    defaults, bit for bit; counts those of the reference's Rosenbrock23 oracle."""
+    from gradsolve_b200 import engine
+    g = load_golden(case)
+    spec = _spec("robertson")
+    y0 = torch.tensor(g["y0"], device=cuda)
+    p = torch.tensor(g["params"], device=cuda)
+    fwd = engine.occ_choices(spec, "forward", "rosenbrock23")
+    rev = engine.occ_choices(spec, "reverse", "rosenbrock23")
+    assert fwd == [0, 4, 6] and rev == [0, 3, 5]
+    saved = dict(engine._OCC), dict(engine._OCC_REV)
+
+    def solve():
+        r = engine.forward_record("rosenbrock23", spec, y0, p, t0=float(g["t0"]),
+                                  t1=float(g["t1"]), rtol=float(g["rtol"]),
+                                  atol=float(g["atol"]), max_steps=50000, checkpoint=2)
+        gy0, gp = engine.adjoint(r, p, torch.ones_like(r.y_final))
+        torch.cuda.synchronize()
+        return [r.padded_dts().cpu(), r.y_final.cpu(), r.n_acc.cpu(), r.n_rej.cpu(),
+                r.status.cpu(), gy0.cpu(), gp.cpu()]
+
+    outs = {}
+    try:
+        for pass_, choices in (("forward", fwd), ("reverse", rev[1:])):
+            for b in choices:
+                engine.set_occupancy(spec, 0, "forward", "rosenbrock23")
+                engine.set_occupancy(spec, 0, "reverse", "rosenbrock23")
+                engine.set_occupancy(spec, b, pass_, "rosenbrock23")
+                outs[(pass_, b)] = solve()
+        engine._OCC_REV[("rosenbrock23", spec.key)] = 4  # not built: the library refuses
+        with pytest.raises(Exception, match="GS_OCC"):
+            solve()
+    finally:
+        _restore(engine, saved)
+    base = outs[("forward", 0)]
+    np.testing.assert_array_equal(base[2].numpy(), g["n_acc"])
+    np.testing.assert_array_equal(base[3].numpy(), g["n_rej"])
+    for key, out in outs.items():
+        for x, y in zip(base, out):
+            assert torch.equal(x, y), f"{key} differs from the default instances"

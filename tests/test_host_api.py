@@ -179,3 +179,64 @@ def test_record_row_gather_follows_the_chunked_layout():
         want[: n_acc[j]] = 100 * j + np.arange(n_acc[j]) + 1
         np.testing.assert_array_equal(got[k], want)
     assert r.dts_rows(rows, S=12).shape == (3, 12)
+
+
+def test_occupancy_flags_and_choice_rule():
+    """Which calls carry GS_OCC, and the autotuner's keep-the-default margin (host logic; the
+    instances themselves are checked bit for bit on the GPU)."""
+    import re
+
+    import torch
+
+    from gradsolve_b200 import engine
+    hdr = (Path(__file__).resolve().parents[1] / "include" / "gsolve.h").read_text()
+    val = {m.group(1): int(m.group(2), 0)
+           for m in re.finditer(r"#define (GS_\w+_MASK) (0x[0-9A-Fa-f]+)", hdr)}
+    assert val["GS_OCC_MASK"] == 0x78000
+    # the occupancy bits overlap no other flag field; the engine shifts by the header's shift
+    for k, v in val.items():
+        if k != "GS_OCC_MASK":
+            assert v & val["GS_OCC_MASK"] == 0, k
+    assert int(re.search(r"#define GS_OCC_SHIFT (\d+)", hdr).group(1)) == 15
+    spec = field_spec("lorenz")
+    saved = dict(engine._OCC), dict(engine._OCC_REV)
+    try:
+        engine._OCC[("tsit5", spec.key)] = 5
+        engine._OCC_REV[("tsit5", spec.key)] = 4
+        f = engine._occ_flag
+        assert f("tsit5", spec, "float64", "auto", None, None) == 5 << 15
+        assert f("tsit5", spec, "float64", "static", torch.zeros(1), None) == 5 << 15
+        assert f("tsit5", spec, "float64", "auto", torch.zeros(1), None) == 0   # refilled
+        assert f("tsit5", spec, "mixed", "auto", None, None) == 0
+        assert f("tsit5", spec, "float32", "auto", None, None) == 0
+        assert f("tsit5", spec, "float64", "auto", None, torch.zeros(2)) == 0   # saveat
+        assert f("tsit5", spec, "float64", "refill", None, None) == 0
+        assert f("rosenbrock23", spec, "float64", "auto", None, None) == 0    # not tuned
+
+        class R:
+            method, ckpt_every = "tsit5", 2
+        R.spec = spec
+        g = engine._occ_rev_flag
+        assert g(R, "float64", "auto", "auto") == 4 << 15
+        assert g(R, "float64", "static", "stages") == 4 << 15
+        assert g(R, "float64", "auto", "recompute") == 0
+        assert g(R, "float64", "refill", "auto") == 0
+        assert g(R, "mixed", "auto", "auto") == 0
+        R.ckpt_every = 3
+        assert g(R, "float64", "auto", "auto") == 0
+    finally:
+        engine._OCC.clear()
+        engine._OCC.update(saved[0])
+        engine._OCC_REV.clear()
+        engine._OCC_REV.update(saved[1])
+    # another instance replaces the default only when faster by more than the margin
+    m = engine.OCC_MARGIN
+    assert engine._pick({0: 10.0, 5: 10.0 * (1 - m / 2)}) == 0
+    assert engine._pick({0: 10.0, 5: 10.0 * (1 - 2 * m), 7: 10.5}) == 5
+    assert engine._pick({0: 10.0, 4: 11.0}) == 0
+
+
+def test_replay_graph_refuses_record_sets():
+    from gradsolve_b200 import engine
+    with pytest.raises(TypeError, match="single Record"):
+        engine.ReplayGraph(object(), None, None, lambda yf: yf)

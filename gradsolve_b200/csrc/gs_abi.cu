@@ -352,7 +352,8 @@ int lane_choices(int* out, int cap) {
 // forward, whose default instance is bounded for 6 blocks per SM, also has instances bounded
 // for 4 and 5 (more registers: longer-range scheduling, no spills where the default spills),
 // 7 and 8 (fewer registers, more resident warps); the float64 reverse pass's K = 2
-// stage-keeping instance (default 5 blocks) has 3, 4 and 6.  Larger fields keep the compiler's
+// stage-keeping instance (default 5 blocks) has 3, 4 and 6, the float32-stage one (default
+// 6) 4 and 5.  Larger fields keep the compiler's
 // allocation alone.
 template <class F>
 int occ_choices(int pass, int* out, int cap) {
@@ -361,9 +362,10 @@ int occ_choices(int pass, int* out, int cap) {
   ++k;
   if constexpr (F::D <= 4) {
     const std::initializer_list<int> fwd = {4, 5, 7, 8}, rev = {3, 4, 6}, rfwd = {4, 6},
-                                     rrev = {3, 5};
+                                     rrev = {3, 5}, mrev = {4, 5};
     for (int b : (pass == GS_OCC_REVERSE ? rev : pass == GS_OCC_ROS23_FORWARD ? rfwd
-                  : pass == GS_OCC_ROS23_REVERSE ? rrev : fwd)) {
+                  : pass == GS_OCC_ROS23_REVERSE ? rrev
+                  : pass == GS_OCC_MIXED_REVERSE ? mrev : fwd)) {
       if (cap > k) out[k] = b;
       ++k;
     }
@@ -372,9 +374,10 @@ int occ_choices(int pass, int* out, int cap) {
 }
 
 template <class F>
-int launch_adjoint_k2_occ(const gs::AdjointArgs& a, cudaStream_t s, int occ) {
+int launch_adjoint_k2_occ(const gs::AdjointArgs& a, cudaStream_t s, int occ, bool mixed) {
   if constexpr (F::D <= 4) {
-    const int sd = gs::adjoint_stages_smem_doubles<F::D>(2);
+    const int sd = mixed ? gs::mixed_stages_smem_doubles<F::D>(2)
+                         : gs::adjoint_stages_smem_doubles<F::D>(2);
     auto go = [&](auto kern) -> int {
       SegCfg c{0, 0, 0};
       int rc;
@@ -385,11 +388,19 @@ int launch_adjoint_k2_occ(const gs::AdjointArgs& a, cudaStream_t s, int occ) {
       kern<<<grid_for_block(a.n, c.block), c.block, c.smem, s>>>(a);
       return cuda_check("tsit5_adjoint_stages_kernel");
     };
-    switch (occ) {
-      case 3: return go(gs::tsit5_adjoint_stages_k2_kernel<F, 3>);
-      case 4: return go(gs::tsit5_adjoint_stages_k2_kernel<F, 4>);
-      case 6: return go(gs::tsit5_adjoint_stages_k2_kernel<F, 6>);
-      default: break;
+    if (mixed) {
+      switch (occ) {
+        case 4: return go(gs::tsit5_mixed_adjoint_stages_k2_kernel<F, 4>);
+        case 5: return go(gs::tsit5_mixed_adjoint_stages_k2_kernel<F, 5>);
+        default: break;
+      }
+    } else {
+      switch (occ) {
+        case 3: return go(gs::tsit5_adjoint_stages_k2_kernel<F, 3>);
+        case 4: return go(gs::tsit5_adjoint_stages_k2_kernel<F, 4>);
+        case 6: return go(gs::tsit5_adjoint_stages_k2_kernel<F, 6>);
+        default: break;
+      }
     }
   }
   return fail(GS_ERR_ARG, "GS_OCC: no reverse-pass instance bounded for " + std::to_string(occ) +
@@ -534,9 +545,9 @@ template <class F>
 int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool mixed,
                          int sched, int variant, int precision) {
   const int occ = (precision & GS_OCC_MASK) >> GS_OCC_SHIFT;
-  if (occ && (kCoop<F> || mixed || sched != GS_SCHED_STATIC || variant == GS_ADJ_RECOMPUTE ||
+  if (occ && (kCoop<F> || sched != GS_SCHED_STATIC || variant == GS_ADJ_RECOMPUTE ||
               a.ck_every != 2))
-    return fail(GS_ERR_ARG, "GS_OCC applies to the float64 reverse pass's K = 2 stage-keeping "
+    return fail(GS_ERR_ARG, "GS_OCC applies to the reverse pass's K = 2 stage-keeping "
                             "instance, one thread per trajectory");
   if constexpr (kCoop<F>) {
     (void)cap; (void)sched; (void)variant;
@@ -544,7 +555,7 @@ int launch_tsit5_adjoint(const gs::AdjointArgs& a, int cap, cudaStream_t s, bool
   } else {
   if (precision & GS_LANES_MASK)
     return fail(GS_ERR_ARG, "lanes per trajectory apply to fields of more than 8 components only");
-  if (occ) return launch_adjoint_k2_occ<F>(a, s, occ);
+  if (occ) return launch_adjoint_k2_occ<F>(a, s, occ, mixed);
   if (sched == GS_SCHED_STATIC) {
     int rc;
     if (!mixed) {
@@ -1118,7 +1129,7 @@ int gs_occ_choices(int field, int pass, int* out, int cap) {
   if (pass == GS_OCC_ROS23_FORWARD || pass == GS_OCC_ROS23_REVERSE) {
     GS_ROS23_DISPATCH(field, occ_choices, pass, out, cap)
   }
-  if (pass != GS_OCC_FORWARD && pass != GS_OCC_REVERSE)
+  if (pass != GS_OCC_FORWARD && pass != GS_OCC_REVERSE && pass != GS_OCC_MIXED_REVERSE)
     return fail(GS_ERR_ARG, "gs_occ_choices: unknown pass " + std::to_string(pass));
   GS_TSIT5_DISPATCH(field, occ_choices, pass, out, cap)
 }

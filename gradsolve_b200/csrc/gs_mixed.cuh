@@ -597,9 +597,11 @@ __global__ void __launch_bounds__(128) tsit5_mixed_adjoint_stages_kernel(const A
 
 // K = 2 with the segment loops unrolled (the autotuned interval of the small built-in fields),
 // bounded to 6 blocks of 128 per SM: unbounded, Lorenz's instance takes 94 registers (5 blocks)
-// where the general stage-keeping kernel holds 6
-template <class F>
-__global__ void __launch_bounds__(128, 6) tsit5_mixed_adjoint_stages_k2_kernel(const AdjointArgs a) {
+// where the general stage-keeping kernel holds 6.  kMinB > 0 bounds it for kMinB blocks
+// instead (the occupancy autotuner's instances; same arithmetic, bit for bit).
+template <class F, int kMinB = 0>
+__global__ void __launch_bounds__(128, (kMinB > 0 ? kMinB : 6))
+    tsit5_mixed_adjoint_stages_k2_kernel(const AdjointArgs a) {
   tsit5_mixed_adjoint_stages_body<F, 2>(a);
 }
 

@@ -564,8 +564,10 @@ def _lanes_flag(method: str, spec: FieldSpec) -> int:
 _OCC: dict = {}      # (method, field key) -> GS_OCC blocks per SM of the forward (0: default)
 _OCC_REV: dict = {}  # (method, field key) -> the same for the reverse pass at K = 2
 OCC_MARGIN = 0.01    # another instance replaces the default only when faster by more than 1%
+MIXED = "tsit5/mixed"  # the tables' method key of the Tsit5 float32-stage reverse pass
 _OCC_PASS = {(METHOD_TSIT5, "forward"): 0, (METHOD_TSIT5, "reverse"): 1,
-             (METHOD_ROS23, "forward"): 2, (METHOD_ROS23, "reverse"): 3}
+             (METHOD_ROS23, "forward"): 2, (METHOD_ROS23, "reverse"): 3,
+             (MIXED, "reverse"): 4}
 
 
 def occ_choices(spec: FieldSpec, pass_: str = "forward", method: str = METHOD_TSIT5) -> list:
@@ -607,12 +609,19 @@ def _occ_flag(method, spec, precision, schedule, t1v, saveat_ts) -> int:
 
 
 def _occ_rev_flag(r, precision: str, schedule: str, variant: str) -> int:
-    """The reverse pass's GS_OCC: float64 at K = 2, the instance that keeps the replayed
-    steps' stage inputs (Tsit5) or factors (Rosenbrock23), one thread per trajectory."""
-    if (precision != "float64" or r.ckpt_every != 2 or schedule not in ("auto", "static") or
+    """The reverse pass's GS_OCC: at K = 2, the instance that keeps the replayed steps' stage
+    inputs (Tsit5, float64 or float32-stage) or factors (Rosenbrock23, float64), one thread
+    per trajectory."""
+    if (r.ckpt_every != 2 or schedule not in ("auto", "static") or
             (r.method == METHOD_TSIT5 and variant == "recompute")):
         return 0
-    return int(_OCC_REV.get((r.method, r.spec.key)) or 0) << 15
+    if precision == "float64":
+        key = (r.method, r.spec.key)
+    elif precision == "mixed" and r.method == METHOD_TSIT5:
+        key = (MIXED, r.spec.key)
+    else:
+        return 0
+    return int(_OCC_REV.get(key) or 0) << 15
 
 
 def _time_ms(fn, reps: int) -> float:
@@ -679,6 +688,32 @@ def autotune_occupancy(spec: FieldSpec, y0: torch.Tensor, p: torch.Tensor, *, t0
             times[b] = _time_ms(lambda: adjoint(r, ps, ybar), reps)
         _OCC_REV[key] = _pick(times)
     return _OCC[key], _OCC_REV[key]
+
+
+@_tuner
+def autotune_mixed_reverse(spec: FieldSpec, y0: torch.Tensor, p: torch.Tensor, *, t0: float,
+                           t1: float, rtol: float, atol: float, max_steps: int = 100000,
+                           checkpoint="auto", sample: int = 1 << 20, reps: int = 3) -> int:
+    """The float32-stage Tsit5 reverse pass's occupancy instance at K = 2, timed like
+    ``autotune_occupancy``'s reverse half on a float32-stage record of up to ``sample`` of
+    the caller's trajectories (0 where the record's interval is not 2)."""
+    key = (MIXED, spec.key)
+    choices = occ_choices(spec, "reverse", MIXED)
+    _OCC_REV[key] = 0
+    m = min(y0.shape[0], sample)
+    ys, ps = y0[:m].contiguous(), p[:m].contiguous()
+    r = forward_record(METHOD_TSIT5, spec, ys, ps, t0=t0, t1=t1, rtol=rtol, atol=atol,
+                       max_steps=max_steps, checkpoint=checkpoint, precision="mixed")
+    if len(choices) < 2 or any(rr.ckpt_every != 2 for _rows, rr in _parts(r)):
+        return 0
+    ybar = torch.ones_like(r.y_final)
+    times = {}
+    for b in choices:
+        _OCC_REV[key] = b
+        adjoint(r, ps, ybar, precision="mixed")  # warm
+        times[b] = _time_ms(lambda: adjoint(r, ps, ybar, precision="mixed"), reps)
+    _OCC_REV[key] = _pick(times)
+    return _OCC_REV[key]
 
 
 @_tuner
@@ -766,6 +801,11 @@ def forward_record(method: str, spec: FieldSpec, y0: torch.Tensor, p: torch.Tens
                             max_steps=max_steps, precision=precision)
     occ_sched = "static" if method == METHOD_ROS23 and schedule == "auto" and isinstance(
         ws, RecordSet) else schedule  # (planned Rosenbrock23 tiers run one thread per row)
+    if (precision == "mixed" and method == METHOD_TSIT5 and (MIXED, spec.key) not in _OCC_REV
+            and not _IN_TUNER[0] and n >= 4096 and
+            _occ_applies(method, "float64", occ_sched, t1v, saveat_ts)):
+        autotune_mixed_reverse(spec, y0, p, t0=t0, t1=t1, rtol=rtol, atol=atol,
+                               max_steps=max_steps, checkpoint=checkpoint)
     if ((method, spec.key) not in _OCC and not _IN_TUNER[0] and n >= 4096 and
             _occ_applies(method, precision, occ_sched, t1v, saveat_ts)):
         autotune_occupancy(spec, y0, p, t0=t0, t1=t1, rtol=rtol, atol=atol,

@@ -113,13 +113,13 @@ extern "C" {
 
 /* Registers and occupancy, OR-ed into the precision argument of gs_tsit5_fwd_record /
  * gs_ros23_fwd_record (the float64 recording forward, one thread per trajectory) and of
- * gs_tsit5_adjoint / gs_ros23_adjoint / gs_adjoint_ordered (the float64 reverse pass's K = 2
- * instance that keeps the replayed steps' stage inputs or factors, one thread per
- * trajectory): GS_OCC(b) runs the kernel instance whose registers are bounded for b resident
+ * gs_tsit5_adjoint / gs_ros23_adjoint / gs_adjoint_ordered (the reverse pass's K = 2
+ * instance that keeps the replayed steps' stage inputs or factors, float64 or, for Tsit5,
+ * float32-stage, one thread per trajectory): GS_OCC(b) runs the kernel instance whose registers are bounded for b resident
  * blocks of 128 threads per SM; 0 takes the default instance.  gs_occ_choices lists the
  * values built for a field and pass (0 first); any other value, and any nonzero value on
- * another path (float32 stages, the float32 route, the forward without a record, persistent
- * schedules, another checkpoint interval or reverse-pass variant), is refused with
+ * another path (the float32-stage forward, the float32 route, the forward without a record,
+ * persistent schedules, another checkpoint interval or reverse-pass variant), is refused with
  * GS_ERR_ARG.  The instances run the same arithmetic: results are bit for bit those of the
  * default. */
 #define GS_OCC_SHIFT 15
@@ -129,6 +129,7 @@ extern "C" {
 #define GS_OCC_REVERSE 1       /* Tsit5 reverse pass at K = 2 */
 #define GS_OCC_ROS23_FORWARD 2 /* Rosenbrock23 recording forward */
 #define GS_OCC_ROS23_REVERSE 3 /* Rosenbrock23 reverse pass at K = 2 */
+#define GS_OCC_MIXED_REVERSE 4 /* Tsit5 float32-stage reverse pass at K = 2 */
 
 /* per-trajectory status values written to status[] */
 #define GS_TRAJ_OK 0          /* reached t1 */
@@ -189,7 +190,8 @@ int gs_lane_choices(int field, int* out, int cap);
  * forward; default instance bounded for 6 blocks per SM at up to 4 components, unbounded
  * above), GS_OCC_REVERSE (the float64 Tsit5 reverse pass at K = 2; default 5 blocks),
  * GS_OCC_ROS23_FORWARD (Rosenbrock23 forward; default unbounded) or GS_OCC_ROS23_REVERSE
- * (Rosenbrock23 reverse pass at K = 2; default 4 blocks): writes up to cap GS_OCC values to
+ * (Rosenbrock23 reverse pass at K = 2; default 4 blocks) or GS_OCC_MIXED_REVERSE (the Tsit5
+ * float32-stage reverse pass at K = 2; default 6 blocks): writes up to cap GS_OCC values to
  * out (0, the default instance, first) and returns how many, or a negative GS_ERR_* for an
  * unknown field or pass (or a field without a Jacobian for the Rosenbrock23 passes).  No counterpart in the
  * reference, whose kernels take the compiler's register allocation

@@ -212,3 +212,31 @@ def test_ros23_occupancy_instances_bitwise(gslib, cuda, case):
     for key, out in outs.items():
         for x, y in zip(base, out):
             assert torch.equal(x, y), f"{key} differs from the default instances"
+
+
+def test_mixed_reverse_occupancy_bitwise(gslib, cuda):
+    """The float32-stage reverse pass's K = 2 instances against its default, bit for bit."""
+    from gradsolve_b200 import engine
+    g = load_golden("lorenz_scale")
+    spec = _spec("lorenz")
+    y0, p = _inputs(cuda, spec, g)
+    rev = engine.occ_choices(spec, "reverse", engine.MIXED)
+    assert rev == [0, 4, 5]
+    saved = dict(engine._OCC), dict(engine._OCC_REV)
+    try:
+        r = engine.forward_record("tsit5", spec, y0, p, t0=float(g["t0"]), t1=float(g["t1"]),
+                                  rtol=float(g["rtol"]), atol=float(g["atol"]), checkpoint=2,
+                                  precision="mixed")
+        ybar = 2.0 * r.y_final
+        outs = {}
+        for b in rev:
+            engine.set_occupancy(spec, b, "reverse", engine.MIXED)
+            outs[b] = [t.cpu() for t in engine.adjoint(r, p, ybar, precision="mixed")]
+        engine._OCC_REV[(engine.MIXED, spec.key)] = 6  # not built: the library refuses
+        with pytest.raises(Exception, match="GS_OCC"):
+            engine.adjoint(r, p, ybar, precision="mixed")
+    finally:
+        _restore(engine, saved)
+    for b in rev[1:]:
+        for x, y in zip(outs[0], outs[b]):
+            assert torch.equal(x, y), f"instance {b} differs from the default"
